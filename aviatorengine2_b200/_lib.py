@@ -1,0 +1,148 @@
+"""ctypes binding of libae_b200.so and numpy dtypes of its byte contract.
+
+Loading fails loudly when the library is missing: there is no fallback path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libae_b200.so")
+
+# --- byte contract (include/ae_b200.h) --------------------------------------
+VERTEX = np.dtype([("px", "<f4"), ("py", "<f4"), ("pz", "<f4"), ("nx", "<f4"), ("ny", "<f4"), ("nz", "<f4"),
+                   ("u", "<f4"), ("v", "<f4")])
+NODE = np.dtype([("min_x", "<f4"), ("min_y", "<f4"), ("min_z", "<f4"), ("pad0", "<f4"), ("max_x", "<f4"),
+                 ("max_y", "<f4"), ("max_z", "<f4"), ("left", "<i4"), ("right", "<i4"), ("count", "<i4"),
+                 ("padding", "<i4"), ("pad_trailing", "<i4")])
+OBJECT = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("prevRotX", "<f4"), ("x2", "<f4"), ("y2", "<f4"),
+                   ("z2", "<f4"), ("radius", "<f4"), ("u_x", "<f4"), ("u_y", "<f4"), ("u_z", "<f4"),
+                   ("prevRotY", "<f4"), ("v_x", "<f4"), ("v_y", "<f4"), ("v_z", "<f4"), ("prevRotZ", "<f4"),
+                   ("half_x", "<f4"), ("half_y", "<f4"), ("half_z", "<f4"), ("rotation", "<f4"),
+                   ("density", "<f4"), ("emission", "<f4"), ("instanceIndex", "<u4"), ("textureTint", "<f4"),
+                   ("r", "<f4"), ("g", "<f4"), ("b", "<f4"), ("fuzz", "<f4"), ("refraction", "<f4"),
+                   ("shapeType", "<u4"), ("colorType", "<u4"), ("textureID", "<u4")])
+INSTANCE = np.dtype([("px", "<f4"), ("py", "<f4"), ("pz", "<f4"), ("scale", "<f4"), ("qx", "<f4"), ("qy", "<f4"),
+                     ("qz", "<f4"), ("qw", "<f4"), ("vertexBase", "<u4"), ("indexBase", "<u4"),
+                     ("triangleCount", "<u4"), ("blasBase", "<u4")])
+AABB = np.dtype([("min_x", "<f4"), ("min_y", "<f4"), ("min_z", "<f4"), ("max_x", "<f4"), ("max_y", "<f4"),
+                 ("max_z", "<f4")])
+RAY = np.dtype([("ox", "<f4"), ("oy", "<f4"), ("oz", "<f4"), ("tnear", "<f4"), ("dx", "<f4"), ("dy", "<f4"),
+                ("dz", "<f4"), ("time", "<f4")])
+HIT = np.dtype([("t", "<f4"), ("alpha", "<f4"), ("beta", "<f4"), ("object", "<u4"), ("prim", "<u4")])
+CONFIG = np.dtype([("source_x", "<f4"), ("source_y", "<f4"), ("source_z", "<f4"), ("fov", "<f4"),
+                   ("target_x", "<f4"), ("target_y", "<f4"), ("target_z", "<f4"), ("focus_dist", "<f4"),
+                   ("defocus_angle", "<f4"), ("padding", "<f4", 3), ("up_x", "<f4"), ("up_y", "<f4"),
+                   ("up_z", "<f4"), ("oof", "<f4"), ("sky_r", "<f4"), ("sky_g", "<f4"), ("sky_b", "<f4"),
+                   ("width", "<u4"), ("horizon_r", "<f4"), ("horizon_g", "<f4"), ("horizon_b", "<f4"),
+                   ("height", "<u4"), ("samples", "<u4"), ("batches", "<u4"), ("batch", "<u4"), ("depth", "<u4"),
+                   ("num_spheres", "<u4"), ("renderType", "<u4"), ("num_lights", "<u4"), ("exposure", "<f4"),
+                   ("debugView", "<u4"), ("zNear", "<f4"), ("zFar", "<f4"), ("jitter_x", "<f4"),
+                   ("jitter_y", "<f4"), ("displayOnly", "<u4"), ("traceScale", "<f4"), ("frameIndex", "<u4"),
+                   ("historyReset", "<u4"), ("cameraMoved", "<u4"), ("historyCap", "<f4"), ("padding3", "<f4"),
+                   ("prevViewProj", "<f4", 16)])
+ENTITY = np.dtype([("shape", "<u4"), ("material", "<u4"), ("position", "<f4", 3), ("rotation", "<f4", 4),
+                   ("scale", "<f4"), ("albedo", "<f4", 3), ("fuzz", "<f4"), ("ior", "<f4"), ("emission", "<f4"),
+                   ("density", "<f4"), ("texture_tint", "<f4"), ("texture_id", "<u4"), ("radius", "<f4"),
+                   ("u", "<f4", 3), ("v", "<f4", 3), ("half_extent", "<f4", 3), ("mesh", "<u4"),
+                   ("prev_position", "<f4", 3), ("prev_rotation", "<f4", 4)])
+SETTINGS = np.dtype([("width", "<u4"), ("height", "<u4"), ("samples", "<u4"), ("max_samples", "<u4"),
+                     ("hybrid", "<u4"), ("hybrid_max_depth", "<u4"), ("trace_scale", "<f4"),
+                     ("history_while_moving", "<u4"), ("device", "<i4"), ("reserved", "<u4", 7)])
+MESH_RANGE = np.dtype([("vertexBase", "<u4"), ("indexBase", "<u4"), ("triangleCount", "<u4"), ("blasBase", "<u4"),
+                       ("localBounds", AABB), ("doubleSided", "<u4")])
+
+for _dt, _size in ((VERTEX, 32), (NODE, 48), (OBJECT, 128), (INSTANCE, 48), (RAY, 32), (HIT, 20), (CONFIG, 240),
+                   (AABB, 24), (SETTINGS, 64)):
+    assert _dt.itemsize == _size, (_dt, _size)
+
+# Enumerations (include/ae_b200.h)
+SHAPE_SPHERE, SHAPE_QUAD, SHAPE_BOX, SHAPE_TRIANGLE, SHAPE_MESH = range(5)
+MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_DIFFUSE_LIGHT, MAT_ISOTROPIC = range(5)
+NO_TEXTURE = 0xFFFFFFFF
+MISS = 0xFFFFFFFF
+VARIANT_PLAIN, VARIANT_FAST, VARIANT_QUANT = 0, 1, 2
+MODE_COMPUTE_ONLY, MODE_DEFERRED, MODE_WAVEFRONT = 0, 1, 2
+IMAGE_ACCUM, IMAGE_DISPLAY, IMAGE_FRAME, IMAGE_REDUCED, IMAGE_HISTORY_GEOMETRY = range(5)
+STATUS = {0: "AE_OK", -1: "AE_ERR_INVALID", -2: "AE_ERR_OOM", -3: "AE_ERR_OVERSIZE", -4: "AE_ERR_LAYOUT",
+          -5: "AE_ERR_CUDA", -6: "AE_ERR_TIMEOUT", -7: "AE_ERR_STATE", -8: "AE_ERR_REJECTED"}
+
+# Every symbol include/ae_b200.h declares, with (restype, argtypes).
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_I = ctypes.c_int
+SIGNATURES = {
+    "ae_build_bvh": (_I, [_P, _U32, _P, _P, _P]),
+    "ae_mesh_library_create": (_P, []),
+    "ae_mesh_library_destroy": (None, [_P]),
+    "ae_mesh_library_add": (_I, [_P, _P, _U32, _P, _U32, _I]),
+    "ae_mesh_library_range": (_I, [_P, _U32, _P]),
+    "ae_mesh_library_sizes": (None, [_P, _P, _P, _P]),
+    "ae_mesh_library_vertices": (_P, [_P]),
+    "ae_mesh_library_indices": (_P, [_P]),
+    "ae_mesh_library_blas": (_P, [_P]),
+    "ae_pack_scene": (_I, [_P, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "ae_entity_bounds": (_I, [_P, _P, _P]),
+    "ae_create": (_P, [_P]),
+    "ae_destroy": (None, [_P]),
+    "ae_last_error": (ctypes.c_char_p, [_P]),
+    "ae_upload_geometry": (_I, [_P, _P, _U32, _P, _U32, _P, _U32]),
+    "ae_reserve_scene": (_I, [_P, _U32, _U32]),
+    "ae_upload_scene": (_I, [_P, _P, _U32, _P, _U32, _P, _U32, _P, _U32]),
+    "ae_set_config": (_I, [_P, _P]),
+    "ae_get_config": (_I, [_P, _P]),
+    "ae_reset_accumulation": (_I, [_P]),
+    "ae_render_frame": (_I, [_P, _I, _P]),
+    "ae_build_gbuffer": (_I, [_P]),
+    "ae_read_image": (_I, [_P, _I, _P, ctypes.c_size_t]),
+    "ae_closest_hit": (_I, [_P, _P, _U32, _P, _I]),
+    "ae_closest_hit_device": (_I, [_P, _P, _U32, _P, _I]),
+    "ae_any_hit": (_I, [_P, _P, _P, _U32, _P]),
+    "ae_camera_rays": (_I, [_P, _P]),
+    "ae_bounce_rays": (_I, [_P, _P, _P, _U32, _P, _P]),
+    "ae_trace_counters": (_I, [_P, _P, _U32, _P]),
+    "ae_synchronize": (_I, [_P]),
+    "ae_last_kernel_ms": (_I, [_P, _P]),
+    "ae_stream": (_P, [_P]),
+    "ae_launch_count": (ctypes.c_uint64, [_P]),
+    "ae_prepare_fast": (_I, [_P]),
+    "ae_refit_instances": (_I, [_P, _P, _U32]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded library (built by aviatorengine2_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m aviatorengine2_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def ptr(a):
+    """Address of a numpy array's data (None for None)."""
+    if a is None:
+        return None
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class AeError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def check(code, ctx=None, what=""):
+    if code != 0:
+        msg = lib().ae_last_error(ctx).decode() if ctx else what
+        raise AeError(code, msg or what)
+    return code

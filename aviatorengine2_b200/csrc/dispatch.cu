@@ -1,0 +1,66 @@
+// dispatch.cu - kernel-family selection for closest hit, and the context's
+// destructor (it owns the optimised structures).
+#include "context.h"
+#include "kernels.h"
+#include "fast.h"
+
+namespace ae {
+
+Ctx::~Ctx() {
+    destroy_fast(this);
+    destroy_wavefront(this);
+    destroy_deferred(this);
+    if (side_stream) cudaStreamDestroy(side_stream);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+int prepare_variant(Ctx *c, int variant) {
+    switch (variant) {
+    case AE_VARIANT_PLAIN: return AE_OK;
+    case AE_VARIANT_FAST:
+    case AE_VARIANT_QUANT: return prepare_fast(c);
+    default: return c->fail(AE_ERR_INVALID, "unknown kernel variant %d", variant);
+    }
+}
+
+int closest_hit_dispatch(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, int variant, cudaStream_t st,
+                         bool timed) {
+    int rc = prepare_variant(c, variant);
+    if (rc) return rc;
+    if (n == 0) return AE_OK;
+    if (timed && (rc = c->cuda(cudaEventRecord(c->ev0, st), "event"))) return rc;
+    cudaError_t e;
+    if (variant == AE_VARIANT_PLAIN) e = launch_closest_plain(c->scene(), rays, n, hits, st);
+    else e = launch_closest_fast(c, rays, n, hits, variant == AE_VARIANT_QUANT, st);
+    if ((rc = c->cuda(e, "closest hit launch"))) return rc;
+    c->launches++;
+    if (timed) {
+        c->timed = true;
+        if ((rc = c->cuda(cudaEventRecord(c->ev1, st), "event"))) return rc;
+    }
+    return AE_OK;
+}
+
+}  // namespace ae
+
+extern "C" int ae_trace_counters(ae_ctx *ctx, const ae_ray *d_rays, uint32_t n, uint64_t *counters) {
+    ae::Ctx *c = reinterpret_cast<ae::Ctx *>(ctx);
+    if (!c || !counters || (n && !d_rays)) return AE_ERR_INVALID;
+    if (!c->scene_uploaded) return c->fail(AE_ERR_STATE, "counters before ae_upload_scene");
+    ae::DevBuf<unsigned long long> tot;
+    if (tot.reserve(6)) return c->fail(AE_ERR_OOM, "counter buffer");
+    int rc = c->cuda(cudaMemsetAsync(tot.ptr, 0, 6 * sizeof(unsigned long long), c->stream), "memset");
+    if (!rc) rc = c->cuda(ae::launch_count_plain(c->scene(), d_rays, n, tot.ptr, c->stream), "count launch");
+    c->launches++;
+    if (!rc) rc = c->cuda(cudaMemcpyAsync(counters, tot.ptr, 6 * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream), "copy");
+    if (!rc) rc = c->cuda(cudaStreamSynchronize(c->stream), "counters");
+    return rc;
+}
+
+extern "C" int ae_prepare_fast(ae_ctx *ctx) {
+    ae::Ctx *c = reinterpret_cast<ae::Ctx *>(ctx);
+    if (!c) return AE_ERR_INVALID;
+    return ae::prepare_fast(c);
+}

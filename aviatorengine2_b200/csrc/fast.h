@@ -1,0 +1,12 @@
+// fast.h - entry points of the optimised closest-hit path and the other
+// kernel families that own per-context state.
+#pragma once
+#include "context.h"
+
+namespace ae {
+int prepare_fast(Ctx *c);
+void destroy_fast(Ctx *c);
+cudaError_t launch_closest_fast(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, bool quant, cudaStream_t st);
+void destroy_wavefront(Ctx *c);
+void destroy_deferred(Ctx *c);
+}  // namespace ae

@@ -1,0 +1,333 @@
+"""Scene authoring and the seeded synthetic scenes of the measured workloads.
+
+Mirrors the reference's authoring split: meshes go into a MeshLibrary (one BLAS
+each, scene/mesh_library.h:91-159), renderable entities carry a transform and
+a material (scene/components.h), and packing builds the TLAS and the byte
+arrays the device reads (renderer/renderer.cpp:1087-1130).  Emissive surfaces
+are analytic quads, as Scene::MeshEligible routes them (scene/scene.h:543-546).
+
+Workloads (all inputs seeded; no dataset is involved):
+  cornell_box      320x240 closed box: 5 mesh-quad walls, 2 rotated mesh cubes,
+                   1 analytic emissive quad (radiance 15), 8 TLAS objects,
+                   albedo uniform in [0.2, 0.8]^3, fov 40, black sky.
+  instanced_meshes 64 instances of 8 procedural meshes (3 value-noise
+                   heightfields of 512x512 vertices, icospheres at levels
+                   7, 6, 6, 5, 5), 2,099,206 unique triangles; random rotation,
+                   uniform scale in [0.5, 2], translation in a 100^3 box.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib, ptr
+
+
+# ---------------------------------------------------------------------------
+# Mesh library
+# ---------------------------------------------------------------------------
+class MeshLibrary:
+    """MeshLibrary of scene/mesh_library.h over the C ABI."""
+
+    def __init__(self):
+        self._h = lib().ae_mesh_library_create()
+        if not self._h:
+            raise MemoryError("ae_mesh_library_create")
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            lib().ae_mesh_library_destroy(h)
+
+    def add(self, vertices, indices, double_sided=False):
+        v = np.ascontiguousarray(vertices, dtype=_lib.VERTEX)
+        i = np.ascontiguousarray(indices, dtype=np.uint32).ravel()
+        handle = lib().ae_mesh_library_add(self._h, ptr(v), len(v), ptr(i), len(i), int(double_sided))
+        if handle < 0:
+            raise _lib.AeError(handle, "ae_mesh_library_add")
+        return handle
+
+    def range(self, handle):
+        r = np.zeros(1, _lib.MESH_RANGE)
+        check(lib().ae_mesh_library_range(self._h, handle, ptr(r)), what="ae_mesh_library_range")
+        return r[0]
+
+    def arrays(self):
+        nv, ni, nb = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        L = lib()
+        L.ae_mesh_library_sizes(self._h, ctypes.byref(nv), ctypes.byref(ni), ctypes.byref(nb))
+
+        def view(p, n, dt):
+            if n == 0:
+                return np.zeros(0, dt)
+            buf = (ctypes.c_char * (n * dt.itemsize)).from_address(p)
+            return np.frombuffer(buf, dtype=dt).copy()
+
+        return (view(L.ae_mesh_library_vertices(self._h), nv.value, _lib.VERTEX),
+                view(L.ae_mesh_library_indices(self._h), ni.value, np.dtype(np.uint32)),
+                view(L.ae_mesh_library_blas(self._h), nb.value, _lib.NODE))
+
+    @property
+    def handle(self):
+        return self._h
+
+
+def build_bvh(bounds):
+    """BuildBVH (scene/bvh.h:275-295) over an (n, 6) float32 array of boxes."""
+    b = np.ascontiguousarray(bounds, dtype=np.float32).reshape(-1, 6)
+    n = len(b)
+    nodes = np.zeros(max(2 * n, 1), _lib.NODE)
+    order = np.zeros(max(n, 1), np.uint32)
+    count = ctypes.c_uint32()
+    check(lib().ae_build_bvh(ptr(b), n, ptr(nodes), ctypes.byref(count), ptr(order)), what="ae_build_bvh")
+    return nodes[:count.value].copy(), order[:n].copy()
+
+
+# ---------------------------------------------------------------------------
+# Mesh generators (local space, outward normals, counter-clockwise winding)
+# ---------------------------------------------------------------------------
+def _verts(p, n, uv):
+    v = np.zeros(len(p), _lib.VERTEX)
+    v["px"], v["py"], v["pz"] = p[:, 0], p[:, 1], p[:, 2]
+    v["nx"], v["ny"], v["nz"] = n[:, 0], n[:, 1], n[:, 2]
+    v["u"], v["v"] = uv[:, 0], uv[:, 1]
+    return v
+
+
+def quad_mesh(u, v):
+    """A parallelogram spanning u and v, centred on its middle (the mesh twin of
+    an analytic quad, Mesh::CreateQuad in scene/mesh.h:248-268)."""
+    u = np.asarray(u, np.float32)
+    v = np.asarray(v, np.float32)
+    n = np.cross(u, v)
+    n = (n / np.linalg.norm(n)).astype(np.float32)
+    corners = np.array([0 * u, u, u + v, v], np.float32) - (u + v) * np.float32(0.5)
+    uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    return _verts(corners, np.tile(n, (4, 1)), uv), np.array([0, 1, 2, 0, 2, 3], np.uint32)
+
+
+def box_mesh(half):
+    """A box of 12 triangles with per-face normals (Mesh::CreateBox layout)."""
+    hx, hy, hz = (np.float32(h) for h in half)
+    faces = [((0, 0, 1), [(-hx, -hy, hz), (hx, -hy, hz), (hx, hy, hz), (-hx, hy, hz)]),
+             ((0, 0, -1), [(hx, -hy, -hz), (-hx, -hy, -hz), (-hx, hy, -hz), (hx, hy, -hz)]),
+             ((-1, 0, 0), [(-hx, -hy, -hz), (-hx, -hy, hz), (-hx, hy, hz), (-hx, hy, -hz)]),
+             ((1, 0, 0), [(hx, -hy, hz), (hx, -hy, -hz), (hx, hy, -hz), (hx, hy, hz)]),
+             ((0, 1, 0), [(-hx, hy, hz), (hx, hy, hz), (hx, hy, -hz), (-hx, hy, -hz)]),
+             ((0, -1, 0), [(-hx, -hy, -hz), (hx, -hy, -hz), (hx, -hy, hz), (-hx, -hy, hz)])]
+    p, n, uv, idx = [], [], [], []
+    for k, (nrm, quad) in enumerate(faces):
+        p += quad
+        n += [nrm] * 4
+        uv += [(0, 0), (1, 0), (1, 1), (0, 1)]
+        b = 4 * k
+        idx += [b, b + 1, b + 2, b, b + 2, b + 3]
+    return _verts(np.array(p, np.float32), np.array(n, np.float32), np.array(uv, np.float32)), np.array(idx, np.uint32)
+
+
+def icosphere(level, radius=1.0):
+    """Icosahedron subdivided `level` times, projected to a sphere:
+    20 * 4^level triangles."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    p = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5], [2, 4, 11],
+                  [6, 2, 10], [8, 6, 7], [9, 8, 1]], np.int64)
+    p /= np.linalg.norm(p, axis=1, keepdims=True)
+    for _ in range(level):
+        e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        e.sort(axis=1)
+        key = e[:, 0] * (len(p) + 1) + e[:, 1]
+        uniq, inv = np.unique(key, return_inverse=True)
+        a, b = uniq // (len(p) + 1), uniq % (len(p) + 1)
+        mid = p[a] + p[b]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        m = (inv + len(p)).reshape(3, -1).T  # mids of edges 01, 12, 20
+        p = np.concatenate([p, mid])
+        f = np.concatenate([np.stack([f[:, 0], m[:, 0], m[:, 2]], 1), np.stack([f[:, 1], m[:, 1], m[:, 0]], 1),
+                            np.stack([f[:, 2], m[:, 2], m[:, 1]], 1), m])
+    n = p.astype(np.float32)
+    pos = (p * radius).astype(np.float32)
+    uv = np.stack([0.5 + np.arctan2(p[:, 2], p[:, 0]) / (2 * np.pi), 0.5 - np.arcsin(p[:, 1]) / np.pi], 1)
+    return _verts(pos, n, uv.astype(np.float32)), f.astype(np.uint32).ravel()
+
+
+def _value_noise(n, cells, rng):
+    """Smooth value noise on an n x n grid: random lattice values on a
+    (cells+1)^2 lattice, bicubic-smoothstep interpolated."""
+    lat = rng.uniform(-1.0, 1.0, size=(cells + 1, cells + 1))
+    x = np.linspace(0, cells, n, endpoint=False)
+    i = np.floor(x).astype(int)
+    fr = x - i
+    s = fr * fr * (3 - 2 * fr)
+    a = lat[np.ix_(i, i)]
+    b = lat[np.ix_(i + 1, i)]
+    c = lat[np.ix_(i, i + 1)]
+    d = lat[np.ix_(i + 1, i + 1)]
+    sy, sx = s[:, None], s[None, :]
+    return (a * (1 - sy) + b * sy) * (1 - sx) + (c * (1 - sy) + d * sy) * sx
+
+
+def heightfield(n, size, amplitude, rng):
+    """n x n vertex grid over [-size/2, size/2]^2 in x/z with value-noise height
+    (three octaves); 2 (n-1)^2 triangles."""
+    h = (_value_noise(n, 8, rng) + 0.5 * _value_noise(n, 16, rng) + 0.25 * _value_noise(n, 32, rng)) * amplitude
+    g = np.linspace(-size / 2, size / 2, n)
+    X, Z = np.meshgrid(g, g, indexing="xy")
+    pos = np.stack([X, h, Z], -1).reshape(-1, 3)
+    dx = np.gradient(h, g, axis=1)
+    dz = np.gradient(h, g, axis=0)
+    nrm = np.stack([-dx, np.ones_like(h), -dz], -1).reshape(-1, 3)
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    uu, vv = np.meshgrid(np.linspace(0, 1, n), np.linspace(0, 1, n), indexing="xy")
+    uv = np.stack([uu, vv], -1).reshape(-1, 2)
+    r = np.arange(n - 1)
+    i00 = (r[:, None] * n + r[None, :]).ravel()
+    i10, i01, i11 = i00 + 1, i00 + n, i00 + n + 1
+    tris = np.stack([np.stack([i00, i01, i10], 1), np.stack([i10, i01, i11], 1)], 1).reshape(-1, 3)
+    return _verts(pos.astype(np.float32), nrm.astype(np.float32), uv.astype(np.float32)), tris.astype(np.uint32).ravel()
+
+
+# ---------------------------------------------------------------------------
+# Entities and packing
+# ---------------------------------------------------------------------------
+def entity(shape, material, position, rotation=(0.0, 0.0, 0.0, 1.0), albedo=(1, 1, 1), **kw):
+    e = np.zeros(1, _lib.ENTITY)[0]
+    e["shape"], e["material"] = shape, material
+    e["position"], e["rotation"] = position, rotation
+    e["prev_position"], e["prev_rotation"] = position, rotation
+    e["albedo"] = albedo
+    e["scale"] = kw.pop("scale", 1.0)
+    e["ior"] = kw.pop("ior", 1.0)
+    e["texture_id"] = _lib.NO_TEXTURE
+    e["texture_tint"] = 0.25
+    for k, v in kw.items():
+        e[k] = v
+    return e
+
+
+def yaw_quat(radians):
+    """Rotation about +Y, x,y,z,w (QuatY, math/quat.hpp:238)."""
+    h = np.float32(radians) * np.float32(0.5)
+    return (0.0, float(np.sin(h)), 0.0, float(np.cos(h)))
+
+
+def random_quat(rng):
+    """Uniform random rotation (Shoemake's method), x,y,z,w."""
+    u1, u2, u3 = rng.random(3)
+    a, b = np.sqrt(1 - u1), np.sqrt(u1)
+    return (a * np.sin(2 * np.pi * u2), a * np.cos(2 * np.pi * u2), b * np.sin(2 * np.pi * u3),
+            b * np.cos(2 * np.pi * u3))
+
+
+class PackedScene:
+    """The seven device arrays of RenderFrame's bind order
+    (renderer/renderer.cpp:1456-1459) plus the config they were made for."""
+
+    def __init__(self, objects, tlas, lights, vertices, indices, blas, instances, config, order=None, name=""):
+        self.objects, self.tlas, self.lights = objects, tlas, lights
+        self.vertices, self.indices, self.blas, self.instances = vertices, indices, blas, instances
+        self.config = config
+        self.order = order
+        self.name = name
+
+    @property
+    def triangles(self):
+        return len(self.indices) // 3
+
+    def device_bytes(self):
+        return sum(a.nbytes for a in (self.objects, self.tlas, self.lights, self.vertices, self.indices, self.blas,
+                                      self.instances))
+
+
+def pack(entities, meshes):
+    """RebuildAcceleration minus the upload: TLAS over the entities, objects in
+    slot order, light IDs, instances (renderer/renderer.cpp:1087-1130)."""
+    ents = np.ascontiguousarray(np.array(entities, dtype=_lib.ENTITY))
+    n = len(ents)
+    objects = np.zeros(max(n, 1), _lib.OBJECT)
+    nodes = np.zeros(2 * n + 1, _lib.NODE)
+    lights = np.zeros(max(n, 1), np.uint32)
+    insts = np.zeros(max(n, 1), _lib.INSTANCE)
+    order = np.zeros(max(n, 1), np.uint32)
+    nn, nl, ni = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    check(lib().ae_pack_scene(ptr(ents), n, meshes.handle if meshes else None, ptr(objects), ptr(nodes),
+                              ctypes.byref(nn), ptr(lights), ctypes.byref(nl), ptr(insts), ctypes.byref(ni),
+                              ptr(order)), what="ae_pack_scene")
+    return objects[:n].copy(), nodes[:nn.value].copy(), lights[:nl.value].copy(), insts[:ni.value].copy(), order[:n]
+
+
+def make_config(width, height, source, target, fov=40.0, depth=8, sky=(0, 0, 0), samples=1, exposure=1.0):
+    c = np.zeros(1, _lib.CONFIG)[0]
+    c["source_x"], c["source_y"], c["source_z"] = source
+    c["target_x"], c["target_y"], c["target_z"] = target
+    c["up_x"], c["up_y"], c["up_z"] = 0.0, 1.0, 0.0
+    c["fov"], c["focus_dist"] = fov, 1.0
+    c["width"], c["height"] = width, height
+    c["samples"], c["batches"], c["depth"] = samples, 1, depth
+    c["sky_r"], c["sky_g"], c["sky_b"] = sky
+    c["exposure"] = exposure
+    c["traceScale"] = 1.0
+    c["historyCap"] = 32.0
+    c["zNear"], c["zFar"] = 0.1, 10000.0
+    return c
+
+
+def _finish(entities, meshes, config, name):
+    objects, tlas, lights, insts, order = pack(entities, meshes)
+    v, i, b = meshes.arrays()
+    config = config.copy()
+    config["num_lights"] = len(lights)
+    config["num_spheres"] = len(objects)
+    return PackedScene(objects, tlas, lights, v, i, b, insts, config, order, name)
+
+
+def cornell_box(seed=1, width=320, height=240, depth=8):
+    """Closed box of 5 mesh-quad walls, 2 yawed mesh cubes and an analytic
+    emissive quad (8 objects, 36 triangles counting the light as 2)."""
+    rng = np.random.default_rng(seed)
+    meshes = MeshLibrary()
+    ents = []
+    L = 10.0
+
+    def alb():
+        return tuple(float(x) for x in rng.uniform(0.2, 0.8, 3))
+
+    # The light first: the reference gathers quads before meshes.
+    ents.append(entity(_lib.SHAPE_QUAD, _lib.MAT_DIFFUSE_LIGHT, (3.5, L - 0.01, 3.5), albedo=(1, 1, 1),
+                       emission=15.0, u=(3.0, 0.0, 0.0), v=(0.0, 0.0, 3.0)))
+    walls = [((L / 2, 0.0, L / 2), (0, 0, L), (L, 0, 0)),       # floor, normal +y
+             ((L / 2, L, L / 2), (L, 0, 0), (0, 0, L)),         # ceiling, normal -y
+             ((L / 2, L / 2, 0.0), (L, 0, 0), (0, L, 0)),       # back, normal +z
+             ((0.0, L / 2, L / 2), (0, L, 0), (0, 0, L)),       # left, normal +x
+             ((L, L / 2, L / 2), (0, 0, L), (0, L, 0))]         # right, normal -x
+    for centre, u, v in walls:
+        h = meshes.add(*quad_mesh(u, v), double_sided=True)
+        ents.append(entity(_lib.SHAPE_MESH, _lib.MAT_LAMBERTIAN, centre, albedo=alb(), mesh=h))
+    for centre, half, yaw in (((3.3, 1.5, 3.7), (1.5, 1.5, 1.5), -0.3), ((6.6, 3.0, 6.2), (1.5, 3.0, 1.5), 0.35)):
+        h = meshes.add(*box_mesh(half))
+        ents.append(entity(_lib.SHAPE_MESH, _lib.MAT_LAMBERTIAN, centre, rotation=yaw_quat(yaw), albedo=alb(), mesh=h))
+    cfg = make_config(width, height, (5.0, 5.0, 24.0), (5.0, 5.0, 0.0), fov=40.0, depth=depth, sky=(0, 0, 0))
+    return _finish(ents, meshes, cfg, "cornell_box")
+
+
+def instanced_meshes(seed=2, width=1920, height=1080, levels=(7, 6, 6, 5, 5), grid=512, n_instances=64,
+                     n_heightfields=3):
+    """64 instances over 8 unique meshes; 2,099,206 triangles at the defaults."""
+    rng = np.random.default_rng(seed)
+    meshes = MeshLibrary()
+    handles = []
+    for _ in range(n_heightfields):
+        handles.append(meshes.add(*heightfield(grid, 20.0, 2.5, rng)))
+    for lv in levels:
+        handles.append(meshes.add(*icosphere(lv, 5.0)))
+    ents = []
+    for k in range(n_instances):
+        pos = tuple(float(x) for x in rng.uniform(0.0, 100.0, 3))
+        rot = random_quat(rng)
+        scale = float(rng.uniform(0.5, 2.0))
+        ents.append(entity(_lib.SHAPE_MESH, _lib.MAT_LAMBERTIAN, pos, rotation=rot, scale=scale,
+                           albedo=tuple(float(x) for x in rng.uniform(0.2, 0.8, 3)), mesh=handles[k % len(handles)]))
+    cfg = make_config(width, height, (50.0, 55.0, 175.0), (50.0, 50.0, 50.0), fov=40.0, depth=2, sky=(0.5, 0.6, 0.8))
+    return _finish(ents, meshes, cfg, "instanced_meshes")

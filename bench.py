@@ -1,0 +1,339 @@
+"""Closest-hit throughput of the ray-tracing hot path on one B200 (or N
+independent replicas), with the reference's CPU implementation timed beside it.
+
+Workload (`instanced_meshes`, seeded): 64 instances of 8 procedural meshes,
+2,099,206 unique triangles (3 value-noise heightfields of 512x512 vertices,
+icospheres at levels 7, 6, 6, 5, 5), random rotation, uniform scale in
+[0.5, 2], translation in a 100^3 box.  One step traces the 1920x1080 camera
+rays of frame 0 (2,073,600) and then one diffuse bounce ray per primary hit,
+closest hit each, ray set already resident in HBM.  L2 is flushed (a 512 MB
+write) before every timed step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--variant plain|fast|quant]
+
+Prints one JSON line (rank 0).  Under torchrun each rank is an independent
+replica on its own GPU (the path does not shard across GPUs); value is the
+sum over ranks, timed as the max over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "closest-hit Mrays/s (1080p primary + diffuse bounce rays, 2.1M-triangle instanced scene)"
+UNIT = "Mrays/s"
+VARIANTS = {"plain": 0, "fast": 1, "quant": 2}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[4 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """DRAM bytes per ray of the closest-hit kernel from a committed ncu
+    summary (profiles/closest_hit_traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "closest_hit_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+def make_workload(ctx, scene):
+    """Primary rays of frame 0 and one diffuse bounce per primary hit."""
+    from aviatorengine2_b200 import _lib
+    prim = ctx.camera_rays()
+    hits = ctx.closest_hit(prim, _lib.VARIANT_PLAIN)
+    bounce, valid = ctx.bounce_rays(prim, hits)
+    return prim, bounce[valid].copy()
+
+
+def cpu_reference(scene, rays, budget_s=20.0):
+    """The reference's own traversal (its shader, compiled for the CPU under
+    oracle/_ref) on a bounded sample of the ray set, all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    cores = os.cpu_count() or 1
+    fn = O.ref_closest_hit if kind == "reference" else O.closest_hit
+    rng = np.random.default_rng(0)
+    n = min(len(rays), 65536)
+    sample = rays[np.sort(rng.choice(len(rays), n, replace=False))]
+    t0 = time.perf_counter()
+    fn(scene, sample, threads=cores)
+    dt = time.perf_counter() - t0
+    # Grow the sample to fill about `budget_s` of CPU time (bounded).
+    n2 = int(min(len(rays), max(n, n * budget_s / max(dt, 1e-3) * 0.5)))
+    if n2 > n:
+        sample = rays[np.sort(rng.choice(len(rays), n2, replace=False))]
+        t0 = time.perf_counter()
+        fn(scene, sample, threads=cores)
+        dt = time.perf_counter() - t0
+        n = n2
+    return {"value": n / dt / 1e6, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{n} rays drawn uniformly from the step's {len(rays)} (primary + bounce), {dt:.2f} s"}
+
+
+def run_reference_arm(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    from aviatorengine2_b200 import Context, scenes
+    scene = scenes.instanced_meshes()
+    with Context(int(scene.config["width"]), int(scene.config["height"]), device=local) as ctx:
+        ctx.upload(scene)
+        prim, bounce = make_workload(ctx, scene)
+    rays = np.concatenate([prim, bounce])
+    steps = []
+    for _ in range(args.warmup):
+        cpu_reference(scene, rays[:20000], budget_s=0.0)
+    base = None
+    for _ in range(args.steps):
+        base = cpu_reference(scene, rays, budget_s=8.0)
+        steps.append(base["value"])
+    v = float(np.median(steps))
+    base["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": len(rays) / (v * 1e6) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": "instanced_meshes 1920x1080 primary+bounce closest hit",
+                       "rays_per_step": int(len(rays)), "triangles": int(scene.triangles)},
+            "cpu_baseline": base, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--variant", default=os.environ.get("AE_BENCH_VARIANT", "best"))
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    from aviatorengine2_b200 import Context, _lib, scenes
+    scene = scenes.instanced_meshes()
+    W, H = int(scene.config["width"]), int(scene.config["height"])
+    ctx = Context(W, H, device=local)
+    ctx.upload(scene)
+    prim, bounce = make_workload(ctx, scene)
+    n1, n2 = len(prim), len(bounce)
+    variant = args.variant
+    if variant == "best":
+        try:
+            ctx.prepare_fast()
+            variant = "fast"
+        except Exception:
+            variant = "plain"
+    vid = VARIANTS[variant]
+
+    dev = torch.device("cuda", local)
+    d_prim = torch.from_numpy(prim.view(np.uint8)).to(dev)
+    d_bounce = torch.from_numpy(bounce.view(np.uint8)).to(dev)
+    d_hits1 = torch.empty(n1 * 20, dtype=torch.uint8, device=dev)
+    d_hits2 = torch.empty(n2 * 20, dtype=torch.uint8, device=dev)
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+    ext = torch.cuda.ExternalStream(ctx.stream)
+
+    def step():
+        ctx.closest_hit_device(d_prim.data_ptr(), n1, d_hits1.data_ptr(), vid)
+        ctx.closest_hit_device(d_bounce.data_ptr(), n2, d_hits2.data_ptr(), vid)
+
+    for _ in range(args.warmup):
+        step()
+    ctx.synchronize()
+
+    # Algorithmic bytes of the reference traversal over this ray set.
+    cnt = np.zeros(6, np.uint64)
+    _lib.check(_lib.lib().ae_trace_counters(ctx.handle, d_prim.data_ptr(), n1, _lib.ptr(cnt)), ctx.handle)
+    cnt2 = np.zeros(6, np.uint64)
+    _lib.check(_lib.lib().ae_trace_counters(ctx.handle, d_bounce.data_ptr(), n2, _lib.ptr(cnt2)), ctx.handle)
+    per = np.array([48, 128, 48, 48, 48, 60], np.float64)
+    alg_bytes_step = float((cnt.astype(np.float64) * per).sum() + (cnt2.astype(np.float64) * per).sum())
+
+    launches0 = ctx.launch_count
+    times = []
+    with ClockSampler(local) as clk:
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(ext):
+                e0.record()
+                step()
+                e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+    launches = ctx.launch_count - launches0
+    ms = float(np.sum(times)) / args.steps
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    rays_step = n1 + n2
+    value = rays_step * world / (ms / 1e3) / 1e6
+
+    # End to end through the public call with host buffers: pinned host rays
+    # in, hits out, per step.
+    h_prim = torch.from_numpy(prim.view(np.uint8)).pin_memory()
+    h_bounce = torch.from_numpy(bounce.view(np.uint8)).pin_memory()
+    h_h1 = torch.empty(n1 * 20, dtype=torch.uint8).pin_memory()
+    h_h2 = torch.empty(n2 * 20, dtype=torch.uint8).pin_memory()
+    L = _lib.lib()
+
+    def e2e_step():
+        _lib.check(L.ae_closest_hit(ctx.handle, h_prim.data_ptr(), n1, h_h1.data_ptr(), vid), ctx.handle)
+        _lib.check(L.ae_closest_hit(ctx.handle, h_bounce.data_ptr(), n2, h_h2.data_ptr(), vid), ctx.handle)
+
+    for _ in range(2):
+        e2e_step()
+    et = []
+    for _ in range(max(3, args.steps // 2)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        et.append(time.perf_counter() - t0)
+    e2e_s = float(np.mean(et))
+    if pg:
+        t = torch.tensor([e2e_s], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": rays_step * world / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": int((n1 + n2) * 32),
+           "d2h_bytes_per_step": int((n1 + n2) * 20)}
+
+    peak, peak_kind = load_peaks()
+    achieved = alg_bytes_step / (ms / 1e3) / 1e9
+    traffic = load_traffic()
+    traffic_bytes = None
+    if traffic and traffic.get("variant") == variant:
+        traffic_bytes = float(traffic["dram_bytes_per_ray"]) * rays_step / 2
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic_bytes, "peak_source": peak_kind,
+                "algorithmic_bytes_per_ray": alg_bytes_step / rays_step,
+                "note": "algorithmic bytes = reference-walk touches (48 B node, 128 B object, 48 B instance, "
+                        "48 B triangle, 60 B winner) counted on the device over the step's ray set; achieved = "
+                        "those bytes / measured step time; traffic = per launch (mean of the two launches)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_reference(scene, np.concatenate([prim, bounce]))
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene and camera)",
+            "config": {"workload": "instanced_meshes 1920x1080 primary+bounce closest hit", "variant": variant,
+                       "rays_per_step": rays_step, "primary_rays": n1, "bounce_rays": n2,
+                       "triangles": int(scene.triangles), "instances": int(len(scene.instances)),
+                       "l2": "flushed before every step (512 MB write)", "parallelism": f"replicas x{world}"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "per_step_ms": [round(t, 4) for t in times]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,437 @@
+/*
+ * ae_b200.h - C ABI of the B200 ray/path-tracing library.
+ *
+ * This header is the drop-in boundary that replaces the SDL_gpu compute
+ * dispatch of AviatorEngine2's renderer.  Everything crossing it is a plain C
+ * type: byte layouts identical to the reference's shader contract, pointers
+ * and sizes.  No CUDA or torch type appears in a signature.
+ *
+ * Byte contract (each struct re-declared here with its size pinned):
+ *   ae_object      == Object_GPU        scene/gpu_types.h:26-81     (128 B)
+ *   ae_instance    == MeshInstance_GPU  scene/gpu_types.h:84-96     (48 B)
+ *   ae_bvh_node    == BVHNode_GPU       scene/bvh.h:31-43           (48 B)
+ *   ae_vertex      == Vertex_GPU        scene/mesh_library.h:39-46  (32 B)
+ *   ae_config      == Config            renderer/renderer.h:76-147  (240 B)
+ *
+ * Extension: ae_instance.scale occupies MeshInstance_GPU::pad0 (offset 12).
+ * The reference transform is rigid (scene/gpu_types.h:83); a value of 0 or 1
+ * means "no scale", so reference-packed instances (pad0 = 0) trace unchanged.
+ *
+ * Every entry point returns AE_OK (0) or a negative ae_status; the message of
+ * the last failure on a context is available from ae_last_error().  The
+ * reference returns bool + SDL_Log (renderer/renderer.cpp:938-949); the status
+ * codes name the same failure classes.
+ *
+ * Threading: one host thread per context, as the reference drives its Renderer
+ * from the main loop (main.cpp:157-369).  Calls on one context are not
+ * re-entrant.  The serving API (ae_serve_*) is internally threaded and is the
+ * one exception: it may be called from any thread.
+ */
+#ifndef AE_B200_H
+#define AE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+typedef enum ae_status {
+    AE_OK = 0,
+    AE_ERR_INVALID = -1,     /* bad argument (null pointer, zero size, bad enum) */
+    AE_ERR_OOM = -2,         /* device or host allocation failed                 */
+    AE_ERR_OVERSIZE = -3,    /* upload larger than the buffers sized at creation  */
+    AE_ERR_LAYOUT = -4,      /* scene arrays are inconsistent (index out of range) */
+    AE_ERR_CUDA = -5,        /* a CUDA runtime call failed                        */
+    AE_ERR_TIMEOUT = -6,     /* a bounded device-side wait gave up                */
+    AE_ERR_STATE = -7,       /* call order violated (e.g. trace before upload)    */
+    AE_ERR_REJECTED = -8     /* serving: request refused at admission             */
+} ae_status;
+
+/* ------------------------------------------------------------------------ */
+/* Byte contract                                                             */
+/* ------------------------------------------------------------------------ */
+
+/* BodyShape, scene/gpu_types.h:14-21 */
+enum { AE_SHAPE_SPHERE = 0, AE_SHAPE_QUAD = 1, AE_SHAPE_BOX = 2, AE_SHAPE_TRIANGLE = 3, AE_SHAPE_MESH = 4 };
+/* MaterialType, scene/material.h:11-18 */
+enum { AE_MAT_LAMBERTIAN = 0, AE_MAT_METAL = 1, AE_MAT_DIELECTRIC = 2, AE_MAT_DIFFUSE_LIGHT = 3, AE_MAT_ISOTROPIC = 4 };
+/* kNoTexture, scene/texture.h:19 */
+#define AE_NO_TEXTURE 0xFFFFFFFFu
+
+/* Object_GPU, scene/gpu_types.h:26-81 (128 B). */
+typedef struct ae_object {
+    float x, y, z;          /*   0 position                        */
+    float prevRotX;         /*  12                                  */
+    float x2, y2, z2;       /*  16 previous position                */
+    float radius;           /*  28                                  */
+    float u_x, u_y, u_z;    /*  32 quad/triangle edge u             */
+    float prevRotY;         /*  44                                  */
+    float v_x, v_y, v_z;    /*  48 quad/triangle edge v             */
+    float prevRotZ;         /*  60                                  */
+    float half_x, half_y, half_z; /* 64 box half extents            */
+    float rotation;         /*  76 yaw                              */
+    float density;          /*  80                                  */
+    float emission;         /*  84                                  */
+    uint32_t instanceIndex; /*  88                                  */
+    float textureTint;      /*  92                                  */
+    float r, g, b;          /*  96 albedo                           */
+    float fuzz;             /* 108                                  */
+    float refraction;       /* 112                                  */
+    uint32_t shapeType;     /* 116                                  */
+    uint32_t colorType;     /* 120                                  */
+    uint32_t textureID;     /* 124                                  */
+} ae_object;
+
+/* MeshInstance_GPU, scene/gpu_types.h:84-96 (48 B).  `scale` is pad0. */
+typedef struct ae_instance {
+    float px, py, pz;
+    float scale;            /* 12: uniform scale, 0 or 1 = rigid (reference) */
+    float qx, qy, qz, qw;   /* 16: rotation, x,y,z,w memory order            */
+    uint32_t vertexBase;    /* 32 */
+    uint32_t indexBase;     /* 36 */
+    uint32_t triangleCount; /* 40 */
+    uint32_t blasBase;      /* 44 */
+} ae_instance;
+
+/* BVHNode_GPU, scene/bvh.h:31-43 (48 B).  count > 0: leaf, left = first slot. */
+typedef struct ae_bvh_node {
+    float min_x, min_y, min_z;
+    float pad0;
+    float max_x, max_y, max_z;
+    int32_t left;
+    int32_t right;
+    int32_t count;
+    int32_t padding;
+    int32_t pad_trailing;
+} ae_bvh_node;
+
+/* Vertex_GPU, scene/mesh_library.h:39-46 (32 B). */
+typedef struct ae_vertex {
+    float px, py, pz;
+    float nx, ny, nz;
+    float u, v;
+} ae_vertex;
+
+/* AABB, scene/aabb.h:14-22 (24 B). */
+typedef struct ae_aabb {
+    float min_x, min_y, min_z;
+    float max_x, max_y, max_z;
+} ae_aabb;
+
+/* Config, renderer/renderer.h:76-147 (240 B). */
+typedef struct ae_config {
+    float source_x, source_y, source_z;
+    float fov;
+    float target_x, target_y, target_z;
+    float focus_dist;
+    float defocus_angle;
+    float padding[3];
+    float up_x, up_y, up_z;
+    float oof;
+    float sky_r, sky_g, sky_b;
+    uint32_t width;
+    float horizon_r, horizon_g, horizon_b;
+    uint32_t height;
+    uint32_t samples;
+    uint32_t batches;
+    uint32_t batch;
+    uint32_t depth;
+    uint32_t num_spheres;
+    uint32_t renderType;
+    uint32_t num_lights;
+    float exposure;          /* 124 */
+    uint32_t debugView;      /* 128 */
+    float zNear, zFar;
+    float jitter_x, jitter_y;
+    uint32_t displayOnly;    /* 148 */
+    float traceScale;        /* 152 */
+    uint32_t frameIndex;     /* 156 */
+    uint32_t historyReset;
+    uint32_t cameraMoved;
+    float historyCap;        /* 168 */
+    float padding3;
+    float prevViewProj[16];  /* 176, row-major Mat4 (math/mat4.h) */
+} ae_config;
+
+/* ------------------------------------------------------------------------ */
+/* Ray and hit records of the closest-hit / any-hit entry points             */
+/* ------------------------------------------------------------------------ */
+
+/* A ray as the shaders build it (hybrid:32-41): origin, near bound, direction,
+ * time.  The far bound starts at 1e6 as TraverseBVH does (hybrid:869). */
+typedef struct ae_ray {
+    float ox, oy, oz;
+    float tnear;
+    float dx, dy, dz;
+    float time;
+} ae_ray;
+
+/* The closest hit.  object = slot in the object buffer (the TLAS leaf order),
+ * AE_MISS on a miss.  prim = triangle slot inside the mesh (leaf order of its
+ * BLAS, i.e. (bestBase - indexBase) / 3 in hybrid:600-707), AE_MISS for
+ * analytic objects.  alpha/beta are HitMeshTriangle's weights of v1 and v2
+ * (hybrid:564-598) or HitQuad's plane coordinates for quads. */
+typedef struct ae_hit {
+    float t;
+    float alpha;
+    float beta;
+    uint32_t object;
+    uint32_t prim;
+} ae_hit;
+#define AE_MISS 0xFFFFFFFFu
+
+/* ------------------------------------------------------------------------ */
+/* Host-side acceleration structure (the reference's CPU side)               */
+/* ------------------------------------------------------------------------ */
+
+/* Binned-SAH BVH over `n` boxes; BuildBVH, scene/bvh.h:275-295.
+ * out_nodes must hold 2*n nodes (the builder never emits more than 2n-1);
+ * out_order receives the n-entry leaf-slot permutation.  *out_node_count is
+ * set to the number of nodes written.  n == 0 writes nothing. */
+int ae_build_bvh(const ae_aabb *bounds, uint32_t n,
+                 ae_bvh_node *out_nodes, uint32_t *out_node_count,
+                 uint32_t *out_order);
+
+/* Mesh library: MeshLibrary, scene/mesh_library.h:64-159, with 32-bit input
+ * indices (the reference's Mesh is uint16, scene/mesh.h:24, too small for a
+ * 512x512 grid).  Add() appends local vertices, builds the BLAS over the
+ * triangles' AABBs and appends the indices in BLAS leaf order. */
+typedef struct ae_mesh_library ae_mesh_library;
+typedef struct ae_mesh_range {
+    uint32_t vertexBase, indexBase, triangleCount, blasBase;
+    ae_aabb localBounds;
+    uint32_t doubleSided;
+} ae_mesh_range;
+
+ae_mesh_library *ae_mesh_library_create(void);
+void ae_mesh_library_destroy(ae_mesh_library *lib);
+/* Returns the mesh handle (>= 0) or a negative ae_status. */
+int ae_mesh_library_add(ae_mesh_library *lib, const ae_vertex *vertices, uint32_t nv,
+                        const uint32_t *indices, uint32_t ni, int double_sided);
+int ae_mesh_library_range(const ae_mesh_library *lib, uint32_t handle, ae_mesh_range *out);
+/* Sizes of the flattened arrays (elements). */
+void ae_mesh_library_sizes(const ae_mesh_library *lib, uint64_t *nv, uint64_t *ni, uint64_t *nb);
+/* Borrowed pointers into the flattened arrays; valid until the next add. */
+const ae_vertex *ae_mesh_library_vertices(const ae_mesh_library *lib);
+const uint32_t *ae_mesh_library_indices(const ae_mesh_library *lib);
+const ae_bvh_node *ae_mesh_library_blas(const ae_mesh_library *lib);
+
+/* One renderable entity, the host-side union of TransformComponent,
+ * MaterialComponent and the shape component (scene/components.h:31-148). */
+typedef struct ae_entity {
+    uint32_t shape;          /* AE_SHAPE_*                                   */
+    uint32_t material;       /* AE_MAT_*                                     */
+    float position[3];       /* TransformComponent::position                 */
+    float rotation[4];       /* TransformComponent::rotation, x,y,z,w        */
+    float scale;             /* mesh instances only: uniform scale (1 = rigid) */
+    float albedo[3];
+    float fuzz, ior, emission, density;
+    float texture_tint;
+    uint32_t texture_id;
+    float radius;            /* sphere                                       */
+    float u[3], v[3];        /* quad / triangle edges (local, unrotated)     */
+    float half_extent[3];    /* box                                          */
+    uint32_t mesh;           /* mesh handle for AE_SHAPE_MESH                */
+    float prev_position[3];  /* last frame's transform (Object_GPU x2..)     */
+    float prev_rotation[4];
+} ae_entity;
+
+/* TLAS assembly: GatherRenderables (scene/shapes.h:379-426) + BuildBVH +
+ * entity reorder + LightIndices (renderer/renderer.cpp:803-813) + PackObjects
+ * (renderer/renderer.cpp:815-929).  Entities are taken in the caller's order
+ * (the reference's gather order is per shape type: spheres, quads, boxes,
+ * triangles, meshes; callers that need its exact slot order pass them so).
+ * Capacities: out_objects/out_instances n, out_nodes 2n+1, out_lights n,
+ * out_order n.  Counts are written through the count pointers. */
+int ae_pack_scene(const ae_entity *entities, uint32_t n, const ae_mesh_library *lib,
+                  ae_object *out_objects, ae_bvh_node *out_nodes, uint32_t *out_node_count,
+                  uint32_t *out_lights, uint32_t *out_light_count,
+                  ae_instance *out_instances, uint32_t *out_instance_count,
+                  uint32_t *out_order);
+
+/* World bounds of one entity (SphereBounds/QuadBounds/BoxBounds/
+ * TriangleBounds/MeshBounds, scene/shapes.h:70-145). */
+int ae_entity_bounds(const ae_entity *e, const ae_mesh_library *lib, ae_aabb *out);
+
+/* ------------------------------------------------------------------------ */
+/* Device context: Renderer, renderer/renderer.h:325-411                     */
+/* ------------------------------------------------------------------------ */
+
+typedef struct ae_ctx ae_ctx;
+
+/* RendererSettings, renderer/renderer.h:225-274 (window/shader-name fields
+ * dropped: there is no window; the kernels are compiled in). */
+typedef struct ae_settings {
+    uint32_t width, height;
+    uint32_t samples;          /* samples per pixel per frame                 */
+    uint32_t max_samples;      /* 0 = accumulate forever                      */
+    uint32_t hybrid;           /* 1 = deferred resolve, 0 = compute-only      */
+    uint32_t hybrid_max_depth; /* path segments in hybrid mode (default 3)    */
+    float trace_scale;         /* 1, 0.75, 0.5 (TraceResolution)              */
+    uint32_t history_while_moving;
+    int32_t device;            /* CUDA device ordinal                         */
+    uint32_t reserved[7];
+} ae_settings;
+
+/* Kernel families.  PLAIN reproduces the reference order of operations;
+ * FAST is the optimised closest-hit (ordered traversal, packed triangles);
+ * QUANT adds 8-bit child bounds and the watertight triangle test. */
+enum { AE_VARIANT_PLAIN = 0, AE_VARIANT_FAST = 1, AE_VARIANT_QUANT = 2 };
+
+/* Render modes for ae_render_frame. */
+enum { AE_MODE_COMPUTE_ONLY = 0, AE_MODE_DEFERRED = 1, AE_MODE_WAVEFRONT = 2 };
+
+/* Image identifiers for ae_read_image. */
+enum {
+    AE_IMAGE_ACCUM = 0,    /* float4 linear accumulation (RGBA32F)           */
+    AE_IMAGE_DISPLAY = 1,  /* uint8x4 sRGB display image                     */
+    AE_IMAGE_FRAME = 2,    /* float4 this frame's radiance before blending   */
+    AE_IMAGE_REDUCED = 3,  /* float4 lightingReduced (deferred, reduced grid) */
+    AE_IMAGE_HISTORY_GEOMETRY = 4 /* float4 historyGeometry[write]           */
+};
+
+/* Renderer::Initialize.  Returns NULL on failure; the reason is printed to
+ * stderr (there is no context to hold it yet). */
+ae_ctx *ae_create(const ae_settings *settings);
+/* Renderer::Shutdown. */
+void ae_destroy(ae_ctx *ctx);
+const char *ae_last_error(const ae_ctx *ctx);
+
+/* Renderer::UploadMeshGeometry (renderer/renderer.cpp:706-785): vertices,
+ * indices and BLAS nodes, once.  Sizes the geometry buffers. */
+int ae_upload_geometry(ae_ctx *ctx, const ae_vertex *vertices, uint32_t nv,
+                       const uint32_t *indices, uint32_t ni,
+                       const ae_bvh_node *blas, uint32_t nb);
+
+/* Renderer::CreateSceneBuffers (renderer/renderer.cpp:553-628): worst-case
+ * capacities for the per-frame arrays.  Optional: ae_upload_scene sizes them
+ * on first use. */
+int ae_reserve_scene(ae_ctx *ctx, uint32_t max_objects, uint32_t max_lights);
+
+/* Renderer::UploadScene (renderer/renderer.cpp:931-1027): objects, TLAS,
+ * light IDs and instances, in the storage-buffer order of RenderFrame
+ * (renderer/renderer.cpp:1456-1459).  Fails with AE_ERR_OVERSIZE beyond the
+ * reserved capacity, like the reference. */
+int ae_upload_scene(ae_ctx *ctx, const ae_object *objects, uint32_t n_objects,
+                    const ae_bvh_node *tlas, uint32_t n_nodes,
+                    const uint32_t *light_ids, uint32_t n_lights,
+                    const ae_instance *instances, uint32_t n_instances);
+
+/* SDL_PushGPUComputeUniformData(Config) (renderer/renderer.cpp:1426). */
+int ae_set_config(ae_ctx *ctx, const ae_config *config);
+int ae_get_config(const ae_ctx *ctx, ae_config *config);
+
+/* Per-frame state of RenderFrame (renderer/renderer.cpp:1332-1588):
+ * Renderer::ResetAccumulation / CameraMoved / MarkSceneDirty equivalents. */
+int ae_reset_accumulation(ae_ctx *ctx);
+
+/* G-buffer planes consumed by the deferred resolve, host or device pointers
+ * per `on_device`.  Layout of renderer/renderer.cpp:370-421: position RGBA32F
+ * (w = object slot as float), normal RGBA32F here (w = coverage; the
+ * reference stores RGBA16F), albedo RGBA8 (a = 0 for view-dependent), depth
+ * float. */
+typedef struct ae_gbuffer {
+    const float *position;
+    const float *normal;
+    const uint8_t *albedo;
+    const float *depth;
+    uint32_t on_device;
+} ae_gbuffer;
+
+/* One dispatch: the compute-only megakernel (hybrid:1328-1404), or the
+ * deferred resolve (deferred:1879-2010) followed by the temporal upsample
+ * (upsample:280-390) when config.traceScale < 1, or the wavefront path
+ * tracer.  Uses the config set by ae_set_config (batch/frameIndex included). */
+int ae_render_frame(ae_ctx *ctx, int mode, const ae_gbuffer *gbuffer);
+
+/* Produce the G-buffer on the device by ray casting the primary hit with the
+ * reference camera (the raster pass gbuffer.vert/frag writes the same planes).
+ * The planes stay resident and feed the next deferred frame. */
+int ae_build_gbuffer(ae_ctx *ctx);
+
+/* Copy an image to host memory.  dst_bytes must be >= the image size. */
+int ae_read_image(ae_ctx *ctx, int which, void *dst, size_t dst_bytes);
+
+/* Closest hit for a batch of HOST rays: copies in, traces, copies out,
+ * pipelined in chunks over streams.  variant = AE_VARIANT_*. */
+int ae_closest_hit(ae_ctx *ctx, const ae_ray *rays, uint32_t n, ae_hit *hits, int variant);
+/* Same with DEVICE pointers, on the context's stream, no synchronisation. */
+int ae_closest_hit_device(ae_ctx *ctx, const ae_ray *d_rays, uint32_t n, ae_hit *d_hits, int variant);
+/* Any hit in [tnear, tmax] with the deferred shader's rules (Occluded,
+ * deferred:1115-1171: glass and lights do not block).  out[i] = 1 when
+ * occluded.  Host pointers. */
+int ae_any_hit(ae_ctx *ctx, const ae_ray *rays, const float *tmax, uint32_t n, uint8_t *out);
+
+/* Ray sets of the closest-hit workload, host buffers.
+ * ae_camera_rays: the width*height primary rays of the current config's
+ * Batch in row-major pixel order, as main builds them (hybrid:1346-1373).
+ * ae_bounce_rays: for ray i (pixel i) and its closest hit, one diffuse
+ * bounce (n + RandomDirection(), hybrid:980-986) drawn from pixel i's RNG
+ * stream after its camera ray, origin offset 0.001 along the facing normal
+ * (hybrid:1294-1296).  valid[i] = 0 where the primary missed (out[i] is then
+ * a copy of the primary ray). */
+int ae_camera_rays(ae_ctx *ctx, ae_ray *out);
+int ae_bounce_rays(ae_ctx *ctx, const ae_ray *primary, const ae_hit *hits, uint32_t n, ae_ray *out, uint8_t *valid);
+
+/* Algorithmic traffic of the reference traversal over DEVICE rays: the
+ * touches of TraverseBVH/HitMesh (hybrid:600-917) summed over the set, as
+ * counters[6] = TLAS nodes, object records, instance records, BLAS nodes,
+ * triangles tested, closest-hit winners.  The roofline's bytes per ray are
+ * 48, 128, 48, 48, 48 and 60 bytes per touch respectively. */
+int ae_trace_counters(ae_ctx *ctx, const ae_ray *d_rays, uint32_t n, uint64_t *counters);
+
+/* Synchronise the context's stream.  Returns AE_ERR_CUDA on a sticky error. */
+int ae_synchronize(ae_ctx *ctx);
+/* Device time in milliseconds of the last kernel launch that the context
+ * timed (events recorded on the launching stream). */
+int ae_last_kernel_ms(ae_ctx *ctx, float *ms);
+/* Raw CUDA stream of the context (cudaStream_t), for callers that order their
+ * own work against it. */
+void *ae_stream(ae_ctx *ctx);
+/* Number of kernel launches issued by this context since creation. */
+uint64_t ae_launch_count(const ae_ctx *ctx);
+
+/* Rebuild the derived device structures (packed triangles, 4-wide quantised
+ * BVH) after ae_upload_geometry.  Called implicitly on first use. */
+int ae_prepare_fast(ae_ctx *ctx);
+
+/* GPU TLAS refit: new instance transforms on the device; recompute world
+ * bounds of every mesh object bottom-up without rebuilding topology
+ * (replaces the per-frame CPU rebuild of renderer/renderer.cpp:1087-1130
+ * when only transforms changed). */
+int ae_refit_instances(ae_ctx *ctx, const ae_instance *instances, uint32_t n);
+
+#ifdef __cplusplus
+} /* extern "C" */
+
+static_assert(sizeof(ae_object) == 128, "Object_GPU stride");
+static_assert(offsetof(ae_object, radius) == 28, "Object_GPU layout");
+static_assert(offsetof(ae_object, rotation) == 76, "Object_GPU layout");
+static_assert(offsetof(ae_object, density) == 80, "Object_GPU layout");
+static_assert(offsetof(ae_object, emission) == 84, "Object_GPU layout");
+static_assert(offsetof(ae_object, textureTint) == 92, "Object_GPU layout");
+static_assert(offsetof(ae_object, r) == 96, "Object_GPU layout");
+static_assert(offsetof(ae_object, fuzz) == 108, "Object_GPU layout");
+static_assert(offsetof(ae_object, textureID) == 124, "Object_GPU layout");
+static_assert(sizeof(ae_instance) == 48, "MeshInstance_GPU stride");
+static_assert(sizeof(ae_bvh_node) == 48, "BVHNode_GPU stride");
+static_assert(sizeof(ae_vertex) == 32, "Vertex_GPU stride");
+static_assert(offsetof(ae_config, exposure) == 124, "Config layout");
+static_assert(offsetof(ae_config, debugView) == 128, "Config layout");
+static_assert(offsetof(ae_config, jitter_y) == 144, "Config layout");
+static_assert(offsetof(ae_config, displayOnly) == 148, "Config layout");
+static_assert(offsetof(ae_config, traceScale) == 152, "Config layout");
+static_assert(offsetof(ae_config, frameIndex) == 156, "Config layout");
+static_assert(offsetof(ae_config, historyCap) == 168, "Config layout");
+static_assert(offsetof(ae_config, prevViewProj) == 176, "Config layout");
+static_assert(sizeof(ae_config) == 240, "Config size");
+static_assert(sizeof(ae_ray) == 32, "ray record");
+static_assert(sizeof(ae_hit) == 20, "hit record");
+#endif
+
+#endif /* AE_B200_H */

@@ -1,0 +1,871 @@
+// oracle.cpp - TEST INFRASTRUCTURE ONLY.  A CPU restatement of AviatorEngine2's
+// ray/path-tracing hot path, used by tests/ as the parity checker and by
+// bench.py as the timed CPU baseline.  The library never links or calls it.
+//
+// Parity pinning: the reference has no CPU ray tracer and no golden vectors
+// for this path.  This restatement is pinned against the reference's own
+// shader code run on the CPU (oracle/_ref, built by the Makefile from
+// shaders/ray_trace.comp.hybrid.hlsl through hlsl2cpp.py) on identical inputs:
+// closest hits and rendered frames must agree bit for bit
+// (tests/test_oracle_pin.py), and against golden fixtures generated that way
+// (tests/golden/).
+//
+// Templated on the arithmetic type.  float reproduces the reference's order of
+// operations with ae_math.h intrinsics (the ones the kernels use); double is
+// the FP64 oracle for image error, with libm transcendentals, the same RNG
+// stream (each draw widened exactly) and the same estimator.
+//
+// Every function cites the reference lines it restates.  `hybrid:N` is
+// shaders/ray_trace.comp.hybrid.hlsl line N.
+#include <omp.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+
+#include "../aviatorengine2_b200/csrc/ae_math.h"
+#include "../include/ae_b200.h"
+
+namespace oracle {
+
+// ---------------------------------------------------------------------------
+// Arithmetic per type
+// ---------------------------------------------------------------------------
+template <class T> struct M;
+template <> struct M<float> {
+    static float sqrt(float x) { return AE_SQRT(x); }
+    static float sin(float x) { return ae::sinf_(x); }
+    static float cos(float x) { return ae::cosf_(x); }
+    static float tan(float x) { return ae::tanf_(x); }
+    static float pow(float x, float y) { return ae::powf_(x, y); }
+    static float log(float x) { return ae::logf_(x); }
+    static float acos(float x) { return ae::acosf_(x); }
+    static float atan2(float y, float x) { return ae::atan2f_(y, x); }
+    static float fmin(float a, float b) { return AE_FMIN(a, b); }
+    static float fmax(float a, float b) { return AE_FMAX(a, b); }
+    static float rnd(float u) { return u; }
+};
+template <> struct M<double> {
+    static double sqrt(double x) { return std::sqrt(x); }
+    static double sin(double x) { return std::sin(x); }
+    static double cos(double x) { return std::cos(x); }
+    static double tan(double x) { return std::tan(x); }
+    static double pow(double x, double y) {
+        // Integer exponents multiply exactly, as the float intrinsic does.
+        if (y == std::floor(y) && std::fabs(y) <= 64) {
+            int n = int(std::fabs(y));
+            double b = x, a = 1;
+            while (n) { if (n & 1) a *= b; n >>= 1; if (n) b *= b; }
+            return y < 0 ? 1 / a : a;
+        }
+        return std::pow(x, y);
+    }
+    static double log(double x) { return std::log(x); }
+    static double acos(double x) { return std::acos(x); }
+    static double atan2(double y, double x) { return std::atan2(y, x); }
+    static double fmin(double a, double b) { return std::fmin(a, b); }
+    static double fmax(double a, double b) { return std::fmax(a, b); }
+};
+
+template <class T> struct V {
+    T x, y, z;
+};
+template <class T> V<T> v3(T x, T y, T z) { return V<T>{x, y, z}; }
+template <class T> V<T> operator+(V<T> a, V<T> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class T> V<T> operator-(V<T> a, V<T> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class T> V<T> operator*(V<T> a, V<T> b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+template <class T> V<T> operator/(V<T> a, V<T> b) { return {a.x / b.x, a.y / b.y, a.z / b.z}; }
+template <class T> V<T> operator*(V<T> a, T s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class T> V<T> operator*(T s, V<T> a) { return {s * a.x, s * a.y, s * a.z}; }
+template <class T> V<T> operator/(V<T> a, T s) { return {a.x / s, a.y / s, a.z / s}; }
+template <class T> V<T> operator/(T s, V<T> a) { return {s / a.x, s / a.y, s / a.z}; }
+template <class T> V<T> operator-(V<T> a) { return {-a.x, -a.y, -a.z}; }
+template <class T> T dot(V<T> a, V<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class T> V<T> cross(V<T> a, V<T> b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+template <class T> T len(V<T> a) { return M<T>::sqrt(dot(a, a)); }
+template <class T> V<T> nrm(V<T> a) { return a * (T(1) / M<T>::sqrt(dot(a, a))); }
+template <class T> V<T> vmin(V<T> a, V<T> b) { return {M<T>::fmin(a.x, b.x), M<T>::fmin(a.y, b.y), M<T>::fmin(a.z, b.z)}; }
+template <class T> V<T> vmax(V<T> a, V<T> b) { return {M<T>::fmax(a.x, b.x), M<T>::fmax(a.y, b.y), M<T>::fmax(a.z, b.z)}; }
+template <class T> T maxc(V<T> a) { return M<T>::fmax(a.x, M<T>::fmax(a.y, a.z)); }
+template <class T> T sat(T x) { return M<T>::fmin(M<T>::fmax(x, T(0)), T(1)); }
+template <class T> T sgn(T x) { return x > 0 ? T(1) : (x < 0 ? T(-1) : T(0)); }
+template <class T> V<T> reflectv(V<T> i, V<T> n) { return i - (T(2) * dot(n, i)) * n; }
+template <class T> V<T> refractv(V<T> i, V<T> n, T eta) {
+    const T c = dot(n, i);
+    const T k = T(1) - eta * eta * (T(1) - c * c);
+    if (k < 0) return v3<T>(0, 0, 0);
+    return eta * i - (eta * c + M<T>::sqrt(k)) * n;
+}
+// rotate(q, v), math/quat.hpp:211-217; hybrid:521-526
+template <class T> V<T> qrot(T qx, T qy, T qz, T qw, V<T> v) {
+    const V<T> u{qx, qy, qz};
+    const V<T> t = T(2) * cross(u, v);
+    return v + qw * t + cross(u, t);
+}
+
+// The per-invocation RNG (hybrid:238-243).  The draw is computed in float
+// and widened exactly for the FP64 oracle, so both consume one stream.
+struct Rng {
+    uint32_t seed;
+    template <class T> T next() { return T(ae::rng_next(seed)); }
+};
+
+// Traffic counters: what a ray touches, by the formula of the roofline
+// (48 B per node, 128 B per object record, 48 B per instance record, 48 B per
+// triangle = 12 B indices + 36 B positions, 60 B for the winner's attributes).
+struct Counters {
+    uint64_t tlas_nodes = 0, objects = 0, instances = 0, blas_nodes = 0, tris = 0, winners = 0;
+    uint64_t bytes() const {
+        return 48 * tlas_nodes + 128 * objects + 48 * instances + 48 * blas_nodes + 48 * tris + 60 * winners;
+    }
+};
+
+struct Scene {
+    const ae_object *objects;
+    uint32_t n_objects;
+    const ae_bvh_node *tlas;
+    uint32_t n_nodes;
+    const uint32_t *lights;
+    uint32_t n_lights;
+    const ae_vertex *vertices;
+    const uint32_t *indices;
+    const ae_bvh_node *blas;
+    const ae_instance *instances;
+};
+
+template <class T> struct Ray {
+    V<T> o, d;
+    T time;
+};
+
+template <class T> struct Hit {
+    T t = 0;
+    V<T> p{0, 0, 0}, n{0, 0, 0};
+    T u = 0, v = 0;     // surface uv (interpolated for meshes)
+    bool front = true;
+    const ae_object *obj = nullptr;
+    uint32_t slot = AE_MISS, prim = AE_MISS;
+    T alpha = 0, beta = 0;
+};
+
+template <class T> V<T> pos(const ae_object &o) { return v3<T>(o.x, o.y, o.z); }
+template <class T> V<T> pos2(const ae_object &o) { return v3<T>(o.x2, o.y2, o.z2); }
+template <class T> V<T> edge_u(const ae_object &o) { return v3<T>(o.u_x, o.u_y, o.u_z); }
+template <class T> V<T> edge_v(const ae_object &o) { return v3<T>(o.v_x, o.v_y, o.v_z); }
+template <class T> V<T> albedo(const ae_object &o) { return v3<T>(o.r, o.g, o.b); }
+
+// ---------------------------------------------------------------------------
+// Intersection
+// ---------------------------------------------------------------------------
+
+// Slab test, hybrid:547-562.
+template <class T> bool slab(V<T> o, V<T> inv, const ae_bvh_node &n, T tnear, T tfar) {
+    const V<T> t0 = (v3<T>(n.min_x, n.min_y, n.min_z) - o) * inv;
+    const V<T> t1 = (v3<T>(n.max_x, n.max_y, n.max_z) - o) * inv;
+    const V<T> lo = vmin(t0, t1), hi = vmax(t0, t1);
+    const T tmin = M<T>::fmax(M<T>::fmax(lo.x, lo.y), M<T>::fmax(lo.z, tnear));
+    const T tmax = M<T>::fmin(M<T>::fmin(hi.x, hi.y), M<T>::fmin(hi.z, tfar));
+    return tmin <= tmax;
+}
+
+// Sphere span, hybrid:285-297.
+template <class T> bool sphere_span(const ae_object &s, const Ray<T> &r, T &t0, T &t1) {
+    const V<T> c = pos<T>(s) + r.time * (pos2<T>(s) - pos<T>(s));
+    const V<T> oc = c - r.o;
+    const T a = dot(r.d, r.d), b = dot(r.d, oc);
+    const T cc = dot(oc, oc) - T(s.radius) * T(s.radius);
+    const T disc = b * b - a * cc;
+    if (disc < 0) { t0 = t1 = 0; return false; }
+    const T sq = M<T>::sqrt(disc);
+    t0 = (b - sq) / a;
+    t1 = (b + sq) / a;
+    return true;
+}
+
+// Box in its yawed frame, hybrid:315-348.
+template <class T> struct BoxLocal {
+    V<T> o, d;
+    T tin, tout;
+    V<T> nin, nout;
+};
+template <class T> V<T> yaw_rotate(V<T> v, T s, T c) { return v3<T>(c * v.x + s * v.z, v.y, -s * v.x + c * v.z); }
+template <class T> bool box_span(const ae_object &b, const Ray<T> &r, BoxLocal<T> &L) {
+    const T s = M<T>::sin(T(b.rotation)), c = M<T>::cos(T(b.rotation));
+    L.o = yaw_rotate(r.o - pos<T>(b), -s, c);
+    L.d = yaw_rotate(r.d, -s, c);
+    const V<T> inv = T(1) / L.d;
+    const V<T> h = v3<T>(b.half_x, b.half_y, b.half_z);
+    const V<T> t0 = (-h - L.o) * inv, t1 = (h - L.o) * inv;
+    const V<T> lo = vmin(t0, t1), hi = vmax(t0, t1);
+    L.tin = M<T>::fmax(M<T>::fmax(lo.x, lo.y), lo.z);
+    L.tout = M<T>::fmin(M<T>::fmin(hi.x, hi.y), hi.z);
+    L.nin = v3<T>(0, 0, -sgn(L.d.z));
+    if (L.tin == lo.x) L.nin = v3<T>(-sgn(L.d.x), 0, 0);
+    else if (L.tin == lo.y) L.nin = v3<T>(0, -sgn(L.d.y), 0);
+    L.nout = v3<T>(0, 0, sgn(L.d.z));
+    if (L.tout == hi.x) L.nout = v3<T>(sgn(L.d.x), 0, 0);
+    else if (L.tout == hi.y) L.nout = v3<T>(0, sgn(L.d.y), 0);
+    return L.tout > L.tin;
+}
+
+template <class T> void face(Hit<T> &h, V<T> d) {
+    h.front = dot(d, h.n) < 0;
+    if (!h.front) h.n = -h.n;
+}
+
+// get_sphere_uv, hybrid:257-265.
+template <class T> void sphere_uv(V<T> p, T rot, T &u, T &v) {
+    const T tau = T(6.2831853f), pi = T(3.14159265f);
+    const T theta = M<T>::acos(-p.y);
+    const T phi = M<T>::atan2(-p.z, p.x) + pi;
+    const T x = phi / tau - rot / tau;
+    u = x - std::floor(x);
+    v = theta / pi;
+}
+
+// HitSphere, hybrid:382-423.
+template <class T> bool hit_sphere(const ae_object &s, const Ray<T> &r, T tn, T tf, Hit<T> &h) {
+    T t0, t1;
+    if (!sphere_span(s, r, t0, t1)) return false;
+    T root = t0;
+    if (root <= tn || tf <= root) {
+        root = t1;
+        if (root <= tn || tf <= root) return false;
+    }
+    const V<T> c = pos<T>(s) + r.time * (pos2<T>(s) - pos<T>(s));
+    h.t = root;
+    h.p = r.o + r.d * root;
+    h.n = (h.p - c) / T(s.radius);
+    face(h, r.d);
+    sphere_uv(h.n, T(s.rotation), h.u, h.v);
+    return true;
+}
+
+// HitQuad, hybrid:425-478; HitTriangle, hybrid:480-513 (tri = true).
+template <class T> bool hit_planar(const ae_object &q, const Ray<T> &r, T tn, T tf, Hit<T> &h, bool tri) {
+    const V<T> U = edge_u<T>(q), W = edge_v<T>(q), P = pos<T>(q);
+    const V<T> n = cross(U, W);
+    const T nn = dot(n, n);
+    if (nn < T(1e-8f)) return false;
+    const V<T> unit = n / M<T>::sqrt(nn);
+    const V<T> w = n / nn;
+    T t;
+    if (!tri) {
+        const T D = dot(n, P);
+        const T den = dot(n, r.d);
+        if (std::fabs(den) < T(1e-8f)) return false;
+        t = (D - dot(n, r.o)) / den;
+    } else {
+        const T den = dot(n, r.d);
+        if (std::fabs(den) < T(1e-8f)) return false;
+        t = (dot(n, P) - dot(n, r.o)) / den;
+    }
+    if (t < tn || t > tf) return false;
+    const V<T> X = r.o + r.d * t;
+    const V<T> pl = X - P;
+    const T a = dot(w, cross(pl, W));
+    const T b = dot(w, cross(U, pl));
+    if (!tri) {
+        if (a < 0 || a > 1 || b < 0 || b > 1) return false;
+    } else {
+        if (a < 0 || b < 0 || a + b > 1) return false;
+    }
+    h.u = a; h.v = b; h.alpha = a; h.beta = b;
+    h.t = t; h.p = X; h.n = unit;
+    face(h, r.d);
+    return true;
+}
+
+// HitMeshTriangle, hybrid:564-598.
+template <class T>
+bool hit_mesh_triangle(const Ray<T> &r, T tn, T tf, V<T> p0, V<T> p1, V<T> p2, T &t, T &a, T &b, V<T> &geo) {
+    t = 0; a = 0; b = 0; geo = v3<T>(0, 0, 1);
+    const V<T> e1 = p1 - p0, e2 = p2 - p0;
+    const V<T> n = cross(e1, e2);
+    const T nn = dot(n, n);
+    if (nn < T(1e-12f)) return false;
+    const T den = dot(n, r.d);
+    if (std::fabs(den) < T(1e-12f)) return false;
+    t = (dot(n, p0) - dot(n, r.o)) / den;
+    if (t < tn || t > tf) return false;
+    const V<T> w = n / nn;
+    const V<T> pl = r.o + r.d * t - p0;
+    a = dot(w, cross(pl, e2));
+    b = dot(w, cross(e1, pl));
+    if (a < 0 || b < 0 || a + b > 1) return false;
+    geo = n / M<T>::sqrt(nn);
+    return true;
+}
+
+template <class T> V<T> vpos(const ae_vertex &v) { return v3<T>(v.px, v.py, v.pz); }
+
+// HitMesh, hybrid:600-707, with ToLocal (hybrid:534-543).  A non-rigid
+// instance (scale in pad0, neither 0 nor 1) maps the local ray through 1/s;
+// t is unchanged by an affine map applied to origin and direction alike.
+template <class T>
+bool hit_mesh(const Scene &S, const ae_object &obj, const Ray<T> &r, T tn, T tf, Hit<T> &h, Counters *C) {
+    const ae_instance &I = S.instances[obj.instanceIndex];
+    if (C) C->instances++;
+    const T qx = I.qx, qy = I.qy, qz = I.qz, qw = I.qw;
+    Ray<T> L;
+    L.o = qrot<T>(-qx, -qy, -qz, qw, r.o - v3<T>(I.px, I.py, I.pz));
+    L.d = qrot<T>(-qx, -qy, -qz, qw, r.d);
+    L.time = r.time;
+    if (I.scale != 0.0f && I.scale != 1.0f) {
+        const T inv = T(1) / T(I.scale);
+        L.o = L.o * inv;
+        L.d = L.d * inv;
+    }
+    const V<T> invd = T(1) / L.d;
+    int stack[64];
+    int sp = 0;
+    stack[sp++] = 0;
+    bool found = false;
+    T closest = tf, ba = 0, bb = 0;
+    uint32_t best = 0;
+    V<T> bgeo = v3<T>(0, 0, 1);
+    while (sp > 0) {
+        const ae_bvh_node &n = S.blas[I.blasBase + uint32_t(stack[--sp])];
+        if (C) C->blas_nodes++;
+        if (!slab(L.o, invd, n, tn, closest)) continue;
+        if (n.count > 0) {
+            for (int i = 0; i < n.count; i++) {
+                const uint32_t base = I.indexBase + uint32_t(n.left + i) * 3u;
+                if (C) C->tris++;
+                const V<T> p0 = vpos<T>(S.vertices[I.vertexBase + S.indices[base]]);
+                const V<T> p1 = vpos<T>(S.vertices[I.vertexBase + S.indices[base + 1]]);
+                const V<T> p2 = vpos<T>(S.vertices[I.vertexBase + S.indices[base + 2]]);
+                T t, a, b;
+                V<T> g;
+                if (hit_mesh_triangle(L, tn, closest, p0, p1, p2, t, a, b, g)) {
+                    closest = t; found = true; ba = a; bb = b; best = base; bgeo = g;
+                }
+            }
+        } else {
+            stack[sp++] = n.left;
+            stack[sp++] = n.right;
+        }
+    }
+    if (!found) return false;
+    if (C) C->winners++;
+    const ae_vertex &A = S.vertices[I.vertexBase + S.indices[best]];
+    const ae_vertex &B = S.vertices[I.vertexBase + S.indices[best + 1]];
+    const ae_vertex &Cv = S.vertices[I.vertexBase + S.indices[best + 2]];
+    const T w0 = T(1) - ba - bb;
+    const V<T> sh = nrm(w0 * v3<T>(A.nx, A.ny, A.nz) + ba * v3<T>(B.nx, B.ny, B.nz) + bb * v3<T>(Cv.nx, Cv.ny, Cv.nz));
+    V<T> geo = bgeo;
+    if (dot(geo, sh) < 0) geo = -geo;
+    h.t = closest;
+    h.p = r.o + r.d * closest;
+    h.n = nrm(qrot<T>(qx, qy, qz, qw, sh));
+    h.front = dot(r.d, qrot<T>(qx, qy, qz, qw, geo)) < 0;
+    if (!h.front) h.n = -h.n;
+    h.u = w0 * T(A.u) + ba * T(B.u) + bb * T(Cv.u);
+    h.v = w0 * T(A.v) + ba * T(B.v) + bb * T(Cv.v);
+    h.prim = (best - I.indexBase) / 3u;
+    h.alpha = ba;
+    h.beta = bb;
+    return true;
+}
+
+// BoxFaceUV, hybrid:711-727; HitBox, hybrid:729-773.
+template <class T> bool hit_box(const ae_object &b, const Ray<T> &r, T tn, T tf, Hit<T> &h) {
+    BoxLocal<T> L;
+    if (!box_span(b, r, L)) return false;
+    T t = L.tin;
+    V<T> ln = L.nin;
+    bool outside = true;
+    if (t <= tn || tf <= t) {
+        t = L.tout; ln = L.nout; outside = false;
+        if (t <= tn || tf <= t) return false;
+    }
+    const T s = M<T>::sin(T(b.rotation)), c = M<T>::cos(T(b.rotation));
+    h.t = t;
+    h.p = r.o + r.d * t;
+    const V<T> lp = L.o + L.d * t;
+    const V<T> he = v3<T>(b.half_x, b.half_y, b.half_z);
+    T uu, vv;
+    if (std::fabs(ln.x) > T(0.5f)) { uu = lp.z / he.z; vv = lp.y / he.y; }
+    else if (std::fabs(ln.y) > T(0.5f)) { uu = lp.x / he.x; vv = lp.z / he.z; }
+    else { uu = lp.x / he.x; vv = lp.y / he.y; }
+    h.u = sat(uu * T(0.5f) + T(0.5f));
+    h.v = sat(vv * T(0.5f) + T(0.5f));
+    h.n = yaw_rotate(ln, s, c);
+    h.front = outside;
+    if (!h.front) h.n = -h.n;
+    return true;
+}
+
+// HitVolume, hybrid:779-822.  Consumes one draw.
+template <class T> bool hit_volume(const ae_object &o, const Ray<T> &r, T tn, T tf, Hit<T> &h, Rng &rng) {
+    T a = 0, b = 0;
+    if (o.shapeType == AE_SHAPE_SPHERE) {
+        if (!sphere_span(o, r, a, b)) return false;
+    } else if (o.shapeType == AE_SHAPE_BOX) {
+        BoxLocal<T> L;
+        if (!box_span(o, r, L)) return false;
+        a = L.tin; b = L.tout;
+    } else {
+        return false;
+    }
+    a = M<T>::fmax(a, tn);
+    b = M<T>::fmin(b, tf);
+    if (a >= b) return false;
+    const T rl = len(r.d);
+    const T inside = (b - a) * rl;
+    const T d = -M<T>::log(M<T>::fmax(rng.next<T>(), T(1e-8f))) / M<T>::fmax(T(o.density), T(1e-8f));
+    if (d > inside) return false;
+    h.t = a + d / rl;
+    h.p = r.o + r.d * h.t;
+    h.n = v3<T>(0, 1, 0);
+    h.front = true;
+    h.u = h.v = 0;
+    return true;
+}
+
+// HitObject dispatch, hybrid:827-856.
+template <class T>
+bool hit_object(const Scene &S, const ae_object &o, const Ray<T> &r, T tn, T tf, Hit<T> &h, Rng &rng, Counters *C) {
+    if (o.colorType == AE_MAT_ISOTROPIC) return hit_volume(o, r, tn, tf, h, rng);
+    switch (o.shapeType) {
+    case AE_SHAPE_SPHERE: return hit_sphere(o, r, tn, tf, h);
+    case AE_SHAPE_QUAD: return hit_planar(o, r, tn, tf, h, false);
+    case AE_SHAPE_TRIANGLE: return hit_planar(o, r, tn, tf, h, true);
+    case AE_SHAPE_MESH: return hit_mesh(S, o, r, tn, tf, h, C);
+    default: return hit_box(o, r, tn, tf, h);
+    }
+}
+
+// TraverseBVH, hybrid:862-917: depth-first, interior nodes push left then
+// right, far starts at 1e6 and shrinks with each hit; ties go to the later hit.
+template <class T> bool traverse(const Scene &S, const Ray<T> &r, T tn, Hit<T> &out, Rng &rng, Counters *C) {
+    if (S.n_nodes == 0) return false;
+    const V<T> inv = T(1) / r.d;
+    int stack[64];
+    int sp = 0;
+    stack[sp++] = 0;
+    bool found = false;
+    T tf = T(1000000.0f);
+    while (sp > 0) {
+        const int ni = stack[--sp];
+        const ae_bvh_node &n = S.tlas[ni];
+        if (C) C->tlas_nodes++;
+        if (!slab(r.o, inv, n, tn, tf)) continue;
+        if (n.count > 0) {
+            for (int i = 0; i < n.count; i++) {
+                const uint32_t slot = uint32_t(n.left + i);
+                const ae_object &o = S.objects[slot];
+                if (C) C->objects++;
+                Hit<T> h;
+                if (hit_object(S, o, r, tn, tf, h, rng, C)) {
+                    tf = h.t;
+                    h.obj = &o;
+                    h.slot = slot;
+                    out = h;
+                    found = true;
+                }
+            }
+        } else {
+            stack[sp++] = n.left;
+            stack[sp++] = n.right;
+        }
+    }
+    return found;
+}
+
+// ---------------------------------------------------------------------------
+// Shading
+// ---------------------------------------------------------------------------
+
+// SurfaceAlbedo without textures, hybrid:940-949.
+template <class T> V<T> surface_albedo(const Hit<T> &h) { return albedo<T>(*h.obj); }
+
+template <class T> V<T> random_direction(Rng &rng) {
+    // hybrid:245-251
+    const T z = rng.next<T>() * T(2) - T(1);
+    const T a = rng.next<T>() * T(6.2831853f);
+    const T rr = M<T>::sqrt(T(1) - z * z);
+    return v3<T>(rr * M<T>::cos(a), rr * M<T>::sin(a), z);
+}
+
+// GetBounce, hybrid:965-1033.
+template <class T> bool bounce(const Ray<T> &r, const Hit<T> &h, V<T> &dir, Rng &rng) {
+    dir = v3<T>(0, 0, 0);
+    switch (h.obj->colorType) {
+    case AE_MAT_LAMBERTIAN:
+        dir = h.n + random_direction<T>(rng);
+        if (dot(dir, dir) < T(0.001f)) dir = h.n;
+        return true;
+    case AE_MAT_METAL: {
+        dir = nrm(reflectv(r.d, h.n));
+        dir = dir + random_direction<T>(rng) * T(h.obj->fuzz);
+        return dot(dir, h.n) > 0;
+    }
+    case AE_MAT_DIELECTRIC: {
+        const T ior = h.obj->refraction;
+        const T ri = h.front ? T(1) / ior : ior;
+        const V<T> d = nrm(r.d);
+        const T ct = M<T>::fmin(dot(-d, h.n), T(1));
+        const T st = M<T>::sqrt(M<T>::fmax(T(0), T(1) - ct * ct));
+        const T r0 = M<T>::pow((T(1) - ri) / (T(1) + ri), T(2));
+        const T refl = r0 + (T(1) - r0) * M<T>::pow(T(1) - ct, T(5));
+        if (ri * st > T(1) || refl > rng.next<T>()) dir = reflectv(d, h.n);
+        else dir = refractv(d, h.n, ri);
+        return true;
+    }
+    case AE_MAT_ISOTROPIC:
+        dir = random_direction<T>(rng);
+        return true;
+    default:
+        return false;
+    }
+}
+
+// SampleLight, hybrid:1057-1119.
+template <class T> void sample_light(const ae_object &L, V<T> from, V<T> &p, T &omega, Rng &rng) {
+    p = pos<T>(L);
+    omega = 0;
+    if (L.shapeType == AE_SHAPE_QUAD) {
+        const T r1 = rng.next<T>();
+        const T r2 = rng.next<T>();
+        p = pos<T>(L) + r1 * edge_u<T>(L) + r2 * edge_v<T>(L);
+        const V<T> cuv = cross(edge_u<T>(L), edge_v<T>(L));
+        const T area = len(cuv);
+        const V<T> ln = cuv / M<T>::fmax(area, T(1e-8f));
+        V<T> ts = from - p;
+        const T d2 = dot(ts, ts);
+        ts = nrm(ts);
+        const T cl = std::fabs(dot(ln, ts));
+        omega = (cl * area) / M<T>::fmax(d2, T(1e-8f));
+        return;
+    }
+    if (L.shapeType == AE_SHAPE_SPHERE) {
+        const V<T> tl = pos<T>(L) - from;
+        const T d2 = M<T>::fmax(dot(tl, tl), T(1e-8f));
+        const T r2 = T(L.radius) * T(L.radius);
+        p = pos<T>(L);
+        if (d2 <= r2) { omega = T(4) * T(3.14159265f); return; }
+        const T ctm = M<T>::sqrt(M<T>::fmax(T(0), T(1) - r2 / d2));
+        omega = T(2) * T(3.14159265f) * (T(1) - ctm);
+        return;
+    }
+    const V<T> tl = pos<T>(L) - from;
+    const T d2 = M<T>::fmax(dot(tl, tl), T(1e-8f));
+    const T area = T(4) * (T(L.half_x) * T(L.half_y) + T(L.half_y) * T(L.half_z) + T(L.half_z) * T(L.half_x)) / T(6);
+    omega = area / d2;
+}
+
+// CalculateDirectLight, hybrid:1122-1212: every light, one sample each; the
+// shadow ray steps through up to four dielectric hits.
+template <class T> V<T> direct_light(const Scene &S, const Hit<T> &h, const Ray<T> &r, Rng &rng, Counters *C) {
+    V<T> acc = v3<T>(0, 0, 0);
+    for (uint32_t i = 0; i < S.n_lights; i++) {
+        const ae_object &L = S.objects[S.lights[i]];
+        V<T> lp;
+        T omega;
+        sample_light(L, h.p, lp, omega, rng);
+        if (omega <= 0) continue;
+        V<T> sd = lp - h.p;
+        const T dist = len(sd);
+        if (dist <= T(1e-6f)) continue;
+        sd = sd / dist;
+        const T ct = dot(h.n, sd);
+        if (ct <= 0) continue;
+        Ray<T> sr;
+        sr.o = h.p + h.n * T(0.001f);
+        sr.d = sd;
+        sr.time = r.time;
+        bool occluded = false;
+        for (int k = 0; k < 4; k++) {
+            Hit<T> sh;
+            if (!traverse(S, sr, T(0.001f), sh, rng, C)) break;
+            if (sh.t >= len(lp - sr.o) - T(0.001f)) break;
+            if (sh.obj->colorType == AE_MAT_DIFFUSE_LIGHT) break;
+            if (sh.obj->colorType != AE_MAT_DIELECTRIC) { occluded = true; break; }
+            sr.o = sh.p + sr.d * T(0.001f);
+        }
+        if (!occluded) {
+            const V<T> rad = T(L.emission) * albedo<T>(L);
+            const V<T> brdf = surface_albedo(h);
+            acc = acc + brdf * rad * ct * omega;
+        }
+    }
+    return acc;
+}
+
+// ColorRay, hybrid:1230-1325.
+template <class T> V<T> color_ray(const Scene &S, const ae_config &cfg, Ray<T> ray, Rng &rng, Counters *C) {
+    V<T> thr = v3<T>(1, 1, 1), acc = v3<T>(0, 0, 0);
+    const V<T> sky = v3<T>(cfg.sky_r, cfg.sky_g, cfg.sky_b);
+    for (uint32_t b = 0; b < cfg.depth; b++) {
+        Hit<T> h;
+        if (!traverse(S, ray, T(0.001f), h, rng, C)) {
+            acc = acc + thr * sky;
+            break;
+        }
+        if (h.obj->colorType == AE_MAT_DIFFUSE_LIGHT) {
+            acc = acc + thr * (T(h.obj->emission) * albedo<T>(*h.obj));
+            break;
+        }
+        if (h.obj->colorType == AE_MAT_LAMBERTIAN) {
+            V<T> dl = direct_light(S, h, ray, rng, C);
+            const T luma = maxc(dl);
+            if (luma > T(8)) dl = dl * (T(8) / luma);
+            acc = acc + thr * dl;
+        }
+        V<T> sd;
+        if (!bounce(ray, h, sd, rng)) break;
+        ray.d = nrm(sd);
+        const T sign = dot(ray.d, h.n) < 0 ? T(-1) : T(1);
+        ray.o = h.p + h.n * (T(0.001f) * sign);
+        if (h.obj->colorType != AE_MAT_DIELECTRIC) thr = thr * surface_albedo(h);
+        if (b > 0) {
+            T p = maxc(thr);
+            p = M<T>::fmin(M<T>::fmax(p, T(0.1f)), T(1));
+            if (rng.next<T>() > p) break;
+            thr = thr / p;
+        }
+    }
+    return acc;
+}
+
+// Camera basis of main, hybrid:1347-1361.
+template <class T> struct Camera {
+    V<T> src, u, v, pu, pv, p0, du, dv;
+    T defocus;
+};
+template <class T> Camera<T> camera(const ae_config &c) {
+    Camera<T> K;
+    K.src = v3<T>(c.source_x, c.source_y, c.source_z);
+    const V<T> tgt = v3<T>(c.target_x, c.target_y, c.target_z), up = v3<T>(c.up_x, c.up_y, c.up_z);
+    const V<T> w = nrm(K.src - tgt);
+    K.u = nrm(cross(up, w));
+    K.v = cross(w, K.u);
+    const T deg = T(0.017453292519943295f);
+    const T vh = T(2) * M<T>::tan((T(c.fov) / T(2)) * deg) * T(c.focus_dist);
+    const T vw = vh * T(c.width) / T(c.height);
+    const V<T> vu = vw * K.u, vv = vh * -K.v;
+    K.pu = vu / T(c.width);
+    K.pv = vv / T(c.height);
+    K.p0 = K.src - T(c.focus_dist) * w - vu / T(2) - vv / T(2) + K.pu / T(2) + K.pv / T(2);
+    const T dr = T(c.focus_dist) * M<T>::tan((T(c.defocus_angle) / T(2)) * deg);
+    K.du = K.u * dr;
+    K.dv = K.v * dr;
+    K.defocus = c.defocus_angle;
+    return K;
+}
+
+// One pixel's frame radiance (main, hybrid:1346-1386), before blending.
+template <class T> V<T> pixel_radiance(const Scene &S, const ae_config &c, const Camera<T> &K, uint32_t x, uint32_t y, Counters *C) {
+    Rng rng{x + y * c.width + c.batch * c.width * c.height + 1u};
+    V<T> color = v3<T>(0, 0, 0);
+    const uint32_t spp = c.batches ? (c.samples / c.batches > 1u ? c.samples / c.batches : 1u) : 1u;
+    for (uint32_t s = 0; s < spp; s++) {
+        const T jx = rng.next<T>() - T(0.5f);
+        const T jy = rng.next<T>() - T(0.5f);
+        const V<T> tgt = K.p0 + (T(x) + jx) * K.pu + (T(y) + jy) * K.pv;
+        Ray<T> r;
+        if (K.defocus <= 0) {
+            r.o = K.src;
+        } else {
+            T px, py;
+            for (;;) {  // random_in_unit_disk, hybrid:1215-1221
+                const T a = rng.next<T>(), b = rng.next<T>();
+                px = a * T(2) - T(1);
+                py = b * T(2) - T(1);
+                if (M<T>::sqrt(px * px + py * py + T(0) * T(0)) < T(1)) break;
+            }
+            r.o = K.src + px * K.du + py * K.dv;
+        }
+        r.d = nrm(tgt - r.o);
+        r.time = rng.next<T>();
+        color = color + color_ray(S, c, r, rng, C);
+    }
+    return color / T(spp);
+}
+
+// ToneMapACES and LinearToSRGB, hybrid:213-233.
+template <class T> V<T> aces(V<T> x) {
+    const T a = T(2.51f), b = T(0.03f), c = T(2.43f), d = T(0.59f), e = T(0.14f);
+    const V<T> n = x * (a * x + v3<T>(b, b, b));
+    const V<T> m = x * (c * x + v3<T>(d, d, d)) + v3<T>(e, e, e);
+    const V<T> q = n / m;
+    return v3<T>(sat(q.x), sat(q.y), sat(q.z));
+}
+template <class T> T srgb1(T c) {
+    const T lo = c * T(12.92f);
+    const T hi = T(1.055f) * M<T>::pow(c, T(1.0f) / T(2.4f)) - T(0.055f);
+    return c <= T(0.0031308f) ? lo : hi;
+}
+template <class T> V<T> srgb(V<T> c) {
+    c = v3<T>(sat(c.x), sat(c.y), sat(c.z));
+    return v3<T>(srgb1(c.x), srgb1(c.y), srgb1(c.z));
+}
+
+template <class T>
+void render_frame(const Scene &S, const ae_config &c, T *accum, T *display, T *frame, const uint32_t *xy, uint32_t n_px,
+                  int threads) {
+    if (threads > 0) omp_set_num_threads(threads);
+    const Camera<T> K = camera<T>(c);
+    const int64_t total = xy ? int64_t(n_px) : int64_t(c.width) * c.height;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t i = 0; i < total; i++) {
+        uint32_t x, y;
+        if (xy) { x = xy[2 * i]; y = xy[2 * i + 1]; }
+        else { x = uint32_t(i % c.width); y = uint32_t(i / c.width); }
+        const size_t px = size_t(y) * c.width + x;
+        T *acc = accum + 4 * px;
+        if (c.displayOnly) {
+            const V<T> g = srgb(aces(v3<T>(acc[0], acc[1], acc[2]) * T(c.exposure)));
+            T *d = display + 4 * px;
+            d[0] = g.x; d[1] = g.y; d[2] = g.z; d[3] = 1;
+            continue;
+        }
+        const V<T> col = pixel_radiance<T>(S, c, K, x, y, nullptr);
+        if (frame) { T *f = frame + 4 * px; f[0] = col.x; f[1] = col.y; f[2] = col.z; f[3] = 1; }
+        V<T> a;
+        if (c.batch == 0) a = col;
+        else {
+            const T w = T(1) / T(c.batch + 1);
+            const V<T> prev = v3<T>(acc[0], acc[1], acc[2]);
+            a = prev + w * (col - prev);
+        }
+        acc[0] = a.x; acc[1] = a.y; acc[2] = a.z; acc[3] = 1;
+        const V<T> g = srgb(aces(a * T(c.exposure)));
+        T *d = display + 4 * px;
+        d[0] = g.x; d[1] = g.y; d[2] = g.z; d[3] = 1;
+    }
+}
+
+}  // namespace oracle
+
+using namespace oracle;
+
+extern "C" {
+
+// ae_hit per ray; counters (optional) receive 6 aggregates:
+// tlas_nodes, objects, instances, blas_nodes, tris, winners.
+int oracle_closest_hit(const Scene *S, const ae_ray *rays, uint32_t n, ae_hit *hits, uint64_t *counters, int threads) {
+    if (threads > 0) omp_set_num_threads(threads);
+    uint64_t agg[6] = {0, 0, 0, 0, 0, 0};
+#pragma omp parallel
+    {
+        Counters C;
+#pragma omp for schedule(dynamic, 1024)
+        for (int64_t i = 0; i < int64_t(n); i++) {
+            const ae_ray &q = rays[i];
+            Ray<float> r;
+            r.o = v3<float>(q.ox, q.oy, q.oz);
+            r.d = v3<float>(q.dx, q.dy, q.dz);
+            r.time = q.time;
+            Rng rng{1u};
+            Hit<float> h;
+            ae_hit out{0, 0, 0, AE_MISS, AE_MISS};
+            if (traverse(*S, r, q.tnear, h, rng, counters ? &C : nullptr)) {
+                out.t = h.t;
+                out.alpha = h.alpha;
+                out.beta = h.beta;
+                out.object = h.slot;
+                out.prim = h.prim;
+            }
+            hits[i] = out;
+        }
+        if (counters) {
+#pragma omp critical
+            {
+                agg[0] += C.tlas_nodes; agg[1] += C.objects; agg[2] += C.instances;
+                agg[3] += C.blas_nodes; agg[4] += C.tris; agg[5] += C.winners;
+            }
+        }
+    }
+    if (counters) std::memcpy(counters, agg, sizeof(agg));
+    return 0;
+}
+
+// Frame render in float (parity) or double (image-error oracle).  Buffers are
+// width*height*4 of the precision's type.  xy (optional) restricts the frame
+// to n_px listed pixels.
+int oracle_render_frame_f32(const Scene *S, const ae_config *c, float *accum, float *display, float *frame,
+                            const uint32_t *xy, uint32_t n_px, int threads) {
+    render_frame<float>(*S, *c, accum, display, frame, xy, n_px, threads);
+    return 0;
+}
+int oracle_render_frame_f64(const Scene *S, const ae_config *c, double *accum, double *display, double *frame,
+                            const uint32_t *xy, uint32_t n_px, int threads) {
+    render_frame<double>(*S, *c, accum, display, frame, xy, n_px, threads);
+    return 0;
+}
+
+// The shared intrinsics on the host, for their accuracy tests:
+// fn 0 sin, 1 cos, 2 tan, 3 exp, 4 log, 5 pow(x, y), 6 atan2(x, y), 7 acos, 8 rng draw of seed x.
+int oracle_math(int fn, const float *x, const float *y, float *out, uint32_t n) {
+    for (uint32_t i = 0; i < n; i++) {
+        switch (fn) {
+        case 0: out[i] = ae::sinf_(x[i]); break;
+        case 1: out[i] = ae::cosf_(x[i]); break;
+        case 2: out[i] = ae::tanf_(x[i]); break;
+        case 3: out[i] = ae::expf_(x[i]); break;
+        case 4: out[i] = ae::logf_(x[i]); break;
+        case 5: out[i] = ae::powf_(x[i], y[i]); break;
+        case 6: out[i] = ae::atan2f_(x[i], y[i]); break;
+        case 7: out[i] = ae::acosf_(x[i]); break;
+        default: { uint32_t sd; std::memcpy(&sd, &x[i], 4); out[i] = ae::rng_next(sd); }
+        }
+    }
+    return 0;
+}
+
+// Camera rays of a frame (main, hybrid:1346-1373), row-major.
+int oracle_camera_rays(const ae_config *c, ae_ray *out) {
+    const Camera<float> K = camera<float>(*c);
+    for (uint32_t y = 0; y < c->height; y++)
+        for (uint32_t x = 0; x < c->width; x++) {
+            Rng rng{x + y * c->width + c->batch * c->width * c->height + 1u};
+            const float jx = rng.next<float>() - 0.5f;
+            const float jy = rng.next<float>() - 0.5f;
+            const V<float> tgt = K.p0 + (float(x) + jx) * K.pu + (float(y) + jy) * K.pv;
+            V<float> o = K.src;
+            if (K.defocus > 0) {
+                float px, py;
+                for (;;) {
+                    const float a = rng.next<float>(), b = rng.next<float>();
+                    px = a * 2.0f - 1.0f;
+                    py = b * 2.0f - 1.0f;
+                    if (M<float>::sqrt(px * px + py * py + 0.0f * 0.0f) < 1.0f) break;
+                }
+                o = K.src + px * K.du + py * K.dv;
+            }
+            const V<float> d = nrm(tgt - o);
+            ae_ray &r = out[size_t(y) * c->width + x];
+            r.ox = o.x; r.oy = o.y; r.oz = o.z; r.tnear = 0.001f;
+            r.dx = d.x; r.dy = d.y; r.dz = d.z; r.time = rng.next<float>();
+        }
+    return 0;
+}
+
+// Per-path traffic of one frame's paths (camera, bounce and shadow rays),
+// for the Mpaths/s roofline: counters as oracle_closest_hit.
+int oracle_path_counters(const Scene *S, const ae_config *c, const uint32_t *xy, uint32_t n_px, uint64_t *counters,
+                         uint64_t *rays_traced, int threads) {
+    if (threads > 0) omp_set_num_threads(threads);
+    const Camera<float> K = camera<float>(*c);
+    uint64_t agg[6] = {0, 0, 0, 0, 0, 0};
+#pragma omp parallel
+    {
+        Counters C;
+#pragma omp for schedule(dynamic, 64)
+        for (int64_t i = 0; i < int64_t(n_px); i++) pixel_radiance<float>(*S, *c, K, xy[2 * i], xy[2 * i + 1], &C);
+#pragma omp critical
+        {
+            agg[0] += C.tlas_nodes; agg[1] += C.objects; agg[2] += C.instances;
+            agg[3] += C.blas_nodes; agg[4] += C.tris; agg[5] += C.winners;
+        }
+    }
+    std::memcpy(counters, agg, sizeof(agg));
+    if (rays_traced) *rays_traced = 0;
+    return 0;
+}
+
+}  // extern "C"

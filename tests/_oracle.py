@@ -1,0 +1,183 @@
+"""Test-side bindings of the oracle (oracle/liboracle.so) and of the
+reference's own code compiled for the CPU pin (oracle/_ref/*.so).
+
+Only tests/, bench.py's CPU baseline and __graft_entry__.smoke() use this.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from aviatorengine2_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE = os.path.join(ROOT, "oracle", "liboracle.so")
+REF_SCENE = os.path.join(ROOT, "oracle", "_ref", "libaeref_scene.so")
+REF_SHADER = os.path.join(ROOT, "oracle", "_ref", "libaeref_shader.so")
+
+_P = ctypes.c_void_p
+
+
+class OScene(ctypes.Structure):
+    _fields_ = [("objects", _P), ("n_objects", ctypes.c_uint32), ("tlas", _P), ("n_nodes", ctypes.c_uint32),
+                ("lights", _P), ("n_lights", ctypes.c_uint32), ("vertices", _P), ("indices", _P), ("blas", _P),
+                ("instances", _P)]
+
+
+def ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+_cache = {}
+
+
+def _load(path):
+    if path not in _cache:
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        _cache[path] = ctypes.CDLL(path)
+    return _cache[path]
+
+
+def oracle():
+    return _load(ORACLE)
+
+
+def ref_available():
+    return os.path.exists(REF_SCENE) and os.path.exists(REF_SHADER)
+
+
+def ref_scene():
+    return _load(REF_SCENE)
+
+
+def ref_shader():
+    return _load(REF_SHADER)
+
+
+def oscene(scene):
+    """An oracle Scene view; keeps the arrays alive on the returned object."""
+    keep = [np.ascontiguousarray(a) for a in (scene.objects, scene.tlas, scene.lights, scene.vertices, scene.indices,
+                                              scene.blas, scene.instances)]
+    o, t, l, v, i, b, ins = keep
+    s = OScene(ptr(o), len(o), ptr(t), len(t), ptr(l), len(l), ptr(v), ptr(i), ptr(b), ptr(ins))
+    s._keep = keep
+    return s
+
+
+def closest_hit(scene, rays, threads=0, counters=False):
+    s = oscene(scene)
+    r = np.ascontiguousarray(rays, dtype=_lib.RAY)
+    hits = np.zeros(len(r), _lib.HIT)
+    cnt = np.zeros(6, np.uint64)
+    f = oracle().oracle_closest_hit
+    f.restype = ctypes.c_int
+    f(ctypes.byref(s), ptr(r), ctypes.c_uint32(len(r)), ptr(hits), ptr(cnt) if counters else None, ctypes.c_int(threads))
+    return (hits, cnt) if counters else hits
+
+
+def camera_rays(config):
+    c = np.ascontiguousarray(np.array(config, dtype=_lib.CONFIG).reshape(1))
+    out = np.zeros(int(c["width"][0]) * int(c["height"][0]), _lib.RAY)
+    oracle().oracle_camera_rays(ptr(c), ptr(out))
+    return out
+
+
+def render_frame(scene, config, accum=None, precision=32, pixels=None, threads=0):
+    """One frame; returns (accum, display, frame) as (H, W, 4) arrays."""
+    s = oscene(scene)
+    c = np.ascontiguousarray(np.array(config, dtype=_lib.CONFIG).reshape(1))
+    w, h = int(c["width"][0]), int(c["height"][0])
+    dt = np.float32 if precision == 32 else np.float64
+    acc = np.zeros((h, w, 4), dt) if accum is None else np.ascontiguousarray(accum, dtype=dt).copy()
+    disp = np.zeros((h, w, 4), dt)
+    frame = np.zeros((h, w, 4), dt)
+    xy = None if pixels is None else np.ascontiguousarray(pixels, dtype=np.uint32).reshape(-1, 2)
+    fn = oracle().oracle_render_frame_f32 if precision == 32 else oracle().oracle_render_frame_f64
+    fn(ctypes.byref(s), ptr(c), ptr(acc), ptr(disp), ptr(frame), ptr(xy), ctypes.c_uint32(0 if xy is None else len(xy)),
+       ctypes.c_int(threads))
+    return acc, disp, frame
+
+
+def counters_bytes(cnt):
+    """Algorithmic bytes of the counted touches (the roofline's formula)."""
+    t, o, i, b, tri, win = (int(x) for x in cnt)
+    return 48 * t + 128 * o + 48 * i + 48 * b + 48 * tri + 60 * win
+
+
+# --- the reference's own code ------------------------------------------------
+def ref_bind(scene):
+    L = ref_shader()
+    keep = [np.ascontiguousarray(a) for a in (scene.objects, scene.tlas, scene.lights, scene.vertices, scene.indices,
+                                              scene.blas, scene.instances)]
+    o, t, l, v, i, b, ins = keep
+    u32 = ctypes.c_uint32
+    L.aeref_bind(ptr(o), u32(len(o)), ptr(t), u32(len(t)), ptr(l), u32(len(l)), ptr(v), u32(len(v)), ptr(i),
+                 u32(len(i)), ptr(b), u32(len(b)), ptr(ins), u32(len(ins)))
+    _cache["_ref_keep"] = keep
+
+
+def ref_set_config(config):
+    c = np.ascontiguousarray(np.array(config, dtype=_lib.CONFIG).reshape(1))
+    ref_shader().aeref_set_config(ptr(c))
+
+
+def ref_closest_hit(scene, rays, threads=0):
+    ref_bind(scene)
+    r = np.ascontiguousarray(rays, dtype=_lib.RAY)
+    hits = np.zeros(len(r), _lib.HIT)
+    ref_shader().aeref_closest_hit(ptr(r), ctypes.c_uint32(len(r)), ptr(hits), ctypes.c_int(threads))
+    return hits
+
+
+def ref_render(scene, config, accum=None, threads=0, pixels=None):
+    ref_bind(scene)
+    ref_set_config(config)
+    w, h = int(config["width"]), int(config["height"])
+    acc = np.zeros((h, w, 4), np.float32) if accum is None else np.ascontiguousarray(accum, np.float32).copy()
+    disp = np.zeros((h, w, 4), np.float32)
+    if pixels is None:
+        ref_shader().aeref_render(ptr(acc), ptr(disp), ctypes.c_int(threads))
+    else:
+        xy = np.ascontiguousarray(pixels, dtype=np.uint32).reshape(-1, 2)
+        ref_shader().aeref_render_pixels(ptr(xy), ctypes.c_uint32(len(xy)), ptr(acc), ptr(disp), ctypes.c_int(threads))
+    return acc, disp
+
+
+def ref_build_bvh(bounds):
+    b = np.ascontiguousarray(bounds, dtype=np.float32).reshape(-1, 6)
+    n = len(b)
+    nodes = np.zeros(max(2 * n, 1), _lib.NODE)
+    order = np.zeros(max(n, 1), np.uint32)
+    cnt = ctypes.c_uint32()
+    ref_scene().aeref_build_bvh(ptr(b), ctypes.c_uint32(n), ptr(nodes), ctypes.byref(cnt), ptr(order))
+    return nodes[:cnt.value].copy(), order[:n].copy()
+
+
+def ref_mesh_add(vertices, indices16):
+    v = np.ascontiguousarray(np.stack([vertices[k] for k in ("px", "py", "pz", "nx", "ny", "nz", "u", "v")], 1),
+                             np.float32)
+    i = np.ascontiguousarray(indices16, np.uint16)
+    ov = np.zeros(len(v), _lib.VERTEX)
+    oi = np.zeros(len(i), np.uint32)
+    ob = np.zeros(max(2 * (len(i) // 3), 1), _lib.NODE)
+    nb = ctypes.c_uint32()
+    ref_scene().aeref_mesh_add(ptr(v), ctypes.c_uint32(len(v)), ptr(i), ctypes.c_uint32(len(i)), ptr(ov), ptr(oi),
+                               ptr(ob), ctypes.byref(nb))
+    return ov, oi, ob[:nb.value].copy()
+
+
+def ref_bounds(kind, position, rotation, a, b=None):
+    p = np.asarray(position, np.float32)
+    q = np.asarray(rotation, np.float32)
+    a = np.asarray(a, np.float32)
+    b = None if b is None else np.asarray(b, np.float32)
+    out = np.zeros(6, np.float32)
+    L = ref_scene()
+    if kind == "mesh":
+        L.aeref_mesh_bounds(ptr(p), ptr(q), ptr(a), ptr(out))
+    elif kind == "quad":
+        L.aeref_quad_bounds(ptr(p), ptr(q), ptr(a), ptr(b), ptr(out))
+    elif kind == "box":
+        L.aeref_box_bounds(ptr(p), ptr(q), ptr(a), ptr(out))
+    return out
