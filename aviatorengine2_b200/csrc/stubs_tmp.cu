@@ -1,9 +1,6 @@
 // Temporary: families not yet built report so loudly.
 #include "fast.h"
 namespace ae {
-int prepare_fast(Ctx *c) { return c->fail(AE_ERR_STATE, "optimised closest-hit kernels not built"); }
-void destroy_fast(Ctx *) {}
-cudaError_t launch_closest_fast(Ctx *, const ae_ray *, uint32_t, ae_hit *, bool, cudaStream_t) { return cudaErrorNotSupported; }
 void destroy_wavefront(Ctx *) {}
 void destroy_deferred(Ctx *) {}
 int render_deferred(Ctx *c, const ae_gbuffer *) { return c->fail(AE_ERR_STATE, "deferred resolve not built"); }
