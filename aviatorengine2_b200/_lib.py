@@ -50,11 +50,13 @@ ENTITY = np.dtype([("shape", "<u4"), ("material", "<u4"), ("position", "<f4", 3)
 SETTINGS = np.dtype([("width", "<u4"), ("height", "<u4"), ("samples", "<u4"), ("max_samples", "<u4"),
                      ("hybrid", "<u4"), ("hybrid_max_depth", "<u4"), ("trace_scale", "<f4"),
                      ("history_while_moving", "<u4"), ("device", "<i4"), ("reserved", "<u4", 7)])
+QNODE = np.dtype([("origin", "<f4", 3), ("exp", "i1", 3), ("nchild", "u1"), ("lo", "u1", (3, 4)),
+                  ("hi", "u1", (3, 4)), ("child", "<u4", 4), ("pad", "<u4", 2)])
 MESH_RANGE = np.dtype([("vertexBase", "<u4"), ("indexBase", "<u4"), ("triangleCount", "<u4"), ("blasBase", "<u4"),
                        ("localBounds", AABB), ("doubleSided", "<u4")])
 
 for _dt, _size in ((VERTEX, 32), (NODE, 48), (OBJECT, 128), (INSTANCE, 48), (RAY, 32), (HIT, 20), (CONFIG, 240),
-                   (AABB, 24), (SETTINGS, 64)):
+                   (AABB, 24), (SETTINGS, 64), (QNODE, 64)):
     assert _dt.itemsize == _size, (_dt, _size)
 
 # Enumerations (include/ae_b200.h)
@@ -108,6 +110,7 @@ SIGNATURES = {
     "ae_launch_count": (ctypes.c_uint64, [_P]),
     "ae_prepare_fast": (_I, [_P]),
     "ae_refit_instances": (_I, [_P, _P, _U32]),
+    "ae_build_wide_bvh": (_I, [_P, _U32, _U32, _P, _U32, _P, _P, _P]),
 }
 
 _lib = None

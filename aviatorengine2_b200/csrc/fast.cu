@@ -33,9 +33,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <string>
 #include <tuple>
 #include <vector>
 
@@ -89,7 +91,13 @@ struct FastScene {
     std::vector<float> host_tris;
 };
 
-constexpr int kFastStack = 24;  // shared-memory stack entries per thread
+// Traversal stack per thread: the first kSharedStack entries in shared
+// memory, the rest (rarely reached: only along the deepest paths of the
+// largest meshes) in a per-thread local array.  prepare_fast checks that no
+// tree needs more than kFastStack entries.
+constexpr int kSharedStack = 24;
+constexpr int kLocalStack = 40;
+constexpr int kFastStack = kSharedStack + kLocalStack;
 
 // ---------------------------------------------------------------------------
 // Host: 4-wide collapse and quantisation
@@ -218,6 +226,66 @@ int stack_need(const std::vector<QNode> &nodes, uint32_t root) {
 
 }  // namespace
 
+// The 4-wide quantised BVH of one mesh from its binary BLAS (mesh-relative
+// node links, `tri_count` triangles).  Node indices in `out` start at 0; the
+// root is returned in `root` (a node index, or a leaf ref for a one-leaf
+// mesh).  Checks, before anything reaches a device: every link stays inside
+// the tree, every leaf inside the mesh's triangles, every quantised box
+// contains its exact box, and the traversal stack bound.
+bool build_qbvh(const ae_bvh_node *bin, uint32_t n_bin, uint32_t tri_count, std::vector<QNode> &out, uint32_t &root,
+                int &stack, std::string &err) {
+    out.clear();
+    stack = 0;
+    if (n_bin == 0) { err = "empty BLAS"; return false; }
+    // The binary tree itself: links in range, acyclic, leaves in range.
+    {
+        std::vector<uint8_t> seen(n_bin, 0);
+        std::vector<uint32_t> todo = {0};
+        while (!todo.empty()) {
+            const uint32_t i = todo.back();
+            todo.pop_back();
+            if (i >= n_bin || seen[i]++) { err = "binary BLAS link out of range or repeated"; return false; }
+            const ae_bvh_node &n = bin[i];
+            if (n.count > 0) {
+                if (n.left < 0 || uint64_t(n.left) + uint64_t(n.count) > tri_count) { err = "leaf outside the mesh"; return false; }
+                if (uint32_t(n.count) > kMaxLeafCount || uint32_t(n.left) >= kMaxLeafFirst) {
+                    err = "leaf beyond the packed reference limits";
+                    return false;
+                }
+            } else {
+                if (n.left < 0 || n.right < 0) { err = "negative link"; return false; }
+                todo.push_back(uint32_t(n.left));
+                todo.push_back(uint32_t(n.right));
+            }
+        }
+    }
+    if (bin[0].count > 0) {
+        root = leaf_ref(uint32_t(bin[0].left), uint32_t(bin[0].count));
+        stack = 0;
+        return true;
+    }
+    Collapser col{bin, out};
+    root = col.emit(0);
+    if (!col.ok) { err = "a child box cannot be quantised conservatively"; return false; }
+    // Final structural check of what the kernel will follow.
+    for (size_t i = 0; i < out.size(); i++) {
+        const QNode &q = out[i];
+        if (q.nchild < 2 || q.nchild > 4) { err = "node child count"; return false; }
+        for (int k = 0; k < q.nchild; k++) {
+            const uint32_t r = q.child[k];
+            if (r & kLeafBit) {
+                if (leaf_count(r) == 0 || uint64_t(leaf_first(r)) + leaf_count(r) > tri_count) { err = "leaf ref"; return false; }
+            } else if (r >= out.size()) {
+                err = "node ref";
+                return false;
+            }
+        }
+    }
+    stack = stack_need(out, root);
+    if (stack + 1 > kFastStack) { err = "tree needs more stack than the kernel holds"; return false; }
+    return true;
+}
+
 int prepare_fast(Ctx *c) {
     if (!c->geometry_uploaded || !c->scene_uploaded) return c->fail(AE_ERR_STATE, "prepare before uploads");
     if (!c->fast) c->fast = new (std::nothrow) FastScene();
@@ -243,25 +311,19 @@ int prepare_fast(Ctx *c) {
             dst[12 * t + 9] = dst[12 * t + 10] = dst[12 * t + 11] = 0.0f;
         }
         uint32_t root;
-        const ae_bvh_node &r = c->host_blas[m.blasBase];
-        if (r.count > 0) {
-            if (uint32_t(r.count) > kMaxLeafCount || uint32_t(r.left) >= kMaxLeafFirst)
-                return c->fail(AE_ERR_LAYOUT, "mesh leaf outside the 4-wide BVH's limits");
-            root = leaf_ref(uint32_t(r.left), uint32_t(r.count));
-        } else {
-            const size_t before = F.host_nodes.size();
-            // Node indices are global: offset the collapse into the shared array.
-            std::vector<QNode> local;
-            Collapser lc{c->host_blas.data() + m.blasBase, local};
-            lc.emit(0);
-            if (!lc.ok) return c->fail(AE_ERR_LAYOUT, "mesh cannot be quantised (leaf too large or extent)");
-            for (QNode &q : local)
-                for (int k = 0; k < q.nchild; k++)
-                    if (!(q.child[k] & kLeafBit)) q.child[k] += uint32_t(before);
-            F.host_nodes.insert(F.host_nodes.end(), local.begin(), local.end());
-            root = uint32_t(before);
-            F.max_stack = std::max(F.max_stack, stack_need(F.host_nodes, root));
-        }
+        std::vector<QNode> local;
+        int need = 0;
+        std::string err;
+        if (!build_qbvh(c->host_blas.data() + m.blasBase, uint32_t(c->n_blas - m.blasBase), m.triangleCount, local,
+                        root, need, err))
+            return c->fail(AE_ERR_LAYOUT, "4-wide BVH of instance %u: %s", i, err.c_str());
+        const uint32_t before = uint32_t(F.host_nodes.size());
+        for (QNode &q : local)
+            for (int k = 0; k < q.nchild; k++)
+                if (!(q.child[k] & kLeafBit)) q.child[k] += before;
+        if (!(root & kLeafBit)) root += before;
+        F.host_nodes.insert(F.host_nodes.end(), local.begin(), local.end());
+        F.max_stack = std::max(F.max_stack, need);
         F.mesh_roots[key] = std::make_pair(root, tri_base);
         rebuilt = true;
     }
@@ -472,6 +534,7 @@ AE_DEV void trace_mesh(const FastView &V, const FastInst &I, uint32_t slot, uint
     WtRay W;
     if (WT) W = wt_setup(ld);
     const float4 *tris = V.tris + size_t(I.tri_base) * 3;
+    uint2 spill[kLocalStack];
     int sp = 0;
     uint32_t cur = I.root;
     for (;;) {
@@ -511,10 +574,9 @@ AE_DEV void trace_mesh(const FastView &V, const FastInst &I, uint32_t slot, uint
                 // than kFastStack entries; the bound check keeps that true for
                 // any input.
                 for (int k = nh - 1; k >= 1; k--) {
-                    if (sp < kFastStack) {
-                        stk[sp * nthreads + tid] = make_uint2(ch[k], __float_as_uint(tm[k]));
-                        sp++;
-                    }
+                    if (sp < kSharedStack) stk[sp * nthreads + tid] = make_uint2(ch[k], __float_as_uint(tm[k]));
+                    else if (sp < kFastStack) spill[sp - kSharedStack] = make_uint2(ch[k], __float_as_uint(tm[k]));
+                    sp = sp < kFastStack ? sp + 1 : sp;
                 }
                 cur = ch[0];
                 continue;
@@ -524,7 +586,7 @@ AE_DEV void trace_mesh(const FastView &V, const FastInst &I, uint32_t slot, uint
         bool found = false;
         while (sp > 0) {
             sp--;
-            const uint2 e = stk[sp * nthreads + tid];
+            const uint2 e = sp < kSharedStack ? stk[sp * nthreads + tid] : spill[sp - kSharedStack];
             if (__uint_as_float(e.y) <= best.t) {
                 cur = e.x;
                 found = true;
@@ -643,7 +705,7 @@ cudaError_t launch_closest_fast(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *
     FastScene &F = *c->fast;
     FastView V{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr};
     const int threads = 128;
-    const size_t smem = size_t(kFastStack) * threads * sizeof(uint2);
+    const size_t smem = size_t(kSharedStack) * threads * sizeof(uint2);
     if (quant) {
         cudaFuncSetAttribute(k_closest_fast<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         k_closest_fast<true><<<(n + threads - 1) / threads, threads, smem, st>>>(c->scene(), V, rays, n, hits);
@@ -655,3 +717,22 @@ cudaError_t launch_closest_fast(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *
 }
 
 }  // namespace ae
+
+extern "C" int ae_build_wide_bvh(const ae_bvh_node *blas, uint32_t n_nodes, uint32_t tri_count, void *out_nodes,
+                                 uint32_t capacity, uint32_t *out_count, uint32_t *out_root, int32_t *out_stack) {
+    if (!blas || !out_count || !out_root || !out_stack) return AE_ERR_INVALID;
+    std::vector<ae::QNode> nodes;
+    uint32_t root = 0;
+    int stack = 0;
+    std::string err;
+    if (!ae::build_qbvh(blas, n_nodes, tri_count, nodes, root, stack, err)) {
+        fprintf(stderr, "ae_build_wide_bvh: %s\n", err.c_str());
+        return AE_ERR_LAYOUT;
+    }
+    *out_count = uint32_t(nodes.size());
+    *out_root = root;
+    *out_stack = stack;
+    if (nodes.size() > capacity || (!out_nodes && !nodes.empty())) return AE_ERR_OVERSIZE;
+    if (!nodes.empty()) std::memcpy(out_nodes, nodes.data(), nodes.size() * sizeof(ae::QNode));
+    return AE_OK;
+}

@@ -154,12 +154,17 @@ def run_reference_arm(args):
     rank, world, local = dist_env()
     if rank != 0:
         return 0
-    from aviatorengine2_b200 import Context, scenes
+    # No library kernel on this path: the ray set is generated on the CPU with
+    # the same rules (camera rays, reference closest hits, one diffuse bounce).
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle as O
+    from aviatorengine2_b200 import scenes
     scene = scenes.instanced_meshes()
-    with Context(int(scene.config["width"]), int(scene.config["height"]), device=local) as ctx:
-        ctx.upload(scene)
-        prim, bounce = make_workload(ctx, scene)
-    rays = np.concatenate([prim, bounce])
+    cores = os.cpu_count() or 1
+    prim = O.camera_rays(scene.config)
+    hits = (O.ref_closest_hit if O.ref_available() else O.closest_hit)(scene, prim, threads=cores)
+    bounce, valid = O.bounce_rays(scene, scene.config, prim, hits)
+    rays = np.concatenate([prim, bounce[valid]])
     steps = []
     for _ in range(args.warmup):
         cpu_reference(scene, rays[:20000], budget_s=0.0)
@@ -182,11 +187,14 @@ def run_reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--variant", default=os.environ.get("AE_BENCH_VARIANT", "best"))
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -203,7 +211,7 @@ def main():
         pg = dist
 
     from aviatorengine2_b200 import Context, _lib, scenes
-    scene = scenes.instanced_meshes()
+    scene = scenes.instanced_meshes(width=args.width, height=args.height)
     W, H = int(scene.config["width"]), int(scene.config["height"])
     ctx = Context(W, H, device=local)
     ctx.upload(scene)
@@ -271,34 +279,36 @@ def main():
     rays_step = n1 + n2
     value = rays_step * world / (ms / 1e3) / 1e6
 
-    # End to end through the public call with host buffers: pinned host rays
-    # in, hits out, per step.
-    h_prim = torch.from_numpy(prim.view(np.uint8)).pin_memory()
-    h_bounce = torch.from_numpy(bounce.view(np.uint8)).pin_memory()
-    h_h1 = torch.empty(n1 * 20, dtype=torch.uint8).pin_memory()
-    h_h2 = torch.empty(n2 * 20, dtype=torch.uint8).pin_memory()
-    L = _lib.lib()
+    e2e = None
+    if not args.no_e2e:
+        # End to end through the public call with host buffers: pinned host rays
+        # in, hits out, per step.
+        h_prim = torch.from_numpy(prim.view(np.uint8)).pin_memory()
+        h_bounce = torch.from_numpy(bounce.view(np.uint8)).pin_memory()
+        h_h1 = torch.empty(n1 * 20, dtype=torch.uint8).pin_memory()
+        h_h2 = torch.empty(n2 * 20, dtype=torch.uint8).pin_memory()
+        L = _lib.lib()
 
-    def e2e_step():
-        _lib.check(L.ae_closest_hit(ctx.handle, h_prim.data_ptr(), n1, h_h1.data_ptr(), vid), ctx.handle)
-        _lib.check(L.ae_closest_hit(ctx.handle, h_bounce.data_ptr(), n2, h_h2.data_ptr(), vid), ctx.handle)
+        def e2e_step():
+            _lib.check(L.ae_closest_hit(ctx.handle, h_prim.data_ptr(), n1, h_h1.data_ptr(), vid), ctx.handle)
+            _lib.check(L.ae_closest_hit(ctx.handle, h_bounce.data_ptr(), n2, h_h2.data_ptr(), vid), ctx.handle)
 
-    for _ in range(2):
-        e2e_step()
-    et = []
-    for _ in range(max(3, args.steps // 2)):
-        flush.zero_()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        e2e_step()
-        et.append(time.perf_counter() - t0)
-    e2e_s = float(np.mean(et))
-    if pg:
-        t = torch.tensor([e2e_s], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": rays_step * world / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": int((n1 + n2) * 32),
-           "d2h_bytes_per_step": int((n1 + n2) * 20)}
+        for _ in range(2):
+            e2e_step()
+        et = []
+        for _ in range(max(3, args.steps // 2)):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            e2e_step()
+            et.append(time.perf_counter() - t0)
+        e2e_s = float(np.mean(et))
+        if pg:
+            t = torch.tensor([e2e_s], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": rays_step * world / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": int((n1 + n2) * 32),
+               "d2h_bytes_per_step": int((n1 + n2) * 20)}
 
     peak, peak_kind = load_peaks()
     achieved = alg_bytes_step / (ms / 1e3) / 1e9
@@ -320,7 +330,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene and camera)",
-            "config": {"workload": "instanced_meshes 1920x1080 primary+bounce closest hit", "variant": variant,
+            "config": {"workload": f"instanced_meshes {W}x{H} primary+bounce closest hit", "variant": variant,
                        "rays_per_step": rays_step, "primary_rays": n1, "bounce_rays": n2,
                        "triangles": int(scene.triangles), "instances": int(len(scene.instances)),
                        "l2": "flushed before every step (512 MB write)", "parallelism": f"replicas x{world}"},

@@ -400,6 +400,18 @@ uint64_t ae_launch_count(const ae_ctx *ctx);
  * BVH) after ae_upload_geometry.  Called implicitly on first use. */
 int ae_prepare_fast(ae_ctx *ctx);
 
+/* The 4-wide BVH of the optimised kernels, host side, for one mesh: binary
+ * BLAS nodes (mesh-relative links, scene/bvh.h layout) collapsed to 64-byte
+ * nodes holding four child boxes quantised to 8 bits and rounded outward.
+ * Leaves are the binary tree's (same triangle slots).  Layout of a node:
+ * float origin[3]; int8 exp[3]; uint8 nchild; uint8 lo[3][4]; uint8 hi[3][4];
+ * uint32 child[4] (bit 31 = leaf: count in bits 24-30, first slot in 0-23);
+ * uint32 pad[2].  Writes up to `capacity` nodes; *out_count, *out_root (node
+ * index or leaf ref) and *out_stack (worst-case traversal stack) are always
+ * set on AE_OK or AE_ERR_OVERSIZE. */
+int ae_build_wide_bvh(const ae_bvh_node *blas, uint32_t n_nodes, uint32_t tri_count, void *out_nodes,
+                      uint32_t capacity, uint32_t *out_count, uint32_t *out_root, int32_t *out_stack);
+
 /* GPU TLAS refit: new instance transforms on the device; recompute world
  * bounds of every mesh object bottom-up without rebuilding topology
  * (replaces the per-frame CPU rebuild of renderer/renderer.cpp:1087-1130

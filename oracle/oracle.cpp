@@ -845,6 +845,72 @@ int oracle_camera_rays(const ae_config *c, ae_ray *out) {
     return 0;
 }
 
+// One diffuse bounce per hit, as the library's ray-set generator defines it:
+// the pixel's RNG stream after its camera ray, direction n + RandomDirection()
+// (hybrid:980-986), origin offset 0.001 along the facing shading normal
+// (hybrid:1294-1296); the normal recomputed as HitMesh finishes
+// (hybrid:655-706).  valid[i] = 0 where the primary missed or hit a
+// non-planar analytic object.
+int oracle_bounce_rays(const Scene *S, const ae_config *c, const ae_ray *prim, const ae_hit *hits, uint32_t n,
+                       ae_ray *out, uint8_t *valid) {
+    const Camera<float> K = camera<float>(*c);
+    for (uint32_t i = 0; i < n; i++) {
+        out[i] = prim[i];
+        valid[i] = 0;
+        const ae_hit &h = hits[i];
+        if (h.object == AE_MISS) continue;
+        const ae_object &obj = S->objects[h.object];
+        const V<float> d = v3<float>(prim[i].dx, prim[i].dy, prim[i].dz);
+        V<float> sn;
+        if (obj.shapeType == AE_SHAPE_MESH) {
+            const ae_instance &I = S->instances[obj.instanceIndex];
+            const uint32_t base = I.indexBase + h.prim * 3u;
+            const ae_vertex &A = S->vertices[I.vertexBase + S->indices[base]];
+            const ae_vertex &B = S->vertices[I.vertexBase + S->indices[base + 1]];
+            const ae_vertex &C = S->vertices[I.vertexBase + S->indices[base + 2]];
+            const float w0 = 1.0f - h.alpha - h.beta;
+            const V<float> sh = nrm(w0 * v3<float>(A.nx, A.ny, A.nz) + h.alpha * v3<float>(B.nx, B.ny, B.nz) +
+                                    h.beta * v3<float>(C.nx, C.ny, C.nz));
+            const V<float> p0 = vpos<float>(A);
+            const V<float> gn = cross(vpos<float>(B) - p0, vpos<float>(C) - p0);
+            V<float> geo = gn / M<float>::sqrt(dot(gn, gn));
+            if (dot(geo, sh) < 0) geo = -geo;
+            sn = nrm(qrot<float>(I.qx, I.qy, I.qz, I.qw, sh));
+            if (!(dot(d, qrot<float>(I.qx, I.qy, I.qz, I.qw, geo)) < 0)) sn = -sn;
+        } else if (obj.shapeType == AE_SHAPE_QUAD || obj.shapeType == AE_SHAPE_TRIANGLE) {
+            const V<float> nn = cross(edge_u<float>(obj), edge_v<float>(obj));
+            sn = nn / M<float>::sqrt(dot(nn, nn));
+            if (!(dot(d, sn) < 0)) sn = -sn;
+        } else {
+            continue;
+        }
+        const uint32_t x = i % c->width, y = i / c->width;
+        Rng rng{x + y * c->width + c->batch * c->width * c->height + 1u};
+        rng.next<float>();
+        rng.next<float>();
+        if (K.defocus > 0) {
+            for (;;) {
+                const float a = rng.next<float>(), b = rng.next<float>();
+                const float px = a * 2.0f - 1.0f, py = b * 2.0f - 1.0f;
+                if (M<float>::sqrt(px * px + py * py + 0.0f * 0.0f) < 1.0f) break;
+            }
+        }
+        rng.next<float>();
+        V<float> dir = sn + random_direction<float>(rng);
+        if (dot(dir, dir) < 0.001f) dir = sn;
+        dir = nrm(dir);
+        const V<float> o = v3<float>(prim[i].ox, prim[i].oy, prim[i].oz);
+        const V<float> p = o + d * h.t;
+        const float sgn = dot(dir, sn) < 0 ? -1.0f : 1.0f;
+        const V<float> no = p + sn * (0.001f * sgn);
+        ae_ray &r = out[i];
+        r.ox = no.x; r.oy = no.y; r.oz = no.z; r.tnear = 0.001f;
+        r.dx = dir.x; r.dy = dir.y; r.dz = dir.z;
+        valid[i] = 1;
+    }
+    return 0;
+}
+
 // Per-path traffic of one frame's paths (camera, bounce and shadow rays),
 // for the Mpaths/s roofline: counters as oracle_closest_hit.
 int oracle_path_counters(const Scene *S, const ae_config *c, const uint32_t *xy, uint32_t n_px, uint64_t *counters,

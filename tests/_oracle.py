@@ -181,3 +181,14 @@ def ref_bounds(kind, position, rotation, a, b=None):
     elif kind == "box":
         L.aeref_box_bounds(ptr(p), ptr(q), ptr(a), ptr(out))
     return out
+
+
+def bounce_rays(scene, config, primary, hits):
+    s = oscene(scene)
+    c = np.ascontiguousarray(np.array(config, dtype=_lib.CONFIG).reshape(1))
+    p = np.ascontiguousarray(primary, dtype=_lib.RAY)
+    h = np.ascontiguousarray(hits, dtype=_lib.HIT)
+    out = np.zeros(len(p), _lib.RAY)
+    valid = np.zeros(len(p), np.uint8)
+    oracle().oracle_bounce_rays(ctypes.byref(s), ptr(c), ptr(p), ptr(h), ctypes.c_uint32(len(p)), ptr(out), ptr(valid))
+    return out, valid.astype(bool)

@@ -67,6 +67,8 @@ def test_closest_hit_camera_and_bounce(instanced):
         assert same(hits, O.closest_hit(s, prim))
         assert (hits["object"] != _lib.MISS).mean() > 0.3
         bounce, valid = c.bounce_rays(prim, hits)
+        ob, ov = O.bounce_rays(s, s.config, prim, hits)
+        assert np.array_equal(valid, ov) and same(bounce[valid], ob[ov])
         b = bounce[valid]
         bh = c.closest_hit(b)
         assert same(bh, O.closest_hit(s, b))
