@@ -108,6 +108,24 @@ class Context:
         self._chk(lib().ae_read_image(self._h, which, ptr(out), out.nbytes))
         return out
 
+    def read_planes(self):
+        """The deferred path's G-buffer planes (position, normal, albedo bytes,
+        depth) as the last ae_build_gbuffer / G-buffer upload left them."""
+        h, w = self.height, self.width
+        out = (np.zeros((h, w, 4), np.float32), np.zeros((h, w, 4), np.float32), np.zeros((h, w, 4), np.uint8),
+               np.zeros((h, w), np.float32))
+        for k, a in enumerate(out):
+            self._chk(lib().ae_read_image(self._h, 101 + k, ptr(a), a.nbytes))
+        return out
+
+    def read_deferred_accum(self):
+        out = np.zeros((self.height, self.width, 4), np.float32)
+        self._chk(lib().ae_read_image(self._h, 100, ptr(out), out.nbytes))
+        return out
+
+    def build_gbuffer(self):
+        self._chk(lib().ae_build_gbuffer(self._h))
+
     # --- rays --------------------------------------------------------------
     def closest_hit(self, rays, variant=_lib.VARIANT_PLAIN):
         r = np.ascontiguousarray(rays, dtype=_lib.RAY)

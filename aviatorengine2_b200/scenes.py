@@ -331,3 +331,36 @@ def instanced_meshes(seed=2, width=1920, height=1080, levels=(7, 6, 6, 5, 5), gr
                            albedo=tuple(float(x) for x in rng.uniform(0.2, 0.8, 3)), mesh=handles[k % len(handles)]))
     cfg = make_config(width, height, (50.0, 55.0, 175.0), (50.0, 50.0, 50.0), fov=40.0, depth=2, sky=(0.5, 0.6, 0.8))
     return _finish(ents, meshes, cfg, "instanced_meshes")
+
+
+def hybrid_box(seed=3, width=160, height=120, depth=4):
+    """The Cornell box with every kind of primitive the hybrid renderer sorts:
+    mesh walls and a mesh cube (rasterized), an unrotated solid box (raster
+    proxy), a yawed box, a metal sphere and a glass sphere (analytic), and the
+    emissive quad light."""
+    s = cornell_box(seed=seed, width=width, height=height, depth=depth)
+    rng = np.random.default_rng(seed)
+    meshes = MeshLibrary()
+    ents = []
+    L = 10.0
+    ents.append(entity(_lib.SHAPE_QUAD, _lib.MAT_DIFFUSE_LIGHT, (3.5, L - 0.01, 3.5), emission=15.0,
+                       u=(3.0, 0.0, 0.0), v=(0.0, 0.0, 3.0)))
+    ents.append(entity(_lib.SHAPE_SPHERE, _lib.MAT_METAL, (7.0, 1.2, 3.0), albedo=(0.8, 0.7, 0.5), radius=1.2,
+                       fuzz=0.1))
+    ents.append(entity(_lib.SHAPE_SPHERE, _lib.MAT_DIELECTRIC, (2.5, 4.5, 6.5), radius=1.0, ior=1.5))
+    ents.append(entity(_lib.SHAPE_BOX, _lib.MAT_LAMBERTIAN, (2.0, 0.75, 7.5), albedo=(0.6, 0.3, 0.3),
+                       half_extent=(0.75, 0.75, 0.75)))
+    ents.append(entity(_lib.SHAPE_BOX, _lib.MAT_LAMBERTIAN, (8.0, 4.0, 7.0), rotation=yaw_quat(0.4),
+                       albedo=(0.3, 0.6, 0.3), half_extent=(0.6, 1.0, 0.6)))
+    walls = [((L / 2, 0.0, L / 2), (0, 0, L), (L, 0, 0)), ((L / 2, L, L / 2), (L, 0, 0), (0, 0, L)),
+             ((L / 2, L / 2, 0.0), (L, 0, 0), (0, L, 0)), ((0.0, L / 2, L / 2), (0, L, 0), (0, 0, L)),
+             ((L, L / 2, L / 2), (0, 0, L), (0, L, 0))]
+    for centre, u, v in walls:
+        h = meshes.add(*quad_mesh(u, v), double_sided=True)
+        ents.append(entity(_lib.SHAPE_MESH, _lib.MAT_LAMBERTIAN, centre,
+                           albedo=tuple(float(x) for x in rng.uniform(0.2, 0.8, 3)), mesh=h))
+    h = meshes.add(*box_mesh((1.2, 1.2, 1.2)))
+    ents.append(entity(_lib.SHAPE_MESH, _lib.MAT_LAMBERTIAN, (5.0, 1.2, 5.0), rotation=yaw_quat(0.5),
+                       albedo=(0.7, 0.7, 0.2), mesh=h))
+    cfg = s.config.copy()
+    return _finish(ents, meshes, cfg, "hybrid_box")

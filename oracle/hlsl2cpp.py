@@ -16,14 +16,17 @@ Every rewrite is token level and changes no arithmetic:
      HLSL code names them;
   5. parameter qualifiers: "out T x" / "inout T x" -> "T &x",
      "const in T x" -> "const T &x", "in T x" -> "T x";
-  6. swizzle reads become calls: ".xyz" -> ".xyz()" (also .rgb .xy .zw);
+  6. swizzle reads become calls: ".xyz" -> ".xyz()" (also .rgb .xy .zw), and
+     the colour alias ".a" reads ".w";
   7. file-scope "static T x;" becomes thread_local (the RNG state `seed` is
      per invocation in HLSL; per host thread here);
   8. a statement with two or more Random() calls gets its calls hoisted into
      temporaries in textual order, since C++ leaves the evaluation order of
      operands and constructor arguments unspecified and the shader's stream
      order is left to right;
-  9. optional instrumentation (--instrument): extra fields on the Hit struct
+  9. "row_major" is dropped (the shim's float4x4 is row-major), "(T)0"
+     becomes "T{}" and a scalar's ".xxx" becomes "float3(...)";
+ 10. optional instrumentation (--instrument): extra fields on the Hit struct
      that record the winning triangle and object slot, which the shader keeps
      only in locals.  Each anchor must match exactly once.
 
@@ -131,11 +134,15 @@ def transpile(src: str, kind: str | None) -> str:
     s = re.sub(r":\s*register\([^)]*\)", "", s)
     s = re.sub(r":\s*SV_\w+", "", s)
     s = unwrap_cbuffer(s)
+    s = re.sub(r"\brow_major\s+", "", s)
+    s = re.sub(r"\((\w+)\)0\b", r"\1{}", s)                 # (Hit)0 -> Hit{}
+    s = re.sub(r"\(([^()]*)\)\.xxx\b", r"float3(\1)", s)   # (scalar).xxx -> float3(scalar)
     s = re.sub(r"\bconst\s+in\s+(\w+)\s+(\w+)", r"const \1 &\2", s)
     s = re.sub(r"\binout\s+(\w+)\s+(\w+)", r"\1 &\2", s)
     s = re.sub(r"\bout\s+(\w+)\s+(\w+)", r"\1 &\2", s)
     s = re.sub(r"\bin\s+(\w+)\s+(\w+)", r"\1 \2", s)
     s = re.sub(r"\.(xyz|rgb|xy|zw)\b(?!\s*\()", r".\1()", s)
+    s = re.sub(r"\.a\b(?!\s*\()", ".w", s)                  # colour alpha is the w member
     s = re.sub(r"(?m)^static\s+(?!const\b)(\w+)\s+(\w+)\s*;", r"static thread_local \1 \2;", s)
     s = hoist_random(s)
     if kind:

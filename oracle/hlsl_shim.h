@@ -22,11 +22,13 @@ struct float2;
 struct float3;
 struct float4;
 
+struct uint2;
 struct float2 {
     float x, y;
     float2() : x(0), y(0) {}
     float2(float s) : x(s), y(s) {}
     float2(float a, float b) : x(a), y(b) {}
+    explicit float2(const uint2 &u);
 };
 struct float3 {
     float x, y, z;
@@ -56,7 +58,10 @@ struct uint2 {
     uint x, y;
     uint2() : x(0), y(0) {}
     uint2(uint a, uint b) : x(a), y(b) {}
+    explicit uint2(float2 f) : x(uint(f.x)), y(uint(f.y)) {}
+    explicit uint2(const struct int2 &v);
 };
+inline uint2 min(uint2 a, uint2 b) { return uint2(a.x < b.x ? a.x : b.x, a.y < b.y ? a.y : b.y); }
 struct uint3 {
     uint x, y, z;
     uint3() : x(0), y(0), z(0) {}
@@ -67,7 +72,40 @@ struct int2 {
     int x, y;
     int2() : x(0), y(0) {}
     int2(int a, int b) : x(a), y(b) {}
+    explicit int2(uint2 u) : x(int(u.x)), y(int(u.y)) {}
+    explicit int2(float2 f) : x(int(f.x)), y(int(f.y)) {}
 };
+struct int3 {
+    int x, y, z;
+    int3(int a, int b, int c) : x(a), y(b), z(c) {}
+    int3(int2 a, int c) : x(a.x), y(a.y), z(c) {}
+    int3(uint2 a, int c) : x(int(a.x)), y(int(a.y)), z(c) {}
+};
+struct bool2 {
+    bool x, y;
+};
+inline uint2::uint2(const int2 &v) : x(uint(v.x)), y(uint(v.y)) {}
+inline float2::float2(const uint2 &u) : x(float(u.x)), y(float(u.y)) {}
+inline bool all(bool2 b) { return b.x && b.y; }
+inline bool2 operator>=(int2 a, int b) { return bool2{a.x >= b, a.y >= b}; }
+inline bool2 operator<(int2 a, int2 b) { return bool2{a.x < b.x, a.y < b.y}; }
+inline int2 operator+(int2 a, int2 b) { return int2(a.x + b.x, a.y + b.y); }
+inline int2 operator-(int2 a, int b) { return int2(a.x - b, a.y - b); }
+inline int2 clamp(int2 v, int2 lo, int2 hi) {
+    return int2(v.x < lo.x ? lo.x : (v.x > hi.x ? hi.x : v.x), v.y < lo.y ? lo.y : (v.y > hi.y ? hi.y : v.y));
+}
+inline float2 to_float2(uint2 u) { return float2(float(u.x), float(u.y)); }
+struct float4x4 {
+    float m[4][4];
+};
+// mul(M, v) for a row-major matrix: each row dotted with v, left to right.
+inline float4 mul(const float4x4 &M, const float4 &v) {
+    float r[4];
+    for (int i = 0; i < 4; i++)
+        r[i] = AE_ADD(AE_ADD(AE_ADD(AE_MUL(M.m[i][0], v.x), AE_MUL(M.m[i][1], v.y)), AE_MUL(M.m[i][2], v.z)),
+                      AE_MUL(M.m[i][3], v.w));
+    return float4(r[0], r[1], r[2], r[3]);
+}
 
 // --- float3 arithmetic through ae:: (IEEE, no contraction) ---------------
 inline ae::f3 A(const float3 &v) { return ae::mk(v.x, v.y, v.z); }
@@ -141,6 +179,8 @@ inline float pow(float x, float y) { return ae::powf_(x, y); }
 inline float3 pow(const float3 &x, float y) { return float3(ae::powf_(x.x, y), ae::powf_(x.y, y), ae::powf_(x.z, y)); }
 inline float floor(float x) { return AE_FLOOR(x); }
 inline float2 floor(const float2 &v) { return float2(AE_FLOOR(v.x), AE_FLOOR(v.y)); }
+inline float2 ceil(const float2 &v) { return float2(__builtin_ceilf(v.x), __builtin_ceilf(v.y)); }
+inline float3 frac(const float3 &v) { return float3(ae::fracf(v.x), ae::fracf(v.y), ae::fracf(v.z)); }
 inline float frac(float x) { return ae::fracf(x); }
 inline float sign(float x) { return ae::signf(x); }
 inline float saturate(float x) { return ae::saturate(x); }
@@ -172,6 +212,7 @@ template <typename T>
 struct Texture2D {
     const T *data = nullptr;
     uint width = 0, height = 0;
+    T Load(const int3 &p) const { return data[size_t(p.y) * width + size_t(p.x)]; }
     T operator[](uint2 id) const { return data[size_t(id.y) * width + id.x]; }
 };
 struct SamplerState {};

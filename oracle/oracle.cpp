@@ -935,3 +935,723 @@ int oracle_path_counters(const Scene *S, const ae_config *c, const uint32_t *xy,
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Hybrid renderer passes (float only): deferred resolve, temporal upsample,
+// and the library's ray-cast G-buffer.  `deferred:N` is
+// shaders/deferred.comp.hlsl line N, `upsample:N` shaders/upsample.comp.hlsl.
+// ===========================================================================
+namespace oracle {
+
+using Vf = V<float>;
+
+// AABBEntry, deferred:635-646.
+inline float aabb_entry(Vf o, Vf inv, const ae_bvh_node &n, float tn, float tf) {
+    const Vf t0 = (v3<float>(n.min_x, n.min_y, n.min_z) - o) * inv;
+    const Vf t1 = (v3<float>(n.max_x, n.max_y, n.max_z) - o) * inv;
+    const Vf lo = vmin(t0, t1), hi = vmax(t0, t1);
+    const float tmin = M<float>::fmax(M<float>::fmax(lo.x, lo.y), M<float>::fmax(lo.z, tn));
+    const float tmax = M<float>::fmin(M<float>::fmin(hi.x, hi.y), M<float>::fmin(hi.z, tf));
+    return tmin <= tmax ? tmin : 1e30f;
+}
+
+inline void to_local(const ae_instance &I, const Ray<float> &r, Ray<float> &L) {
+    L.o = qrot<float>(-I.qx, -I.qy, -I.qz, I.qw, r.o - v3<float>(I.px, I.py, I.pz));
+    L.d = qrot<float>(-I.qx, -I.qy, -I.qz, I.qw, r.d);
+    L.time = r.time;
+    if (I.scale != 0.0f && I.scale != 1.0f) {
+        const float inv = 1.0f / I.scale;
+        L.o = L.o * inv;
+        L.d = L.d * inv;
+    }
+}
+
+// HitMesh with nearest-first children, deferred:684-806.
+inline bool hit_mesh_ordered(const Scene &S, const ae_object &obj, const Ray<float> &r, float tn, float tf,
+                             Hit<float> &h) {
+    const ae_instance &I = S.instances[obj.instanceIndex];
+    Ray<float> L;
+    to_local(I, r, L);
+    const Vf invd = 1.0f / L.d;
+    int stack[64];
+    int sp = 0;
+    stack[sp++] = 0;
+    bool found = false;
+    float closest = tf, ba = 0, bb = 0;
+    uint32_t best = 0;
+    Vf bgeo = v3<float>(0, 0, 1);
+    while (sp > 0) {
+        const ae_bvh_node &n = S.blas[I.blasBase + uint32_t(stack[--sp])];
+        if (!slab(L.o, invd, n, tn, closest)) continue;
+        if (n.count > 0) {
+            for (int i = 0; i < n.count; i++) {
+                const uint32_t base = I.indexBase + uint32_t(n.left + i) * 3u;
+                const Vf p0 = vpos<float>(S.vertices[I.vertexBase + S.indices[base]]);
+                const Vf p1 = vpos<float>(S.vertices[I.vertexBase + S.indices[base + 1]]);
+                const Vf p2 = vpos<float>(S.vertices[I.vertexBase + S.indices[base + 2]]);
+                float t, a, b;
+                Vf g;
+                if (hit_mesh_triangle(L, tn, closest, p0, p1, p2, t, a, b, g)) {
+                    closest = t; found = true; ba = a; bb = b; best = base; bgeo = g;
+                }
+            }
+        } else {
+            const ae_bvh_node &Ln = S.blas[I.blasBase + uint32_t(n.left)];
+            const ae_bvh_node &Rn = S.blas[I.blasBase + uint32_t(n.right)];
+            const float tl = aabb_entry(L.o, invd, Ln, tn, closest);
+            const float tr = aabb_entry(L.o, invd, Rn, tn, closest);
+            const bool lf = tl <= tr;
+            if (M<float>::fmax(tl, tr) < 1e30f) stack[sp++] = lf ? n.right : n.left;
+            if (M<float>::fmin(tl, tr) < 1e30f) stack[sp++] = lf ? n.left : n.right;
+        }
+    }
+    if (!found) return false;
+    const ae_vertex &A = S.vertices[I.vertexBase + S.indices[best]];
+    const ae_vertex &B = S.vertices[I.vertexBase + S.indices[best + 1]];
+    const ae_vertex &C = S.vertices[I.vertexBase + S.indices[best + 2]];
+    const float w0 = 1.0f - ba - bb;
+    const Vf sh = nrm(w0 * v3<float>(A.nx, A.ny, A.nz) + ba * v3<float>(B.nx, B.ny, B.nz) + bb * v3<float>(C.nx, C.ny, C.nz));
+    Vf geo = bgeo;
+    if (dot(geo, sh) < 0) geo = -geo;
+    h.t = closest;
+    h.p = r.o + r.d * closest;
+    h.n = nrm(qrot<float>(I.qx, I.qy, I.qz, I.qw, sh));
+    h.front = dot(r.d, qrot<float>(I.qx, I.qy, I.qz, I.qw, geo)) < 0;
+    if (!h.front) h.n = -h.n;
+    h.prim = (best - I.indexBase) / 3u;
+    h.alpha = ba;
+    h.beta = bb;
+    return true;
+}
+
+// OccludedMesh, deferred:812-854.
+inline bool occluded_mesh(const Scene &S, const ae_object &obj, const Ray<float> &r, float tn, float tf) {
+    const ae_instance &I = S.instances[obj.instanceIndex];
+    Ray<float> L;
+    to_local(I, r, L);
+    const Vf invd = 1.0f / L.d;
+    int stack[64];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const ae_bvh_node &n = S.blas[I.blasBase + uint32_t(stack[--sp])];
+        if (!slab(L.o, invd, n, tn, tf)) continue;
+        if (n.count > 0) {
+            for (int i = 0; i < n.count; i++) {
+                const uint32_t base = I.indexBase + uint32_t(n.left + i) * 3u;
+                float t, a, b;
+                Vf g;
+                if (hit_mesh_triangle(L, tn, tf, vpos<float>(S.vertices[I.vertexBase + S.indices[base]]),
+                                      vpos<float>(S.vertices[I.vertexBase + S.indices[base + 1]]),
+                                      vpos<float>(S.vertices[I.vertexBase + S.indices[base + 2]]), t, a, b, g))
+                    return true;
+            }
+        } else {
+            stack[sp++] = n.left;
+            stack[sp++] = n.right;
+        }
+    }
+    return false;
+}
+
+// IsRasterProxy, deferred:1011-1017.
+inline bool raster_proxy(const ae_object &o) {
+    return o.shapeType == AE_SHAPE_BOX && o.colorType != AE_MAT_ISOTROPIC && o.textureID == AE_NO_TEXTURE &&
+           o.rotation == 0.0f;
+}
+
+// HitObject as deferred.comp dispatches it (its HitMesh is the ordered one).
+inline bool hit_object_d(const Scene &S, const ae_object &o, const Ray<float> &r, float tn, float tf, Hit<float> &h,
+                         Rng &rng) {
+    if (o.colorType == AE_MAT_ISOTROPIC) return hit_volume(o, r, tn, tf, h, rng);
+    switch (o.shapeType) {
+    case AE_SHAPE_SPHERE: return hit_sphere(o, r, tn, tf, h);
+    case AE_SHAPE_QUAD: return hit_planar(o, r, tn, tf, h, false);
+    case AE_SHAPE_TRIANGLE: return hit_planar(o, r, tn, tf, h, true);
+    case AE_SHAPE_MESH: return hit_mesh_ordered(S, o, r, tn, tf, h);
+    default: return hit_box(o, r, tn, tf, h);
+    }
+}
+
+// TraverseBVHBounded, deferred:1027-1099.
+inline bool traverse_bounded(const Scene &S, const Ray<float> &r, float tn, float far_limit, bool skip, Hit<float> &out,
+                             Rng &rng) {
+    if (S.n_nodes == 0) return false;
+    const Vf inv = 1.0f / r.d;
+    int stack[64];
+    int sp = 0;
+    stack[sp++] = 0;
+    bool found = false;
+    float tf = far_limit;
+    while (sp > 0) {
+        const ae_bvh_node &n = S.tlas[stack[--sp]];
+        if (!slab(r.o, inv, n, tn, tf)) continue;
+        if (n.count > 0) {
+            for (int i = 0; i < n.count; i++) {
+                const uint32_t slot = uint32_t(n.left + i);
+                const ae_object &o = S.objects[slot];
+                if (skip && (o.shapeType == AE_SHAPE_MESH || raster_proxy(o))) continue;
+                Hit<float> h;
+                if (hit_object_d(S, o, r, tn, tf, h, rng)) {
+                    tf = h.t;
+                    h.obj = &o;
+                    h.slot = slot;
+                    out = h;
+                    found = true;
+                }
+            }
+        } else {
+            const float tl = aabb_entry(r.o, inv, S.tlas[n.left], tn, tf);
+            const float tr = aabb_entry(r.o, inv, S.tlas[n.right], tn, tf);
+            const bool lf = tl <= tr;
+            if (M<float>::fmax(tl, tr) < 1e30f) stack[sp++] = lf ? n.right : n.left;
+            if (M<float>::fmin(tl, tr) < 1e30f) stack[sp++] = lf ? n.left : n.right;
+        }
+    }
+    return found;
+}
+
+// Occluded, deferred:1115-1171.
+inline bool occluded(const Scene &S, const Ray<float> &r, float tn, float tf, Rng &rng) {
+    if (S.n_nodes == 0) return false;
+    const Vf inv = 1.0f / r.d;
+    int stack[64];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const ae_bvh_node &n = S.tlas[stack[--sp]];
+        if (!slab(r.o, inv, n, tn, tf)) continue;
+        if (n.count > 0) {
+            for (int i = 0; i < n.count; i++) {
+                const ae_object &o = S.objects[n.left + i];
+                if (o.colorType == AE_MAT_DIELECTRIC || o.colorType == AE_MAT_DIFFUSE_LIGHT) continue;
+                if (o.shapeType == AE_SHAPE_MESH) {
+                    if (occluded_mesh(S, o, r, tn, tf)) return true;
+                    continue;
+                }
+                Hit<float> h;
+                if (hit_object_d(S, o, r, tn, tf, h, rng)) return true;
+            }
+        } else {
+            stack[sp++] = n.left;
+            stack[sp++] = n.right;
+        }
+    }
+    return false;
+}
+
+// The deferred Hit: geometry plus the (possibly G-buffer) albedo it shades with.
+struct DSurf {
+    Hit<float> h;
+    Vf albedo;
+    const ae_object *obj = nullptr;
+};
+
+// CalculateDirectLight (deferred:1376-1446) + ClampedDirectLight (1556-1569).
+inline Vf clamped_direct(const Scene &S, const DSurf &s, float time, Rng &rng) {
+    Vf acc = v3<float>(0, 0, 0);
+    for (uint32_t i = 0; i < S.n_lights; i++) {
+        const ae_object &L = S.objects[S.lights[i]];
+        Vf lp;
+        float omega;
+        sample_light(L, s.h.p, lp, omega, rng);
+        if (omega <= 0) continue;
+        Vf sd = lp - s.h.p;
+        const float dist = len(sd);
+        if (dist <= 1e-6f) continue;
+        sd = sd / dist;
+        const float ct = dot(s.h.n, sd);
+        if (ct <= 0) continue;
+        Ray<float> sr;
+        sr.o = s.h.p + s.h.n * 0.001f;
+        sr.d = sd;
+        sr.time = time;
+        if (!occluded(S, sr, 0.001f, dist - 0.001f, rng)) {
+            const Vf rad = float(L.emission) * albedo<float>(L);
+            acc = acc + s.albedo * rad * ct * omega;
+        }
+    }
+    const float luma = maxc(acc);
+    if (luma > 8.0f) acc = acc * (8.0f / luma);
+    return acc;
+}
+
+inline DSurf surf_of(const Hit<float> &h) {
+    DSurf s;
+    s.h = h;
+    s.obj = h.obj;
+    s.albedo = albedo<float>(*h.obj);
+    return s;
+}
+
+// GetBounce on a deferred surface (deferred:1219-1288).
+inline bool bounce_d(const Ray<float> &r, const DSurf &s, Vf &dir, Rng &rng) { return bounce(r, s.h, dir, rng); }
+
+// TraceIndirect, deferred:1575-1646.
+inline Vf trace_indirect(const Scene &S, const ae_config &c, const Ray<float> &primary, const DSurf &surf, Rng &rng) {
+    Vf bd;
+    if (!bounce_d(primary, surf, bd, rng)) return v3<float>(0, 0, 0);
+    Ray<float> ray;
+    ray.d = nrm(bd);
+    const float s0 = dot(ray.d, surf.h.n) < 0 ? -1.0f : 1.0f;
+    ray.o = surf.h.p + surf.h.n * (0.001f * s0);
+    ray.time = primary.time;
+    Vf thr = surf.obj->colorType != AE_MAT_DIELECTRIC ? surf.albedo : v3<float>(1, 1, 1);
+    Vf acc = v3<float>(0, 0, 0);
+    const Vf sky = v3<float>(c.sky_r, c.sky_g, c.sky_b);
+    for (uint32_t b = 1; b < c.depth; b++) {
+        Hit<float> h;
+        if (!traverse_bounded(S, ray, 0.001f, 1000000.0f, false, h, rng)) {
+            acc = acc + thr * sky;
+            break;
+        }
+        if (h.obj->colorType == AE_MAT_DIFFUSE_LIGHT) {
+            acc = acc + thr * (float(h.obj->emission) * albedo<float>(*h.obj));
+            break;
+        }
+        const DSurf s = surf_of(h);
+        if (h.obj->colorType == AE_MAT_LAMBERTIAN) acc = acc + thr * clamped_direct(S, s, ray.time, rng);
+        Vf nx;
+        if (!bounce(ray, h, nx, rng)) break;
+        ray.d = nrm(nx);
+        const float sg = dot(ray.d, h.n) < 0 ? -1.0f : 1.0f;
+        ray.o = h.p + h.n * (0.001f * sg);
+        if (h.obj->colorType != AE_MAT_DIELECTRIC) thr = thr * albedo<float>(*h.obj);
+        float p = maxc(thr);
+        p = M<float>::fmin(M<float>::fmax(p, 0.1f), 1.0f);
+        if (rng.next<float>() > p) break;
+        thr = thr / p;
+    }
+    return acc;
+}
+
+struct Planes {  // all W*H texels; albedo as float4 = byte/255
+    const float *gpos, *gnrm, *galb, *gdepth;
+    const float *prev_img, *prev_geo;
+    float *img, *display, *reduced, *cur_geo;
+    uint32_t red_w, red_h;
+};
+
+inline const float *at4(const float *p, uint32_t w, uint32_t x, uint32_t y) { return p + 4 * (size_t(y) * w + x); }
+
+// CurrentRotation / PreviousRotation / PreviousPosition, deferred:1759-1793.
+inline Vf previous_position(const Scene &S, const ae_object &o, Vf p) {
+    float qx = 0, qy = 0, qz = 0, qw = 1;
+    if (o.shapeType == AE_SHAPE_MESH) {
+        const ae_instance &I = S.instances[o.instanceIndex];
+        qx = I.qx; qy = I.qy; qz = I.qz; qw = I.qw;
+    } else if (o.shapeType == AE_SHAPE_SPHERE || o.shapeType == AE_SHAPE_BOX) {
+        const float half = 0.5f * o.rotation;
+        qy = M<float>::sin(half);
+        qw = M<float>::cos(half);
+    }
+    const Vf local = qrot<float>(-qx, -qy, -qz, qw, p - pos<float>(o));
+    const Vf v = v3<float>(o.prevRotX, o.prevRotY, o.prevRotZ);
+    const float w = M<float>::sqrt(M<float>::fmax(0.0f, 1.0f - dot(v, v)));
+    return qrot<float>(v.x, v.y, v.z, w, local) + pos2<float>(o);
+}
+
+// ReprojectHistory, deferred:1810-1875 (same as upsample:218-278).
+inline void reproject(const ae_config &c, uint32_t px, uint32_t py, Vf color, bool surface, Vf position, Vf prev_pos,
+                      Vf normal, bool vd, const float *prev_img, const float *prev_geo, Vf &result, float &count) {
+    const uint32_t W = c.width, H = c.height;
+    int hx = int(px), hy = int(py);
+    bool valid = c.historyReset == 0;
+    const Vf src = v3<float>(c.source_x, c.source_y, c.source_z);
+    if (valid && c.cameraMoved != 0) {
+        valid = false;
+        if (surface) {
+            const float v[4] = {prev_pos.x, prev_pos.y, prev_pos.z, 1.0f};
+            float clip[4];
+            for (int r = 0; r < 4; r++) {
+                const float *m = c.prevViewProj + 4 * r;
+                clip[r] = m[0] * v[0] + m[1] * v[1] + m[2] * v[2] + m[3] * v[3];
+            }
+            if (clip[3] > 0) {
+                const float ux = clip[0] / clip[3] * 0.5f + 0.5f;
+                const float uy = clip[1] / clip[3] * -0.5f + 0.5f;
+                const float fx = std::floor(ux * float(W)), fy = std::floor(uy * float(H));
+                hx = int(std::fmax(std::fmin(fx, 2.0e9f), -2.0e9f));
+                hy = int(std::fmax(std::fmin(fy, 2.0e9f), -2.0e9f));
+                if (hx >= 0 && hy >= 0 && hx < int(W) && hy < int(H)) {
+                    const float *pg = at4(prev_geo, W, hx, hy);
+                    const Vf pp = v3<float>(pg[0], pg[1], pg[2]);
+                    const float plane = std::fabs(dot(pp - prev_pos, normal));
+                    const float tol = 0.01f * len(position - src) + 0.01f;
+                    const float fp = len(position - src) * 2.0f * M<float>::tan(ae::radians(c.fov * 0.5f)) / float(H);
+                    const float facing = M<float>::fmax(std::fabs(dot(normal, nrm(src - position))), 0.33f);
+                    const float drift = len(pp - prev_pos);
+                    valid = pg[3] > 0 && plane < tol && drift < M<float>::fmax(2.5f * fp / facing, 0.01f);
+                }
+            }
+        }
+    }
+    if (!valid) {
+        count = 1.0f;
+        result = color;
+        return;
+    }
+    const float prev_count = std::fabs(at4(prev_geo, W, hx, hy)[3]);
+    const float moving = vd ? M<float>::fmin(c.historyCap, 4.0f) : c.historyCap;
+    const float cap = c.cameraMoved != 0 ? moving : 1e7f;
+    count = M<float>::fmin(prev_count + 1.0f, cap);
+    const float *pi = at4(prev_img, W, hx, hy);
+    const Vf prev = v3<float>(pi[0], pi[1], pi[2]);
+    result = prev + (1.0f / count) * (color - prev);
+}
+
+// TracedTexel, deferred:1742-1747.
+inline void traced_texel(const ae_config &c, uint32_t cx, uint32_t cy, uint32_t &tx, uint32_t &ty) {
+    static const float off[4][2] = {{0.0f, 0.0f}, {0.5f, 0.5f}, {0.5f, 0.0f}, {0.0f, 0.5f}};
+    const uint32_t k = c.frameIndex % 4u;
+    const float fx = std::floor((float(cx) + off[k][0]) / c.traceScale);
+    const float fy = std::floor((float(cy) + off[k][1]) / c.traceScale);
+    tx = std::min(uint32_t(fx), c.width - 1);
+    ty = std::min(uint32_t(fy), c.height - 1);
+}
+
+inline void put4(float *p, uint32_t w, uint32_t x, uint32_t y, Vf v, float a) {
+    float *q = p + 4 * (size_t(y) * w + x);
+    q[0] = v.x; q[1] = v.y; q[2] = v.z; q[3] = a;
+}
+
+// ResolvePrimary with HitFromGBuffer, deferred:1452-1548: 0 sky, 1 raster, 2 analytic.
+inline int resolve_primary(const Scene &S, const ae_config &c, const Planes &P, uint32_t x, uint32_t y,
+                           const Ray<float> &primary, Rng &rng, DSurf &hit) {
+    const uint32_t W = c.width;
+    DSurf raster;
+    bool has_raster = false;
+    float far_limit = 1000000.0f;
+    const float *pn = at4(P.gnrm, W, x, y);
+    if (!(pn[3] < 0.5f)) {
+        const float *pp = at4(P.gpos, W, x, y);
+        const uint32_t slot = uint32_t(pp[3] + 0.5f);
+        if (slot < S.n_objects) {
+            raster.obj = &S.objects[slot];
+            raster.h.obj = raster.obj;
+            raster.h.slot = slot;
+            raster.h.p = v3<float>(pp[0], pp[1], pp[2]);
+            raster.h.n = nrm(v3<float>(pn[0], pn[1], pn[2]));
+            const float *pa = at4(P.galb, W, x, y);
+            raster.albedo = v3<float>(pa[0], pa[1], pa[2]);
+            raster.h.front = dot(primary.d, raster.h.n) < 0;
+            if (!raster.h.front) raster.h.n = -raster.h.n;
+            raster.h.t = len(raster.h.p - primary.o);
+            far_limit = raster.h.t;
+            has_raster = true;
+        }
+    }
+    Hit<float> ah;
+    if (traverse_bounded(S, primary, 0.001f, far_limit, true, ah, rng)) {
+        hit = surf_of(ah);
+        return 2;
+    }
+    if (has_raster) {
+        hit = raster;
+        return 1;
+    }
+    return 0;
+}
+
+// MaterialFalseColour, deferred:1652-1663.
+inline Vf false_colour(uint32_t t) {
+    switch (t) {
+    case AE_MAT_LAMBERTIAN: return v3<float>(0.55f, 0.55f, 0.55f);
+    case AE_MAT_METAL: return v3<float>(1.0f, 0.75f, 0.1f);
+    case AE_MAT_DIELECTRIC: return v3<float>(0.1f, 0.85f, 1.0f);
+    case AE_MAT_DIFFUSE_LIGHT: return v3<float>(1.0f, 1.0f, 1.0f);
+    case AE_MAT_ISOTROPIC: return v3<float>(0.7f, 0.3f, 1.0f);
+    default: return v3<float>(1.0f, 0.0f, 1.0f);
+    }
+}
+
+// DebugColour, deferred:1667-1722 (with WorldFromDepth, 1503-1514).
+inline Vf debug_colour(const Scene &S, const ae_config &c, const Planes &P, uint32_t x, uint32_t y,
+                       const Ray<float> &primary, Rng &rng, const Camera<float> &K) {
+    const uint32_t W = c.width;
+    const float *pn = at4(P.gnrm, W, x, y);
+    const bool covered = pn[3] >= 0.5f;
+    const Vf bg = v3<float>(0, 0, 0);
+    if (c.debugView == 1) {
+        const float *pa = at4(P.galb, W, x, y);
+        return covered ? v3<float>(pa[0], pa[1], pa[2]) : bg;
+    }
+    if (c.debugView == 2) return covered ? v3<float>(pn[0], pn[1], pn[2]) * 0.5f + v3<float>(0.5f, 0.5f, 0.5f) : bg;
+    if (c.debugView == 3) {
+        if (!covered) return bg;
+        const float *pp = at4(P.gpos, W, x, y);
+        const Vf q = v3<float>(pp[0], pp[1], pp[2]) / 100.0f;
+        return v3<float>(ae::fracf(q.x), ae::fracf(q.y), ae::fracf(q.z));
+    }
+    if (c.debugView == 6) {
+        if (!covered) return v3<float>(0.0f, 0.0f, 0.2f);
+        const float *pp = at4(P.gpos, W, x, y);
+        const Vf stored = v3<float>(pp[0], pp[1], pp[2]);
+        const float dd = P.gdepth[size_t(y) * W + x];
+        const float vz = (c.zNear * c.zFar) / (c.zFar + dd * (c.zNear - c.zFar));
+        const Vf fwd = -nrm(K.src - v3<float>(c.target_x, c.target_y, c.target_z));
+        const float t = vz / dot(primary.d, fwd);
+        const Vf rebuilt = K.src + primary.d * t;
+        const float rel = len(rebuilt - stored) / M<float>::fmax(len(stored - K.src), 1e-4f);
+        const float v = rel * 100.0f;
+        return v3<float>(v, v, v);
+    }
+    DSurf hit;
+    const int source = resolve_primary(S, c, P, x, y, primary, rng, hit);
+    if (c.debugView == 4) return source != 0 ? false_colour(hit.obj->colorType) : bg;
+    if (source == 1) return v3<float>(0.1f, 0.8f, 0.2f);
+    if (source == 2) return v3<float>(0.85f, 0.15f, 0.1f);
+    return v3<float>(0.1f, 0.15f, 0.5f);
+}
+
+// main, deferred:1879-2010 (final view).
+inline void deferred_cell(const Scene &S, const ae_config &c, const Planes &P, uint32_t cx, uint32_t cy) {
+    const bool reduced = c.traceScale < 1.0f;
+    uint32_t x = cx, y = cy;
+    if (reduced) traced_texel(c, cx, cy, x, y);
+    const uint32_t W = c.width;
+    if (c.displayOnly) {
+        if (!reduced) {
+            const float *a = at4(P.img, W, x, y);
+            put4(P.display, W, x, y, srgb(aces(v3<float>(a[0], a[1], a[2]) * c.exposure)), 1.0f);
+        }
+        return;
+    }
+    Rng rng{x + y * c.width + c.frameIndex * c.width * c.height + 1u};
+    const Camera<float> K = camera<float>(c);
+    const Vf sample = K.p0 + (float(x) + c.jitter_x) * K.pu + (float(y) + c.jitter_y) * K.pv;
+    Ray<float> primary;
+    primary.o = K.src;
+    primary.d = nrm(sample - K.src);
+    primary.time = rng.next<float>();
+    if (c.debugView != 0) {
+        put4(P.display, W, x, y, debug_colour(S, c, P, x, y, primary, rng, K), 1.0f);
+        return;
+    }
+    // ResolvePrimary + HitFromGBuffer, deferred:1452-1548.
+    DSurf raster;
+    bool has_raster = false;
+    float far_limit = 1000000.0f;
+    const float *pn = at4(P.gnrm, W, x, y);
+    if (!(pn[3] < 0.5f)) {
+        const float *pp = at4(P.gpos, W, x, y);
+        const uint32_t slot = uint32_t(pp[3] + 0.5f);
+        if (slot < S.n_objects) {
+            raster.obj = &S.objects[slot];
+            raster.h.obj = raster.obj;
+            raster.h.slot = slot;
+            raster.h.p = v3<float>(pp[0], pp[1], pp[2]);
+            raster.h.n = nrm(v3<float>(pn[0], pn[1], pn[2]));
+            const float *pa = at4(P.galb, W, x, y);
+            raster.albedo = v3<float>(pa[0], pa[1], pa[2]);
+            raster.h.front = dot(primary.d, raster.h.n) < 0;
+            if (!raster.h.front) raster.h.n = -raster.h.n;
+            raster.h.t = len(raster.h.p - K.src);
+            far_limit = raster.h.t;
+            has_raster = true;
+        }
+    }
+    DSurf hit;
+    int source = 0;
+    Hit<float> ah;
+    if (traverse_bounded(S, primary, 0.001f, far_limit, true, ah, rng)) {
+        hit = surf_of(ah);
+        source = 2;
+    } else if (has_raster) {
+        hit = raster;
+        source = 1;
+    }
+    Vf color = v3<float>(0, 0, 0);
+    if (source == 0) {
+        color = v3<float>(c.sky_r, c.sky_g, c.sky_b);
+    } else if (hit.obj->colorType == AE_MAT_DIFFUSE_LIGHT) {
+        color = float(hit.obj->emission) * hit.albedo;
+    } else {
+        const uint32_t per = c.batches ? c.samples / c.batches : c.samples;
+        const uint32_t spp = per > 1u ? per : 1u;
+        for (uint32_t s = 0; s < spp; s++) {
+            if (hit.obj->colorType == AE_MAT_LAMBERTIAN) color = color + clamped_direct(S, hit, primary.time, rng);
+            color = color + trace_indirect(S, c, primary, hit, rng);
+        }
+        color = color / float(spp);
+    }
+    if (reduced) {
+        const bool demod = source == 1 && hit.obj->colorType != AE_MAT_DIELECTRIC;
+        Vf alb = v3<float>(1, 1, 1);
+        if (demod) alb = vmax(hit.albedo, v3<float>(0.01f, 0.01f, 0.01f));
+        put4(P.reduced, P.red_w, cx, cy, color / alb, demod ? 1.0f : 0.0f);
+        return;
+    }
+    const bool surface = source != 0;
+    const bool vd = surface && (hit.obj->colorType == AE_MAT_METAL || hit.obj->colorType == AE_MAT_DIELECTRIC);
+    const Vf hp = surface ? hit.h.p : v3<float>(0, 0, 0);
+    const Vf prev = surface ? previous_position(S, *hit.obj, hit.h.p) : hp;
+    Vf acc;
+    float hl;
+    reproject(c, x, y, color, surface, hp, prev, surface ? hit.h.n : v3<float>(0, 0, 0), vd, P.prev_img, P.prev_geo, acc,
+              hl);
+    put4(P.img, W, x, y, acc, 1.0f);
+    put4(P.cur_geo, W, x, y, hp, surface ? hl : -hl);
+    put4(P.display, W, x, y, srgb(aces(acc * c.exposure)), 1.0f);
+}
+
+// main, upsample:280-390.
+inline void upsample_pixel(const Scene &S, const ae_config &c, const Planes &P, uint32_t x, uint32_t y) {
+    const uint32_t W = c.width;
+    if (c.displayOnly) {
+        const float *a = at4(P.img, W, x, y);
+        put4(P.display, W, x, y, srgb(aces(v3<float>(a[0], a[1], a[2]) * c.exposure)), 1.0f);
+        return;
+    }
+    const Vf src = v3<float>(c.source_x, c.source_y, c.source_z);
+    const int cmx = int(P.red_w) - 1, cmy = int(P.red_h) - 1;
+    const float *np = at4(P.gnrm, W, x, y);
+    const bool covp = np[3] > 0.5f;
+    const float *gp = at4(P.gpos, W, x, y);
+    const float dp = len(v3<float>(gp[0], gp[1], gp[2]) - src);
+    const float *ap = at4(P.galb, W, x, y);
+    const Vf albp = v3<float>(ap[0], ap[1], ap[2]);
+    const float cpx = (float(x) + 0.5f) * c.traceScale - 0.5f, cpy = (float(y) + 0.5f) * c.traceScale - 0.5f;
+    const int bx = int(std::floor(cpx)), by = int(std::floor(cpy));
+    Vf sum = v3<float>(0, 0, 0), nearest = v3<float>(0, 0, 0);
+    float wsum = 0, nd = 1e30f;
+    for (int j = 0; j < 2; j++)
+        for (int i = 0; i < 2; i++) {
+            const uint32_t cx = uint32_t(std::min(std::max(bx + i, 0), cmx)), cy = uint32_t(std::min(std::max(by + j, 0), cmy));
+            uint32_t tx, ty;
+            traced_texel(c, cx, cy, tx, ty);
+            const float *lit = at4(P.reduced, P.red_w, cx, cy);
+            const float *nt = at4(P.gnrm, W, tx, ty);
+            const bool covt = nt[3] > 0.5f;
+            Vf alb = albp;
+            if (!covp) { const float *at = at4(P.galb, W, tx, ty); alb = v3<float>(at[0], at[1], at[2]); }
+            const Vf l = v3<float>(lit[0], lit[1], lit[2]);
+            const Vf rad = lit[3] > 0.5f ? l * alb : l;
+            const float ox = float(tx) - float(x), oy = float(ty) - float(y);
+            const float d2 = ox * ox + oy * oy;
+            if (d2 < nd) { nd = d2; nearest = rad; }
+            float w = ae::expf_(-d2 * c.traceScale * c.traceScale);
+            if (covt != covp) {
+                w = 0;
+            } else if (covp) {
+                const float *gt = at4(P.gpos, W, tx, ty);
+                const float dt = len(v3<float>(gt[0], gt[1], gt[2]) - src);
+                w *= ae::expf_(-std::fabs(dp - dt) / (0.01f * dp + 0.001f));
+                w *= ae::powf_(sat(np[0] * nt[0] + np[1] * nt[1] + np[2] * nt[2]), 32.0f);
+            }
+            sum = sum + w * rad;
+            wsum += w;
+        }
+    const Vf color = wsum > 1e-4f ? sum / wsum : nearest;
+    const Vf posp = v3<float>(gp[0], gp[1], gp[2]);
+    const bool vd = covp && ap[3] < 0.5f;
+    Vf prev = posp;
+    if (covp) {
+        const uint32_t slot = uint32_t(gp[3]);
+        if (slot < S.n_objects) prev = previous_position(S, S.objects[slot], posp);
+    }
+    Vf acc;
+    float hl;
+    reproject(c, x, y, color, covp, posp, prev, v3<float>(np[0], np[1], np[2]), vd, P.prev_img, P.prev_geo, acc, hl);
+    put4(P.img, W, x, y, acc, 1.0f);
+    put4(P.cur_geo, W, x, y, posp, covp ? hl : -hl);
+    put4(P.display, W, x, y, srgb(aces(acc * c.exposure)), 1.0f);
+}
+
+}  // namespace oracle
+
+extern "C" {
+
+int oracle_deferred(const Scene *S, const ae_config *c, const Planes *P, int threads) {
+    if (threads > 0) omp_set_num_threads(threads);
+    const bool reduced = c->traceScale < 1.0f;
+    const uint32_t ew = reduced ? P->red_w : c->width, eh = reduced ? P->red_h : c->height;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < int(eh); y++)
+        for (uint32_t x = 0; x < ew; x++) deferred_cell(*S, *c, *P, x, uint32_t(y));
+    return 0;
+}
+
+int oracle_upsample(const Scene *S, const ae_config *c, const Planes *P, int threads) {
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < int(c->height); y++)
+        for (uint32_t x = 0; x < c->width; x++) upsample_pixel(*S, *c, *P, x, uint32_t(y));
+    return 0;
+}
+
+}  // extern "C"
+
+// The library's ray-cast G-buffer (in place of gbuffer.vert/frag.hlsl): the
+// closest hit through pixel centre + jitter over what the raster pass draws
+// (meshes and raster proxies), by the compute-only walk.  Planes as the
+// kernel writes them: position (w = slot), outward normal (w = coverage),
+// albedo bytes (a = 0 view-dependent), depth.
+extern "C" int oracle_gbuffer(const oracle::Scene *S, const ae_config *c, float *gpos, float *gnrm, uint8_t *galb,
+                              float *gdepth, int threads) {
+    using namespace oracle;
+    if (threads > 0) omp_set_num_threads(threads);
+    const Camera<float> K = camera<float>(*c);
+    const Vf fwd = -nrm(K.src - v3<float>(c->target_x, c->target_y, c->target_z));
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int y = 0; y < int(c->height); y++)
+        for (uint32_t x = 0; x < c->width; x++) {
+            const size_t px = size_t(y) * c->width + x;
+            const Vf sample = K.p0 + (float(x) + c->jitter_x) * K.pu + (float(uint32_t(y)) + c->jitter_y) * K.pv;
+            Ray<float> r;
+            r.o = K.src;
+            r.d = nrm(sample - K.src);
+            r.time = 0;
+            float *P = gpos + 4 * px, *N = gnrm + 4 * px;
+            uint8_t *A = galb + 4 * px;
+            P[0] = P[1] = P[2] = P[3] = 0;
+            N[0] = N[1] = N[2] = N[3] = 0;
+            A[0] = A[1] = A[2] = A[3] = 0;
+            gdepth[px] = 1.0f;
+            if (S->n_nodes == 0) continue;
+            const Vf inv = 1.0f / r.d;
+            int stack[64];
+            int sp = 0;
+            stack[sp++] = 0;
+            float tf = 1000000.0f;
+            bool found = false;
+            Hit<float> best;
+            Rng rng{1u};
+            while (sp > 0) {
+                const ae_bvh_node &n = S->tlas[stack[--sp]];
+                if (!slab(r.o, inv, n, 0.001f, tf)) continue;
+                if (n.count > 0) {
+                    for (int i = 0; i < n.count; i++) {
+                        const uint32_t slot = uint32_t(n.left + i);
+                        const ae_object &o = S->objects[slot];
+                        Hit<float> h;
+                        bool hit = false;
+                        if (o.shapeType == AE_SHAPE_MESH) hit = hit_mesh(*S, o, r, 0.001f, tf, h, nullptr);
+                        else if (raster_proxy(o)) hit = hit_box(o, r, 0.001f, tf, h);
+                        if (hit) {
+                            tf = h.t;
+                            h.obj = &o;
+                            h.slot = slot;
+                            best = h;
+                            found = true;
+                        }
+                    }
+                } else {
+                    stack[sp++] = n.left;
+                    stack[sp++] = n.right;
+                }
+            }
+            (void)rng;
+            if (!found) continue;
+            const Vf nn = best.front ? best.n : -best.n;
+            P[0] = best.p.x; P[1] = best.p.y; P[2] = best.p.z; P[3] = float(best.slot);
+            N[0] = nn.x; N[1] = nn.y; N[2] = nn.z; N[3] = 1.0f;
+            const ae_object &o = *best.obj;
+            const float al[3] = {o.r, o.g, o.b};
+            for (int k = 0; k < 3; k++) A[k] = uint8_t(int(std::rint(std::fmin(std::fmax(al[k], 0.0f), 1.0f) * 255.0f)));
+            A[3] = (o.colorType == AE_MAT_METAL || o.colorType == AE_MAT_DIELECTRIC) ? 0 : 255;
+            const float vz = dot(best.p - r.o, fwd);
+            gdepth[px] = c->zFar * (c->zNear - vz) / ((c->zNear - c->zFar) * vz);
+        }
+    return 0;
+}

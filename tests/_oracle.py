@@ -192,3 +192,90 @@ def bounce_rays(scene, config, primary, hits):
     valid = np.zeros(len(p), np.uint8)
     oracle().oracle_bounce_rays(ctypes.byref(s), ptr(c), ptr(p), ptr(h), ctypes.c_uint32(len(p)), ptr(out), ptr(valid))
     return out, valid.astype(bool)
+
+
+class Planes(ctypes.Structure):
+    _fields_ = [("gpos", _P), ("gnrm", _P), ("galb", _P), ("gdepth", _P), ("prev_img", _P), ("prev_geo", _P),
+                ("img", _P), ("display", _P), ("reduced", _P), ("cur_geo", _P), ("red_w", ctypes.c_uint32),
+                ("red_h", ctypes.c_uint32)]
+
+
+def gbuffer(scene, config, threads=0):
+    """The oracle's ray-cast G-buffer: (pos, nrm, alb_bytes, depth)."""
+    s = oscene(scene)
+    c = np.ascontiguousarray(np.array(config, dtype=_lib.CONFIG).reshape(1))
+    w, h = int(c["width"][0]), int(c["height"][0])
+    pos = np.zeros((h, w, 4), np.float32)
+    nrm = np.zeros((h, w, 4), np.float32)
+    alb = np.zeros((h, w, 4), np.uint8)
+    dep = np.zeros((h, w), np.float32)
+    oracle().oracle_gbuffer(ctypes.byref(s), ptr(c), ptr(pos), ptr(nrm), ptr(alb), ptr(dep), ctypes.c_int(threads))
+    return pos, nrm, alb, dep
+
+
+def albedo_float(alb):
+    """RGBA8 UNORM as the shader reads it: byte / 255."""
+    return (alb.astype(np.float32) / np.float32(255.0)).astype(np.float32)
+
+
+def reduced_extent(config):
+    s = np.float32(config["traceScale"])
+    if s >= 1.0:
+        return int(config["width"]), int(config["height"])
+    return int(np.ceil(np.float32(config["width"]) * s)), int(np.ceil(np.float32(config["height"]) * s))
+
+
+class HybridState:
+    """Ping-pong history of the hybrid renderer for the CPU implementations."""
+
+    def __init__(self, w, h):
+        self.img = [np.zeros((h, w, 4), np.float32) for _ in range(2)]
+        self.geo = [np.zeros((h, w, 4), np.float32) for _ in range(2)]
+        self.display = np.zeros((h, w, 4), np.float32)
+        self.history = 0
+        self.reduced = None
+
+
+def hybrid_frame(scene, config, gb, state, impl="oracle", threads=0):
+    """One hybrid frame (deferred, then upsample when reduced) on the CPU by the
+    oracle or by the reference's own shaders; mutates `state`."""
+    pos, nrm, alb, dep = gb
+    albf = albedo_float(alb)
+    c = np.ascontiguousarray(np.array(config, dtype=_lib.CONFIG).reshape(1))
+    w, h = int(c["width"][0]), int(c["height"][0])
+    rw, rh = reduced_extent(c[0])
+    reduced = np.zeros((rh, rw, 4), np.float32) if state.reduced is None or state.reduced.shape[:2] != (rh, rw) \
+        else state.reduced
+    writes = int(c["debugView"][0]) == 0 and int(c["displayOnly"][0]) == 0
+    ws = 1 - state.history if writes else state.history
+    rs = 1 - ws
+    red = float(c["traceScale"][0]) < 1.0
+    if impl == "oracle":
+        s = oscene(scene)
+        P = Planes(ptr(pos), ptr(nrm), ptr(albf), ptr(dep), ptr(state.img[rs]), ptr(state.geo[rs]), ptr(state.img[ws]),
+                   ptr(state.display), ptr(reduced), ptr(state.geo[ws]), rw, rh)
+        if not (red and int(c["displayOnly"][0])):
+            oracle().oracle_deferred(ctypes.byref(s), ptr(c), ctypes.byref(P), ctypes.c_int(threads))
+        if red:
+            oracle().oracle_upsample(ctypes.byref(s), ptr(c), ctypes.byref(P), ctypes.c_int(threads))
+    else:
+        L = _load(os.path.join(ROOT, "oracle", "_ref", "libaeref_deferred.so"))
+        keep = [np.ascontiguousarray(a) for a in (scene.objects, scene.tlas, scene.lights, scene.vertices,
+                                                  scene.indices, scene.blas, scene.instances)]
+        o, t, l, v, i, b, ins = keep
+        u32 = ctypes.c_uint32
+        L.aeref_d_bind(ptr(o), u32(len(o)), ptr(t), u32(len(t)), ptr(l), u32(len(l)), ptr(v), u32(len(v)), ptr(i),
+                       u32(len(i)), ptr(b), u32(len(b)), ptr(ins), u32(len(ins)))
+        L.aeref_d_set_config(ptr(c))
+        if not (red and int(c["displayOnly"][0])):
+            L.aeref_deferred(ptr(pos), ptr(nrm), ptr(albf), ptr(dep), ptr(state.img[rs]), ptr(state.geo[rs]),
+                             ptr(state.img[ws]), ptr(state.display), ptr(reduced), u32(rw), u32(rh), ptr(state.geo[ws]),
+                             ctypes.c_int(threads))
+        if red:
+            L.aeref_upsample(ptr(pos), ptr(nrm), ptr(albf), ptr(reduced), u32(rw), u32(rh), ptr(state.img[rs]),
+                             ptr(state.geo[rs]), ptr(state.img[ws]), ptr(state.display), ptr(state.geo[ws]),
+                             ctypes.c_int(threads))
+    state.reduced = reduced
+    if writes:
+        state.history = ws
+    return state
