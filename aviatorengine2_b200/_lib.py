@@ -104,6 +104,7 @@ SIGNATURES = {
     "ae_camera_rays": (_I, [_P, _P]),
     "ae_bounce_rays": (_I, [_P, _P, _P, _U32, _P, _P]),
     "ae_trace_counters": (_I, [_P, _P, _U32, _P]),
+    "ae_wavefront_info": (_I, [_P, _P, _P, _P, _P]),
     "ae_synchronize": (_I, [_P]),
     "ae_last_kernel_ms": (_I, [_P, _P]),
     "ae_stream": (_P, [_P]),

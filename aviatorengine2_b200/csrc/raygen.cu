@@ -5,31 +5,10 @@
 // and the incoherent bounce set that follows it.
 #include "context.h"
 #include "kernels.h"
+#include "shade.cuh"
 #include "trace_common.cuh"
 
 namespace ae {
-
-// Primary ray of pixel (x, y) and the RNG state after it (jitter, defocus
-// disk when the angle is positive, then the time draw).
-AE_DEV void camera_ray(const FrameParams &F, uint32_t x, uint32_t y, f3 &o, f3 &d, float &time, uint32_t &seed) {
-    seed = x + y * F.width + F.batch * F.width * F.height + 1u;
-    const float jx = AE_SUB(rng_next(seed), 0.5f);
-    const float jy = AE_SUB(rng_next(seed), 0.5f);
-    const f3 tgt = F.pixel0 + AE_ADD(AE_U2F(x), jx) * F.pixel_u + AE_ADD(AE_U2F(y), jy) * F.pixel_v;
-    o = F.source;
-    if (F.defocus_angle > 0.0f) {
-        float px, py;
-        for (;;) {
-            const float a = rng_next(seed), b = rng_next(seed);
-            px = AE_SUB(AE_MUL(a, 2.0f), 1.0f);
-            py = AE_SUB(AE_MUL(b, 2.0f), 1.0f);
-            if (length(mk(px, py, 0.0f)) < 1.0f) break;
-        }
-        o = F.source + px * F.defocus_u + py * F.defocus_v;
-    }
-    d = normalize(tgt - o);
-    time = rng_next(seed);
-}
 
 __global__ void k_camera_rays(FrameParams F, ae_ray *__restrict__ out) {
     const uint32_t x = blockIdx.x * 16 + (threadIdx.x & 15);
@@ -42,43 +21,6 @@ __global__ void k_camera_rays(FrameParams F, ae_ray *__restrict__ out) {
     float4 *p = reinterpret_cast<float4 *>(out + size_t(y) * F.width + x);
     p[0] = make_float4(o.x, o.y, o.z, 0.001f);
     p[1] = make_float4(d.x, d.y, d.z, time);
-}
-
-// World shading normal and facing of a mesh hit, recomputed from the hit
-// record exactly as HitMesh finishes (hybrid:655-706).
-AE_DEV bool hit_normal(const DevScene &S, const ae_hit &h, f3 d, f3 &n) {
-    if (h.object == AE_MISS) return false;
-    const ae_object *obj = S.objects + h.object;
-    const ObjHead hd = load_head(obj);
-    if (hd.shape != AE_SHAPE_MESH) {
-        // Planar objects: the unit plane normal facing the ray.
-        const char *b = reinterpret_cast<const char *>(obj);
-        const float4 q2 = ld4(b + 32), q3 = ld4(b + 48);
-        const f3 nn = cross(mk(q2.x, q2.y, q2.z), mk(q3.x, q3.y, q3.z));
-        n = nn / AE_SQRT(dot(nn, nn));
-        if (!(dot(d, n) < 0.0f)) n = -n;
-        return hd.shape == AE_SHAPE_QUAD || hd.shape == AE_SHAPE_TRIANGLE;
-    }
-    const uint32_t ii = __float_as_uint(ld4(reinterpret_cast<const char *>(obj) + 80).z);
-    const float4 *ip = reinterpret_cast<const float4 *>(S.instances + ii);
-    const float4 i1 = __ldg(ip + 1), i2 = __ldg(ip + 2);
-    const uint32_t vbase = __float_as_uint(i2.x), ibase = __float_as_uint(i2.y);
-    const uint32_t base = ibase + h.prim * 3u;
-    const ae_vertex *A = S.vertices + vbase + __ldg(S.indices + base);
-    const ae_vertex *B = S.vertices + vbase + __ldg(S.indices + base + 1);
-    const ae_vertex *C = S.vertices + vbase + __ldg(S.indices + base + 2);
-    const float4 a0 = ld4(A), b0 = ld4(B), c0 = ld4(C);
-    const float4 a1 = ld4(reinterpret_cast<const char *>(A) + 16), b1 = ld4(reinterpret_cast<const char *>(B) + 16),
-                 c1 = ld4(reinterpret_cast<const char *>(C) + 16);
-    const float w0 = AE_SUB(AE_SUB(1.0f, h.alpha), h.beta);
-    const f3 sh = normalize(w0 * mk(a0.w, a1.x, a1.y) + h.alpha * mk(b0.w, b1.x, b1.y) + h.beta * mk(c0.w, c1.x, c1.y));
-    const f3 p0 = mk(a0.x, a0.y, a0.z);
-    const f3 gn = cross(mk(b0.x, b0.y, b0.z) - p0, mk(c0.x, c0.y, c0.z) - p0);
-    f3 geo = gn / AE_SQRT(dot(gn, gn));
-    if (dot(geo, sh) < 0.0f) geo = -geo;
-    n = normalize(quat_rotate(i1.x, i1.y, i1.z, i1.w, sh));
-    if (!(dot(d, quat_rotate(i1.x, i1.y, i1.z, i1.w, geo)) < 0.0f)) n = -n;
-    return true;
 }
 
 __global__ void k_bounce_rays(DevScene S, FrameParams F, const ae_ray *__restrict__ prim, const ae_hit *__restrict__ hits,

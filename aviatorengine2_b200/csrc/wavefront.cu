@@ -1,0 +1,688 @@
+// wavefront.cu - the compute-only path tracer (ColorRay, hybrid:1230-1325)
+// restructured into persistent stages over compacted queues, so every stage
+// runs coherent work at full occupancy instead of one divergent megakernel:
+//
+//   generate  camera rays (main, hybrid:1346-1373) into the ray queue
+//   extend    closest hit of every queued ray (the optimised 4-wide walk);
+//             each CTA stages a tile of the ray queue in shared memory with a
+//             bulk asynchronous copy (cp.async.bulk, completion on an
+//             mbarrier with a bounded wait)
+//   shade     miss / emission / NEE light sampling / bounce / Russian
+//             roulette; surviving paths are appended to the next ray queue
+//             and shadow rays to the shadow queue with warp-aggregated
+//             atomics (ballot + prefix over the warp)
+//   shadow    the reference's shadow test: up to four closest hits stepping
+//             through glass (hybrid:1167-1191)
+//   connect   NEE sums in light order, the luma clamp of 8, added to the path
+//   finish    samples into the frame, the running accumulation and display
+//
+// RNG draws happen in shade in the reference's order (two per quad light,
+// then the bounce, then roulette), and every arithmetic step is the plain
+// megakernel's, so a wavefront frame equals the plain frame bit for bit.
+//
+// One frame is captured into a CUDA graph (all stage launches for Depth
+// bounces, queue counts read on the device), replayed per frame with only the
+// frame parameters copied in.  The extend stage's block size, queue tile and
+// shared-memory stack depth come from an autotuner that times the candidates
+// on the scene's own first-bounce queue.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "context.h"
+#include "fast.h"
+#include "fast_trace.cuh"
+#include "kernels.h"
+#include "shade.cuh"
+#include "trace_common.cuh"
+
+namespace ae {
+
+constexpr int kMaxLights = 64;  // NEE entries per path vertex
+
+struct WfParams {
+    FrameParams F;
+    uint32_t n_paths, sample, spp, n_lights;
+};
+
+// Device counters: [0],[1] ray queue sizes (ping-pong), [2] shadow queue,
+// [3] error flags, [4..4+kMaxBounce) extend tile counters, then shadow tiles.
+constexpr int kMaxBounce = 64;
+enum { C_Q0 = 0, C_Q1 = 1, C_SH = 2, C_ERR = 3, C_TILE = 4, C_SHTILE = 4 + kMaxBounce, C_COUNT = 4 + 2 * kMaxBounce };
+
+struct WfView {
+    ae_ray *qray[2];
+    uint32_t *qpid[2];
+    ae_hit *qhit;
+    float4 *thr, *acc, *col, *pend;
+    uint32_t *seed;
+    uint8_t *nee;
+    // shadow entries, slot = path * n_lights + light
+    float4 *sh_o, *sh_d, *sh_lp, *sh_c;  // origin+tnear, dir+time, light point, contribution
+    uint8_t *sh_valid, *sh_occ;
+    uint32_t *sq;
+    uint32_t *cnt;
+    const WfParams *P;
+    float4 *accum, *frame;
+    uchar4 *display;
+};
+
+struct Wavefront {
+    uint32_t cap = 0, n_lights = 0;
+    DevBuf<ae_ray> qray[2];
+    DevBuf<uint32_t> qpid[2];
+    DevBuf<ae_hit> qhit;
+    DevBuf<float4> thr, acc, col, pend;
+    DevBuf<uint32_t> seed;
+    DevBuf<uint8_t> nee;
+    DevBuf<float4> sh_o, sh_d, sh_lp, sh_c;
+    DevBuf<uint8_t> sh_valid, sh_occ;
+    DevBuf<uint32_t> sq;
+    DevBuf<uint32_t> cnt;
+    DevBuf<WfParams> params;
+    WfParams *host_params = nullptr;  // pinned
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_key = ~0ull;
+    int sms = 148;
+    // autotuned extend configuration
+    int ext_threads = 128, ext_stack = 24;
+    bool tuned = false;
+    float tune_ms[9] = {0};
+    ~Wavefront() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (host_params) cudaFreeHost(host_params);
+    }
+};
+
+void destroy_wavefront(Ctx *c) {
+    delete c->wave;
+    c->wave = nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// Warp-aggregated queue append: one atomic per warp, lanes get consecutive
+// slots in lane order.
+// ---------------------------------------------------------------------------
+AE_DEV uint32_t warp_append(uint32_t *counter, uint32_t want) {
+    const uint32_t lane = threadIdx.x & 31;
+    const unsigned mask = __activemask();
+    // inclusive prefix of `want` over the active lanes
+    uint32_t incl = want;
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t v = __shfl_up_sync(mask, incl, off);
+        if (lane >= uint32_t(off) && ((mask >> (lane - off)) & 1u)) incl += v;
+    }
+    const int leader = 31 - __clz(mask);  // highest active lane holds the total
+    uint32_t base = 0;
+    if (int(lane) == leader) base = atomicAdd(counter, incl);
+    base = __shfl_sync(mask, base, leader);
+    return base + incl - want;
+}
+
+// ---------------------------------------------------------------------------
+// Bulk-copy staging of a queue tile into shared memory.
+// ---------------------------------------------------------------------------
+AE_DEV uint32_t smem_addr(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+AE_DEV void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+AE_DEV void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+AE_DEV void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+// Waits for `phase` to complete; gives up after `limit` polls and reports it.
+AE_DEV bool mbar_wait(uint64_t *bar, uint32_t phase, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// Stages
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_wf_generate(WfView W) {
+    const WfParams &P = *W.P;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        W.cnt[C_Q0] = P.n_paths;
+        W.cnt[C_Q1] = 0;
+        W.cnt[C_SH] = 0;
+        for (int k = 0; k < 2 * kMaxBounce; k++) W.cnt[C_TILE + k] = 0;
+    }
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P.n_paths; p += gridDim.x * blockDim.x) {
+        const uint32_t x = p % P.F.width, y = p / P.F.width;
+        uint32_t seed;
+        f3 o, d;
+        float time;
+        if (P.sample == 0) {
+            camera_ray(P.F, x, y, o, d, time, seed);
+        } else {
+            // Later samples of the frame continue the pixel's stream (the
+            // samples loop of main, hybrid:1366-1381).
+            seed = W.seed[p];
+            const float jx = AE_SUB(rng_next(seed), 0.5f);
+            const float jy = AE_SUB(rng_next(seed), 0.5f);
+            const f3 tgt = P.F.pixel0 + AE_ADD(AE_U2F(x), jx) * P.F.pixel_u + AE_ADD(AE_U2F(y), jy) * P.F.pixel_v;
+            o = P.F.source;
+            if (P.F.defocus_angle > 0.0f) {
+                float px, py;
+                for (;;) {
+                    const float a = rng_next(seed), b = rng_next(seed);
+                    px = AE_SUB(AE_MUL(a, 2.0f), 1.0f);
+                    py = AE_SUB(AE_MUL(b, 2.0f), 1.0f);
+                    if (length(mk(px, py, 0.0f)) < 1.0f) break;
+                }
+                o = P.F.source + px * P.F.defocus_u + py * P.F.defocus_v;
+            }
+            d = normalize(tgt - o);
+            time = rng_next(seed);
+        }
+        W.seed[p] = seed;
+        ae_ray r;
+        r.ox = o.x; r.oy = o.y; r.oz = o.z; r.tnear = 0.001f;
+        r.dx = d.x; r.dy = d.y; r.dz = d.z; r.time = time;
+        W.qray[0][p] = r;
+        W.qpid[0][p] = p;
+        W.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        W.acc[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (P.sample == 0) W.col[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        W.nee[p] = 0;
+    }
+}
+
+// Extend: persistent CTAs take tiles of the ray queue; one elected thread
+// bulk-copies the tile into shared memory and every thread traces one ray.
+template <int THREADS, int SS>
+__global__ void __launch_bounds__(THREADS) k_wf_extend(DevScene S, FastView V, WfView W, int bounce) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ae_ray *tile = reinterpret_cast<ae_ray *>(smem_raw);
+    uint2 *stk = reinterpret_cast<uint2 *>(smem_raw + THREADS * sizeof(ae_ray));
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tile_index;
+    const int q = bounce & 1;
+    const uint32_t count = W.cnt[q];
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    uint32_t phase = 0;
+    for (;;) {
+        if (threadIdx.x == 0) tile_index = atomicAdd(&W.cnt[C_TILE + bounce], 1u);
+        __syncthreads();
+        const uint32_t start = tile_index * THREADS;
+        if (start >= count) break;
+        const uint32_t m = min(uint32_t(THREADS), count - start);
+        if (threadIdx.x == 0) {
+            mbar_expect_tx(&bar, m * uint32_t(sizeof(ae_ray)));
+            bulk_g2s(tile, W.qray[q] + start, m * uint32_t(sizeof(ae_ray)), &bar);
+        }
+        // Every thread polls the barrier (bounded); the block then agrees on
+        // the outcome so no thread leaves while others wait at a barrier.
+        const bool ok = __syncthreads_and(mbar_wait(&bar, phase, 1u << 24) ? 1 : 0) != 0;
+        if (!ok) {
+            // Give the copy in flight a second bounded chance to land before
+            // the block exits, then report the timeout.
+            mbar_wait(&bar, phase, 1u << 24);
+            if (threadIdx.x == 0) atomicOr(&W.cnt[C_ERR], 1u);
+            break;
+        }
+        phase ^= 1u;
+        if (threadIdx.x < m) {
+            const ae_ray r = tile[threadIdx.x];
+            const Best b = closest_fast<false, SS>(S, V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time,
+                                                   stk, threadIdx.x, THREADS);
+            const bool any = b.object != AE_MISS;
+            ae_hit h;
+            h.t = any ? b.t : 0.0f;
+            h.alpha = any ? b.alpha : 0.0f;
+            h.beta = any ? b.beta : 0.0f;
+            h.object = b.object;
+            h.prim = b.prim;
+            W.qhit[start + threadIdx.x] = h;
+        }
+        __syncthreads();  // the tile buffer is reused by the next copy
+    }
+}
+
+// Shade: one queued path per thread (ColorRay's body after the traversal).
+__global__ void __launch_bounds__(256) k_wf_shade(DevScene S, WfView W, int bounce) {
+    const WfParams &P = *W.P;
+    const int q = bounce & 1;
+    const uint32_t count = W.cnt[q];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t pid = W.qpid[q][k];
+        const ae_ray r = W.qray[q][k];
+        const ae_hit hr = W.qhit[k];
+        const f3 o = mk(r.ox, r.oy, r.oz), d = mk(r.dx, r.dy, r.dz);
+        float4 t4 = W.thr[pid], a4 = W.acc[pid];
+        f3 thr = mk(t4.x, t4.y, t4.z), acc = mk(a4.x, a4.y, a4.z);
+        uint32_t seed = W.seed[pid];
+        bool next = false;
+        ae_ray nr = r;
+        uint32_t n_shadow = 0;
+        DHit h;
+        if (!surface_from_hit(S, hr, o, d, r.time, h)) {
+            acc = acc + thr * P.F.sky;
+        } else {
+            const MatRec m = load_mat(S.objects + h.slot);
+            if (m.type == AE_MAT_DIFFUSE_LIGHT) {
+                acc = acc + thr * (m.emission * m.albedo);
+            } else {
+                if (m.type == AE_MAT_LAMBERTIAN) {
+                    // Light samples in light order (CalculateDirectLight,
+                    // hybrid:1122-1212); occlusion is resolved by the shadow stage.
+                    W.nee[pid] = 1;
+                    W.pend[pid] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+                    for (uint32_t i = 0; i < P.n_lights; i++) {
+                        const size_t e = size_t(pid) * P.n_lights + i;
+                        const ae_object *L = S.objects + __ldg(S.lights + i);
+                        const ObjHead lh = load_head(L);
+                        f3 lp;
+                        float omega;
+                        sample_light(L, lh.shape, h.p, lp, omega, seed);
+                        uint8_t valid = 0;
+                        if (omega > 0.0f) {
+                            f3 sd = lp - h.p;
+                            const float dist = length(sd);
+                            if (dist > 1e-6f) {
+                                sd = sd / dist;
+                                const float ct = dot(h.n, sd);
+                                if (ct > 0.0f) {
+                                    const MatRec lm = load_mat(L);
+                                    const f3 rad = lm.emission * lm.albedo;
+                                    const f3 c = m.albedo * rad * ct * omega;
+                                    const f3 so = h.p + h.n * 0.001f;
+                                    W.sh_o[e] = make_float4(so.x, so.y, so.z, 0.001f);
+                                    W.sh_d[e] = make_float4(sd.x, sd.y, sd.z, r.time);
+                                    W.sh_lp[e] = make_float4(lp.x, lp.y, lp.z, 0.0f);
+                                    W.sh_c[e] = make_float4(c.x, c.y, c.z, 0.0f);
+                                    valid = 1;
+                                    n_shadow++;
+                                }
+                            }
+                        }
+                        W.sh_valid[e] = valid;
+                        W.sh_occ[e] = 0;
+                    }
+                }
+                f3 sd;
+                if (get_bounce(d, h, m, sd, seed)) {
+                    const f3 nd = normalize(sd);
+                    const float sgn = dot(nd, h.n) < 0.0f ? -1.0f : 1.0f;
+                    const f3 no = h.p + h.n * AE_MUL(0.001f, sgn);
+                    if (m.type != AE_MAT_DIELECTRIC) thr = thr * m.albedo;
+                    bool alive = true;
+                    if (bounce > 0) {
+                        const float p = clampf(maxc(thr), 0.1f, 1.0f);
+                        if (rng_next(seed) > p) alive = false;
+                        else thr = thr / p;
+                    }
+                    if (alive && uint32_t(bounce + 1) < P.F.depth) {
+                        next = true;
+                        nr.ox = no.x; nr.oy = no.y; nr.oz = no.z; nr.tnear = 0.001f;
+                        nr.dx = nd.x; nr.dy = nd.y; nr.dz = nd.z;
+                    }
+                }
+            }
+        }
+        W.thr[pid] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+        W.acc[pid] = make_float4(acc.x, acc.y, acc.z, 0.0f);
+        W.seed[pid] = seed;
+        // Compaction into the next ray queue and the shadow queue.
+        const uint32_t slot = warp_append(&W.cnt[q ^ 1], next ? 1u : 0u);
+        if (next) {
+            W.qray[q ^ 1][slot] = nr;
+            W.qpid[q ^ 1][slot] = pid;
+        }
+        const uint32_t sbase = warp_append(&W.cnt[C_SH], n_shadow);
+        if (n_shadow) {
+            uint32_t j = 0;
+            for (uint32_t i = 0; i < P.n_lights; i++) {
+                const uint32_t e = pid * P.n_lights + i;
+                if (W.sh_valid[e]) W.sq[sbase + j++] = e;
+            }
+        }
+    }
+}
+
+// Shadow: the reference's occlusion loop per entry.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_wf_shadow(DevScene S, FastView V, WfView W) {
+    extern __shared__ uint2 stk[];
+    const uint32_t count = W.cnt[C_SH];
+    for (uint32_t k = blockIdx.x * THREADS + threadIdx.x; k < count; k += gridDim.x * THREADS) {
+        const uint32_t e = W.sq[k];
+        const float4 o4 = W.sh_o[e], d4 = W.sh_d[e], l4 = W.sh_lp[e];
+        f3 so = mk(o4.x, o4.y, o4.z);
+        const f3 sd = mk(d4.x, d4.y, d4.z), lp = mk(l4.x, l4.y, l4.z);
+        bool occluded = false;
+        for (int step = 0; step < 4; step++) {
+            const Best b = closest_fast<false>(S, V, so, sd, 0.001f, d4.w, stk, threadIdx.x, THREADS);
+            if (b.object == AE_MISS) break;
+            if (b.t >= AE_SUB(distance(lp, so), 0.001f)) break;
+            const uint32_t mt = load_head(S.objects + b.object).material;
+            if (mt == AE_MAT_DIFFUSE_LIGHT) break;
+            if (mt != AE_MAT_DIELECTRIC) { occluded = true; break; }
+            so = (so + sd * b.t) + sd * 0.001f;
+        }
+        W.sh_occ[e] = occluded ? 1 : 0;
+    }
+}
+
+// Connect: NEE in light order, clamped, onto the path radiance.
+__global__ void __launch_bounds__(256) k_wf_connect(WfView W, int bounce) {
+    const WfParams &P = *W.P;
+    const int q = bounce & 1;
+    const uint32_t count = W.cnt[q];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t pid = W.qpid[q][k];
+        if (!W.nee[pid]) continue;
+        W.nee[pid] = 0;
+        f3 dl = splat(0.0f);
+        for (uint32_t i = 0; i < P.n_lights; i++) {
+            const size_t e = size_t(pid) * P.n_lights + i;
+            if (W.sh_valid[e] && !W.sh_occ[e]) {
+                const float4 c = W.sh_c[e];
+                dl = dl + mk(c.x, c.y, c.z);
+            }
+        }
+        const float luma = maxc(dl);
+        if (luma > 8.0f) dl = dl * AE_DIV(8.0f, luma);
+        const float4 t4 = W.pend[pid], a4 = W.acc[pid];
+        const f3 acc = mk(a4.x, a4.y, a4.z) + mk(t4.x, t4.y, t4.z) * dl;
+        W.acc[pid] = make_float4(acc.x, acc.y, acc.z, 0.0f);
+    }
+}
+
+// The shadow queue of a bounce starts empty; the next ray queue too.
+__global__ void k_wf_reset(WfView W, int bounce) {
+    W.cnt[(bounce & 1) ^ 1] = 0;
+    W.cnt[C_SH] = 0;
+}
+
+// Finish: this sample's path radiance into the pixel's sum; at the last
+// sample, the frame colour, the running accumulation and the display
+// (hybrid:1383-1403).
+__global__ void __launch_bounds__(256) k_wf_finish(WfView W) {
+    const WfParams &P = *W.P;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P.n_paths; p += gridDim.x * blockDim.x) {
+        const float4 a = W.acc[p], c0 = W.col[p];
+        const f3 col = mk(c0.x, c0.y, c0.z) + mk(a.x, a.y, a.z);
+        W.col[p] = make_float4(col.x, col.y, col.z, 0.0f);
+        if (P.sample + 1 < P.spp) continue;
+        const f3 color = col / AE_U2F(P.spp);
+        if (W.frame) W.frame[p] = make_float4(color.x, color.y, color.z, 1.0f);
+        f3 accum;
+        if (P.F.batch == 0) {
+            accum = color;
+        } else {
+            const float4 prev = W.accum[p];
+            accum = lerp(mk(prev.x, prev.y, prev.z), color, AE_DIV(1.0f, AE_U2F(P.F.batch + 1)));
+        }
+        W.accum[p] = make_float4(accum.x, accum.y, accum.z, 1.0f);
+        W.display[p] = display_texel(accum, P.F.exposure);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host
+// ---------------------------------------------------------------------------
+typedef void (*ExtendFn)(DevScene, FastView, WfView, int);
+struct ExtendCfg {
+    int threads, stack;
+    ExtendFn fn;
+};
+static const ExtendCfg kExtendCfgs[9] = {
+    {64, 16, k_wf_extend<64, 16>},   {64, 24, k_wf_extend<64, 24>},   {64, 32, k_wf_extend<64, 32>},
+    {128, 16, k_wf_extend<128, 16>}, {128, 24, k_wf_extend<128, 24>}, {128, 32, k_wf_extend<128, 32>},
+    {256, 16, k_wf_extend<256, 16>}, {256, 24, k_wf_extend<256, 24>}, {256, 32, k_wf_extend<256, 32>},
+};
+
+static size_t extend_smem(int threads, int stack) {
+    return size_t(threads) * sizeof(ae_ray) + size_t(threads) * stack * sizeof(uint2);
+}
+
+static int extend_grid(Ctx *c, const ExtendCfg &e) {
+    int per_sm = 0;
+    cudaFuncSetAttribute(reinterpret_cast<const void *>(e.fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(extend_smem(e.threads, e.stack)));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void *>(e.fn), e.threads,
+                                                  extend_smem(e.threads, e.stack));
+    return std::max(1, per_sm) * c->wave->sms;
+}
+
+static WfView view_of(Ctx *c) {
+    Wavefront &Wf = *c->wave;
+    WfView W;
+    for (int k = 0; k < 2; k++) { W.qray[k] = Wf.qray[k].ptr; W.qpid[k] = Wf.qpid[k].ptr; }
+    W.qhit = Wf.qhit.ptr;
+    W.thr = Wf.thr.ptr; W.acc = Wf.acc.ptr; W.col = Wf.col.ptr; W.pend = Wf.pend.ptr;
+    W.seed = Wf.seed.ptr;
+    W.nee = Wf.nee.ptr;
+    W.sh_o = Wf.sh_o.ptr; W.sh_d = Wf.sh_d.ptr; W.sh_lp = Wf.sh_lp.ptr; W.sh_c = Wf.sh_c.ptr;
+    W.sh_valid = Wf.sh_valid.ptr; W.sh_occ = Wf.sh_occ.ptr;
+    W.sq = Wf.sq.ptr;
+    W.cnt = Wf.cnt.ptr;
+    W.P = Wf.params.ptr;
+    W.accum = c->accum.ptr;
+    W.frame = c->frame.ptr;
+    W.display = c->display.ptr;
+    return W;
+}
+
+static int ensure_wavefront(Ctx *c) {
+    int rc = prepare_fast(c);
+    if (rc) return rc;
+    if (!c->wave) c->wave = new (std::nothrow) Wavefront();
+    if (!c->wave) return c->fail(AE_ERR_OOM, "wavefront state");
+    Wavefront &Wf = *c->wave;
+    const uint32_t n = c->settings.width * c->settings.height;
+    const uint32_t nl = c->n_lights;
+    if (nl > uint32_t(kMaxLights)) return c->fail(AE_ERR_LAYOUT, "wavefront NEE supports at most %d lights", kMaxLights);
+    if (c->config.depth > uint32_t(kMaxBounce)) return c->fail(AE_ERR_INVALID, "depth above %d", kMaxBounce);
+    if (Wf.cap < n || Wf.n_lights < std::max(nl, 1u)) {
+        const size_t ne = size_t(n) * std::max(nl, 1u);
+        if (Wf.qray[0].reserve(n) || Wf.qray[1].reserve(n) || Wf.qpid[0].reserve(n) || Wf.qpid[1].reserve(n) ||
+            Wf.qhit.reserve(n) || Wf.thr.reserve(n) || Wf.acc.reserve(n) || Wf.col.reserve(n) || Wf.pend.reserve(n) ||
+            Wf.seed.reserve(n) || Wf.nee.reserve(n) || Wf.sh_o.reserve(ne) || Wf.sh_d.reserve(ne) ||
+            Wf.sh_lp.reserve(ne) || Wf.sh_c.reserve(ne) || Wf.sh_valid.reserve(ne) || Wf.sh_occ.reserve(ne) ||
+            Wf.sq.reserve(ne) || Wf.cnt.reserve(C_COUNT) || Wf.params.reserve(1))
+            return c->fail(AE_ERR_OOM, "wavefront queues (%u paths x %u lights)", n, nl);
+        Wf.cap = n;
+        Wf.n_lights = std::max(nl, 1u);
+        if (Wf.graph) { cudaGraphExecDestroy(Wf.graph); Wf.graph = nullptr; }
+        cudaMemsetAsync(Wf.cnt.ptr, 0, C_COUNT * sizeof(uint32_t), c->stream);
+    }
+    if (!Wf.host_params) {
+        if (cudaMallocHost(&Wf.host_params, sizeof(WfParams)) != cudaSuccess)
+            return c->fail(AE_ERR_OOM, "pinned frame parameters");
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&Wf.sms, cudaDevAttrMultiProcessorCount, dev);
+    return AE_OK;
+}
+
+// Records one sample's stages onto `st` (graph capture or direct).
+struct Grids {
+    int grid256, egrid, shgrid;
+    size_t esmem, shsmem;
+};
+
+// Launch shapes, fixed before capture (no attribute or occupancy query runs
+// while a stream is being captured).
+static Grids grids_for(Ctx *c, int cfg_index) {
+    Wavefront &Wf = *c->wave;
+    Grids g;
+    g.grid256 = Wf.sms * 8;
+    const ExtendCfg &e = kExtendCfgs[cfg_index];
+    g.egrid = extend_grid(c, e);
+    g.esmem = extend_smem(e.threads, e.stack);
+    g.shsmem = size_t(kSharedStack) * 128 * sizeof(uint2);
+    cudaFuncSetAttribute(reinterpret_cast<const void *>(k_wf_shadow<128>), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(g.shsmem));
+    int sh_per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh_per_sm, reinterpret_cast<const void *>(k_wf_shadow<128>), 128,
+                                                  g.shsmem);
+    g.shgrid = std::max(1, sh_per_sm) * Wf.sms;
+    return g;
+}
+
+static int record_sample(Ctx *c, cudaStream_t st, int cfg_index, const Grids &G) {
+    const WfView W = view_of(c);
+    const DevScene S = c->scene();
+    FastScene &F = *c->fast;
+    const FastView V{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr};
+    const ExtendCfg &e = kExtendCfgs[cfg_index];
+    const int grid256 = G.grid256, egrid = G.egrid, shgrid = G.shgrid;
+    const size_t esmem = G.esmem, shsmem = G.shsmem;
+    k_wf_generate<<<grid256, 256, 0, st>>>(W);
+    for (uint32_t b = 0; b < c->config.depth; b++) {
+        k_wf_reset<<<1, 1, 0, st>>>(W, int(b));
+        e.fn<<<egrid, e.threads, esmem, st>>>(S, V, W, int(b));
+        k_wf_shade<<<grid256, 256, 0, st>>>(S, W, int(b));
+        k_wf_shadow<128><<<shgrid, 128, shsmem, st>>>(S, V, W);
+        k_wf_connect<<<grid256, 256, 0, st>>>(W, int(b));
+    }
+    k_wf_finish<<<grid256, 256, 0, st>>>(W);
+    return c->cuda(cudaGetLastError(), "wavefront launch");
+}
+
+static uint64_t launches_per_sample(const Ctx *c) { return 2 + 5ull * c->config.depth; }
+
+// Times every extend configuration on this scene's first bounce and keeps
+// the fastest.
+static int autotune(Ctx *c) {
+    Wavefront &Wf = *c->wave;
+    const WfView W = view_of(c);
+    const DevScene S = c->scene();
+    FastScene &F = *c->fast;
+    const FastView V{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr};
+    int best = 4;
+    float best_ms = 1e30f;
+    for (int k = 0; k < 9; k++) {
+        const ExtendCfg &e = kExtendCfgs[k];
+        const int egrid = extend_grid(c, e);
+        float total = 0.0f;
+        for (int rep = 0; rep < 2; rep++) {
+            k_wf_generate<<<Wf.sms * 8, 256, 0, c->stream>>>(W);
+            k_wf_reset<<<1, 1, 0, c->stream>>>(W, 0);
+            cudaEventRecord(c->ev0, c->stream);
+            e.fn<<<egrid, e.threads, extend_smem(e.threads, e.stack), c->stream>>>(S, V, W, 0);
+            cudaEventRecord(c->ev1, c->stream);
+            int rc = c->cuda(cudaEventSynchronize(c->ev1), "autotune");
+            if (rc) return rc;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+            if (rep == 1) total = ms;
+            c->launches += 3;
+        }
+        Wf.tune_ms[k] = total;
+        if (total < best_ms) { best_ms = total; best = k; }
+    }
+    Wf.ext_threads = kExtendCfgs[best].threads;
+    Wf.ext_stack = kExtendCfgs[best].stack;
+    Wf.tuned = true;
+    return c->cuda(cudaGetLastError(), "autotune");
+}
+
+static int best_cfg_index(const Wavefront &Wf) {
+    for (int k = 0; k < 9; k++)
+        if (kExtendCfgs[k].threads == Wf.ext_threads && kExtendCfgs[k].stack == Wf.ext_stack) return k;
+    return 4;
+}
+
+int render_wavefront(Ctx *c) {
+    int rc = ensure_wavefront(c);
+    if (rc) return rc;
+    Wavefront &Wf = *c->wave;
+    WfParams hp;
+    std::memset(&hp, 0, sizeof(hp));
+    hp.F = make_frame_params(c->config);
+    hp.n_paths = c->settings.width * c->settings.height;
+    hp.spp = hp.F.spp;
+    hp.n_lights = c->n_lights;
+    if (hp.F.display_only) {
+        // Re-grade only: the compute-only kernel's display-only branch.
+        if ((rc = c->timed_begin())) return rc;
+        if ((rc = c->cuda(launch_render_plain(c->scene(), hp.F, c->accum.ptr, c->display.ptr, c->frame.ptr, c->stream),
+                          "display only")))
+            return rc;
+        return c->timed_end();
+    }
+    if (!Wf.tuned) {
+        *Wf.host_params = hp;
+        if ((rc = c->cuda(cudaMemcpyAsync(Wf.params.ptr, Wf.host_params, sizeof(WfParams), cudaMemcpyHostToDevice,
+                                          c->stream), "params")))
+            return rc;
+        if ((rc = autotune(c))) return rc;
+    }
+    // One graph per (scene upload, frame shape); frame parameters travel
+    // through device memory so the graph is replayed unchanged.
+    const uint64_t key = (c->scene_version << 20) ^ (uint64_t(c->config.depth) << 8) ^ hp.n_lights;
+    if (!Wf.graph || Wf.graph_key != key) {
+        if (Wf.graph) { cudaGraphExecDestroy(Wf.graph); Wf.graph = nullptr; }
+        cudaGraph_t g;
+        const int ci = best_cfg_index(Wf);
+        const Grids G = grids_for(c, ci);
+        if ((rc = c->cuda(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "capture"))) return rc;
+        rc = record_sample(c, c->stream, ci, G);
+        cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+        if (rc) return rc;
+        if ((rc = c->cuda(ce, "end capture"))) return rc;
+        ce = cudaGraphInstantiate(&Wf.graph, g, 0);
+        cudaGraphDestroy(g);
+        if ((rc = c->cuda(ce, "graph instantiate"))) return rc;
+        Wf.graph_key = key;
+    }
+    if ((rc = c->timed_begin())) return rc;
+    for (uint32_t s = 0; s < hp.spp; s++) {
+        hp.sample = s;
+        // The pinned block is rewritten only after the previous copy finished.
+        if ((rc = c->cuda(cudaStreamSynchronize(c->stream), "params"))) return rc;
+        *Wf.host_params = hp;
+        if ((rc = c->cuda(cudaMemcpyAsync(Wf.params.ptr, Wf.host_params, sizeof(WfParams), cudaMemcpyHostToDevice,
+                                          c->stream), "params")))
+            return rc;
+        if ((rc = c->cuda(cudaGraphLaunch(Wf.graph, c->stream), "graph launch"))) return rc;
+        c->launches += launches_per_sample(c);
+    }
+    c->launches--;  // timed_end counts one
+    if ((rc = c->timed_end())) return rc;
+    return AE_OK;
+}
+
+}  // namespace ae
+
+using namespace ae;
+
+// Wavefront statistics: the autotuned extend configuration and the error flag.
+extern "C" int ae_wavefront_info(ae_ctx *ctx, int32_t *threads, int32_t *stack, float *tune_ms9, uint32_t *errors) {
+    Ctx *c = reinterpret_cast<Ctx *>(ctx);
+    if (!c) return AE_ERR_INVALID;
+    if (!c->wave) return c->fail(AE_ERR_STATE, "no wavefront frame yet");
+    if (threads) *threads = c->wave->ext_threads;
+    if (stack) *stack = c->wave->ext_stack;
+    if (tune_ms9) std::memcpy(tune_ms9, c->wave->tune_ms, sizeof(c->wave->tune_ms));
+    if (errors) {
+        uint32_t e = 0;
+        int rc = c->cuda(cudaMemcpyAsync(&e, c->wave->cnt.ptr + C_ERR, 4, cudaMemcpyDeviceToHost, c->stream), "copy");
+        if (!rc) rc = c->cuda(cudaStreamSynchronize(c->stream), "sync");
+        if (rc) return rc;
+        *errors = e;
+    }
+    return AE_OK;
+}

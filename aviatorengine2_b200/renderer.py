@@ -156,6 +156,12 @@ class Context:
         self._chk(lib().ae_bounce_rays(self._h, ptr(p), ptr(h), len(p), ptr(out), ptr(valid)))
         return out, valid.astype(bool)
 
+    def wavefront_info(self):
+        th, st, err = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_uint32()
+        ms = np.zeros(9, np.float32)
+        self._chk(lib().ae_wavefront_info(self._h, ctypes.byref(th), ctypes.byref(st), ptr(ms), ctypes.byref(err)))
+        return {"threads": th.value, "stack": st.value, "tune_ms": ms.tolist(), "errors": err.value}
+
     def prepare_fast(self):
         self._chk(lib().ae_prepare_fast(self._h))
 

@@ -14,6 +14,13 @@ Workloads (all inputs seeded; no dataset is involved):
                    heightfields of 512x512 vertices, icospheres at levels
                    7, 6, 6, 5, 5), 2,099,206 unique triangles; random rotation,
                    uniform scale in [0.5, 2], translation in a 100^3 box.
+  wavefront_scene  1024 instances of 32 meshes (heightfields and icospheres
+                   from the generators above), about 10M unique triangles;
+                   materials per mesh 60% Lambertian, 25% metal (fuzz =
+                   roughness in [0.05, 0.6]), 15% dielectric (IOR 1.5); 16
+                   emissive quads above the field.
+  hybrid_box       the Cornell box plus analytic spheres and boxes, for the
+                   hybrid renderer's raster/analytic split.
 """
 import ctypes
 
@@ -364,3 +371,44 @@ def hybrid_box(seed=3, width=160, height=120, depth=4):
                        albedo=(0.7, 0.7, 0.2), mesh=h))
     cfg = s.config.copy()
     return _finish(ents, meshes, cfg, "hybrid_box")
+
+
+def wavefront_scene(seed=4, width=1920, height=1080, depth=12, n_meshes=32, n_instances=1024, n_lights=16,
+                    target_tris=10_000_000):
+    """The wavefront workload: meshes drawn from the heightfield and icosphere
+    generators until about `target_tris` unique triangles, instanced 1024
+    times, lit by 16 emissive quads."""
+    rng = np.random.default_rng(seed)
+    meshes = MeshLibrary()
+    handles, kinds = [], []
+    budget = target_tris
+    for k in range(n_meshes):
+        remaining = n_meshes - k
+        want = budget / remaining
+        if k % 2 == 0:
+            n = int(max(16, min(1024, round((want / 2) ** 0.5 + 1))))
+            v, i = heightfield(n, 20.0, 2.5, rng)
+        else:
+            lv = int(max(2, min(8, round(np.log(max(want, 80) / 20) / np.log(4)))))
+            v, i = icosphere(lv, 5.0)
+        budget -= len(i) // 3
+        handles.append(meshes.add(v, i))
+        r = rng.random()
+        kinds.append(_lib.MAT_LAMBERTIAN if r < 0.6 else (_lib.MAT_METAL if r < 0.85 else _lib.MAT_DIELECTRIC))
+    mat = []
+    for k in range(n_meshes):
+        mat.append(dict(albedo=tuple(float(x) for x in rng.uniform(0.2, 0.8, 3)),
+                        fuzz=float(rng.uniform(0.05, 0.6)), ior=1.5))
+    ents = []
+    for q in range(n_lights):
+        x, z = (q % 4) * 50.0 + 5.0, (q // 4) * 50.0 + 5.0
+        ents.append(entity(_lib.SHAPE_QUAD, _lib.MAT_DIFFUSE_LIGHT, (x, 120.0, z), emission=15.0,
+                           u=(15.0, 0.0, 0.0), v=(0.0, 0.0, 15.0)))
+    for k in range(n_instances):
+        m = k % n_meshes
+        pos = (float(rng.uniform(0, 200)), float(rng.uniform(0, 60)), float(rng.uniform(0, 200)))
+        ents.append(entity(_lib.SHAPE_MESH, kinds[m], pos, rotation=random_quat(rng),
+                           scale=float(rng.uniform(0.5, 2.0)), mesh=handles[m], **mat[m]))
+    cfg = make_config(width, height, (100.0, 90.0, 330.0), (100.0, 30.0, 100.0), fov=40.0, depth=depth,
+                      sky=(0.0, 0.0, 0.0))
+    return _finish(ents, meshes, cfg, "wavefront_scene")

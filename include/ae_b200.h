@@ -385,6 +385,12 @@ int ae_bounce_rays(ae_ctx *ctx, const ae_ray *primary, const ae_hit *hits, uint3
  * 48, 128, 48, 48, 48 and 60 bytes per touch respectively. */
 int ae_trace_counters(ae_ctx *ctx, const ae_ray *d_rays, uint32_t n, uint64_t *counters);
 
+/* Wavefront path tracer state after an AE_MODE_WAVEFRONT frame: the extend
+ * stage's autotuned block size and shared-memory stack depth, the nine
+ * candidate timings in milliseconds (threads 64/128/256 x stack 16/24/32),
+ * and the device error flags (non-zero: a bounded wait gave up). */
+int ae_wavefront_info(ae_ctx *ctx, int32_t *threads, int32_t *stack, float *tune_ms9, uint32_t *errors);
+
 /* Synchronise the context's stream.  Returns AE_ERR_CUDA on a sticky error. */
 int ae_synchronize(ae_ctx *ctx);
 /* Device time in milliseconds of the last kernel launch that the context
