@@ -111,6 +111,7 @@ SIGNATURES = {
     "ae_launch_count": (ctypes.c_uint64, [_P]),
     "ae_prepare_fast": (_I, [_P]),
     "ae_refit_instances": (_I, [_P, _P, _U32]),
+    "ae_download_scene": (_I, [_P, _P, _P, _P]),
     "ae_build_wide_bvh": (_I, [_P, _U32, _U32, _P, _U32, _P, _P, _P]),
 }
 

@@ -302,6 +302,7 @@ int ae_upload_scene(ae_ctx *ctx, const ae_object *objects, uint32_t n_objects, c
     c->host_lights.assign(light_ids, light_ids + n_lights);
     c->scene_uploaded = true;
     c->scene_version++;
+    c->scene_version_layout++;
     c->config.num_spheres = n_objects;
     c->config.num_lights = n_lights;
     return c->cuda(cudaStreamSynchronize(c->stream), "upload scene");

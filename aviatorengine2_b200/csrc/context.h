@@ -43,6 +43,7 @@ template <class T> struct DevBuf {
 struct FastScene;   // derived structures of the optimised closest-hit kernels
 struct Wavefront;   // queues of the wavefront path tracer
 struct Deferred;    // G-buffer and history of the deferred resolve
+struct Refit;       // bottom-up TLAS refit state
 
 struct Ctx {
     ae_settings settings{};
@@ -78,7 +79,9 @@ struct Ctx {
     std::vector<ae_instance> host_instances;
     std::vector<uint32_t> host_lights;
     bool scene_uploaded = false;
-    uint64_t scene_version = 0;
+    uint64_t scene_version = 0;         // bumps on every change of scene content
+    uint64_t scene_version_layout = 0;  // bumps when arrays are re-uploaded (topology may change)
+    DevBuf<float> obj_box;              // world box per object (refit)
 
     // Images.
     DevBuf<float4> accum, frame;
@@ -94,6 +97,7 @@ struct Ctx {
     uint64_t fast_version = 0;
     Wavefront *wave = nullptr;
     Deferred *deferred = nullptr;
+    Refit *refit = nullptr;
 
     ~Ctx();
     int fail(int code, const char *fmt, ...);

@@ -1010,3 +1010,37 @@ extern "C" int ae_build_gbuffer(ae_ctx *ctx) {
     D.have_gbuffer = true;
     return AE_OK;
 }
+
+// Any hit in [tnear, tmax] with deferred.comp's blocking rules (Occluded,
+// deferred:1115-1171): glass and lights never block; meshes take the any-hit
+// walk (OccludedMesh, deferred:812-854).  One thread per ray.
+__global__ void __launch_bounds__(128) k_any_hit(DevScene S, const ae_ray *__restrict__ rays,
+                                                 const float *__restrict__ tmax, uint32_t n, uint8_t *__restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const ae_ray r = rays[i];
+    uint32_t seed = 1u;
+    out[i] = occluded(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.time, r.tnear, tmax[i], seed) ? 1 : 0;
+}
+
+extern "C" int ae_any_hit(ae_ctx *ctx, const ae_ray *rays, const float *tmax, uint32_t n, uint8_t *out) {
+    Ctx *c = reinterpret_cast<Ctx *>(ctx);
+    if (!c) return AE_ERR_INVALID;
+    if (n && (!rays || !tmax || !out)) return c->fail(AE_ERR_INVALID, "null ray, bound or output buffer");
+    if (!c->scene_uploaded) return c->fail(AE_ERR_STATE, "any hit before ae_upload_scene");
+    if (n == 0) return AE_OK;
+    DevBuf<ae_ray> dr;
+    DevBuf<float> dt;
+    DevBuf<uint8_t> dout;
+    if (dr.reserve(n) || dt.reserve(n) || dout.reserve(n)) return c->fail(AE_ERR_OOM, "any-hit buffers");
+    int rc = c->cuda(cudaMemcpyAsync(dr.ptr, rays, size_t(n) * sizeof(ae_ray), cudaMemcpyHostToDevice, c->stream), "copy");
+    if (!rc) rc = c->cuda(cudaMemcpyAsync(dt.ptr, tmax, size_t(n) * sizeof(float), cudaMemcpyHostToDevice, c->stream), "copy");
+    if (rc) return rc;
+    if ((rc = c->timed_begin())) return rc;
+    k_any_hit<<<(n + 127) / 128, 128, 0, c->stream>>>(c->scene(), dr.ptr, dt.ptr, n, dout.ptr);
+    if ((rc = c->cuda(cudaGetLastError(), "any-hit launch"))) return rc;
+    if ((rc = c->timed_end())) return rc;
+    rc = c->cuda(cudaMemcpyAsync(out, dout.ptr, n, cudaMemcpyDeviceToHost, c->stream), "copy");
+    if (!rc) rc = c->cuda(cudaStreamSynchronize(c->stream), "any hit");
+    return rc;
+}

@@ -10,6 +10,7 @@ Ctx::~Ctx() {
     destroy_fast(this);
     destroy_wavefront(this);
     destroy_deferred(this);
+    destroy_refit(this);
     if (side_stream) cudaStreamDestroy(side_stream);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);

@@ -156,6 +156,18 @@ class Context:
         self._chk(lib().ae_bounce_rays(self._h, ptr(p), ptr(h), len(p), ptr(out), ptr(valid)))
         return out, valid.astype(bool)
 
+    def refit_instances(self, instances):
+        ins = np.ascontiguousarray(instances, dtype=_lib.INSTANCE)
+        self._chk(lib().ae_refit_instances(self._h, ptr(ins), len(ins)))
+
+    def download_scene(self):
+        sc = self.scene
+        o = np.zeros(len(sc.objects), _lib.OBJECT)
+        t = np.zeros(len(sc.tlas), _lib.NODE)
+        i = np.zeros(len(sc.instances), _lib.INSTANCE)
+        self._chk(lib().ae_download_scene(self._h, ptr(o), ptr(t), ptr(i)))
+        return o, t, i
+
     def wavefront_info(self):
         th, st, err = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_uint32()
         ms = np.zeros(9, np.float32)

@@ -424,6 +424,11 @@ int ae_build_wide_bvh(const ae_bvh_node *blas, uint32_t n_nodes, uint32_t tri_co
  * when only transforms changed). */
 int ae_refit_instances(ae_ctx *ctx, const ae_instance *instances, uint32_t n);
 
+/* Copies of the device's per-frame arrays as the kernels see them (after any
+ * refit): objects, TLAS nodes, instances, each sized as last uploaded.  Null
+ * pointers are skipped. */
+int ae_download_scene(ae_ctx *ctx, ae_object *objects, ae_bvh_node *tlas, ae_instance *instances);
+
 #ifdef __cplusplus
 } /* extern "C" */
 

@@ -1655,3 +1655,20 @@ extern "C" int oracle_gbuffer(const oracle::Scene *S, const ae_config *c, float 
         }
     return 0;
 }
+
+// Any hit per ray with deferred.comp's rules (Occluded, deferred:1115-1171).
+extern "C" int oracle_any_hit(const oracle::Scene *S, const ae_ray *rays, const float *tmax, uint32_t n, uint8_t *out,
+                              int threads) {
+    using namespace oracle;
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t i = 0; i < int64_t(n); i++) {
+        Ray<float> r;
+        r.o = v3<float>(rays[i].ox, rays[i].oy, rays[i].oz);
+        r.d = v3<float>(rays[i].dx, rays[i].dy, rays[i].dz);
+        r.time = rays[i].time;
+        Rng rng{1u};
+        out[i] = occluded(*S, r, rays[i].tnear, tmax[i], rng) ? 1 : 0;
+    }
+    return 0;
+}

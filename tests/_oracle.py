@@ -279,3 +279,12 @@ def hybrid_frame(scene, config, gb, state, impl="oracle", threads=0):
     if writes:
         state.history = ws
     return state
+
+
+def any_hit(scene, rays, tmax, threads=0):
+    s = oscene(scene)
+    r = np.ascontiguousarray(rays, dtype=_lib.RAY)
+    t = np.ascontiguousarray(tmax, dtype=np.float32)
+    out = np.zeros(len(r), np.uint8)
+    oracle().oracle_any_hit(ctypes.byref(s), ptr(r), ptr(t), ctypes.c_uint32(len(r)), ptr(out), ctypes.c_int(threads))
+    return out

@@ -76,3 +76,25 @@ def test_deferred_without_gbuffer_is_an_error():
         ctx.upload(s)
         with pytest.raises(_lib.AeError):
             ctx.render_frame(_lib.MODE_DEFERRED)
+
+
+def test_any_hit_matches_oracle():
+    """ae_any_hit: the deferred shader's shadow-ray rules (glass and lights do
+    not block) over random segments in the hybrid box."""
+    s = scenes.hybrid_box()
+    rng = np.random.default_rng(21)
+    n = 100000
+    r = np.zeros(n, _lib.RAY)
+    o = rng.uniform(0.1, 9.9, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r["ox"], r["oy"], r["oz"] = o.T
+    r["dx"], r["dy"], r["dz"] = d.T
+    r["tnear"] = 0.001
+    tmax = rng.uniform(0.5, 12.0, n).astype(np.float32)
+    with Context(64, 48) as ctx:
+        ctx.upload(s)
+        got = ctx.any_hit(r, tmax)
+    want = O.any_hit(s, r, tmax)
+    assert np.array_equal(got, want)
+    assert 0.1 < want.mean() < 0.95
