@@ -100,6 +100,7 @@ SIGNATURES = {
     "ae_read_image": (_I, [_P, _I, _P, ctypes.c_size_t]),
     "ae_closest_hit": (_I, [_P, _P, _U32, _P, _I]),
     "ae_closest_hit_device": (_I, [_P, _P, _U32, _P, _I]),
+    "ae_closest_hit_noalloc": (_I, [_P, _P, _U32, _P, _I]),
     "ae_any_hit": (_I, [_P, _P, _P, _U32, _P]),
     "ae_camera_rays": (_I, [_P, _P]),
     "ae_bounce_rays": (_I, [_P, _P, _P, _U32, _P, _P]),

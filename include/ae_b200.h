@@ -362,6 +362,20 @@ int ae_read_image(ae_ctx *ctx, int which, void *dst, size_t dst_bytes);
 int ae_closest_hit(ae_ctx *ctx, const ae_ray *rays, uint32_t n, ae_hit *hits, int variant);
 /* Same with DEVICE pointers, on the context's stream, no synchronisation. */
 int ae_closest_hit_device(ae_ctx *ctx, const ae_ray *d_rays, uint32_t n, ae_hit *d_hits, int variant);
+/* Closest hit for HOST rays with no device allocation: the variant of
+ * ae_closest_hit for callers that cannot let a library call cudaMalloc (a
+ * frame loop that must not stall on the device synchronisation cudaMalloc and
+ * cudaFree imply, or a process whose device memory another allocator already
+ * holds).  It has no counterpart in the reference.  Rays and hits are staged
+ * through one fixed array compiled into the library, AE_NOALLOC_MAX_RAYS rays
+ * (3.25 MiB, held by every GPU that loads the library until exit); larger
+ * batches are refused with AE_ERR_OVERSIZE.  The first call on a device looks
+ * up the array's device address and should come before any stream capture.
+ * All calls on a device share the array: calls that overlap on the GPU race.
+ * FAST/QUANT need ae_prepare_fast (which allocates) to have run first. */
+#define AE_NOALLOC_MAX_RAYS 65536u
+int ae_closest_hit_noalloc(ae_ctx *ctx, const ae_ray *rays, uint32_t n, ae_hit *hits, int variant);
+
 /* Any hit in [tnear, tmax] with the deferred shader's rules (Occluded,
  * deferred:1115-1171: glass and lights do not block).  out[i] = 1 when
  * occluded.  Host pointers. */
