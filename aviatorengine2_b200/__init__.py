@@ -7,5 +7,6 @@ reference's renderer interface over that ABI.
 from . import _lib
 from ._lib import AeError, lib
 from .renderer import Context, Renderer, RendererSettings
+from .serving import Server
 
-__all__ = ["AeError", "Context", "Renderer", "RendererSettings", "lib", "_lib"]
+__all__ = ["AeError", "Context", "Renderer", "RendererSettings", "Server", "lib", "_lib"]

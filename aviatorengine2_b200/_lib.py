@@ -55,8 +55,27 @@ QNODE = np.dtype([("origin", "<f4", 3), ("exp", "i1", 3), ("nchild", "u1"), ("lo
 MESH_RANGE = np.dtype([("vertexBase", "<u4"), ("indexBase", "<u4"), ("triangleCount", "<u4"), ("blasBase", "<u4"),
                        ("localBounds", AABB), ("doubleSided", "<u4")])
 
+SERVE_SETTINGS = np.dtype([("device", "<i4"), ("slots", "<u4"), ("max_lights", "<u4"), ("max_requests", "<u4"),
+                           ("arena_bytes", "<u8"), ("ticks_per_launch", "<u4"), ("extend_threads", "<u4"),
+                           ("max_scenes", "<u4"), ("reserved", "<u4", 5)])
+SERVE_REQUEST = np.dtype([("scene", "<u4"), ("width", "<u4"), ("height", "<u4"), ("frames", "<u4"),
+                          ("config", CONFIG), ("accum", "<u8"), ("display", "<u8"), ("user", "<u8")])
+SERVE_RESULT = np.dtype([("id", "<u8"), ("user", "<u8"), ("status", "<i4"), ("scene_version", "<u4"),
+                         ("submit_ms", "<f8"), ("admit_ms", "<f8"), ("done_ms", "<f8"), ("paths", "<u8"),
+                         ("footprint", "<u8")])
+SERVE_STATS = np.dtype([("submitted", "<u8"), ("completed", "<u8"), ("rejected", "<u8"), ("failed", "<u8"),
+                        ("paths", "<u8"), ("rays", "<u8"), ("first_submit_ms", "<f8"), ("last_done_ms", "<f8"),
+                        ("p50_ms", "<f8"), ("p99_ms", "<f8"), ("mean_ms", "<f8"), ("max_ms", "<f8"),
+                        ("launches", "<u8"), ("peak_arena_bytes", "<u8"), ("peak_resident", "<u4"),
+                        ("moves_applied", "<u4"), ("errors", "<u4"), ("pad", "<u4")])
+POLICY_EVENT = np.dtype([("kind", "<u4"), ("scene", "<u4"), ("tick", "<u4"), ("service_ticks", "<u4"),
+                         ("footprint", "<u8")])
+POLICY_OUTCOME = np.dtype([("admit_tick", "<i4"), ("done_tick", "<i4"), ("version", "<u4"), ("status", "<i4"),
+                           ("offset", "<u8")])
+
 for _dt, _size in ((VERTEX, 32), (NODE, 48), (OBJECT, 128), (INSTANCE, 48), (RAY, 32), (HIT, 20), (CONFIG, 240),
-                   (AABB, 24), (SETTINGS, 64), (QNODE, 64)):
+                   (AABB, 24), (SETTINGS, 64), (QNODE, 64), (SERVE_SETTINGS, 56), (SERVE_REQUEST, 280),
+                   (SERVE_RESULT, 64), (SERVE_STATS, 128), (POLICY_EVENT, 24), (POLICY_OUTCOME, 24)):
     assert _dt.itemsize == _size, (_dt, _size)
 
 # Enumerations (include/ae_b200.h)
@@ -67,6 +86,7 @@ MISS = 0xFFFFFFFF
 VARIANT_PLAIN, VARIANT_FAST, VARIANT_QUANT = 0, 1, 2
 MODE_COMPUTE_ONLY, MODE_DEFERRED, MODE_WAVEFRONT = 0, 1, 2
 IMAGE_ACCUM, IMAGE_DISPLAY, IMAGE_FRAME, IMAGE_REDUCED, IMAGE_HISTORY_GEOMETRY = range(5)
+POLICY_REQUEST, POLICY_MOVE = 0, 1
 STATUS = {0: "AE_OK", -1: "AE_ERR_INVALID", -2: "AE_ERR_OOM", -3: "AE_ERR_OVERSIZE", -4: "AE_ERR_LAYOUT",
           -5: "AE_ERR_CUDA", -6: "AE_ERR_TIMEOUT", -7: "AE_ERR_STATE", -8: "AE_ERR_REJECTED"}
 
@@ -114,6 +134,17 @@ SIGNATURES = {
     "ae_refit_instances": (_I, [_P, _P, _U32]),
     "ae_download_scene": (_I, [_P, _P, _P, _P]),
     "ae_build_wide_bvh": (_I, [_P, _U32, _U32, _P, _U32, _P, _P, _P]),
+    "ae_serve_create": (_P, [_P]),
+    "ae_serve_destroy": (None, [_P]),
+    "ae_serve_last_error": (ctypes.c_char_p, [_P]),
+    "ae_serve_add_scene": (_I, [_P, _P, _P]),
+    "ae_serve_submit": (_I, [_P, _P, _P]),
+    "ae_serve_move_instances": (_I, [_P, _U32, _P, _U32]),
+    "ae_serve_wait": (_I, [_P, ctypes.c_uint64, ctypes.c_int32, _P]),
+    "ae_serve_drain": (_I, [_P, ctypes.c_int32]),
+    "ae_serve_get_stats": (_I, [_P, _P]),
+    "ae_serve_reset_stats": (_I, [_P]),
+    "ae_serve_policy_simulate": (_I, [_P, _U32, ctypes.c_uint64, _U32, _U32, _U32, _P]),
 }
 
 _lib = None

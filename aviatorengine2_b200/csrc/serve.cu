@@ -1,0 +1,1114 @@
+// serve.cu - the render-serving loop: continuous batching of frame requests
+// over scenes kept resident on one GPU.
+//
+// Device side.  A fixed pool of path slots is shared by every admitted
+// request.  A slot owns one pixel of one request and renders all of that
+// pixel's samples in order (frame by frame, sample by sample), so the
+// pixel's arithmetic - seeds, RNG draws, sample sums, the running
+// accumulation - is exactly that of `frames` compute-only frames of the plain
+// megakernel, whatever else is in flight.  Work moves through one merged ray
+// queue per tick:
+//
+//   begin    resets the next queues; adds the tick's ray counts to the stats
+//   extend   closest hit of every queued ray, each against its own scene's
+//            4-wide BVH (the scene is looked up per ray); CTAs stage queue
+//            tiles in shared memory with a bulk asynchronous copy
+//   shade    ColorRay's vertex work; surviving paths go to the next queue,
+//            light samples to the shadow queue (warp-aggregated appends)
+//   shadow   the reference's occlusion loop per light sample
+//   connect  NEE sums in light order onto the path radiance
+//   advance  finished paths close their sample; finished frames fold into the
+//            pixel's running accumulation; a finished pixel is written to its
+//            request's images, and the slot claims the next unclaimed pixel
+//            of the oldest admitted request (warp-cooperative claim) and
+//            queues that pixel's first camera ray; idle slots claim too
+//
+// A replay of one CUDA graph runs an even number of ticks; every parameter it
+// reads lives in device memory (scene table, request table, admission order),
+// so the graph is captured once.
+//
+// Host side.  A scheduler thread admits queued requests (serve_policy.h:
+// arrival order, by image footprint inside an arena allocated once, and by
+// resident request slots), applies instance moves with the GPU refit when no
+// request of the scene's previous version is outstanding, replays the graph
+// while any request is on the GPU (two replays in flight), and watches the
+// per-request pixel counters.  A completion thread copies finished images to
+// the caller's memory and releases their arena blocks.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "context.h"
+#include "fast.h"
+#include "fast_trace.cuh"
+#include "kernels.h"
+#include "serve_policy.h"
+#include "shade.cuh"
+#include "trace_common.cuh"
+#include "wf_common.cuh"
+
+namespace ae {
+namespace {
+
+constexpr uint32_t kServeMaxLights = 64;
+constexpr uint32_t kServeMaxRequests = 1024;
+constexpr int kServeStack = 24;  // shared-memory traversal entries per thread
+
+struct SceneRec {
+    DevScene S;
+    FastView V;
+};
+
+struct ReqDev {
+    FrameParams F;  // the request's camera at its own resolution; batch is the frame
+    float4 *accum;
+    uchar4 *display;
+    uint32_t scene, n_pixels, frames, spp;
+};
+
+enum { SV_Q0 = 0, SV_Q1 = 1, SV_SH = 2, SV_ERR = 3, SV_TILE = 4, SV_IDLE0 = 5, SV_IDLE1 = 6, SV_NORDER = 7, SV_COUNT = 8 };
+enum { ST_RAYS = 0, ST_SHADOW = 1, ST_COUNT = 2 };
+
+struct SvView {
+    const SceneRec *scenes;
+    const ReqDev *reqs;
+    uint32_t *next, *done;  // per request-table entry: pixels claimed, pixels written
+    const uint32_t *order;  // request-table entries in admission order, cnt[SV_NORDER] of them
+    uint32_t *cnt;
+    unsigned long long *stats;
+    // per slot
+    uint32_t *s_req, *s_pix, *s_frame, *s_sample, *s_bounce, *s_seed, *s_scene;
+    float4 *s_thr, *s_acc, *s_col, *s_accp, *s_pend;
+    uint8_t *s_nee, *s_end;
+    // queues
+    ae_ray *qray[2];
+    uint32_t *qslot[2];
+    ae_hit *qhit;
+    uint32_t *idle[2];
+    ShadowStore sh;  // entry = slot * max_lights + light
+    uint32_t *sq;
+    uint32_t max_lights;
+};
+
+__global__ void k_sv_init(SvView W, uint32_t slots) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < slots; i += gridDim.x * blockDim.x) {
+        W.idle[0][i] = i;
+        W.s_end[i] = 0;
+        W.s_nee[i] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int k = 0; k < SV_COUNT; k++) W.cnt[k] = 0;
+        W.cnt[SV_IDLE0] = slots;
+        W.stats[ST_RAYS] = 0;
+        W.stats[ST_SHADOW] = 0;
+    }
+}
+
+__global__ void k_sv_begin(SvView W, int q) {
+    W.stats[ST_RAYS] += W.cnt[q];
+    W.stats[ST_SHADOW] += W.cnt[SV_SH];
+    W.cnt[q ^ 1] = 0;
+    W.cnt[SV_SH] = 0;
+    W.cnt[SV_TILE] = 0;
+    W.cnt[SV_IDLE0 + (q ^ 1)] = 0;
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_sv_extend(SvView W, int q) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ae_ray *tile = reinterpret_cast<ae_ray *>(smem_raw);
+    uint2 *stk = reinterpret_cast<uint2 *>(smem_raw + THREADS * sizeof(ae_ray));
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tile_index;
+    const uint32_t count = W.cnt[q];
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    uint32_t phase = 0;
+    for (;;) {
+        if (threadIdx.x == 0) tile_index = atomicAdd(&W.cnt[SV_TILE], 1u);
+        __syncthreads();
+        const uint32_t start = tile_index * THREADS;
+        if (start >= count) break;
+        const uint32_t m = min(uint32_t(THREADS), count - start);
+        if (threadIdx.x == 0) {
+            mbar_expect_tx(&bar, m * uint32_t(sizeof(ae_ray)));
+            bulk_g2s(tile, W.qray[q] + start, m * uint32_t(sizeof(ae_ray)), &bar);
+        }
+        const bool ok = __syncthreads_and(mbar_wait(&bar, phase, 1u << 24) ? 1 : 0) != 0;
+        if (!ok) {
+            mbar_wait(&bar, phase, 1u << 24);
+            if (threadIdx.x == 0) atomicOr(&W.cnt[SV_ERR], 1u);
+            break;
+        }
+        phase ^= 1u;
+        if (threadIdx.x < m) {
+            const ae_ray r = tile[threadIdx.x];
+            const uint32_t slot = W.qslot[q][start + threadIdx.x];
+            const SceneRec &R = W.scenes[W.s_scene[slot]];
+            const DevScene S = R.S;
+            const FastView V = R.V;
+            const Best b = closest_fast<false, kServeStack>(S, V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear,
+                                                            r.time, stk, threadIdx.x, THREADS);
+            const bool any = b.object != AE_MISS;
+            ae_hit h;
+            h.t = any ? b.t : 0.0f;
+            h.alpha = any ? b.alpha : 0.0f;
+            h.beta = any ? b.beta : 0.0f;
+            h.object = b.object;
+            h.prim = b.prim;
+            W.qhit[start + threadIdx.x] = h;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_sv_shade(SvView W, int q) {
+    const uint32_t count = W.cnt[q];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t slot = W.qslot[q][k];
+        const ae_ray r = W.qray[q][k];
+        const ae_hit hr = W.qhit[k];
+        const DevScene S = W.scenes[W.s_scene[slot]].S;
+        const ReqDev &R = W.reqs[W.s_req[slot]];
+        const int bounce = int(W.s_bounce[slot]);
+        const float4 t4 = W.s_thr[slot], a4 = W.s_acc[slot];
+        f3 thr = mk(t4.x, t4.y, t4.z), acc = mk(a4.x, a4.y, a4.z);
+        uint32_t seed = W.s_seed[slot];
+        ae_ray nr;
+        uint32_t n_shadow;
+        const uint32_t e0 = slot * W.max_lights;
+        const bool next = shade_vertex(S, R.F.sky, R.F.depth, S.n_lights, bounce, r, hr, thr, acc, seed, W.sh, e0,
+                                       W.s_nee + slot, W.s_pend + slot, n_shadow, nr);
+        W.s_thr[slot] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+        W.s_acc[slot] = make_float4(acc.x, acc.y, acc.z, 0.0f);
+        W.s_seed[slot] = seed;
+        if (next) W.s_bounce[slot] = uint32_t(bounce + 1);
+        else W.s_end[slot] = 1;
+        const uint32_t qi = warp_append(&W.cnt[q ^ 1], next ? 1u : 0u);
+        if (next) {
+            W.qray[q ^ 1][qi] = nr;
+            W.qslot[q ^ 1][qi] = slot;
+        }
+        const uint32_t sbase = warp_append(&W.cnt[SV_SH], n_shadow);
+        if (n_shadow) push_shadow_entries(W.sh, e0, S.n_lights, W.sq, sbase);
+    }
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_sv_shadow(SvView W) {
+    extern __shared__ uint2 stk[];
+    const uint32_t count = W.cnt[SV_SH];
+    for (uint32_t k = blockIdx.x * THREADS + threadIdx.x; k < count; k += gridDim.x * THREADS) {
+        const uint32_t e = W.sq[k];
+        const uint32_t slot = e / W.max_lights;
+        const SceneRec &R = W.scenes[W.s_scene[slot]];
+        const DevScene S = R.S;
+        const FastView V = R.V;
+        const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
+        const bool occluded = shadow_occluded(S, V, mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z), mk(l4.x, l4.y, l4.z),
+                                              d4.w, stk, threadIdx.x, THREADS);
+        W.sh.occ[e] = occluded ? 1 : 0;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_sv_connect(SvView W, int q) {
+    const uint32_t count = W.cnt[q];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint32_t slot = W.qslot[q][k];
+        if (!W.s_nee[slot]) continue;
+        W.s_nee[slot] = 0;
+        const uint32_t n_lights = W.scenes[W.s_scene[slot]].S.n_lights;
+        const f3 dl = nee_total(W.sh, size_t(slot) * W.max_lights, n_lights);
+        const float4 t4 = W.s_pend[slot], a4 = W.s_acc[slot];
+        const f3 acc = mk(a4.x, a4.y, a4.z) + mk(t4.x, t4.y, t4.z) * dl;
+        W.s_acc[slot] = make_float4(acc.x, acc.y, acc.z, 0.0f);
+    }
+}
+
+// Warp-cooperative claim: the lanes with `need` take consecutive pixels of
+// the oldest request that still has unclaimed ones, moving to the next
+// request when it runs out.  A request's counter is only advanced while it
+// has pixels left, so it never runs far past its pixel count.  Every lane of
+// the calling warp that is in the loop must call this.
+AE_DEV bool claim_pixel(const SvView &W, bool need, uint32_t &req, uint32_t &pix) {
+    const unsigned mask = __activemask();
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t n_order = W.cnt[SV_NORDER];
+    bool got = false;
+    for (uint32_t i = 0; i < n_order; i++) {
+        const unsigned want = __ballot_sync(mask, need && !got);
+        if (!want) break;
+        const uint32_t r = W.order[i];
+        const uint32_t n = W.reqs[r].n_pixels;
+        const int leader = __ffs(want) - 1;
+        uint32_t base = n;
+        if (int(lane) == leader) {
+            const uint32_t seen = *reinterpret_cast<volatile const uint32_t *>(W.next + r);
+            if (seen < n) base = atomicAdd(W.next + r, uint32_t(__popc(want)));
+        }
+        base = __shfl_sync(mask, base, leader);
+        if (need && !got) {
+            const uint32_t p = base + uint32_t(__popc(want & ((1u << lane) - 1u)));
+            if (p < n) {
+                req = r;
+                pix = p;
+                got = true;
+            }
+        }
+    }
+    return got;
+}
+
+__global__ void __launch_bounds__(256) k_sv_advance(SvView W, int q) {
+    const uint32_t cq = W.cnt[q], ci = W.cnt[SV_IDLE0 + q];
+    const uint32_t total = cq + ci;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+        uint32_t slot;
+        bool ended = false;
+        const bool idle = k >= cq;
+        if (!idle) {
+            slot = W.qslot[q][k];
+            ended = W.s_end[slot] != 0;
+        } else {
+            slot = W.idle[q][k - cq];
+        }
+        bool need = idle, finished_pixel = false;
+        uint32_t req = 0, pix = 0, frame = 0, sample = 0, seed = 0;
+        if (ended) {
+            W.s_end[slot] = 0;
+            req = W.s_req[slot];
+            pix = W.s_pix[slot];
+            const ReqDev &R = W.reqs[req];
+            frame = W.s_frame[slot];
+            sample = W.s_sample[slot] + 1;
+            seed = W.s_seed[slot];
+            const float4 a4 = W.s_acc[slot], c4 = W.s_col[slot];
+            f3 col = mk(c4.x, c4.y, c4.z) + mk(a4.x, a4.y, a4.z);
+            if (sample == R.spp) {
+                // End of a frame: hybrid:1383-1403 for this pixel.
+                const f3 color = col / AE_U2F(R.spp);
+                f3 accp;
+                if (frame == 0) {
+                    accp = color;
+                } else {
+                    const float4 p4 = W.s_accp[slot];
+                    accp = lerp(mk(p4.x, p4.y, p4.z), color, AE_DIV(1.0f, AE_U2F(frame + 1)));
+                }
+                frame++;
+                sample = 0;
+                col = splat(0.0f);
+                if (frame == R.frames) {
+                    R.accum[pix] = make_float4(accp.x, accp.y, accp.z, 1.0f);
+                    R.display[pix] = display_texel(accp, R.F.exposure);
+                    finished_pixel = true;
+                    need = true;
+                } else {
+                    W.s_accp[slot] = make_float4(accp.x, accp.y, accp.z, 1.0f);
+                }
+            }
+            W.s_col[slot] = make_float4(col.x, col.y, col.z, 0.0f);
+        }
+        // One atomic per request per warp for the finished pixels.
+        {
+            const unsigned amask = __activemask();
+            const unsigned same = __match_any_sync(amask, finished_pixel ? req : 0xffffffffu);
+            if (finished_pixel && int(threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(W.done + req, uint32_t(__popc(same)));
+        }
+        uint32_t creq = 0, cpix = 0;
+        const bool got = claim_pixel(W, need, creq, cpix);
+        if (need && got) {
+            req = creq;
+            pix = cpix;
+            frame = 0;
+            sample = 0;
+            W.s_req[slot] = req;
+            W.s_pix[slot] = pix;
+            W.s_scene[slot] = W.reqs[req].scene;
+            W.s_col[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        const bool start = (ended && !need) || (need && got);
+        ae_ray r;
+        if (start) {
+            const ReqDev &R = W.reqs[req];
+            FrameParams F = R.F;
+            F.batch = frame;
+            const uint32_t x = pix % F.width, y = pix / F.width;
+            f3 o, d;
+            float time;
+            if (sample == 0) camera_ray(F, x, y, o, d, time, seed);
+            else camera_sample(F, x, y, o, d, time, seed);
+            W.s_frame[slot] = frame;
+            W.s_sample[slot] = sample;
+            W.s_seed[slot] = seed;
+            W.s_bounce[slot] = 0;
+            W.s_thr[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+            W.s_acc[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            r.ox = o.x; r.oy = o.y; r.oz = o.z; r.tnear = 0.001f;
+            r.dx = d.x; r.dy = d.y; r.dz = d.z; r.time = time;
+        }
+        const uint32_t qi = warp_append(&W.cnt[q ^ 1], start ? 1u : 0u);
+        if (start) {
+            W.qray[q ^ 1][qi] = r;
+            W.qslot[q ^ 1][qi] = slot;
+        }
+        const bool still_idle = need && !got;
+        const uint32_t ii = warp_append(&W.cnt[SV_IDLE0 + (q ^ 1)], still_idle ? 1u : 0u);
+        if (still_idle) W.idle[q ^ 1][ii] = slot;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host
+// ---------------------------------------------------------------------------
+double now_ms(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+struct HostReq {
+    uint64_t id = 0, user = 0;
+    uint32_t scene = 0, width = 0, height = 0, frames = 0, spp = 0;
+    ae_config config{};
+    float *dst_accum = nullptr;
+    uint8_t *dst_display = nullptr;
+    uint64_t footprint = 0, offset = 0, accum_bytes = 0, display_bytes = 0;
+    uint32_t version = 0;
+    int table = -1;
+    uint64_t admit_launch = 0;
+    double t_submit = 0, t_admit = -1, t_done = -1;
+    int status = 1;  // 1 = not finished
+    int stage = 0;   // 0 queued, 1 on the GPU, 2 result being copied
+};
+
+struct MoveOp {
+    uint32_t scene;
+    std::vector<ae_instance> inst;
+};
+
+typedef void (*SvExtendFn)(SvView, int);
+
+}  // namespace
+
+struct Server {
+    ae_serve_settings st{};
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    cudaStream_t stream = nullptr, copy_stream = nullptr, stats_stream = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool ev_live[2] = {false, false};
+    cudaGraphExec_t graph = nullptr;
+    int sms = 148;
+
+    // slot pool and queues
+    DevBuf<uint32_t> s_u32;  // 7 arrays of slots
+    DevBuf<float4> s_f4;     // 5 arrays of slots
+    DevBuf<uint8_t> s_u8;    // 2 arrays of slots
+    DevBuf<ae_ray> qray;     // 2 x slots
+    DevBuf<uint32_t> qslot, idle;
+    DevBuf<ae_hit> qhit;
+    DevBuf<float4> sh4;      // 4 x slots x max_lights
+    DevBuf<uint8_t> sh8;     // 2 x slots x max_lights
+    DevBuf<uint32_t> sq;
+    DevBuf<uint32_t> cnt, next, done, order;
+    DevBuf<unsigned long long> stats;
+    DevBuf<SceneRec> scenes_d;
+    DevBuf<ReqDev> reqs_d;
+    unsigned char *arena = nullptr;
+    SvView view{};
+
+    // pinned staging
+    ReqDev *h_req = nullptr;      // 2 x max_requests
+    uint32_t *h_order = nullptr;  // 2 x (max_requests + 1)
+    uint32_t *h_done = nullptr;   // 2 x (max_requests + 1): done counters, then the error word
+
+    // state shared with the API threads
+    std::mutex mu;
+    std::condition_variable cv_sched, cv_done, cv_copy;
+    std::string err;
+    Policy policy;
+    std::vector<Ctx *> scene_ctx;
+    std::vector<SceneRec> scene_rec;
+    std::map<uint64_t, std::unique_ptr<HostReq>> reqs;
+    std::vector<std::deque<MoveOp>> moves;
+    std::deque<HostReq *> copy_queue;
+    std::vector<HostReq *> table;
+    std::vector<int> table_free;
+    std::vector<int> order_host;  // table entries in admission order
+    bool order_dirty = true;
+    uint64_t next_id = 1;
+    uint64_t outstanding = 0;  // requests + moves not finished
+    bool stop = false, stop_copy = false, failed = false;
+    std::thread sched, completer;
+
+    // statistics
+    std::vector<double> latencies;
+    uint64_t submitted = 0, completed = 0, rejected = 0, n_failed = 0, paths = 0, launches = 0;
+    double first_submit = -1, last_done = -1;
+    uint64_t peak_arena = 0;
+    uint32_t peak_resident = 0, moves_applied = 0, dev_errors = 0;
+    unsigned long long rays_base = 0;
+
+    int fail_locked(int code, const char *fmt, ...) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        std::vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        err = buf;
+        return code;
+    }
+    int init();
+    int build_graph();
+    void run();
+    void run_completer();
+    void fail_all(int code, const std::string &why);
+    int apply_move(MoveOp &m);
+    ~Server();
+};
+
+namespace {
+
+const SvExtendFn kSvExtend[3] = {k_sv_extend<64>, k_sv_extend<128>, k_sv_extend<256>};
+
+int extend_index(uint32_t threads) { return threads == 256 ? 2 : threads == 128 ? 1 : 0; }
+
+size_t sv_extend_smem(int threads) { return size_t(threads) * sizeof(ae_ray) + size_t(threads) * kServeStack * sizeof(uint2); }
+
+}  // namespace
+
+int Server::init() {
+    const uint32_t S = st.slots, L = st.max_lights, R = st.max_requests;
+    if (cudaSetDevice(st.device) != cudaSuccess) { cudaGetLastError(); err = "cudaSetDevice failed"; return AE_ERR_CUDA; }
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, st.device);
+    if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&stats_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        err = "stream or event creation failed";
+        return AE_ERR_CUDA;
+    }
+    const size_t SL = size_t(S) * L;
+    if (s_u32.reserve(size_t(S) * 7) || s_f4.reserve(size_t(S) * 5) || s_u8.reserve(size_t(S) * 2) ||
+        qray.reserve(size_t(S) * 2) || qslot.reserve(size_t(S) * 2) || idle.reserve(size_t(S) * 2) ||
+        qhit.reserve(S) || sh4.reserve(SL * 4) || sh8.reserve(SL * 2) || sq.reserve(SL) || cnt.reserve(SV_COUNT) ||
+        next.reserve(R) || done.reserve(R) || order.reserve(R) || stats.reserve(ST_COUNT) ||
+        scenes_d.reserve(st.max_scenes) || reqs_d.reserve(R)) {
+        err = "slot pool allocation failed";
+        return AE_ERR_OOM;
+    }
+    if (cudaMalloc(&arena, st.arena_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        arena = nullptr;
+        err = "image arena allocation failed";
+        return AE_ERR_OOM;
+    }
+    if (cudaMallocHost(&h_req, sizeof(ReqDev) * 2 * R) != cudaSuccess ||
+        cudaMallocHost(&h_order, sizeof(uint32_t) * 2 * (R + 1)) != cudaSuccess ||
+        cudaMallocHost(&h_done, sizeof(uint32_t) * 2 * (R + 1)) != cudaSuccess) {
+        cudaGetLastError();
+        err = "pinned staging allocation failed";
+        return AE_ERR_OOM;
+    }
+    SvView &W = view;
+    W.scenes = scenes_d.ptr;
+    W.reqs = reqs_d.ptr;
+    W.next = next.ptr;
+    W.done = done.ptr;
+    W.order = order.ptr;
+    W.cnt = cnt.ptr;
+    W.stats = stats.ptr;
+    uint32_t *u = s_u32.ptr;
+    W.s_req = u; W.s_pix = u + S; W.s_frame = u + 2 * size_t(S); W.s_sample = u + 3 * size_t(S);
+    W.s_bounce = u + 4 * size_t(S); W.s_seed = u + 5 * size_t(S); W.s_scene = u + 6 * size_t(S);
+    float4 *f = s_f4.ptr;
+    W.s_thr = f; W.s_acc = f + S; W.s_col = f + 2 * size_t(S); W.s_accp = f + 3 * size_t(S); W.s_pend = f + 4 * size_t(S);
+    W.s_nee = s_u8.ptr; W.s_end = s_u8.ptr + S;
+    W.qray[0] = qray.ptr; W.qray[1] = qray.ptr + S;
+    W.qslot[0] = qslot.ptr; W.qslot[1] = qslot.ptr + S;
+    W.qhit = qhit.ptr;
+    W.idle[0] = idle.ptr; W.idle[1] = idle.ptr + S;
+    W.sh = ShadowStore{sh4.ptr, sh4.ptr + SL, sh4.ptr + 2 * SL, sh4.ptr + 3 * SL, sh8.ptr, sh8.ptr + SL};
+    W.sq = sq.ptr;
+    W.max_lights = L;
+    cudaMemsetAsync(next.ptr, 0, sizeof(uint32_t) * R, stream);
+    cudaMemsetAsync(done.ptr, 0, sizeof(uint32_t) * R, stream);
+    k_sv_init<<<sms * 4, 256, 0, stream>>>(W, S);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(stream) != cudaSuccess) {
+        cudaGetLastError();
+        err = "slot pool initialisation failed";
+        return AE_ERR_CUDA;
+    }
+    policy.configure(st.arena_bytes, st.max_requests);
+    scene_ctx.reserve(st.max_scenes);
+    scene_rec.reserve(st.max_scenes);
+    moves.reserve(st.max_scenes);
+    table.assign(R, nullptr);
+    for (int i = int(R) - 1; i >= 0; i--) table_free.push_back(i);
+    int rc = build_graph();
+    if (rc) return rc;
+    sched = std::thread([this] { run(); });
+    completer = std::thread([this] { run_completer(); });
+    return AE_OK;
+}
+
+// One replay = ticks_per_launch ticks of six stages; launch shapes fixed here.
+int Server::build_graph() {
+    const int ei = extend_index(st.extend_threads);
+    const int et = ei == 2 ? 256 : ei == 1 ? 128 : 64;
+    const SvExtendFn efn = kSvExtend[ei];
+    const size_t esmem = sv_extend_smem(et);
+    const size_t shsmem = size_t(kSharedStack) * 128 * sizeof(uint2);
+    cudaFuncSetAttribute(reinterpret_cast<const void *>(efn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(esmem));
+    cudaFuncSetAttribute(reinterpret_cast<const void *>(k_sv_shadow<128>), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(shsmem));
+    int e_per_sm = 0, sh_per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e_per_sm, reinterpret_cast<const void *>(efn), et, esmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh_per_sm, reinterpret_cast<const void *>(k_sv_shadow<128>), 128,
+                                                  shsmem);
+    const int egrid = std::max(1, e_per_sm) * sms, shgrid = std::max(1, sh_per_sm) * sms, g256 = sms * 8;
+    if (cudaGetLastError() != cudaSuccess) { err = "launch shape query failed"; return AE_ERR_CUDA; }
+    cudaGraph_t g;
+    if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        err = "graph capture failed";
+        return AE_ERR_CUDA;
+    }
+    const SvView W = view;
+    for (uint32_t t = 0; t < st.ticks_per_launch; t++) {
+        const int q = int(t & 1);
+        k_sv_begin<<<1, 1, 0, stream>>>(W, q);
+        efn<<<egrid, et, esmem, stream>>>(W, q);
+        k_sv_shade<<<g256, 256, 0, stream>>>(W, q);
+        k_sv_shadow<128><<<shgrid, 128, shsmem, stream>>>(W);
+        k_sv_connect<<<g256, 256, 0, stream>>>(W, q);
+        k_sv_advance<<<g256, 256, 0, stream>>>(W, q);
+    }
+    const cudaError_t le = cudaGetLastError();
+    cudaError_t ce = cudaStreamEndCapture(stream, &g);
+    if (le != cudaSuccess || ce != cudaSuccess) { cudaGetLastError(); err = "graph capture failed"; return AE_ERR_CUDA; }
+    ce = cudaGraphInstantiate(&graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) { cudaGetLastError(); err = "graph instantiate failed"; return AE_ERR_CUDA; }
+    return AE_OK;
+}
+
+// Applies one queued move: refit on the scene's context, then the optimised
+// instance records, then the scene's row of the device scene table.
+int Server::apply_move(MoveOp &m) {
+    Ctx *c = scene_ctx[m.scene];
+    int rc = ae_refit_instances(reinterpret_cast<ae_ctx *>(c), m.inst.data(), uint32_t(m.inst.size()));
+    if (rc == AE_OK) rc = prepare_fast(c);
+    if (rc == AE_OK) rc = c->cuda(cudaStreamSynchronize(c->stream), "refit");
+    if (rc != AE_OK) {
+        std::lock_guard<std::mutex> lk(mu);
+        err = "instance move: " + c->err;
+        return rc;
+    }
+    FastScene &F = *c->fast;
+    SceneRec rec{c->scene(), FastView{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr}};
+    if (cudaMemcpyAsync(scenes_d.ptr + m.scene, &rec, sizeof(rec), cudaMemcpyHostToDevice, stream) != cudaSuccess) {
+        cudaGetLastError();
+        return AE_ERR_CUDA;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    scene_rec[m.scene] = rec;
+    return AE_OK;
+}
+
+void Server::fail_all(int code, const std::string &why) {
+    // called with mu held
+    failed = true;
+    if (err.empty()) err = why;
+    for (auto &kv : reqs) {
+        HostReq *r = kv.second.get();
+        if (r->status == 1 && r->stage < 2) {  // results already being copied still complete
+            r->status = code;
+            r->t_done = now_ms(t0);
+            n_failed++;
+        }
+    }
+    outstanding = copy_queue.size();
+    cv_done.notify_all();
+}
+
+void Server::run() {
+    cudaSetDevice(st.device);
+    uint64_t issued = 0, observed = 0;
+    for (;;) {
+        std::vector<MoveOp> todo_moves;
+        std::vector<HostReq *> admitted;
+        bool active;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            if (stop || failed) break;
+            uint32_t s;
+            while (policy.next_move(s)) {
+                if (moves[s].empty()) break;
+                todo_moves.push_back(std::move(moves[s].front()));
+                moves[s].pop_front();
+                policy.move_applied(s);  // requests of the new version wait for this iteration's upload
+            }
+            PolicyRequest pr;
+            uint64_t off;
+            while (!table_free.empty() && policy.next_admission(pr, off)) {
+                HostReq *r = reqs[pr.id].get();
+                r->offset = off;
+                r->table = table_free.back();
+                table_free.pop_back();
+                table[r->table] = r;
+                r->t_admit = now_ms(t0);
+                r->stage = 1;
+                r->admit_launch = issued;
+                order_host.push_back(r->table);
+                order_dirty = true;
+                admitted.push_back(r);
+            }
+            peak_resident = std::max(peak_resident, policy.resident());
+            peak_arena = std::max(peak_arena, policy.arena().used());
+            active = !order_host.empty();
+            if (!active && todo_moves.empty() && issued == observed) {
+                cv_sched.wait_for(lk, std::chrono::milliseconds(20));
+                continue;
+            }
+        }
+        for (MoveOp &m : todo_moves) {
+            if (apply_move(m) != AE_OK) {
+                std::lock_guard<std::mutex> lk(mu);
+                fail_all(AE_ERR_CUDA, err);
+                break;
+            }
+            std::lock_guard<std::mutex> lk(mu);
+            moves_applied++;
+            if (outstanding) outstanding--;
+            cv_done.notify_all();
+        }
+        // Descriptors of the admitted requests and the admission order go
+        // through pinned staging half h = parity of the next replay; the
+        // replay two before it (the last reader of half h) has always been
+        // observed by now, and copies not followed by a replay are waited for.
+        const int h = int(issued & 1);
+        bool staged = false;
+        if (!admitted.empty() || order_dirty) {
+            if (ev_live[h]) cudaEventSynchronize(ev[h]);
+            staged = true;
+            ReqDev *hr = h_req + size_t(h) * st.max_requests;
+            for (size_t i = 0; i < admitted.size(); i++) {
+                HostReq *r = admitted[i];
+                ae_config cfg = r->config;
+                cfg.width = r->width;
+                cfg.height = r->height;
+                cfg.batch = 0;
+                ReqDev &d = hr[i];
+                d.F = make_frame_params(cfg);
+                d.accum = reinterpret_cast<float4 *>(arena + r->offset);
+                d.display = reinterpret_cast<uchar4 *>(arena + r->offset + r->accum_bytes);
+                d.scene = r->scene;
+                d.n_pixels = r->width * r->height;
+                d.frames = r->frames;
+                d.spp = d.F.spp;
+                cudaMemcpyAsync(reqs_d.ptr + r->table, &d, sizeof(ReqDev), cudaMemcpyHostToDevice, stream);
+                cudaMemsetAsync(next.ptr + r->table, 0, sizeof(uint32_t), stream);
+                cudaMemsetAsync(done.ptr + r->table, 0, sizeof(uint32_t), stream);
+            }
+            uint32_t *ho = h_order + size_t(h) * (st.max_requests + 1);
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                for (size_t i = 0; i < order_host.size(); i++) ho[i] = uint32_t(order_host[i]);
+                ho[st.max_requests] = uint32_t(order_host.size());
+                order_dirty = false;
+            }
+            if (ho[st.max_requests]) cudaMemcpyAsync(order.ptr, ho, sizeof(uint32_t) * ho[st.max_requests],
+                                                     cudaMemcpyHostToDevice, stream);
+            cudaMemcpyAsync(cnt.ptr + SV_NORDER, ho + st.max_requests, sizeof(uint32_t), cudaMemcpyHostToDevice, stream);
+        }
+        if (active) {
+            cudaGraphLaunch(graph, stream);
+            uint32_t *hd = h_done + size_t(h) * (st.max_requests + 1);
+            cudaMemcpyAsync(hd, done.ptr, sizeof(uint32_t) * st.max_requests, cudaMemcpyDeviceToHost, stream);
+            cudaMemcpyAsync(hd + st.max_requests, cnt.ptr + SV_ERR, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+            cudaEventRecord(ev[h], stream);
+            ev_live[h] = true;
+            issued++;
+            launches++;
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) {
+                std::lock_guard<std::mutex> lk(mu);
+                fail_all(AE_ERR_CUDA, std::string("graph replay: ") + cudaGetErrorString(e));
+                break;
+            }
+        }
+        else if (staged) {
+            cudaStreamSynchronize(stream);
+        }
+        // Observe finished replays: wait while two are in flight (or nothing
+        // new was queued), otherwise only poll.
+        bool broke = false;
+        while (observed < issued) {
+            const int k = int(observed & 1);
+            const bool must = (issued - observed) >= 2 || !active;
+            cudaError_t e = must ? cudaEventSynchronize(ev[k]) : cudaEventQuery(ev[k]);
+            if (e == cudaErrorNotReady) break;
+            if (e != cudaSuccess) {
+                std::lock_guard<std::mutex> lk(mu);
+                fail_all(AE_ERR_CUDA, std::string("serving replay: ") + cudaGetErrorString(e));
+                broke = true;
+                break;
+            }
+            ev_live[k] = false;
+            const uint32_t *hd = h_done + size_t(k) * (st.max_requests + 1);
+            std::lock_guard<std::mutex> lk(mu);
+            if (hd[st.max_requests]) {
+                dev_errors = hd[st.max_requests];
+                fail_all(AE_ERR_TIMEOUT, "a bounded queue-tile wait gave up on the device");
+                broke = true;
+                break;
+            }
+            for (size_t i = 0; i < order_host.size();) {
+                const int t = order_host[i];
+                HostReq *r = table[t];
+                if (r && r->admit_launch <= observed && hd[t] >= r->width * r->height) {
+                    table[t] = nullptr;
+                    table_free.push_back(t);
+                    order_host.erase(order_host.begin() + long(i));
+                    order_dirty = true;
+                    r->stage = 2;
+                    copy_queue.push_back(r);
+                    cv_copy.notify_one();
+                } else {
+                    i++;
+                }
+            }
+            observed++;
+        }
+        if (broke) break;
+    }
+    cudaStreamSynchronize(stream);
+}
+
+void Server::run_completer() {
+    cudaSetDevice(st.device);
+    for (;;) {
+        HostReq *r;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_copy.wait(lk, [this] { return stop_copy || !copy_queue.empty(); });
+            if (copy_queue.empty()) return;
+            r = copy_queue.front();
+            copy_queue.pop_front();
+        }
+        cudaError_t e = cudaSuccess;
+        if (r->dst_accum)
+            e = cudaMemcpyAsync(r->dst_accum, arena + r->offset, r->accum_bytes, cudaMemcpyDeviceToHost, copy_stream);
+        if (e == cudaSuccess && r->dst_display)
+            e = cudaMemcpyAsync(r->dst_display, arena + r->offset + r->accum_bytes, r->display_bytes,
+                                cudaMemcpyDeviceToHost, copy_stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(copy_stream);
+        std::lock_guard<std::mutex> lk(mu);
+        policy.completed(r->id);
+        if (r->status == 1) {
+            r->t_done = now_ms(t0);
+            if (e == cudaSuccess) {
+                r->status = AE_OK;
+                completed++;
+                paths += uint64_t(r->width) * r->height * r->frames * r->spp;
+                latencies.push_back(r->t_done - r->t_submit);
+                last_done = std::max(last_done, r->t_done);
+            } else {
+                cudaGetLastError();
+                r->status = AE_ERR_CUDA;
+                n_failed++;
+                err = std::string("result copy: ") + cudaGetErrorString(e);
+            }
+            if (outstanding) outstanding--;
+        }
+        cv_done.notify_all();
+        cv_sched.notify_one();
+    }
+}
+
+Server::~Server() {
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        stop = true;
+    }
+    cv_sched.notify_all();
+    cv_copy.notify_all();
+    if (sched.joinable()) sched.join();
+    // Copies already queued still complete; the completer exits after them.
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        stop_copy = true;
+    }
+    cv_copy.notify_all();
+    if (completer.joinable()) completer.join();
+    if (graph) cudaGraphExecDestroy(graph);
+    if (stream) cudaStreamSynchronize(stream);
+    if (arena) cudaFree(arena);
+    if (h_req) cudaFreeHost(h_req);
+    if (h_order) cudaFreeHost(h_order);
+    if (h_done) cudaFreeHost(h_done);
+    for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    if (stats_stream) cudaStreamDestroy(stats_stream);
+}
+
+}  // namespace ae
+
+using namespace ae;
+
+struct ae_server : Server {};
+
+extern "C" ae_server *ae_serve_create(const ae_serve_settings *settings) {
+    ae_serve_settings s{};
+    if (settings) s = *settings;
+    if (!s.slots) s.slots = 1u << 20;
+    if (!s.max_lights) s.max_lights = 16;
+    if (!s.max_requests) s.max_requests = 64;
+    if (!s.arena_bytes) s.arena_bytes = 1ull << 30;
+    if (!s.ticks_per_launch) s.ticks_per_launch = 4;
+    if (!s.extend_threads) s.extend_threads = 64;
+    if (!s.max_scenes) s.max_scenes = 16;
+    if (s.max_lights > kServeMaxLights || s.max_requests > kServeMaxRequests || (s.ticks_per_launch & 1) ||
+        s.slots > (1u << 26) || uint64_t(s.slots) * s.max_lights > 0xffffffffull)
+        return nullptr;
+    ae_server *srv = new (std::nothrow) ae_server();
+    if (!srv) return nullptr;
+    srv->st = s;
+    if (srv->init() != AE_OK) {
+        std::fprintf(stderr, "ae_serve_create: %s\n", srv->err.c_str());
+        delete srv;
+        return nullptr;
+    }
+    return srv;
+}
+
+extern "C" void ae_serve_destroy(ae_server *srv) {
+    if (!srv) return;
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        for (uint64_t id : srv->policy.cancel_pending()) {
+            auto it = srv->reqs.find(id);
+            if (it != srv->reqs.end() && it->second->status == 1) it->second->status = AE_ERR_STATE;
+        }
+        srv->cv_done.notify_all();
+    }
+    delete srv;
+}
+
+extern "C" const char *ae_serve_last_error(ae_server *srv) {
+    if (!srv) return "null server";
+    std::lock_guard<std::mutex> lk(srv->mu);
+    return srv->err.c_str();
+}
+
+extern "C" int ae_serve_add_scene(ae_server *srv, ae_ctx *scene, uint32_t *scene_id) {
+    if (!srv || !scene) return AE_ERR_INVALID;
+    Ctx *c = reinterpret_cast<Ctx *>(scene);
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        if (srv->scene_ctx.size() >= srv->st.max_scenes)
+            return srv->fail_locked(AE_ERR_OVERSIZE, "at most %u resident scenes", srv->st.max_scenes);
+        if (c->settings.device != srv->st.device)
+            return srv->fail_locked(AE_ERR_INVALID, "scene context is on device %d, server on %d", c->settings.device,
+                                    srv->st.device);
+        if (c->n_lights > srv->st.max_lights)
+            return srv->fail_locked(AE_ERR_OVERSIZE, "scene has %u lights; server takes %u", c->n_lights,
+                                    srv->st.max_lights);
+        for (Ctx *o : srv->scene_ctx)
+            if (o == c) return srv->fail_locked(AE_ERR_INVALID, "scene context already resident");
+    }
+    // The optimised BVH build can take seconds; it runs without the lock.
+    int rc = prepare_fast(c);
+    if (rc == AE_OK) rc = c->cuda(cudaStreamSynchronize(c->stream), "prepare scene");
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (rc != AE_OK) return srv->fail_locked(rc, "scene: %s", c->err.c_str());
+    if (srv->scene_ctx.size() >= srv->st.max_scenes)
+        return srv->fail_locked(AE_ERR_OVERSIZE, "at most %u resident scenes", srv->st.max_scenes);
+    FastScene &F = *c->fast;
+    SceneRec rec{c->scene(), FastView{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr}};
+    const uint32_t id = uint32_t(srv->scene_ctx.size());
+    // No replay reads this row before a request of the scene is admitted.
+    if (cudaMemcpyAsync(srv->scenes_d.ptr + id, &rec, sizeof(rec), cudaMemcpyHostToDevice, srv->stats_stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(srv->stats_stream) != cudaSuccess) {
+        cudaGetLastError();
+        return srv->fail_locked(AE_ERR_CUDA, "scene table upload failed");
+    }
+    srv->scene_ctx.push_back(c);  // capacity reserved at creation: the scheduler reads it unlocked
+    srv->scene_rec.push_back(rec);
+    srv->moves.emplace_back();
+    srv->policy.add_scene();
+    if (scene_id) *scene_id = id;
+    return AE_OK;
+}
+
+extern "C" int ae_serve_submit(ae_server *srv, const ae_serve_request *req, uint64_t *id) {
+    if (!srv || !req) return AE_ERR_INVALID;
+    std::unique_ptr<HostReq> r(new (std::nothrow) HostReq());
+    if (!r) return AE_ERR_OOM;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (srv->failed) return AE_ERR_STATE;
+    if (req->scene >= srv->scene_ctx.size()) return srv->fail_locked(AE_ERR_INVALID, "unknown scene %u", req->scene);
+    if (!req->width || !req->height || !req->frames || uint64_t(req->width) * req->height > (1ull << 30))
+        return srv->fail_locked(AE_ERR_INVALID, "bad request size %ux%u x %u frames", req->width, req->height, req->frames);
+    if (req->config.depth == 0 || req->config.depth > 64) return srv->fail_locked(AE_ERR_INVALID, "depth %u outside 1..64", req->config.depth);
+    r->id = srv->next_id++;
+    r->user = req->user;
+    r->scene = req->scene;
+    r->width = req->width;
+    r->height = req->height;
+    r->frames = req->frames;
+    r->config = req->config;
+    const uint32_t per = req->config.batches ? req->config.samples / req->config.batches : req->config.samples;
+    r->spp = per > 1u ? per : 1u;
+    r->dst_accum = req->accum;
+    r->dst_display = req->display;
+    const uint64_t px = uint64_t(req->width) * req->height;
+    r->accum_bytes = align_up(px * 16, Arena::kAlign);
+    r->display_bytes = px * 4;
+    r->footprint = r->accum_bytes + align_up(px * 4, Arena::kAlign);
+    r->t_submit = now_ms(srv->t0);
+    PolicyRequest pr;
+    pr.id = r->id;
+    pr.scene = r->scene;
+    pr.footprint = r->footprint;
+    srv->submitted++;
+    if (srv->first_submit < 0) srv->first_submit = r->t_submit;
+    if (!srv->policy.submit(pr)) {
+        srv->rejected++;
+        return srv->fail_locked(AE_ERR_REJECTED, "request of %llu image bytes exceeds the %llu-byte arena",
+                                (unsigned long long)r->footprint, (unsigned long long)srv->st.arena_bytes);
+    }
+    r->version = pr.version;
+    if (id) *id = r->id;
+    srv->reqs[r->id] = std::move(r);
+    srv->outstanding++;
+    srv->cv_sched.notify_one();
+    return AE_OK;
+}
+
+extern "C" int ae_serve_move_instances(ae_server *srv, uint32_t scene, const ae_instance *instances, uint32_t n) {
+    if (!srv || (n && !instances)) return AE_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (srv->failed) return AE_ERR_STATE;
+    if (scene >= srv->scene_ctx.size()) return srv->fail_locked(AE_ERR_INVALID, "unknown scene %u", scene);
+    Ctx *c = srv->scene_ctx[scene];
+    if (n != c->n_instances) return srv->fail_locked(AE_ERR_INVALID, "scene %u has %u instances, got %u", scene, c->n_instances, n);
+    MoveOp m;
+    m.scene = scene;
+    m.inst.assign(instances, instances + n);
+    srv->moves[scene].push_back(std::move(m));
+    srv->policy.move(scene);
+    srv->outstanding++;
+    srv->cv_sched.notify_one();
+    return AE_OK;
+}
+
+extern "C" int ae_serve_wait(ae_server *srv, uint64_t id, int32_t timeout_ms, ae_serve_result *out) {
+    if (!srv) return AE_ERR_INVALID;
+    std::unique_lock<std::mutex> lk(srv->mu);
+    auto it = srv->reqs.find(id);
+    if (it == srv->reqs.end()) return srv->fail_locked(AE_ERR_INVALID, "unknown request %llu", (unsigned long long)id);
+    HostReq *r = it->second.get();
+    auto ready = [r] { return r->status != 1; };
+    if (timeout_ms < 0) srv->cv_done.wait(lk, ready);
+    else if (!srv->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return AE_ERR_TIMEOUT;
+    if (out) {
+        out->id = r->id;
+        out->user = r->user;
+        out->status = r->status;
+        out->scene_version = r->version;
+        out->submit_ms = r->t_submit;
+        out->admit_ms = r->t_admit;
+        out->done_ms = r->t_done;
+        out->paths = uint64_t(r->width) * r->height * r->frames * r->spp;
+        out->footprint = r->footprint;
+    }
+    const int status = r->status;
+    srv->reqs.erase(it);
+    return status;
+}
+
+extern "C" int ae_serve_drain(ae_server *srv, int32_t timeout_ms) {
+    if (!srv) return AE_ERR_INVALID;
+    std::unique_lock<std::mutex> lk(srv->mu);
+    auto ready = [srv] { return srv->outstanding == 0 || srv->failed; };
+    if (timeout_ms < 0) srv->cv_done.wait(lk, ready);
+    else if (!srv->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return AE_ERR_TIMEOUT;
+    return srv->failed ? AE_ERR_STATE : AE_OK;
+}
+
+extern "C" int ae_serve_get_stats(ae_server *srv, ae_serve_stats *out) {
+    if (!srv || !out) return AE_ERR_INVALID;
+    unsigned long long dev[ST_COUNT] = {0, 0};
+    if (cudaMemcpyAsync(dev, srv->stats.ptr, sizeof(dev), cudaMemcpyDeviceToHost, srv->stats_stream) != cudaSuccess ||
+        cudaStreamSynchronize(srv->stats_stream) != cudaSuccess) {
+        cudaGetLastError();
+        return AE_ERR_CUDA;
+    }
+    std::lock_guard<std::mutex> lk(srv->mu);
+    std::memset(out, 0, sizeof(*out));
+    out->submitted = srv->submitted;
+    out->completed = srv->completed;
+    out->rejected = srv->rejected;
+    out->failed = srv->n_failed;
+    out->paths = srv->paths;
+    out->rays = dev[ST_RAYS] + dev[ST_SHADOW] - srv->rays_base;
+    out->first_submit_ms = srv->first_submit;
+    out->last_done_ms = srv->last_done;
+    std::vector<double> l = srv->latencies;
+    if (!l.empty()) {
+        std::sort(l.begin(), l.end());
+        auto pct = [&l](double p) {
+            const double pos = p * double(l.size() - 1);
+            const size_t lo = size_t(pos);
+            const size_t hi = std::min(lo + 1, l.size() - 1);
+            return l[lo] + (l[hi] - l[lo]) * (pos - double(lo));
+        };
+        out->p50_ms = pct(0.50);
+        out->p99_ms = pct(0.99);
+        double s = 0;
+        for (double v : l) s += v;
+        out->mean_ms = s / double(l.size());
+        out->max_ms = l.back();
+    }
+    out->launches = srv->launches;
+    out->peak_arena_bytes = srv->peak_arena;
+    out->peak_resident = srv->peak_resident;
+    out->moves_applied = srv->moves_applied;
+    out->errors = srv->dev_errors;
+    return AE_OK;
+}
+
+extern "C" int ae_serve_reset_stats(ae_server *srv) {
+    if (!srv) return AE_ERR_INVALID;
+    unsigned long long dev[ST_COUNT] = {0, 0};
+    if (cudaMemcpyAsync(dev, srv->stats.ptr, sizeof(dev), cudaMemcpyDeviceToHost, srv->stats_stream) != cudaSuccess ||
+        cudaStreamSynchronize(srv->stats_stream) != cudaSuccess) {
+        cudaGetLastError();
+        return AE_ERR_CUDA;
+    }
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->latencies.clear();
+    srv->submitted = srv->completed = srv->rejected = srv->n_failed = srv->paths = srv->launches = 0;
+    srv->first_submit = srv->last_done = -1;
+    srv->peak_arena = srv->policy.arena().used();
+    srv->peak_resident = srv->policy.resident();
+    srv->moves_applied = 0;
+    srv->rays_base = dev[ST_RAYS] + dev[ST_SHADOW];
+    return AE_OK;
+}

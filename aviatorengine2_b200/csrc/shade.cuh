@@ -135,10 +135,9 @@ AE_DEV bool get_bounce(f3 d, const DHit &h, const MatRec &m, f3 &dir, uint32_t &
     }
 }
 
-// Primary ray of pixel (x, y) and the RNG state after it (jitter, defocus
-// disk when the angle is positive, then the time draw).
-AE_DEV void camera_ray(const FrameParams &F, uint32_t x, uint32_t y, f3 &o, f3 &d, float &time, uint32_t &seed) {
-    seed = x + y * F.width + F.batch * F.width * F.height + 1u;
+// One camera sample of pixel (x, y) drawn from the pixel's running RNG state:
+// jitter, defocus, direction and time (hybrid:1366-1373).
+AE_DEV void camera_sample(const FrameParams &F, uint32_t x, uint32_t y, f3 &o, f3 &d, float &time, uint32_t &seed) {
     const float jx = AE_SUB(rng_next(seed), 0.5f);
     const float jy = AE_SUB(rng_next(seed), 0.5f);
     const f3 tgt = F.pixel0 + AE_ADD(AE_U2F(x), jx) * F.pixel_u + AE_ADD(AE_U2F(y), jy) * F.pixel_v;
@@ -155,6 +154,12 @@ AE_DEV void camera_ray(const FrameParams &F, uint32_t x, uint32_t y, f3 &o, f3 &
     }
     d = normalize(tgt - o);
     time = rng_next(seed);
+}
+
+// The first sample of a frame: the per-pixel seed, then camera_sample.
+AE_DEV void camera_ray(const FrameParams &F, uint32_t x, uint32_t y, f3 &o, f3 &d, float &time, uint32_t &seed) {
+    seed = x + y * F.width + F.batch * F.width * F.height + 1u;
+    camera_sample(F, x, y, o, d, time, seed);
 }
 
 // World shading normal and facing of a mesh hit, recomputed from the hit

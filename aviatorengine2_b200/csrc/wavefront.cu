@@ -37,6 +37,7 @@
 #include "kernels.h"
 #include "shade.cuh"
 #include "trace_common.cuh"
+#include "wf_common.cuh"
 
 namespace ae {
 
@@ -59,9 +60,7 @@ struct WfView {
     float4 *thr, *acc, *col, *pend;
     uint32_t *seed;
     uint8_t *nee;
-    // shadow entries, slot = path * n_lights + light
-    float4 *sh_o, *sh_d, *sh_lp, *sh_c;  // origin+tnear, dir+time, light point, contribution
-    uint8_t *sh_valid, *sh_occ;
+    ShadowStore sh;  // light-sample entries, index = path * n_lights + light
     uint32_t *sq;
     uint32_t *cnt;
     const WfParams *P;
@@ -102,58 +101,6 @@ void destroy_wavefront(Ctx *c) {
 }
 
 // ---------------------------------------------------------------------------
-// Warp-aggregated queue append: one atomic per warp, lanes get consecutive
-// slots in lane order.
-// ---------------------------------------------------------------------------
-AE_DEV uint32_t warp_append(uint32_t *counter, uint32_t want) {
-    const uint32_t lane = threadIdx.x & 31;
-    const unsigned mask = __activemask();
-    // inclusive prefix of `want` over the active lanes
-    uint32_t incl = want;
-    for (int off = 1; off < 32; off <<= 1) {
-        const uint32_t v = __shfl_up_sync(mask, incl, off);
-        if (lane >= uint32_t(off) && ((mask >> (lane - off)) & 1u)) incl += v;
-    }
-    const int leader = 31 - __clz(mask);  // highest active lane holds the total
-    uint32_t base = 0;
-    if (int(lane) == leader) base = atomicAdd(counter, incl);
-    base = __shfl_sync(mask, base, leader);
-    return base + incl - want;
-}
-
-// ---------------------------------------------------------------------------
-// Bulk-copy staging of a queue tile into shared memory.
-// ---------------------------------------------------------------------------
-AE_DEV uint32_t smem_addr(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
-
-AE_DEV void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-AE_DEV void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
-}
-AE_DEV void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_addr(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
-}
-// Waits for `phase` to complete; gives up after `limit` polls and reports it.
-AE_DEV bool mbar_wait(uint64_t *bar, uint32_t phase, uint32_t limit) {
-    for (uint32_t i = 0; i < limit; i++) {
-        uint32_t done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done)
-            : "r"(smem_addr(bar)), "r"(phase)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-// ---------------------------------------------------------------------------
 // Stages
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_wf_generate(WfView W) {
@@ -175,22 +122,7 @@ __global__ void __launch_bounds__(256) k_wf_generate(WfView W) {
             // Later samples of the frame continue the pixel's stream (the
             // samples loop of main, hybrid:1366-1381).
             seed = W.seed[p];
-            const float jx = AE_SUB(rng_next(seed), 0.5f);
-            const float jy = AE_SUB(rng_next(seed), 0.5f);
-            const f3 tgt = P.F.pixel0 + AE_ADD(AE_U2F(x), jx) * P.F.pixel_u + AE_ADD(AE_U2F(y), jy) * P.F.pixel_v;
-            o = P.F.source;
-            if (P.F.defocus_angle > 0.0f) {
-                float px, py;
-                for (;;) {
-                    const float a = rng_next(seed), b = rng_next(seed);
-                    px = AE_SUB(AE_MUL(a, 2.0f), 1.0f);
-                    py = AE_SUB(AE_MUL(b, 2.0f), 1.0f);
-                    if (length(mk(px, py, 0.0f)) < 1.0f) break;
-                }
-                o = P.F.source + px * P.F.defocus_u + py * P.F.defocus_v;
-            }
-            d = normalize(tgt - o);
-            time = rng_next(seed);
+            camera_sample(P.F, x, y, o, d, time, seed);
         }
         W.seed[p] = seed;
         ae_ray r;
@@ -266,78 +198,14 @@ __global__ void __launch_bounds__(256) k_wf_shade(DevScene S, WfView W, int boun
         const uint32_t pid = W.qpid[q][k];
         const ae_ray r = W.qray[q][k];
         const ae_hit hr = W.qhit[k];
-        const f3 o = mk(r.ox, r.oy, r.oz), d = mk(r.dx, r.dy, r.dz);
         float4 t4 = W.thr[pid], a4 = W.acc[pid];
         f3 thr = mk(t4.x, t4.y, t4.z), acc = mk(a4.x, a4.y, a4.z);
         uint32_t seed = W.seed[pid];
-        bool next = false;
-        ae_ray nr = r;
-        uint32_t n_shadow = 0;
-        DHit h;
-        if (!surface_from_hit(S, hr, o, d, r.time, h)) {
-            acc = acc + thr * P.F.sky;
-        } else {
-            const MatRec m = load_mat(S.objects + h.slot);
-            if (m.type == AE_MAT_DIFFUSE_LIGHT) {
-                acc = acc + thr * (m.emission * m.albedo);
-            } else {
-                if (m.type == AE_MAT_LAMBERTIAN) {
-                    // Light samples in light order (CalculateDirectLight,
-                    // hybrid:1122-1212); occlusion is resolved by the shadow stage.
-                    W.nee[pid] = 1;
-                    W.pend[pid] = make_float4(thr.x, thr.y, thr.z, 0.0f);
-                    for (uint32_t i = 0; i < P.n_lights; i++) {
-                        const size_t e = size_t(pid) * P.n_lights + i;
-                        const ae_object *L = S.objects + __ldg(S.lights + i);
-                        const ObjHead lh = load_head(L);
-                        f3 lp;
-                        float omega;
-                        sample_light(L, lh.shape, h.p, lp, omega, seed);
-                        uint8_t valid = 0;
-                        if (omega > 0.0f) {
-                            f3 sd = lp - h.p;
-                            const float dist = length(sd);
-                            if (dist > 1e-6f) {
-                                sd = sd / dist;
-                                const float ct = dot(h.n, sd);
-                                if (ct > 0.0f) {
-                                    const MatRec lm = load_mat(L);
-                                    const f3 rad = lm.emission * lm.albedo;
-                                    const f3 c = m.albedo * rad * ct * omega;
-                                    const f3 so = h.p + h.n * 0.001f;
-                                    W.sh_o[e] = make_float4(so.x, so.y, so.z, 0.001f);
-                                    W.sh_d[e] = make_float4(sd.x, sd.y, sd.z, r.time);
-                                    W.sh_lp[e] = make_float4(lp.x, lp.y, lp.z, 0.0f);
-                                    W.sh_c[e] = make_float4(c.x, c.y, c.z, 0.0f);
-                                    valid = 1;
-                                    n_shadow++;
-                                }
-                            }
-                        }
-                        W.sh_valid[e] = valid;
-                        W.sh_occ[e] = 0;
-                    }
-                }
-                f3 sd;
-                if (get_bounce(d, h, m, sd, seed)) {
-                    const f3 nd = normalize(sd);
-                    const float sgn = dot(nd, h.n) < 0.0f ? -1.0f : 1.0f;
-                    const f3 no = h.p + h.n * AE_MUL(0.001f, sgn);
-                    if (m.type != AE_MAT_DIELECTRIC) thr = thr * m.albedo;
-                    bool alive = true;
-                    if (bounce > 0) {
-                        const float p = clampf(maxc(thr), 0.1f, 1.0f);
-                        if (rng_next(seed) > p) alive = false;
-                        else thr = thr / p;
-                    }
-                    if (alive && uint32_t(bounce + 1) < P.F.depth) {
-                        next = true;
-                        nr.ox = no.x; nr.oy = no.y; nr.oz = no.z; nr.tnear = 0.001f;
-                        nr.dx = nd.x; nr.dy = nd.y; nr.dz = nd.z;
-                    }
-                }
-            }
-        }
+        ae_ray nr;
+        uint32_t n_shadow;
+        const size_t e0 = size_t(pid) * P.n_lights;
+        const bool next = shade_vertex(S, P.F.sky, P.F.depth, P.n_lights, bounce, r, hr, thr, acc, seed, W.sh, e0,
+                                       W.nee + pid, W.pend + pid, n_shadow, nr);
         W.thr[pid] = make_float4(thr.x, thr.y, thr.z, 0.0f);
         W.acc[pid] = make_float4(acc.x, acc.y, acc.z, 0.0f);
         W.seed[pid] = seed;
@@ -348,13 +216,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(DevScene S, WfView W, int boun
             W.qpid[q ^ 1][slot] = pid;
         }
         const uint32_t sbase = warp_append(&W.cnt[C_SH], n_shadow);
-        if (n_shadow) {
-            uint32_t j = 0;
-            for (uint32_t i = 0; i < P.n_lights; i++) {
-                const uint32_t e = pid * P.n_lights + i;
-                if (W.sh_valid[e]) W.sq[sbase + j++] = e;
-            }
-        }
+        if (n_shadow) push_shadow_entries(W.sh, pid * P.n_lights, P.n_lights, W.sq, sbase);
     }
 }
 
@@ -365,20 +227,10 @@ __global__ void __launch_bounds__(THREADS) k_wf_shadow(DevScene S, FastView V, W
     const uint32_t count = W.cnt[C_SH];
     for (uint32_t k = blockIdx.x * THREADS + threadIdx.x; k < count; k += gridDim.x * THREADS) {
         const uint32_t e = W.sq[k];
-        const float4 o4 = W.sh_o[e], d4 = W.sh_d[e], l4 = W.sh_lp[e];
-        f3 so = mk(o4.x, o4.y, o4.z);
-        const f3 sd = mk(d4.x, d4.y, d4.z), lp = mk(l4.x, l4.y, l4.z);
-        bool occluded = false;
-        for (int step = 0; step < 4; step++) {
-            const Best b = closest_fast<false>(S, V, so, sd, 0.001f, d4.w, stk, threadIdx.x, THREADS);
-            if (b.object == AE_MISS) break;
-            if (b.t >= AE_SUB(distance(lp, so), 0.001f)) break;
-            const uint32_t mt = load_head(S.objects + b.object).material;
-            if (mt == AE_MAT_DIFFUSE_LIGHT) break;
-            if (mt != AE_MAT_DIELECTRIC) { occluded = true; break; }
-            so = (so + sd * b.t) + sd * 0.001f;
-        }
-        W.sh_occ[e] = occluded ? 1 : 0;
+        const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
+        const bool occluded = shadow_occluded(S, V, mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z), mk(l4.x, l4.y, l4.z),
+                                              d4.w, stk, threadIdx.x, THREADS);
+        W.sh.occ[e] = occluded ? 1 : 0;
     }
 }
 
@@ -391,16 +243,7 @@ __global__ void __launch_bounds__(256) k_wf_connect(WfView W, int bounce) {
         const uint32_t pid = W.qpid[q][k];
         if (!W.nee[pid]) continue;
         W.nee[pid] = 0;
-        f3 dl = splat(0.0f);
-        for (uint32_t i = 0; i < P.n_lights; i++) {
-            const size_t e = size_t(pid) * P.n_lights + i;
-            if (W.sh_valid[e] && !W.sh_occ[e]) {
-                const float4 c = W.sh_c[e];
-                dl = dl + mk(c.x, c.y, c.z);
-            }
-        }
-        const float luma = maxc(dl);
-        if (luma > 8.0f) dl = dl * AE_DIV(8.0f, luma);
+        const f3 dl = nee_total(W.sh, size_t(pid) * P.n_lights, P.n_lights);
         const float4 t4 = W.pend[pid], a4 = W.acc[pid];
         const f3 acc = mk(a4.x, a4.y, a4.z) + mk(t4.x, t4.y, t4.z) * dl;
         W.acc[pid] = make_float4(acc.x, acc.y, acc.z, 0.0f);
@@ -472,8 +315,7 @@ static WfView view_of(Ctx *c) {
     W.thr = Wf.thr.ptr; W.acc = Wf.acc.ptr; W.col = Wf.col.ptr; W.pend = Wf.pend.ptr;
     W.seed = Wf.seed.ptr;
     W.nee = Wf.nee.ptr;
-    W.sh_o = Wf.sh_o.ptr; W.sh_d = Wf.sh_d.ptr; W.sh_lp = Wf.sh_lp.ptr; W.sh_c = Wf.sh_c.ptr;
-    W.sh_valid = Wf.sh_valid.ptr; W.sh_occ = Wf.sh_occ.ptr;
+    W.sh = ShadowStore{Wf.sh_o.ptr, Wf.sh_d.ptr, Wf.sh_lp.ptr, Wf.sh_c.ptr, Wf.sh_valid.ptr, Wf.sh_occ.ptr};
     W.sq = Wf.sq.ptr;
     W.cnt = Wf.cnt.ptr;
     W.P = Wf.params.ptr;

@@ -1,0 +1,199 @@
+// wf_common.cuh - device pieces shared by the queue-driven path tracers (the
+// wavefront frame renderer and the serving loop): warp-aggregated queue
+// appends, bulk-copy staging on an mbarrier, and ColorRay's per-vertex work
+// (hybrid:1230-1325) split at the traversals so the shadow tests can run as
+// their own queue.
+//
+// Every arithmetic step is the plain megakernel's (trace_plain.cu,
+// color_ray), in the same order, so a path traced through these pieces gives
+// the plain kernel's radiance bit for bit.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fast_trace.cuh"
+#include "shade.cuh"
+#include "trace_common.cuh"
+
+namespace ae {
+
+// ---------------------------------------------------------------------------
+// Warp-aggregated queue append: one atomic per warp, lanes get consecutive
+// slots in lane order.
+// ---------------------------------------------------------------------------
+AE_DEV uint32_t warp_append(uint32_t *counter, uint32_t want) {
+    const uint32_t lane = threadIdx.x & 31;
+    const unsigned mask = __activemask();
+    // inclusive prefix of `want` over the active lanes
+    uint32_t incl = want;
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t v = __shfl_up_sync(mask, incl, off);
+        if (lane >= uint32_t(off) && ((mask >> (lane - off)) & 1u)) incl += v;
+    }
+    const int leader = 31 - __clz(mask);  // highest active lane holds the total
+    uint32_t base = 0;
+    if (int(lane) == leader) base = atomicAdd(counter, incl);
+    base = __shfl_sync(mask, base, leader);
+    return base + incl - want;
+}
+
+// ---------------------------------------------------------------------------
+// Bulk-copy staging of a queue tile into shared memory (no multicast).
+// ---------------------------------------------------------------------------
+AE_DEV uint32_t smem_addr(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+AE_DEV void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+AE_DEV void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+AE_DEV void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+// Waits for `phase` to complete; gives up after `limit` polls and reports it.
+AE_DEV bool mbar_wait(uint64_t *bar, uint32_t phase, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// ColorRay split at its traversals
+// ---------------------------------------------------------------------------
+
+// Light samples of one path vertex: entry e holds the shadow ray (origin +
+// tnear, direction + time), the sampled light point, the contribution if
+// unoccluded, and the valid / occluded flags.
+struct ShadowStore {
+    float4 *o, *d, *lp, *c;
+    uint8_t *valid, *occ;
+};
+
+// Everything at one path vertex after its closest hit: sky or emission on a
+// miss or a light, the light samples of a Lambertian surface (entries
+// e0 .. e0 + n_lights - 1, throughput at the vertex into *pend, *nee set),
+// then the bounce and Russian roulette.  Returns whether the path goes on,
+// with its next ray in `nr`; `n_shadow` counts the valid light samples.
+AE_DEV bool shade_vertex(const DevScene &S, const f3 &sky, uint32_t depth, uint32_t n_lights, int bounce,
+                         const ae_ray &r, const ae_hit &hr, f3 &thr, f3 &acc, uint32_t &seed, const ShadowStore &SH,
+                         size_t e0, uint8_t *nee, float4 *pend, uint32_t &n_shadow, ae_ray &nr) {
+    const f3 o = mk(r.ox, r.oy, r.oz), d = mk(r.dx, r.dy, r.dz);
+    n_shadow = 0;
+    nr = r;
+    DHit h;
+    if (!surface_from_hit(S, hr, o, d, r.time, h)) {
+        acc = acc + thr * sky;
+        return false;
+    }
+    const MatRec m = load_mat(S.objects + h.slot);
+    if (m.type == AE_MAT_DIFFUSE_LIGHT) {
+        acc = acc + thr * (m.emission * m.albedo);
+        return false;
+    }
+    if (m.type == AE_MAT_LAMBERTIAN) {
+        // Light samples in light order (CalculateDirectLight,
+        // hybrid:1122-1212); occlusion is resolved by the shadow stage.
+        *nee = 1;
+        *pend = make_float4(thr.x, thr.y, thr.z, 0.0f);
+        for (uint32_t i = 0; i < n_lights; i++) {
+            const size_t e = e0 + i;
+            const ae_object *L = S.objects + __ldg(S.lights + i);
+            const ObjHead lh = load_head(L);
+            f3 lp;
+            float omega;
+            sample_light(L, lh.shape, h.p, lp, omega, seed);
+            uint8_t valid = 0;
+            if (omega > 0.0f) {
+                f3 sd = lp - h.p;
+                const float dist = length(sd);
+                if (dist > 1e-6f) {
+                    sd = sd / dist;
+                    const float ct = dot(h.n, sd);
+                    if (ct > 0.0f) {
+                        const MatRec lm = load_mat(L);
+                        const f3 rad = lm.emission * lm.albedo;
+                        const f3 c = m.albedo * rad * ct * omega;
+                        const f3 so = h.p + h.n * 0.001f;
+                        SH.o[e] = make_float4(so.x, so.y, so.z, 0.001f);
+                        SH.d[e] = make_float4(sd.x, sd.y, sd.z, r.time);
+                        SH.lp[e] = make_float4(lp.x, lp.y, lp.z, 0.0f);
+                        SH.c[e] = make_float4(c.x, c.y, c.z, 0.0f);
+                        valid = 1;
+                        n_shadow++;
+                    }
+                }
+            }
+            SH.valid[e] = valid;
+            SH.occ[e] = 0;
+        }
+    }
+    f3 sd;
+    if (!get_bounce(d, h, m, sd, seed)) return false;
+    const f3 nd = normalize(sd);
+    const float sgn = dot(nd, h.n) < 0.0f ? -1.0f : 1.0f;
+    const f3 no = h.p + h.n * AE_MUL(0.001f, sgn);
+    if (m.type != AE_MAT_DIELECTRIC) thr = thr * m.albedo;
+    if (bounce > 0) {
+        const float p = clampf(maxc(thr), 0.1f, 1.0f);
+        if (rng_next(seed) > p) return false;
+        thr = thr / p;
+    }
+    if (uint32_t(bounce + 1) >= depth) return false;
+    nr.ox = no.x; nr.oy = no.y; nr.oz = no.z; nr.tnear = 0.001f;
+    nr.dx = nd.x; nr.dy = nd.y; nr.dz = nd.z;
+    return true;
+}
+
+// Writes the indices of the valid light samples e0 .. e0 + n_lights - 1 to
+// the shadow queue from `base` on, in light order.
+AE_DEV void push_shadow_entries(const ShadowStore &SH, uint32_t e0, uint32_t n_lights, uint32_t *sq, uint32_t base) {
+    uint32_t j = 0;
+    for (uint32_t i = 0; i < n_lights; i++)
+        if (SH.valid[e0 + i]) sq[base + j++] = e0 + i;
+}
+
+// The reference's shadow test (hybrid:1167-1191): up to four closest hits,
+// stepping through glass; lights and anything beyond the light point do not
+// block.
+AE_DEV bool shadow_occluded(const DevScene &S, const FastView &V, f3 so, const f3 &sd, const f3 &lp, float time,
+                            uint2 *stk, int tid, int nthreads) {
+    for (int step = 0; step < 4; step++) {
+        const Best b = closest_fast<false>(S, V, so, sd, 0.001f, time, stk, tid, nthreads);
+        if (b.object == AE_MISS) return false;
+        if (b.t >= AE_SUB(distance(lp, so), 0.001f)) return false;
+        const uint32_t mt = load_head(S.objects + b.object).material;
+        if (mt == AE_MAT_DIFFUSE_LIGHT) return false;
+        if (mt != AE_MAT_DIELECTRIC) return true;
+        so = (so + sd * b.t) + sd * 0.001f;
+    }
+    return false;
+}
+
+// NEE of one vertex: unoccluded contributions in light order, then the luma
+// clamp of 8 (hybrid:1207-1210).
+AE_DEV f3 nee_total(const ShadowStore &SH, size_t e0, uint32_t n_lights) {
+    f3 dl = splat(0.0f);
+    for (uint32_t i = 0; i < n_lights; i++) {
+        const size_t e = e0 + i;
+        if (SH.valid[e] && !SH.occ[e]) {
+            const float4 c = SH.c[e];
+            dl = dl + mk(c.x, c.y, c.z);
+        }
+    }
+    const float luma = maxc(dl);
+    if (luma > 8.0f) dl = dl * AE_DIV(8.0f, luma);
+    return dl;
+}
+
+}  // namespace ae

@@ -21,6 +21,9 @@ Workloads (all inputs seeded; no dataset is involved):
                    emissive quads above the field.
   hybrid_box       the Cornell box plus analytic spheres and boxes, for the
                    hybrid renderer's raster/analytic split.
+  serving_scenes   8 scenes built like wavefront_scene with 50k to 5M unique
+                   triangles and 512 instances each (4096 in all), whose
+                   instances move along seeded random walks (random_walk).
 """
 import ctypes
 
@@ -412,3 +415,42 @@ def wavefront_scene(seed=4, width=1920, height=1080, depth=12, n_meshes=32, n_in
     cfg = make_config(width, height, (100.0, 90.0, 330.0), (100.0, 30.0, 100.0), fov=40.0, depth=depth,
                       sky=(0.0, 0.0, 0.0))
     return _finish(ents, meshes, cfg, "wavefront_scene")
+
+
+SERVING_TRIANGLES = (50_000, 120_000, 250_000, 500_000, 1_000_000, 2_000_000, 3_500_000, 5_000_000)
+
+
+def serving_scenes(seed=5, tri_targets=SERVING_TRIANGLES, instances_per_scene=512, depth=8, n_meshes=8):
+    """The serving workload's resident scenes: wavefront_scene's generators
+    and material mix at each triangle budget, `instances_per_scene` instances
+    each, 16 emissive quads."""
+    return [wavefront_scene(seed=seed + k, width=640, height=480, depth=depth, n_meshes=n_meshes,
+                            n_instances=instances_per_scene, n_lights=16, target_tris=t)
+            for k, t in enumerate(tri_targets)]
+
+
+def random_walk(instances, rng, step=0.5, angle=0.05):
+    """One step of every instance along a seeded random walk: a normal
+    translation of `step` per axis and a rotation by a small random angle
+    about a random axis; meshes, bases and scale are kept."""
+    out = np.array(instances, copy=True)
+    n = len(out)
+    d = rng.normal(0.0, step, (n, 3)).astype(np.float32)
+    out["px"] += d[:, 0]
+    out["py"] += d[:, 1]
+    out["pz"] += d[:, 2]
+    axis = rng.normal(0.0, 1.0, (n, 3))
+    axis /= np.linalg.norm(axis, axis=1, keepdims=True)
+    th = rng.normal(0.0, angle, n) * 0.5
+    dq = np.concatenate([axis * np.sin(th)[:, None], np.cos(th)[:, None]], axis=1)
+    q = np.stack([out["qx"], out["qy"], out["qz"], out["qw"]], axis=1).astype(np.float64)
+    # Hamilton product dq * q (x, y, z, w order).
+    x1, y1, z1, w1 = dq.T
+    x2, y2, z2, w2 = q.T
+    r = np.stack([w1 * x2 + x1 * w2 + y1 * z2 - z1 * y2,
+                  w1 * y2 - x1 * z2 + y1 * w2 + z1 * x2,
+                  w1 * z2 + x1 * y2 - y1 * x2 + z1 * w2,
+                  w1 * w2 - x1 * x2 - y1 * y2 - z1 * z2], axis=1)
+    r /= np.linalg.norm(r, axis=1, keepdims=True)
+    out["qx"], out["qy"], out["qz"], out["qw"] = (r[:, k].astype(np.float32) for k in range(4))
+    return out

@@ -443,6 +443,113 @@ int ae_refit_instances(ae_ctx *ctx, const ae_instance *instances, uint32_t n);
  * pointers are skipped. */
 int ae_download_scene(ae_ctx *ctx, ae_object *objects, ae_bvh_node *tlas, ae_instance *instances);
 
+/* ------------------------------------------------------------------------ */
+/* Render serving (no counterpart in the reference, which renders one scene  */
+/* for one window per process)                                               */
+/* ------------------------------------------------------------------------ */
+
+/* A server keeps several scenes resident on one GPU and renders frame
+ * requests against them with continuous batching: a fixed pool of path slots
+ * is shared by every admitted request, one merged ray queue carries rays of
+ * all requests and scenes, and a request is admitted as soon as resident
+ * slots and image memory free up, while others are still on the GPU.  Each
+ * slot renders all samples of one pixel in order, so a request's image does
+ * not depend on what else is being served: it equals `frames` compute-only
+ * frames (Batch = 0 .. frames-1) of ae_render_frame on the same scene and
+ * config, bit for bit.
+ *
+ * Threading: the server runs a scheduler thread and a completion thread;
+ * every ae_serve_* call may be made from any thread.  A context handed to
+ * ae_serve_add_scene belongs to the server until ae_serve_destroy (no other
+ * call may use it meanwhile) and must outlive the server. */
+typedef struct ae_server ae_server;
+
+typedef struct ae_serve_settings {
+    int32_t device;
+    uint32_t slots;            /* paths in flight over all requests; 0 = 1,048,576 */
+    uint32_t max_lights;       /* light samples per path vertex; 0 = 16, at most 64 */
+    uint32_t max_requests;     /* requests resident at once; 0 = 64, at most 1024 */
+    uint64_t arena_bytes;      /* device memory for request images; 0 = 1 GiB */
+    uint32_t ticks_per_launch; /* queue ticks per graph replay (even); 0 = 4 */
+    uint32_t extend_threads;   /* 64, 128 or 256; 0 = 64 */
+    uint32_t max_scenes;       /* resident scenes; 0 = 16 */
+    uint32_t reserved[5];
+} ae_serve_settings;
+
+typedef struct ae_serve_request {
+    uint32_t scene;            /* id from ae_serve_add_scene */
+    uint32_t width, height;    /* image size (overrides config.width/height) */
+    uint32_t frames;           /* progressive frames; spp = frames x samples */
+    ae_config config;          /* camera, samples per frame, depth, sky, exposure; batch is ignored */
+    float *accum;              /* host destination: width*height RGBA float32, or NULL */
+    uint8_t *display;          /* host destination: width*height RGBA8, or NULL */
+    uint64_t user;             /* opaque tag returned in the result */
+} ae_serve_request;
+
+typedef struct ae_serve_result {
+    uint64_t id, user;
+    int32_t status;            /* AE_OK, or why the request failed */
+    uint32_t scene_version;    /* instance moves of the scene applied before it */
+    double submit_ms, admit_ms, done_ms;  /* server clock: ms since ae_serve_create */
+    uint64_t paths;            /* width * height * frames * samples per frame */
+    uint64_t footprint;        /* bytes of image memory it held */
+} ae_serve_result;
+
+typedef struct ae_serve_stats {
+    uint64_t submitted, completed, rejected, failed;
+    uint64_t paths;            /* paths of completed requests */
+    uint64_t rays;             /* closest-hit rays traced (extend + shadow tests) */
+    double first_submit_ms, last_done_ms;
+    double p50_ms, p99_ms, mean_ms, max_ms;  /* latency: submit -> result in host memory */
+    uint64_t launches;         /* graph replays */
+    uint64_t peak_arena_bytes;
+    uint32_t peak_resident, moves_applied;
+    uint32_t errors;           /* device error flags (bounded waits that gave up) */
+    uint32_t pad;
+} ae_serve_stats;
+
+ae_server *ae_serve_create(const ae_serve_settings *settings);
+/* Stops the threads; queued requests fail with AE_ERR_STATE. */
+void ae_serve_destroy(ae_server *srv);
+const char *ae_serve_last_error(ae_server *srv);
+/* Makes an uploaded context's scene resident (prepares its optimised BVH). */
+int ae_serve_add_scene(ae_server *srv, ae_ctx *scene, uint32_t *scene_id);
+/* Queues a request; AE_ERR_REJECTED when its images exceed the whole arena. */
+int ae_serve_submit(ae_server *srv, const ae_serve_request *req, uint64_t *id);
+/* Queues new transforms for every instance of a scene (refit on the GPU);
+ * requests submitted earlier render the old ones, later ones the new. */
+int ae_serve_move_instances(ae_server *srv, uint32_t scene, const ae_instance *instances, uint32_t n);
+/* Waits for a request (timeout_ms < 0: forever); returns its status, or
+ * AE_ERR_TIMEOUT.  The record is released once it has been returned. */
+int ae_serve_wait(ae_server *srv, uint64_t id, int32_t timeout_ms, ae_serve_result *out);
+/* Waits until every submitted request and move has finished. */
+int ae_serve_drain(ae_server *srv, int32_t timeout_ms);
+int ae_serve_get_stats(ae_server *srv, ae_serve_stats *out);
+/* Clears latency samples and counters (not the resident scenes). */
+int ae_serve_reset_stats(ae_server *srv);
+
+/* The admission policy of the server run on a synthetic event list on the
+ * host, with no GPU: requests (footprint, service ticks) and instance moves
+ * arrive at ticks; out[i] tells when each was admitted / applied and done. */
+enum { AE_POLICY_REQUEST = 0, AE_POLICY_MOVE = 1 };
+typedef struct ae_policy_event {
+    uint32_t kind;             /* AE_POLICY_REQUEST or AE_POLICY_MOVE */
+    uint32_t scene;
+    uint32_t tick;             /* arrival; non-decreasing over the list */
+    uint32_t service_ticks;    /* requests: ticks on the GPU once admitted */
+    uint64_t footprint;        /* requests: image bytes */
+} ae_policy_event;
+typedef struct ae_policy_outcome {
+    int32_t admit_tick;        /* -1 = never; moves: the tick it was applied */
+    int32_t done_tick;
+    uint32_t version;          /* requests: moves of the scene before it; moves: version after */
+    int32_t status;            /* AE_OK or AE_ERR_REJECTED */
+    uint64_t offset;           /* requests: arena offset */
+} ae_policy_outcome;
+int ae_serve_policy_simulate(const ae_policy_event *events, uint32_t n, uint64_t arena_bytes,
+                             uint32_t max_resident, uint32_t n_scenes, uint32_t max_ticks,
+                             ae_policy_outcome *out);
+
 #ifdef __cplusplus
 } /* extern "C" */
 
@@ -469,6 +576,12 @@ static_assert(offsetof(ae_config, prevViewProj) == 176, "Config layout");
 static_assert(sizeof(ae_config) == 240, "Config size");
 static_assert(sizeof(ae_ray) == 32, "ray record");
 static_assert(sizeof(ae_hit) == 20, "hit record");
+static_assert(sizeof(ae_serve_settings) == 56, "serve settings");
+static_assert(sizeof(ae_serve_request) == 280, "serve request");
+static_assert(sizeof(ae_serve_result) == 64, "serve result");
+static_assert(sizeof(ae_serve_stats) == 128, "serve stats");
+static_assert(sizeof(ae_policy_event) == 24, "policy event");
+static_assert(sizeof(ae_policy_outcome) == 24, "policy outcome");
 #endif
 
 #endif /* AE_B200_H */

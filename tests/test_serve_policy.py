@@ -1,0 +1,123 @@
+"""Admission policy of the render server, run on the host through
+ae_serve_policy_simulate (the same C++ Policy and Arena the server's scheduler
+thread uses; no GPU)."""
+import numpy as np
+import pytest
+
+from aviatorengine2_b200 import _lib
+from aviatorengine2_b200.serving import simulate_policy
+
+MB = 1 << 20
+
+
+def _req(tick, fp, service, scene=0):
+    return dict(kind=_lib.POLICY_REQUEST, tick=tick, footprint=fp, service_ticks=service, scene=scene)
+
+
+def _move(tick, scene=0):
+    return dict(kind=_lib.POLICY_MOVE, tick=tick, scene=scene)
+
+
+def _align(x):
+    return (x + 255) // 256 * 256
+
+
+def _check_invariants(events, out, arena, max_resident):
+    reqs = [i for i, e in enumerate(events) if e["kind"] == _lib.POLICY_REQUEST and out[i]["status"] == 0]
+    last = max([int(out[i]["done_tick"]) for i in range(len(events))] + [0])
+    for t in range(last + 1):
+        live = [i for i in reqs if out[i]["admit_tick"] <= t <= out[i]["done_tick"]]
+        assert len(live) <= max_resident
+        spans = sorted((int(out[i]["offset"]), int(out[i]["offset"]) + _align(events[i]["footprint"])) for i in live)
+        assert all(a[1] <= b[0] for a, b in zip(spans, spans[1:])), f"overlapping blocks at tick {t}"
+        assert all(hi <= arena for _, hi in spans)
+    for i in reqs:
+        assert out[i]["admit_tick"] >= events[i]["tick"]
+        assert out[i]["done_tick"] - out[i]["admit_tick"] + 1 == max(events[i]["service_ticks"], 1)
+
+
+def test_fifo_by_footprint():
+    ev = [_req(0, 40 * MB, 3) for _ in range(5)]
+    code, out = simulate_policy(ev, 100 * MB, 16, 1)
+    assert code == 0
+    admits = [int(o["admit_tick"]) for o in out]
+    assert admits == sorted(admits)            # arrival order
+    assert admits[:2] == [0, 0] and admits[2] == 3  # two fit, the third waits for a release
+    _check_invariants(ev, out, 100 * MB, 16)
+
+
+def test_large_request_is_not_starved():
+    # A large request at the head blocks later small ones until it fits.
+    ev = [_req(0, 60 * MB, 4), _req(1, 60 * MB, 2), _req(1, 1 * MB, 1), _req(1, 1 * MB, 1)]
+    code, out = simulate_policy(ev, 100 * MB, 16, 1)
+    assert code == 0
+    assert out[1]["admit_tick"] == 4
+    assert out[2]["admit_tick"] >= out[1]["admit_tick"]
+    _check_invariants(ev, out, 100 * MB, 16)
+
+
+def test_resident_limit():
+    ev = [_req(0, 1 * MB, 2) for _ in range(7)]
+    code, out = simulate_policy(ev, 100 * MB, 3, 1)
+    assert code == 0
+    _check_invariants(ev, out, 100 * MB, 3)
+    assert sorted(int(o["admit_tick"]) for o in out) == [0, 0, 0, 2, 2, 2, 4]
+
+
+def test_oversize_rejected():
+    ev = [_req(0, 200 * MB, 1), _req(0, 1 * MB, 1)]
+    code, out = simulate_policy(ev, 100 * MB, 4, 1)
+    assert code == 0
+    assert out[0]["status"] == -8  # AE_ERR_REJECTED
+    assert out[0]["admit_tick"] == -1
+    assert out[1]["admit_tick"] == 0
+
+
+def test_move_waits_for_earlier_requests_of_its_scene():
+    ev = [_req(0, 1 * MB, 5, scene=0), _req(0, 1 * MB, 2, scene=0), _move(1, scene=0),
+          _req(1, 1 * MB, 1, scene=0), _req(1, 1 * MB, 1, scene=1), _req(2, 1 * MB, 1, scene=0)]
+    code, out = simulate_policy(ev, 100 * MB, 16, 2)
+    assert code == 0
+    # the move applies only after both earlier scene-0 requests finished
+    assert out[2]["admit_tick"] > max(out[0]["done_tick"], out[1]["done_tick"])
+    assert out[2]["version"] == 1
+    # later scene-0 requests see the move; scene 1 is not held up
+    for i in (3, 5):
+        assert out[i]["version"] == 1 and out[i]["admit_tick"] >= out[2]["admit_tick"]
+    assert out[4]["version"] == 0 and out[4]["admit_tick"] == 1
+    _check_invariants(ev, out, 100 * MB, 16)
+
+
+def test_back_to_back_moves_apply_in_order():
+    ev = [_move(0), _move(0), _req(0, 1 * MB, 1), _move(1), _req(1, 1 * MB, 1)]
+    code, out = simulate_policy(ev, 100 * MB, 16, 1)
+    assert code == 0
+    assert out[0]["version"] == 1 and out[1]["version"] == 2
+    assert out[2]["version"] == 2 and out[4]["version"] == 3
+    assert out[3]["admit_tick"] > out[2]["done_tick"]
+    assert out[4]["admit_tick"] >= out[3]["admit_tick"]
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3])
+def test_random_streams_keep_invariants(seed):
+    rng = np.random.default_rng(seed)
+    ev, t = [], 0
+    for _ in range(300):
+        t += int(rng.poisson(1.0))
+        if rng.random() < 0.1:
+            ev.append(_move(t, scene=int(rng.integers(0, 4))))
+        else:
+            ev.append(_req(t, int(rng.choice([1, 4, 16, 33]) * MB), int(rng.integers(1, 8)), scene=int(rng.integers(0, 4))))
+    code, out = simulate_policy(ev, 64 * MB, 8, 4)
+    assert code == 0
+    _check_invariants(ev, out, 64 * MB, 8)
+    # every request renders the version of its scene current at its arrival
+    moves_before = {s: 0 for s in range(4)}
+    for i, e in enumerate(ev):
+        if e["kind"] == _lib.POLICY_MOVE:
+            moves_before[e["scene"]] += 1
+            # applied after every earlier request of that scene finished
+            earlier = [j for j in range(i) if ev[j]["kind"] == _lib.POLICY_REQUEST and ev[j]["scene"] == e["scene"]]
+            assert all(out[j]["done_tick"] < out[i]["admit_tick"] for j in earlier)
+        else:
+            assert out[i]["version"] == moves_before[e["scene"]]
