@@ -57,7 +57,7 @@ MESH_RANGE = np.dtype([("vertexBase", "<u4"), ("indexBase", "<u4"), ("triangleCo
 
 SERVE_SETTINGS = np.dtype([("device", "<i4"), ("slots", "<u4"), ("max_lights", "<u4"), ("max_requests", "<u4"),
                            ("arena_bytes", "<u8"), ("ticks_per_launch", "<u4"), ("extend_threads", "<u4"),
-                           ("max_scenes", "<u4"), ("reserved", "<u4", 5)])
+                           ("max_scenes", "<u4"), ("claim_policy", "<u4"), ("reserved", "<u4", 4)])
 SERVE_REQUEST = np.dtype([("scene", "<u4"), ("width", "<u4"), ("height", "<u4"), ("frames", "<u4"),
                           ("config", CONFIG), ("accum", "<u8"), ("display", "<u8"), ("user", "<u8")])
 SERVE_RESULT = np.dtype([("id", "<u8"), ("user", "<u8"), ("status", "<i4"), ("scene_version", "<u4"),
@@ -84,9 +84,10 @@ MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_DIFFUSE_LIGHT, MAT_ISOTROPIC = ra
 NO_TEXTURE = 0xFFFFFFFF
 MISS = 0xFFFFFFFF
 VARIANT_PLAIN, VARIANT_FAST, VARIANT_QUANT = 0, 1, 2
-MODE_COMPUTE_ONLY, MODE_DEFERRED, MODE_WAVEFRONT = 0, 1, 2
+MODE_COMPUTE_ONLY, MODE_DEFERRED, MODE_WAVEFRONT, MODE_WAVEFRONT_PRECISION = 0, 1, 2, 3
 IMAGE_ACCUM, IMAGE_DISPLAY, IMAGE_FRAME, IMAGE_REDUCED, IMAGE_HISTORY_GEOMETRY = range(5)
 POLICY_REQUEST, POLICY_MOVE = 0, 1
+CLAIM_OLDEST_FIRST, CLAIM_SHARED = 0, 1
 STATUS = {0: "AE_OK", -1: "AE_ERR_INVALID", -2: "AE_ERR_OOM", -3: "AE_ERR_OVERSIZE", -4: "AE_ERR_LAYOUT",
           -5: "AE_ERR_CUDA", -6: "AE_ERR_TIMEOUT", -7: "AE_ERR_STATE", -8: "AE_ERR_REJECTED"}
 
@@ -118,6 +119,7 @@ SIGNATURES = {
     "ae_render_frame": (_I, [_P, _I, _P]),
     "ae_build_gbuffer": (_I, [_P]),
     "ae_read_image": (_I, [_P, _I, _P, ctypes.c_size_t]),
+    "ae_image_error": (_I, [_P, _I, _P, ctypes.c_double, _P]),
     "ae_closest_hit": (_I, [_P, _P, _U32, _P, _I]),
     "ae_closest_hit_device": (_I, [_P, _P, _U32, _P, _I]),
     "ae_closest_hit_noalloc": (_I, [_P, _P, _U32, _P, _I]),
@@ -144,7 +146,7 @@ SIGNATURES = {
     "ae_serve_drain": (_I, [_P, ctypes.c_int32]),
     "ae_serve_get_stats": (_I, [_P, _P]),
     "ae_serve_reset_stats": (_I, [_P]),
-    "ae_serve_policy_simulate": (_I, [_P, _U32, ctypes.c_uint64, _U32, _U32, _U32, _P]),
+    "ae_serve_policy_simulate": (_I, [_P, _U32, ctypes.c_uint64, _U32, _U32, _U32, _U32, _P]),
 }
 
 _lib = None

@@ -350,7 +350,9 @@ int ae_render_frame(ae_ctx *ctx, int mode, const ae_gbuffer *gb) {
     case AE_MODE_DEFERRED:
         return render_deferred(c, gb);
     case AE_MODE_WAVEFRONT:
-        return render_wavefront(c);
+        return render_wavefront(c, false);
+    case AE_MODE_WAVEFRONT_PRECISION:
+        return render_wavefront(c, true);
     default:
         return c->fail(AE_ERR_INVALID, "unknown render mode %d", mode);
     }

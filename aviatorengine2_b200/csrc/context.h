@@ -112,7 +112,7 @@ int prepare_variant(Ctx *c, int variant);
 int closest_hit_dispatch(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, int variant, cudaStream_t st,
                          bool timed);
 int render_deferred(Ctx *c, const ae_gbuffer *gb);
-int render_wavefront(Ctx *c);
+int render_wavefront(Ctx *c, bool precision);
 int read_image_extra(Ctx *c, int which, void *dst, size_t bytes);
 
 }  // namespace ae

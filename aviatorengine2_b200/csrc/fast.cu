@@ -30,6 +30,7 @@
 // correctly rounded binary32, so t and the barycentrics are bit-identical to
 // the plain kernel's; the watertight variant (Woop, Benthin and Wald, "Watertight
 // Ray/Triangle Intersection", JCGT 2013) is selected with `quant`.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -325,6 +326,45 @@ int prepare_fast(Ctx *c) {
     if (F.has_volumes)
         return c->fail(AE_ERR_STATE, "participating media consume RNG in the reference's visit order; use the plain kernel");
     c->fast_ready = true;
+    return AE_OK;
+}
+
+// The precision form's shading records: per triangle, in the optimised
+// BVH's slot order, the three vertex normals and UVs rounded to FP16
+// (round to nearest even), 32 bytes (layout in wf_common.cuh).
+int prepare_precision(Ctx *c) {
+    int rc = prepare_fast(c);
+    if (rc) return rc;
+    FastScene &F = *c->fast;
+    if (F.shade16_tris == F.n_tris && F.shade16.ptr) return AE_OK;
+    std::vector<uint16_t> h(size_t(std::max(F.n_tris, 1u)) * 16, 0);
+    auto half_bits = [](float x) {
+        const __half v = __float2half_rn(x);
+        uint16_t b;
+        std::memcpy(&b, &v, 2);
+        return b;
+    };
+    for (const auto &kv : F.mesh_roots) {
+        const uint32_t vbase = std::get<0>(kv.first), ibase = std::get<1>(kv.first), tris = std::get<2>(kv.first);
+        const uint32_t tri_base = kv.second.second;
+        for (uint32_t t = 0; t < tris; t++) {
+            uint16_t *r = h.data() + (size_t(tri_base) + t) * 16;
+            for (int v = 0; v < 3; v++) {
+                const ae_vertex &vx = c->host_vertices[vbase + c->host_indices[ibase + 3 * t + v]];
+                r[3 * v + 0] = half_bits(vx.nx);
+                r[3 * v + 1] = half_bits(vx.ny);
+                r[3 * v + 2] = half_bits(vx.nz);
+                r[9 + 2 * v] = half_bits(vx.u);
+                r[10 + 2 * v] = half_bits(vx.v);
+            }
+        }
+    }
+    if (F.shade16.reserve(size_t(std::max(F.n_tris, 1u)) * 2)) return c->fail(AE_ERR_OOM, "FP16 shading records");
+    if ((rc = c->cuda(cudaMemcpyAsync(F.shade16.ptr, h.data(), h.size() * 2, cudaMemcpyHostToDevice, c->stream),
+                      "upload FP16 shading records")))
+        return rc;
+    if ((rc = c->cuda(cudaStreamSynchronize(c->stream), "FP16 shading records"))) return rc;
+    F.shade16_tris = F.n_tris;
     return AE_OK;
 }
 

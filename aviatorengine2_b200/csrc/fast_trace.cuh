@@ -49,6 +49,8 @@ struct FastScene {
     DevBuf<float4> tris;     // 3 float4 per triangle
     DevBuf<FastInst> inst;
     DevBuf<uint4> obj_meta;  // per object slot: shape | material << 8, instance
+    DevBuf<uint4> shade16;   // precision form: FP16 normals and UVs, 2 per triangle
+    uint32_t shade16_tris = 0;
     uint32_t n_nodes = 0, n_tris = 0;
     int max_stack = 0;
     uint64_t geometry_key = 0, scene_key = ~0ull;

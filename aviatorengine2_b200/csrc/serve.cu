@@ -100,6 +100,7 @@ struct SvView {
     ShadowStore sh;  // entry = slot * max_lights + light
     uint32_t *sq;
     uint32_t max_lights;
+    uint32_t claim_shared;  // 1: each warp starts its claim at a different request
 };
 
 __global__ void k_sv_init(SvView W, uint32_t slots) {
@@ -180,7 +181,8 @@ __global__ void __launch_bounds__(256) k_sv_shade(SvView W, int q) {
         const uint32_t slot = W.qslot[q][k];
         const ae_ray r = W.qray[q][k];
         const ae_hit hr = W.qhit[k];
-        const DevScene S = W.scenes[W.s_scene[slot]].S;
+        const SceneRec &SR = W.scenes[W.s_scene[slot]];
+        const DevScene S = SR.S;
         const ReqDev &R = W.reqs[W.s_req[slot]];
         const int bounce = int(W.s_bounce[slot]);
         const float4 t4 = W.s_thr[slot], a4 = W.s_acc[slot];
@@ -189,8 +191,8 @@ __global__ void __launch_bounds__(256) k_sv_shade(SvView W, int q) {
         ae_ray nr;
         uint32_t n_shadow;
         const uint32_t e0 = slot * W.max_lights;
-        const bool next = shade_vertex(S, R.F.sky, R.F.depth, S.n_lights, bounce, r, hr, thr, acc, seed, W.sh, e0,
-                                       W.s_nee + slot, W.s_pend + slot, n_shadow, nr);
+        const bool next = shade_vertex<false>(S, SR.V, PrecView{nullptr}, R.F.sky, R.F.depth, S.n_lights, bounce, r, hr,
+                                              thr, acc, seed, W.sh, e0, W.s_nee + slot, W.s_pend + slot, n_shadow, nr);
         W.s_thr[slot] = make_float4(thr.x, thr.y, thr.z, 0.0f);
         W.s_acc[slot] = make_float4(acc.x, acc.y, acc.z, 0.0f);
         W.s_seed[slot] = seed;
@@ -238,8 +240,9 @@ __global__ void __launch_bounds__(256) k_sv_connect(SvView W, int q) {
 }
 
 // Warp-cooperative claim: the lanes with `need` take consecutive pixels of
-// the oldest request that still has unclaimed ones, moving to the next
-// request when it runs out.  A request's counter is only advanced while it
+// the oldest request that still has unclaimed ones (with the shared policy:
+// of the first such request from a per-warp starting point in the admission
+// order), moving to the next request when it runs out.  A request's counter is only advanced while it
 // has pixels left, so it never runs far past its pixel count.  Every lane of
 // the calling warp that is in the loop must call this.
 AE_DEV bool claim_pixel(const SvView &W, bool need, uint32_t &req, uint32_t &pix) {
@@ -247,10 +250,12 @@ AE_DEV bool claim_pixel(const SvView &W, bool need, uint32_t &req, uint32_t &pix
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t n_order = W.cnt[SV_NORDER];
     bool got = false;
+    const uint32_t start =
+        W.claim_shared && n_order ? ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) % n_order : 0u;
     for (uint32_t i = 0; i < n_order; i++) {
         const unsigned want = __ballot_sync(mask, need && !got);
         if (!want) break;
-        const uint32_t r = W.order[i];
+        const uint32_t r = W.order[start + i < n_order ? start + i : start + i - n_order];
         const uint32_t n = W.reqs[r].n_pixels;
         const int leader = __ffs(want) - 1;
         uint32_t base = n;
@@ -393,8 +398,20 @@ struct HostReq {
 
 struct MoveOp {
     uint32_t scene;
+    uint32_t version = 0;  // the scene version this move creates
     std::vector<ae_instance> inst;
 };
+
+// One copy of a scene's per-frame arrays.  Version v of a scene is rendered
+// from copy v % 2, so a move is prepared in the other copy while requests of
+// the current version keep running.
+struct FrameSet {
+    DevBuf<ae_object> objects;
+    DevBuf<ae_bvh_node> tlas;
+    DevBuf<ae_instance> instances;
+    DevBuf<FastInst> inst;
+};
+constexpr uint32_t kFrameSets = 2;
 
 typedef void (*SvExtendFn)(SvView, int);
 
@@ -437,7 +454,7 @@ struct Server {
     std::string err;
     Policy policy;
     std::vector<Ctx *> scene_ctx;
-    std::vector<SceneRec> scene_rec;
+    std::vector<std::unique_ptr<FrameSet[]>> frame_sets;  // kFrameSets per scene
     std::map<uint64_t, std::unique_ptr<HostReq>> reqs;
     std::vector<std::deque<MoveOp>> moves;
     std::deque<HostReq *> copy_queue;
@@ -473,6 +490,7 @@ struct Server {
     void run_completer();
     void fail_all(int code, const std::string &why);
     int apply_move(MoveOp &m);
+    int fill_frame_set(uint32_t scene, uint32_t copy);
     ~Server();
 };
 
@@ -504,7 +522,7 @@ int Server::init() {
         qray.reserve(size_t(S) * 2) || qslot.reserve(size_t(S) * 2) || idle.reserve(size_t(S) * 2) ||
         qhit.reserve(S) || sh4.reserve(SL * 4) || sh8.reserve(SL * 2) || sq.reserve(SL) || cnt.reserve(SV_COUNT) ||
         next.reserve(R) || done.reserve(R) || order.reserve(R) || stats.reserve(ST_COUNT) ||
-        scenes_d.reserve(st.max_scenes) || reqs_d.reserve(R)) {
+        scenes_d.reserve(size_t(st.max_scenes) * kFrameSets) || reqs_d.reserve(R)) {
         err = "slot pool allocation failed";
         return AE_ERR_OOM;
     }
@@ -542,6 +560,7 @@ int Server::init() {
     W.sh = ShadowStore{sh4.ptr, sh4.ptr + SL, sh4.ptr + 2 * SL, sh4.ptr + 3 * SL, sh8.ptr, sh8.ptr + SL};
     W.sq = sq.ptr;
     W.max_lights = L;
+    W.claim_shared = st.claim_policy == AE_CLAIM_SHARED ? 1u : 0u;
     cudaMemsetAsync(next.ptr, 0, sizeof(uint32_t) * R, stream);
     cudaMemsetAsync(done.ptr, 0, sizeof(uint32_t) * R, stream);
     k_sv_init<<<sms * 4, 256, 0, stream>>>(W, S);
@@ -550,9 +569,9 @@ int Server::init() {
         err = "slot pool initialisation failed";
         return AE_ERR_CUDA;
     }
-    policy.configure(st.arena_bytes, st.max_requests);
+    policy.configure(st.arena_bytes, st.max_requests, kFrameSets);
     scene_ctx.reserve(st.max_scenes);
-    scene_rec.reserve(st.max_scenes);
+    frame_sets.reserve(st.max_scenes);
     moves.reserve(st.max_scenes);
     table.assign(R, nullptr);
     for (int i = int(R) - 1; i >= 0; i--) table_free.push_back(i);
@@ -604,27 +623,61 @@ int Server::build_graph() {
     return AE_OK;
 }
 
-// Applies one queued move: refit on the scene's context, then the optimised
-// instance records, then the scene's row of the device scene table.
+// Copies the scene context's current per-frame arrays into one of the
+// scene's frame sets and points that set's row of the device scene table at
+// it (geometry and the optimised BLAS stay shared).
+int Server::fill_frame_set(uint32_t scene, uint32_t copy) {
+    Ctx *c = scene_ctx[scene];
+    FrameSet &fs = frame_sets[scene][copy];
+    FastScene &F = *c->fast;
+    const size_t no = std::max<size_t>(c->n_objects, 1), nn = std::max<size_t>(c->n_nodes, 1),
+                 ni = std::max<size_t>(c->n_instances, 1);
+    if (fs.objects.reserve(no) || fs.tlas.reserve(nn) || fs.instances.reserve(ni) || fs.inst.reserve(ni))
+        return AE_ERR_OOM;
+    cudaStream_t cs = c->stream;
+    cudaError_t e = cudaSuccess;
+    if (c->n_objects)
+        e = cudaMemcpyAsync(fs.objects.ptr, c->objects.ptr, c->n_objects * sizeof(ae_object), cudaMemcpyDeviceToDevice, cs);
+    if (e == cudaSuccess && c->n_nodes)
+        e = cudaMemcpyAsync(fs.tlas.ptr, c->tlas.ptr, c->n_nodes * sizeof(ae_bvh_node), cudaMemcpyDeviceToDevice, cs);
+    if (e == cudaSuccess && c->n_instances)
+        e = cudaMemcpyAsync(fs.instances.ptr, c->instances.ptr, c->n_instances * sizeof(ae_instance),
+                            cudaMemcpyDeviceToDevice, cs);
+    if (e == cudaSuccess && c->n_instances)
+        e = cudaMemcpyAsync(fs.inst.ptr, F.inst.ptr, c->n_instances * sizeof(FastInst), cudaMemcpyDeviceToDevice, cs);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return AE_ERR_CUDA;
+    }
+    DevScene S = c->scene();
+    S.objects = fs.objects.ptr;
+    S.tlas = fs.tlas.ptr;
+    S.instances = fs.instances.ptr;
+    const SceneRec rec{S, FastView{F.nodes.ptr, F.tris.ptr, fs.inst.ptr, F.obj_meta.ptr}};
+    // Stream order puts the row before any replay that reads it.
+    if (cudaMemcpyAsync(scenes_d.ptr + size_t(scene) * kFrameSets + copy, &rec, sizeof(rec), cudaMemcpyHostToDevice,
+                        stream) != cudaSuccess) {
+        cudaGetLastError();
+        return AE_ERR_CUDA;
+    }
+    return AE_OK;
+}
+
+// Applies one queued move: refit on the scene's context (which always holds
+// the newest version), its optimised instance records, then a copy into the
+// frame set of the new version.
 int Server::apply_move(MoveOp &m) {
     Ctx *c = scene_ctx[m.scene];
     int rc = ae_refit_instances(reinterpret_cast<ae_ctx *>(c), m.inst.data(), uint32_t(m.inst.size()));
     if (rc == AE_OK) rc = prepare_fast(c);
     if (rc == AE_OK) rc = c->cuda(cudaStreamSynchronize(c->stream), "refit");
+    if (rc == AE_OK) rc = fill_frame_set(m.scene, m.version % kFrameSets);
     if (rc != AE_OK) {
         std::lock_guard<std::mutex> lk(mu);
-        err = "instance move: " + c->err;
-        return rc;
+        err = "instance move: " + (c->err.empty() ? std::string("frame set copy failed") : c->err);
     }
-    FastScene &F = *c->fast;
-    SceneRec rec{c->scene(), FastView{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr}};
-    if (cudaMemcpyAsync(scenes_d.ptr + m.scene, &rec, sizeof(rec), cudaMemcpyHostToDevice, stream) != cudaSuccess) {
-        cudaGetLastError();
-        return AE_ERR_CUDA;
-    }
-    std::lock_guard<std::mutex> lk(mu);
-    scene_rec[m.scene] = rec;
-    return AE_OK;
+    return rc;
 }
 
 void Server::fail_all(int code, const std::string &why) {
@@ -659,6 +712,7 @@ void Server::run() {
                 todo_moves.push_back(std::move(moves[s].front()));
                 moves[s].pop_front();
                 policy.move_applied(s);  // requests of the new version wait for this iteration's upload
+                todo_moves.back().version = policy.applied(s);
             }
             PolicyRequest pr;
             uint64_t off;
@@ -714,7 +768,7 @@ void Server::run() {
                 d.F = make_frame_params(cfg);
                 d.accum = reinterpret_cast<float4 *>(arena + r->offset);
                 d.display = reinterpret_cast<uchar4 *>(arena + r->offset + r->accum_bytes);
-                d.scene = r->scene;
+                d.scene = r->scene * kFrameSets + r->version % kFrameSets;
                 d.n_pixels = r->width * r->height;
                 d.frames = r->frames;
                 d.spp = d.F.spp;
@@ -883,6 +937,7 @@ extern "C" ae_server *ae_serve_create(const ae_serve_settings *settings) {
     if (!s.extend_threads) s.extend_threads = 64;
     if (!s.max_scenes) s.max_scenes = 16;
     if (s.max_lights > kServeMaxLights || s.max_requests > kServeMaxRequests || (s.ticks_per_launch & 1) ||
+        s.claim_policy > AE_CLAIM_SHARED ||
         s.slots > (1u << 26) || uint64_t(s.slots) * s.max_lights > 0xffffffffull)
         return nullptr;
     ae_server *srv = new (std::nothrow) ae_server();
@@ -938,18 +993,22 @@ extern "C" int ae_serve_add_scene(ae_server *srv, ae_ctx *scene, uint32_t *scene
     if (rc != AE_OK) return srv->fail_locked(rc, "scene: %s", c->err.c_str());
     if (srv->scene_ctx.size() >= srv->st.max_scenes)
         return srv->fail_locked(AE_ERR_OVERSIZE, "at most %u resident scenes", srv->st.max_scenes);
-    FastScene &F = *c->fast;
-    SceneRec rec{c->scene(), FastView{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr}};
     const uint32_t id = uint32_t(srv->scene_ctx.size());
-    // No replay reads this row before a request of the scene is admitted.
-    if (cudaMemcpyAsync(srv->scenes_d.ptr + id, &rec, sizeof(rec), cudaMemcpyHostToDevice, srv->stats_stream) !=
-            cudaSuccess ||
-        cudaStreamSynchronize(srv->stats_stream) != cudaSuccess) {
+    std::unique_ptr<FrameSet[]> sets(new (std::nothrow) FrameSet[kFrameSets]);
+    if (!sets) return srv->fail_locked(AE_ERR_OOM, "frame sets");
+    srv->scene_ctx.push_back(c);  // capacity reserved at creation: the scheduler reads it unlocked
+    srv->frame_sets.push_back(std::move(sets));
+    for (uint32_t k = 0; k < kFrameSets; k++) {
+        if ((rc = srv->fill_frame_set(id, k)) != AE_OK) {
+            srv->scene_ctx.pop_back();
+            srv->frame_sets.pop_back();
+            return srv->fail_locked(rc, "scene %u: frame set copy failed", id);
+        }
+    }
+    if (cudaStreamSynchronize(srv->stream) != cudaSuccess) {
         cudaGetLastError();
         return srv->fail_locked(AE_ERR_CUDA, "scene table upload failed");
     }
-    srv->scene_ctx.push_back(c);  // capacity reserved at creation: the scheduler reads it unlocked
-    srv->scene_rec.push_back(rec);
     srv->moves.emplace_back();
     srv->policy.add_scene();
     if (scene_id) *scene_id = id;

@@ -60,9 +60,10 @@ uint64_t Arena::largest_free() const {
     return m;
 }
 
-void Policy::configure(uint64_t arena_bytes, uint32_t max_resident) {
+void Policy::configure(uint64_t arena_bytes, uint32_t max_resident, uint32_t frame_sets) {
     arena_.reset(arena_bytes);
     max_resident_ = std::max(max_resident, 1u);
+    frame_sets_ = std::max(frame_sets, 1u);
 }
 
 uint32_t Policy::add_scene() {
@@ -89,7 +90,14 @@ bool Policy::move(uint32_t scene) {
 bool Policy::next_move(uint32_t &scene) const {
     for (uint32_t s = 0; s < applied_.size(); s++) {
         if (submitted_moves_[s] == applied_[s]) continue;
-        auto it = outstanding_.find({s, applied_[s]});
+        // The new version applied_ + 1 overwrites the copy of version
+        // applied_ + 1 - frame_sets (none while that is negative).
+        if (applied_[s] + 1 < frame_sets_) {
+            scene = s;
+            return true;
+        }
+        const uint32_t victim = applied_[s] + 1 - frame_sets_;
+        auto it = outstanding_.find({s, victim});
         if (it == outstanding_.end() || it->second == 0) {
             scene = s;
             return true;
@@ -99,14 +107,17 @@ bool Policy::next_move(uint32_t &scene) const {
 }
 
 void Policy::move_applied(uint32_t scene) {
-    outstanding_.erase({scene, applied_[scene]});
+    if (applied_[scene] + 1 >= frame_sets_) outstanding_.erase({scene, applied_[scene] + 1 - frame_sets_});
     applied_[scene]++;
 }
 
 bool Policy::next_admission(PolicyRequest &out, uint64_t &offset) {
     if (resident_ >= max_resident_) return false;
     for (auto it = pending_.begin(); it != pending_.end(); ++it) {
-        if (it->version != applied_[it->scene]) continue;  // waits for a move of its scene
+        // A request waits for the moves submitted before it; its version's
+        // copy stays intact until every request of that version is done.
+        const uint32_t cur = applied_[it->scene];
+        if (it->version > cur || cur - it->version >= frame_sets_) continue;
         const uint64_t off = arena_.alloc(it->footprint);
         if (off == Arena::kNone) return false;  // arrival order: later requests wait too
         out = *it;
@@ -149,11 +160,11 @@ using namespace ae;
 // list order within a tick); each tick applies every move that may apply,
 // admits what fits, then advances admitted requests by one tick of service.
 extern "C" int ae_serve_policy_simulate(const ae_policy_event *events, uint32_t n, uint64_t arena_bytes,
-                                        uint32_t max_resident, uint32_t n_scenes, uint32_t max_ticks,
-                                        ae_policy_outcome *out) {
-    if ((n && (!events || !out)) || n_scenes == 0) return AE_ERR_INVALID;
+                                        uint32_t max_resident, uint32_t n_scenes, uint32_t frame_sets,
+                                        uint32_t max_ticks, ae_policy_outcome *out) {
+    if ((n && (!events || !out)) || n_scenes == 0 || frame_sets == 0) return AE_ERR_INVALID;
     Policy P;
-    P.configure(arena_bytes, max_resident);
+    P.configure(arena_bytes, max_resident, frame_sets);
     for (uint32_t s = 0; s < n_scenes; s++) P.add_scene();
     for (uint32_t i = 0; i < n; i++) {
         out[i].admit_tick = out[i].done_tick = -1;

@@ -6,6 +6,10 @@
 //   * Policy: admission in arrival order by memory footprint and resident
 //     slots, and the ordering of instance moves against the requests of a
 //     scene (a request renders the scene as it was when it was submitted).
+//     Each scene has `frame_sets` copies of its per-frame arrays; version v
+//     lives in copy v % frame_sets, so a move to version v + 1 may be applied
+//     once no request of version v + 1 - frame_sets is outstanding, while
+//     requests of the newer versions still run.
 #pragma once
 #include <cstdint>
 #include <deque>
@@ -48,7 +52,7 @@ struct PolicyRequest {
 
 class Policy {
   public:
-    void configure(uint64_t arena_bytes, uint32_t max_resident);
+    void configure(uint64_t arena_bytes, uint32_t max_resident, uint32_t frame_sets = 2);
     uint32_t add_scene();
     uint32_t scenes() const { return uint32_t(applied_.size()); }
     // Queues a request; fills in its scene version.  False when it can never
@@ -56,8 +60,8 @@ class Policy {
     bool submit(PolicyRequest &r);
     // Queues an instance move of `scene`; requests submitted after it see it.
     bool move(uint32_t scene);
-    // A scene whose oldest queued move may be applied now: every request
-    // submitted before that move has completed.
+    // A scene whose oldest queued move may be applied now: every request of
+    // the version whose copy the move overwrites has completed.
     bool next_move(uint32_t &scene) const;
     void move_applied(uint32_t scene);
     // The next request to admit (arrival order; requests waiting for a move
@@ -76,7 +80,7 @@ class Policy {
 
   private:
     Arena arena_;
-    uint32_t max_resident_ = 1, resident_ = 0;
+    uint32_t max_resident_ = 1, resident_ = 0, frame_sets_ = 2;
     std::deque<PolicyRequest> pending_;
     std::map<uint64_t, std::pair<PolicyRequest, uint64_t>> active_;  // id -> (request, offset)
     std::vector<uint32_t> applied_, submitted_moves_;

@@ -46,6 +46,7 @@ constexpr int kMaxLights = 64;  // NEE entries per path vertex
 struct WfParams {
     FrameParams F;
     uint32_t n_paths, sample, spp, n_lights;
+    uint32_t kahan;  // precision form: compensated accumulation
 };
 
 // Device counters: [0],[1] ray queue sizes (ping-pong), [2] shadow queue,
@@ -66,6 +67,8 @@ struct WfView {
     const WfParams *P;
     float4 *accum, *frame;
     uchar4 *display;
+    float4 *ksum, *kcomp;  // precision form: compensated sum of frame colours
+    PrecView prec;
 };
 
 struct Wavefront {
@@ -81,6 +84,7 @@ struct Wavefront {
     DevBuf<uint32_t> sq;
     DevBuf<uint32_t> cnt;
     DevBuf<WfParams> params;
+    DevBuf<float4> ksum, kcomp;
     WfParams *host_params = nullptr;  // pinned
     cudaGraphExec_t graph = nullptr;
     uint64_t graph_key = ~0ull;
@@ -139,7 +143,7 @@ __global__ void __launch_bounds__(256) k_wf_generate(WfView W) {
 
 // Extend: persistent CTAs take tiles of the ray queue; one elected thread
 // bulk-copies the tile into shared memory and every thread traces one ray.
-template <int THREADS, int SS>
+template <int THREADS, int SS, bool WT>
 __global__ void __launch_bounds__(THREADS) k_wf_extend(DevScene S, FastView V, WfView W, int bounce) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ae_ray *tile = reinterpret_cast<ae_ray *>(smem_raw);
@@ -174,8 +178,8 @@ __global__ void __launch_bounds__(THREADS) k_wf_extend(DevScene S, FastView V, W
         phase ^= 1u;
         if (threadIdx.x < m) {
             const ae_ray r = tile[threadIdx.x];
-            const Best b = closest_fast<false, SS>(S, V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time,
-                                                   stk, threadIdx.x, THREADS);
+            const Best b = closest_fast<WT, SS>(S, V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time,
+                                                stk, threadIdx.x, THREADS);
             const bool any = b.object != AE_MISS;
             ae_hit h;
             h.t = any ? b.t : 0.0f;
@@ -190,7 +194,8 @@ __global__ void __launch_bounds__(THREADS) k_wf_extend(DevScene S, FastView V, W
 }
 
 // Shade: one queued path per thread (ColorRay's body after the traversal).
-__global__ void __launch_bounds__(256) k_wf_shade(DevScene S, WfView W, int bounce) {
+template <bool PREC>
+__global__ void __launch_bounds__(256) k_wf_shade(DevScene S, FastView V, WfView W, int bounce) {
     const WfParams &P = *W.P;
     const int q = bounce & 1;
     const uint32_t count = W.cnt[q];
@@ -204,8 +209,8 @@ __global__ void __launch_bounds__(256) k_wf_shade(DevScene S, WfView W, int boun
         ae_ray nr;
         uint32_t n_shadow;
         const size_t e0 = size_t(pid) * P.n_lights;
-        const bool next = shade_vertex(S, P.F.sky, P.F.depth, P.n_lights, bounce, r, hr, thr, acc, seed, W.sh, e0,
-                                       W.nee + pid, W.pend + pid, n_shadow, nr);
+        const bool next = shade_vertex<PREC>(S, V, W.prec, P.F.sky, P.F.depth, P.n_lights, bounce, r, hr, thr, acc,
+                                             seed, W.sh, e0, W.nee + pid, W.pend + pid, n_shadow, nr);
         W.thr[pid] = make_float4(thr.x, thr.y, thr.z, 0.0f);
         W.acc[pid] = make_float4(acc.x, acc.y, acc.z, 0.0f);
         W.seed[pid] = seed;
@@ -221,15 +226,15 @@ __global__ void __launch_bounds__(256) k_wf_shade(DevScene S, WfView W, int boun
 }
 
 // Shadow: the reference's occlusion loop per entry.
-template <int THREADS>
+template <int THREADS, bool WT>
 __global__ void __launch_bounds__(THREADS) k_wf_shadow(DevScene S, FastView V, WfView W) {
     extern __shared__ uint2 stk[];
     const uint32_t count = W.cnt[C_SH];
     for (uint32_t k = blockIdx.x * THREADS + threadIdx.x; k < count; k += gridDim.x * THREADS) {
         const uint32_t e = W.sq[k];
         const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
-        const bool occluded = shadow_occluded(S, V, mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z), mk(l4.x, l4.y, l4.z),
-                                              d4.w, stk, threadIdx.x, THREADS);
+        const bool occluded = shadow_occluded<WT>(S, V, mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z),
+                                                  mk(l4.x, l4.y, l4.z), d4.w, stk, threadIdx.x, THREADS);
         W.sh.occ[e] = occluded ? 1 : 0;
     }
 }
@@ -269,7 +274,24 @@ __global__ void __launch_bounds__(256) k_wf_finish(WfView W) {
         const f3 color = col / AE_U2F(P.spp);
         if (W.frame) W.frame[p] = make_float4(color.x, color.y, color.z, 1.0f);
         f3 accum;
-        if (P.F.batch == 0) {
+        if (P.kahan) {
+            // Compensated (Kahan) sum of the frame colours, divided by the
+            // frame count: the precision form's accumulation.
+            f3 sum, comp;
+            if (P.F.batch == 0) {
+                sum = color;
+                comp = splat(0.0f);
+            } else {
+                const float4 s4 = W.ksum[p], c4 = W.kcomp[p];
+                const f3 y = color - mk(c4.x, c4.y, c4.z);
+                const f3 prev = mk(s4.x, s4.y, s4.z);
+                sum = prev + y;
+                comp = (sum - prev) - y;
+            }
+            W.ksum[p] = make_float4(sum.x, sum.y, sum.z, 0.0f);
+            W.kcomp[p] = make_float4(comp.x, comp.y, comp.z, 0.0f);
+            accum = sum / AE_U2F(P.F.batch + 1);
+        } else if (P.F.batch == 0) {
             accum = color;
         } else {
             const float4 prev = W.accum[p];
@@ -288,10 +310,16 @@ struct ExtendCfg {
     int threads, stack;
     ExtendFn fn;
 };
-static const ExtendCfg kExtendCfgs[9] = {
-    {64, 16, k_wf_extend<64, 16>},   {64, 24, k_wf_extend<64, 24>},   {64, 32, k_wf_extend<64, 32>},
-    {128, 16, k_wf_extend<128, 16>}, {128, 24, k_wf_extend<128, 24>}, {128, 32, k_wf_extend<128, 32>},
-    {256, 16, k_wf_extend<256, 16>}, {256, 24, k_wf_extend<256, 24>}, {256, 32, k_wf_extend<256, 32>},
+// [0]: the reference triangle test; [1]: the watertight test (precision form).
+static const ExtendCfg kExtendCfgs[2][9] = {
+    {{64, 16, k_wf_extend<64, 16, false>}, {64, 24, k_wf_extend<64, 24, false>}, {64, 32, k_wf_extend<64, 32, false>},
+     {128, 16, k_wf_extend<128, 16, false>}, {128, 24, k_wf_extend<128, 24, false>},
+     {128, 32, k_wf_extend<128, 32, false>}, {256, 16, k_wf_extend<256, 16, false>},
+     {256, 24, k_wf_extend<256, 24, false>}, {256, 32, k_wf_extend<256, 32, false>}},
+    {{64, 16, k_wf_extend<64, 16, true>}, {64, 24, k_wf_extend<64, 24, true>}, {64, 32, k_wf_extend<64, 32, true>},
+     {128, 16, k_wf_extend<128, 16, true>}, {128, 24, k_wf_extend<128, 24, true>},
+     {128, 32, k_wf_extend<128, 32, true>}, {256, 16, k_wf_extend<256, 16, true>},
+     {256, 24, k_wf_extend<256, 24, true>}, {256, 32, k_wf_extend<256, 32, true>}},
 };
 
 static size_t extend_smem(int threads, int stack) {
@@ -322,6 +350,9 @@ static WfView view_of(Ctx *c) {
     W.accum = c->accum.ptr;
     W.frame = c->frame.ptr;
     W.display = c->display.ptr;
+    W.ksum = Wf.ksum.ptr;
+    W.kcomp = Wf.kcomp.ptr;
+    W.prec = PrecView{c->fast->shade16.ptr};
     return W;
 }
 
@@ -366,37 +397,42 @@ struct Grids {
 
 // Launch shapes, fixed before capture (no attribute or occupancy query runs
 // while a stream is being captured).
-static Grids grids_for(Ctx *c, int cfg_index) {
+static Grids grids_for(Ctx *c, int cfg_index, bool prec) {
     Wavefront &Wf = *c->wave;
     Grids g;
     g.grid256 = Wf.sms * 8;
-    const ExtendCfg &e = kExtendCfgs[cfg_index];
+    const ExtendCfg &e = kExtendCfgs[prec][cfg_index];
     g.egrid = extend_grid(c, e);
     g.esmem = extend_smem(e.threads, e.stack);
     g.shsmem = size_t(kSharedStack) * 128 * sizeof(uint2);
-    cudaFuncSetAttribute(reinterpret_cast<const void *>(k_wf_shadow<128>), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         int(g.shsmem));
+    const void *shfn = prec ? reinterpret_cast<const void *>(k_wf_shadow<128, true>)
+                            : reinterpret_cast<const void *>(k_wf_shadow<128, false>);
+    cudaFuncSetAttribute(shfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(g.shsmem));
     int sh_per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh_per_sm, reinterpret_cast<const void *>(k_wf_shadow<128>), 128,
-                                                  g.shsmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh_per_sm, shfn, 128, g.shsmem);
     g.shgrid = std::max(1, sh_per_sm) * Wf.sms;
     return g;
 }
 
-static int record_sample(Ctx *c, cudaStream_t st, int cfg_index, const Grids &G) {
+static int record_sample(Ctx *c, cudaStream_t st, int cfg_index, const Grids &G, bool prec) {
     const WfView W = view_of(c);
     const DevScene S = c->scene();
     FastScene &F = *c->fast;
     const FastView V{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr};
-    const ExtendCfg &e = kExtendCfgs[cfg_index];
+    const ExtendCfg &e = kExtendCfgs[prec][cfg_index];
     const int grid256 = G.grid256, egrid = G.egrid, shgrid = G.shgrid;
     const size_t esmem = G.esmem, shsmem = G.shsmem;
     k_wf_generate<<<grid256, 256, 0, st>>>(W);
     for (uint32_t b = 0; b < c->config.depth; b++) {
         k_wf_reset<<<1, 1, 0, st>>>(W, int(b));
         e.fn<<<egrid, e.threads, esmem, st>>>(S, V, W, int(b));
-        k_wf_shade<<<grid256, 256, 0, st>>>(S, W, int(b));
-        k_wf_shadow<128><<<shgrid, 128, shsmem, st>>>(S, V, W);
+        if (prec) {
+            k_wf_shade<true><<<grid256, 256, 0, st>>>(S, V, W, int(b));
+            k_wf_shadow<128, true><<<shgrid, 128, shsmem, st>>>(S, V, W);
+        } else {
+            k_wf_shade<false><<<grid256, 256, 0, st>>>(S, V, W, int(b));
+            k_wf_shadow<128, false><<<shgrid, 128, shsmem, st>>>(S, V, W);
+        }
         k_wf_connect<<<grid256, 256, 0, st>>>(W, int(b));
     }
     k_wf_finish<<<grid256, 256, 0, st>>>(W);
@@ -416,7 +452,7 @@ static int autotune(Ctx *c) {
     int best = 4;
     float best_ms = 1e30f;
     for (int k = 0; k < 9; k++) {
-        const ExtendCfg &e = kExtendCfgs[k];
+        const ExtendCfg &e = kExtendCfgs[0][k];
         const int egrid = extend_grid(c, e);
         float total = 0.0f;
         for (int rep = 0; rep < 2; rep++) {
@@ -435,28 +471,35 @@ static int autotune(Ctx *c) {
         Wf.tune_ms[k] = total;
         if (total < best_ms) { best_ms = total; best = k; }
     }
-    Wf.ext_threads = kExtendCfgs[best].threads;
-    Wf.ext_stack = kExtendCfgs[best].stack;
+    Wf.ext_threads = kExtendCfgs[0][best].threads;
+    Wf.ext_stack = kExtendCfgs[0][best].stack;
     Wf.tuned = true;
     return c->cuda(cudaGetLastError(), "autotune");
 }
 
 static int best_cfg_index(const Wavefront &Wf) {
     for (int k = 0; k < 9; k++)
-        if (kExtendCfgs[k].threads == Wf.ext_threads && kExtendCfgs[k].stack == Wf.ext_stack) return k;
+        if (kExtendCfgs[0][k].threads == Wf.ext_threads && kExtendCfgs[0][k].stack == Wf.ext_stack) return k;
     return 4;
 }
 
-int render_wavefront(Ctx *c) {
+int render_wavefront(Ctx *c, bool prec) {
     int rc = ensure_wavefront(c);
     if (rc) return rc;
     Wavefront &Wf = *c->wave;
+    const uint32_t n_px = c->settings.width * c->settings.height;
+    if (prec) {
+        if ((rc = prepare_precision(c))) return rc;
+        if (Wf.ksum.reserve(n_px) || Wf.kcomp.reserve(n_px))
+            return c->fail(AE_ERR_OOM, "compensated accumulation (%u pixels)", n_px);
+    }
     WfParams hp;
     std::memset(&hp, 0, sizeof(hp));
     hp.F = make_frame_params(c->config);
-    hp.n_paths = c->settings.width * c->settings.height;
+    hp.n_paths = n_px;
     hp.spp = hp.F.spp;
     hp.n_lights = c->n_lights;
+    hp.kahan = prec ? 1u : 0u;
     if (hp.F.display_only) {
         // Re-grade only: the compute-only kernel's display-only branch.
         if ((rc = c->timed_begin())) return rc;
@@ -474,14 +517,15 @@ int render_wavefront(Ctx *c) {
     }
     // One graph per (scene upload, frame shape); frame parameters travel
     // through device memory so the graph is replayed unchanged.
-    const uint64_t key = (c->scene_version << 20) ^ (uint64_t(c->config.depth) << 8) ^ hp.n_lights;
+    const uint64_t key = (c->scene_version << 21) ^ (uint64_t(prec) << 20) ^ (uint64_t(c->config.depth) << 8) ^
+                         hp.n_lights;
     if (!Wf.graph || Wf.graph_key != key) {
         if (Wf.graph) { cudaGraphExecDestroy(Wf.graph); Wf.graph = nullptr; }
         cudaGraph_t g;
         const int ci = best_cfg_index(Wf);
-        const Grids G = grids_for(c, ci);
+        const Grids G = grids_for(c, ci, prec);
         if ((rc = c->cuda(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "capture"))) return rc;
-        rc = record_sample(c, c->stream, ci, G);
+        rc = record_sample(c, c->stream, ci, G, prec);
         cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
         if (rc) return rc;
         if ((rc = c->cuda(ce, "end capture"))) return rc;

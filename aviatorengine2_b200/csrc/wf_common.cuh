@@ -8,6 +8,7 @@
 // color_ray), in the same order, so a path traced through these pieces gives
 // the plain kernel's radiance bit for bit.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "fast_trace.cuh"
@@ -80,19 +81,69 @@ struct ShadowStore {
     uint8_t *valid, *occ;
 };
 
+// The precision form's shading data: per triangle record (in the optimised
+// BVH's slot order) the three vertex normals and UVs as FP16, 32 bytes:
+//   word 0: n0.x n0.y | n0.z n1.x | n1.y n1.z | n2.x n2.y
+//   word 1: n2.z u0   | v0   u1   | v1   u2   | v2   (pad)
+struct PrecView {
+    const uint4 *shade16;  // 2 per triangle
+};
+
+AE_DEV float half_lo(uint32_t w) { return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu))); }
+AE_DEV float half_hi(uint32_t w) { return __half2float(__ushort_as_half((unsigned short)(w >> 16))); }
+
+// surface_from_hit for the precision form: mesh hits take the shading normal
+// from the FP16 record and the geometric normal from the optimised
+// triangle record (the same FP32 positions); everything else as the plain form.
+AE_DEV bool surface_from_hit_prec(const DevScene &S, const FastView &V, const PrecView &P, const ae_hit &h, f3 o,
+                                  f3 d, float time, DHit &out) {
+    if (h.object == AE_MISS) return false;
+    const uint4 m = __ldg(V.meta + h.object);
+    if ((m.x & 0xffu) != AE_SHAPE_MESH) return surface_from_hit(S, h, o, d, time, out);
+    out.t = h.t;
+    out.slot = h.object;
+    out.prim = h.prim;
+    out.alpha = h.alpha;
+    out.beta = h.beta;
+    out.p = o + d * h.t;
+    const float4 *ip = reinterpret_cast<const float4 *>(V.inst + m.y);
+    const float4 q = __ldg(ip + 1), rb = __ldg(ip + 2);
+    const size_t tri = size_t(__float_as_uint(rb.y)) + h.prim;
+    const float4 *tp = V.tris + 3 * tri;
+    const float4 t0 = __ldg(tp), t1 = __ldg(tp + 1), t2 = __ldg(tp + 2);
+    const f3 p0 = mk(t0.x, t0.y, t0.z), p1 = mk(t0.w, t1.x, t1.y), p2 = mk(t1.z, t1.w, t2.x);
+    const uint4 s0 = __ldg(P.shade16 + 2 * tri), s1 = __ldg(P.shade16 + 2 * tri + 1);
+    const f3 n0 = mk(half_lo(s0.x), half_hi(s0.x), half_lo(s0.y));
+    const f3 n1 = mk(half_hi(s0.y), half_lo(s0.z), half_hi(s0.z));
+    const f3 n2 = mk(half_lo(s0.w), half_hi(s0.w), half_lo(s1.x));
+    const float w0 = AE_SUB(AE_SUB(1.0f, h.alpha), h.beta);
+    const f3 sh = normalize(w0 * n0 + h.alpha * n1 + h.beta * n2);
+    const f3 gn = cross(p1 - p0, p2 - p0);
+    f3 geo = gn / AE_SQRT(dot(gn, gn));
+    if (dot(geo, sh) < 0.0f) geo = -geo;
+    out.front = dot(d, quat_rotate(q.x, q.y, q.z, q.w, geo)) < 0.0f;
+    out.n = normalize(quat_rotate(q.x, q.y, q.z, q.w, sh));
+    if (!out.front) out.n = -out.n;
+    return true;
+}
+
 // Everything at one path vertex after its closest hit: sky or emission on a
 // miss or a light, the light samples of a Lambertian surface (entries
 // e0 .. e0 + n_lights - 1, throughput at the vertex into *pend, *nee set),
 // then the bounce and Russian roulette.  Returns whether the path goes on,
 // with its next ray in `nr`; `n_shadow` counts the valid light samples.
-AE_DEV bool shade_vertex(const DevScene &S, const f3 &sky, uint32_t depth, uint32_t n_lights, int bounce,
-                         const ae_ray &r, const ae_hit &hr, f3 &thr, f3 &acc, uint32_t &seed, const ShadowStore &SH,
-                         size_t e0, uint8_t *nee, float4 *pend, uint32_t &n_shadow, ae_ray &nr) {
+// PREC selects the precision form's FP16 shading normals.
+template <bool PREC>
+AE_DEV bool shade_vertex(const DevScene &S, const FastView &V, const PrecView &PV, const f3 &sky, uint32_t depth,
+                         uint32_t n_lights, int bounce, const ae_ray &r, const ae_hit &hr, f3 &thr, f3 &acc,
+                         uint32_t &seed, const ShadowStore &SH, size_t e0, uint8_t *nee, float4 *pend,
+                         uint32_t &n_shadow, ae_ray &nr) {
     const f3 o = mk(r.ox, r.oy, r.oz), d = mk(r.dx, r.dy, r.dz);
     n_shadow = 0;
     nr = r;
     DHit h;
-    if (!surface_from_hit(S, hr, o, d, r.time, h)) {
+    const bool hit = PREC ? surface_from_hit_prec(S, V, PV, hr, o, d, r.time, h) : surface_from_hit(S, hr, o, d, r.time, h);
+    if (!hit) {
         acc = acc + thr * sky;
         return false;
     }
@@ -165,11 +216,12 @@ AE_DEV void push_shadow_entries(const ShadowStore &SH, uint32_t e0, uint32_t n_l
 
 // The reference's shadow test (hybrid:1167-1191): up to four closest hits,
 // stepping through glass; lights and anything beyond the light point do not
-// block.
+// block.  WT selects the watertight triangle test.
+template <bool WT = false>
 AE_DEV bool shadow_occluded(const DevScene &S, const FastView &V, f3 so, const f3 &sd, const f3 &lp, float time,
                             uint2 *stk, int tid, int nthreads) {
     for (int step = 0; step < 4; step++) {
-        const Best b = closest_fast<false>(S, V, so, sd, 0.001f, time, stk, tid, nthreads);
+        const Best b = closest_fast<WT>(S, V, so, sd, 0.001f, time, stk, tid, nthreads);
         if (b.object == AE_MISS) return false;
         if (b.t >= AE_SUB(distance(lp, so), 0.001f)) return false;
         const uint32_t mt = load_head(S.objects + b.object).material;

@@ -174,6 +174,15 @@ class Context:
         self._chk(lib().ae_wavefront_info(self._h, ctypes.byref(th), ctypes.byref(st), ptr(ms), ctypes.byref(err)))
         return {"threads": th.value, "stack": st.value, "tune_ms": ms.tolist(), "errors": err.value}
 
+    def image_error(self, reference, which=_lib.IMAGE_ACCUM, eps=1e-3):
+        """FP64 error of an image against a reference (H, W, 4) float64 image,
+        reduced on the GPU: (mean relative, mean absolute, max absolute, rms)."""
+        ref = np.ascontiguousarray(reference, dtype=np.float64)
+        assert ref.shape == (self.height, self.width, 4), ref.shape
+        out = np.zeros(4, np.float64)
+        self._chk(lib().ae_image_error(self._h, which, ptr(ref), eps, ptr(out)))
+        return {"mre": out[0], "mae": out[1], "max": out[2], "rmse": out[3]}
+
     def prepare_fast(self):
         self._chk(lib().ae_prepare_fast(self._h))
 

@@ -20,11 +20,11 @@ from ._lib import lib, ptr
 
 class Server:
     def __init__(self, slots=0, max_lights=0, max_requests=0, arena_bytes=0, ticks_per_launch=0, extend_threads=0,
-                 max_scenes=0, device=0):
+                 max_scenes=0, claim_policy=_lib.CLAIM_OLDEST_FIRST, device=0):
         s = np.zeros(1, _lib.SERVE_SETTINGS)
         s["device"], s["slots"], s["max_lights"], s["max_requests"] = device, slots, max_lights, max_requests
         s["arena_bytes"], s["ticks_per_launch"] = arena_bytes, ticks_per_launch
-        s["extend_threads"], s["max_scenes"] = extend_threads, max_scenes
+        s["extend_threads"], s["max_scenes"], s["claim_policy"] = extend_threads, max_scenes, claim_policy
         self._h = lib().ae_serve_create(ptr(s))
         if not self._h:
             raise _lib.AeError(-5, "ae_serve_create failed (see stderr)")
@@ -99,7 +99,7 @@ class Server:
         self._chk(lib().ae_serve_reset_stats(self._h))
 
 
-def simulate_policy(events, arena_bytes, max_resident, n_scenes, max_ticks=100000):
+def simulate_policy(events, arena_bytes, max_resident, n_scenes, frame_sets=2, max_ticks=100000):
     """Runs the server's admission policy on a list of event dicts on the host
     (no GPU).  Returns (status, outcomes array)."""
     ev = np.zeros(len(events), _lib.POLICY_EVENT)
@@ -110,5 +110,6 @@ def simulate_policy(events, arena_bytes, max_resident, n_scenes, max_ticks=10000
         ev[i]["service_ticks"] = e.get("service_ticks", 1)
         ev[i]["footprint"] = e.get("footprint", 0)
     out = np.zeros(len(events), _lib.POLICY_OUTCOME)
-    code = lib().ae_serve_policy_simulate(ptr(ev), len(ev), arena_bytes, max_resident, n_scenes, max_ticks, ptr(out))
+    code = lib().ae_serve_policy_simulate(ptr(ev), len(ev), arena_bytes, max_resident, n_scenes, frame_sets, max_ticks,
+                                          ptr(out))
     return code, out

@@ -150,6 +150,99 @@ def cpu_reference(scene, rays, budget_s=20.0):
             "sample": f"{n} rays drawn uniformly from the step's {len(rays)} (primary + bounce), {dt:.2f} s"}
 
 
+def measure_paths(local, width, height, frames=2):
+    """Mpaths/s of compute-only frames (1 spp) on the wavefront workload:
+    the plain megakernel against the wavefront form (4-wide 8-bit quantised
+    BVH, persistent stages, CUDA graph).  Frames are timed on the device
+    around the whole frame; the images of the two forms are compared."""
+    from aviatorengine2_b200 import Context, _lib, scenes
+    scene = scenes.wavefront_scene(width=width, height=height)
+    out = {"workload": f"wavefront_scene {width}x{height}, 1 spp, depth {int(scene.config['depth'])}, "
+                       f"{len(scene.lights)} lights", "triangles": int(scene.triangles),
+           "instances": int(len(scene.instances)), "paths_per_frame": width * height}
+    imgs = {}
+    with Context(width, height, device=local) as ctx:
+        ctx.upload(scene)
+        for name, mode in (("plain", _lib.MODE_COMPUTE_ONLY), ("wavefront", _lib.MODE_WAVEFRONT)):
+            c = scene.config.copy()
+            ms = []
+            for b in range(frames + 1):  # frame 0 warms up (and autotunes the wavefront)
+                c["batch"] = b
+                ctx.set_config(c)
+                ctx.render_frame(mode)
+                ctx.synchronize()
+                if b:
+                    ms.append(ctx.last_kernel_ms())
+            imgs[name] = ctx.read_image(_lib.IMAGE_FRAME)
+            out[f"{name}_ms"] = float(np.mean(ms))
+            out[f"{name}_mpaths"] = width * height / (float(np.mean(ms)) / 1e3) / 1e6
+        info = ctx.wavefront_info()
+        out["wavefront_extend"] = {"threads": info["threads"], "stack": info["stack"]}
+    out["speedup"] = out["wavefront_mpaths"] / out["plain_mpaths"]
+    a, b = imgs["plain"], imgs["wavefront"]
+    out["frames_bit_exact"] = bool(np.array_equal(a.view(np.uint32), b.view(np.uint32)))
+    out["pixels_differing"] = int(np.any(a.view(np.uint32) != b.view(np.uint32), axis=-1).sum())
+    return out
+
+
+def measure_serving(local, n_requests=16, rate=0.5, seed=7, claim_policy=1):
+    """The serving loop under a Poisson stream of requests over the 8 resident
+    serving scenes: resolution uniform over {256^2, 640x480, 960x540,
+    1920x1080}, spp from {1, 4, 16, 64} (as that many progressive frames),
+    and before each request a random-walk step of all 512 instances of its
+    scene (a GPU refit).  Latency = submit to images in host memory."""
+    from aviatorengine2_b200 import Context, Server, scenes
+    rng = np.random.default_rng(seed)
+    t0 = time.perf_counter()
+    S = scenes.serving_scenes()
+    ctxs = []
+    for s in S:
+        c = Context(256, 256, device=local)
+        c.upload(s)
+        ctxs.append(c)
+    build_s = time.perf_counter() - t0
+    res_choices = [(256, 256), (640, 480), (960, 540), (1920, 1080)]
+    spp_choices = [1, 4, 16, 64]
+    plan = [(int(rng.integers(0, len(S))), res_choices[int(rng.integers(0, 4))], spp_choices[int(rng.integers(0, 4))])
+            for _ in range(n_requests)]
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    inst = [s.instances.copy() for s in S]
+    with Server(device=local, arena_bytes=4 << 30, max_requests=64, claim_policy=claim_policy) as srv:
+        ids = [srv.add_scene(c) for c in ctxs]
+        # warm-up: one small request per scene
+        for k in range(len(S)):
+            c = S[k].config.copy()
+            c["samples"], c["batches"] = 1, 1
+            srv.wait(srv.submit(ids[k], 64, 64, 1, c, accum=False, display=False), 600000)
+        srv.reset_stats()
+        start = time.perf_counter()
+        rids = []
+        for i, (sc, (w, h), spp) in enumerate(plan):
+            while time.perf_counter() - start < arrivals[i]:
+                time.sleep(0.0005)
+            inst[sc] = scenes.random_walk(inst[sc], rng)
+            srv.move_instances(ids[sc], inst[sc])
+            c = S[sc].config.copy()
+            c["samples"], c["batches"] = 1, 1
+            rids.append(srv.submit(ids[sc], w, h, spp, c))
+        lat = []
+        for r in rids:
+            res, _, _ = srv.wait(r, 1800000)
+            lat.append(res["done_ms"] - res["submit_ms"])
+        st = srv.stats()
+    for c in ctxs:
+        c.close()
+    wall = (st["last_done_ms"] - st["first_submit_ms"]) / 1e3
+    return {"workload": "8 resident scenes " + "/".join(f"{s.triangles // 1000}k" for s in S) +
+                        " tris, 512 moving instances each; Poisson arrivals",
+            "requests": n_requests, "rate_per_s": rate, "claim_policy": "shared" if claim_policy else "oldest_first",
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
+            "mpaths": st["paths"] / wall / 1e6, "mrays": st["rays"] / wall / 1e6, "paths": int(st["paths"]),
+            "wall_s": wall, "moves_applied": int(st["moves_applied"]), "peak_resident": int(st["peak_resident"]),
+            "peak_arena_bytes": int(st["peak_arena_bytes"]), "errors": int(st["errors"]),
+            "scene_build_s": build_s}
+
+
 def run_reference_arm(args):
     rank, world, local = dist_env()
     if rank != 0:
@@ -195,6 +288,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--no-paths", action="store_true", help="skip the Mpaths/s leg (plain vs wavefront frames)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serve-requests", type=int, default=16)
+    ap.add_argument("--serve-rate", type=float, default=0.5, help="Poisson arrivals per second")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -327,6 +424,14 @@ def main():
     if rank == 0 and not args.no_cpu:
         cpu = cpu_reference(scene, np.concatenate([prim, bounce]))
 
+    # Frame-level legs: rank 0 only (the other replicas would repeat them).
+    paths = None
+    if not args.no_paths and rank == 0:
+        paths = measure_paths(local, args.width, args.height)
+    serving = None
+    if not args.no_serve and rank == 0:
+        serving = measure_serving(local, args.serve_requests, args.serve_rate)
+
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene and camera)",
@@ -336,7 +441,8 @@ def main():
                        "l2": "flushed before every step (512 MB write)", "parallelism": f"replicas x{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk.summary(),
-            "per_step_ms": [round(t, 4) for t in times]}
+            "per_step_ms": [round(t, 4) for t in times],
+            "paths": paths, "serving": serving}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -283,8 +283,11 @@ typedef struct ae_settings {
  * QUANT adds 8-bit child bounds and the watertight triangle test. */
 enum { AE_VARIANT_PLAIN = 0, AE_VARIANT_FAST = 1, AE_VARIANT_QUANT = 2 };
 
-/* Render modes for ae_render_frame. */
-enum { AE_MODE_COMPUTE_ONLY = 0, AE_MODE_DEFERRED = 1, AE_MODE_WAVEFRONT = 2 };
+/* Render modes for ae_render_frame.  AE_MODE_WAVEFRONT_PRECISION is the
+ * wavefront tracer in the precision form: watertight triangle test, FP16
+ * shading normals and UVs, and the accumulation image kept as a compensated
+ * (Kahan) FP32 sum of the frame colours divided by the frame count. */
+enum { AE_MODE_COMPUTE_ONLY = 0, AE_MODE_DEFERRED = 1, AE_MODE_WAVEFRONT = 2, AE_MODE_WAVEFRONT_PRECISION = 3 };
 
 /* Image identifiers for ae_read_image. */
 enum {
@@ -356,6 +359,15 @@ int ae_build_gbuffer(ae_ctx *ctx);
 
 /* Copy an image to host memory.  dst_bytes must be >= the image size. */
 int ae_read_image(ae_ctx *ctx, int which, void *dst, size_t dst_bytes);
+
+/* Error of an image against a reference image, reduced on the GPU in FP64
+ * (no counterpart in the reference).  `reference` is host memory holding
+ * width*height RGBA doubles (e.g. the FP64 CPU oracle's accumulation); the RGB
+ * channels are compared.  out[0] = mean relative error
+ * mean(|x - r| / (|r| + eps)), out[1] = mean absolute error, out[2] = largest
+ * absolute error, out[3] = root mean square error.  The sums are reduced in a
+ * fixed order, so the result is the same on every run. */
+int ae_image_error(ae_ctx *ctx, int which, const double *reference, double eps, double *out4);
 
 /* Closest hit for a batch of HOST rays: copies in, traces, copies out,
  * pipelined in chunks over streams.  variant = AE_VARIANT_*. */
@@ -473,8 +485,15 @@ typedef struct ae_serve_settings {
     uint32_t ticks_per_launch; /* queue ticks per graph replay (even); 0 = 4 */
     uint32_t extend_threads;   /* 64, 128 or 256; 0 = 64 */
     uint32_t max_scenes;       /* resident scenes; 0 = 16 */
-    uint32_t reserved[5];
+    uint32_t claim_policy;     /* AE_CLAIM_OLDEST_FIRST (0) or AE_CLAIM_SHARED (1) */
+    uint32_t reserved[4];
 } ae_serve_settings;
+
+/* How free slots pick the next pixel: from the oldest admitted request that
+ * still has unclaimed pixels, or spread over all admitted requests (each warp
+ * starts its search at a different request), which lets short requests
+ * finish while long ones run. */
+enum { AE_CLAIM_OLDEST_FIRST = 0, AE_CLAIM_SHARED = 1 };
 
 typedef struct ae_serve_request {
     uint32_t scene;            /* id from ae_serve_add_scene */
@@ -517,7 +536,10 @@ int ae_serve_add_scene(ae_server *srv, ae_ctx *scene, uint32_t *scene_id);
 /* Queues a request; AE_ERR_REJECTED when its images exceed the whole arena. */
 int ae_serve_submit(ae_server *srv, const ae_serve_request *req, uint64_t *id);
 /* Queues new transforms for every instance of a scene (refit on the GPU);
- * requests submitted earlier render the old ones, later ones the new. */
+ * requests submitted earlier render the old ones, later ones the new.  The
+ * server keeps two copies of each scene's per-frame arrays (objects, TLAS,
+ * instances), so a move is applied while requests of the previous version
+ * still run; only requests two versions back must have finished. */
 int ae_serve_move_instances(ae_server *srv, uint32_t scene, const ae_instance *instances, uint32_t n);
 /* Waits for a request (timeout_ms < 0: forever); returns its status, or
  * AE_ERR_TIMEOUT.  The record is released once it has been returned. */
@@ -530,7 +552,8 @@ int ae_serve_reset_stats(ae_server *srv);
 
 /* The admission policy of the server run on a synthetic event list on the
  * host, with no GPU: requests (footprint, service ticks) and instance moves
- * arrive at ticks; out[i] tells when each was admitted / applied and done. */
+ * arrive at ticks; out[i] tells when each was admitted / applied and done.
+ * frame_sets = copies of each scene's per-frame arrays (the server uses 2). */
 enum { AE_POLICY_REQUEST = 0, AE_POLICY_MOVE = 1 };
 typedef struct ae_policy_event {
     uint32_t kind;             /* AE_POLICY_REQUEST or AE_POLICY_MOVE */
@@ -547,8 +570,8 @@ typedef struct ae_policy_outcome {
     uint64_t offset;           /* requests: arena offset */
 } ae_policy_outcome;
 int ae_serve_policy_simulate(const ae_policy_event *events, uint32_t n, uint64_t arena_bytes,
-                             uint32_t max_resident, uint32_t n_scenes, uint32_t max_ticks,
-                             ae_policy_outcome *out);
+                             uint32_t max_resident, uint32_t n_scenes, uint32_t frame_sets,
+                             uint32_t max_ticks, ae_policy_outcome *out);
 
 #ifdef __cplusplus
 } /* extern "C" */

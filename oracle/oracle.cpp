@@ -438,9 +438,22 @@ bool hit_object(const Scene &S, const ae_object &o, const Ray<T> &r, T tn, T tf,
     }
 }
 
+// Optional record of every closest-hit query (test diagnostics: the rays of
+// one pixel's paths, to replay them through the GPU kernels).
+struct RayLog {
+    ae_ray *rays;
+    uint32_t cap, n;
+};
+thread_local RayLog *g_ray_log = nullptr;
+
 // TraverseBVH, hybrid:862-917: depth-first, interior nodes push left then
 // right, far starts at 1e6 and shrinks with each hit; ties go to the later hit.
 template <class T> bool traverse(const Scene &S, const Ray<T> &r, T tn, Hit<T> &out, Rng &rng, Counters *C) {
+    if (g_ray_log && g_ray_log->n < g_ray_log->cap) {
+        ae_ray &q = g_ray_log->rays[g_ray_log->n++];
+        q.ox = float(r.o.x); q.oy = float(r.o.y); q.oz = float(r.o.z); q.tnear = float(tn);
+        q.dx = float(r.d.x); q.dy = float(r.d.y); q.dz = float(r.d.z); q.time = float(r.time);
+    }
     if (S.n_nodes == 0) return false;
     const V<T> inv = T(1) / r.d;
     int stack[64];
@@ -796,6 +809,17 @@ int oracle_render_frame_f64(const Scene *S, const ae_config *c, double *accum, d
                             const uint32_t *xy, uint32_t n_px, int threads) {
     render_frame<double>(*S, *c, accum, display, frame, xy, n_px, threads);
     return 0;
+}
+
+// Every closest-hit query of pixel (x, y)'s samples in one float frame, in
+// order (camera, shadow and bounce rays); returns how many were made.
+uint32_t oracle_pixel_rays(const Scene *S, const ae_config *c, uint32_t x, uint32_t y, ae_ray *out, uint32_t cap) {
+    RayLog log{out, cap, 0};
+    g_ray_log = &log;
+    const Camera<float> K = camera<float>(*c);
+    pixel_radiance<float>(*S, *c, K, x, y, nullptr);
+    g_ray_log = nullptr;
+    return log.n;
 }
 
 // The shared intrinsics on the host, for their accuracy tests:

@@ -99,6 +99,18 @@ def render_frame(scene, config, accum=None, precision=32, pixels=None, threads=0
     return acc, disp, frame
 
 
+def pixel_rays(scene, config, x, y, cap=8192):
+    """Every closest-hit query the float oracle makes for pixel (x, y) in one
+    frame (camera, shadow and bounce rays, in order)."""
+    s = oscene(scene)
+    c = np.ascontiguousarray(np.array(config, dtype=_lib.CONFIG).reshape(1))
+    out = np.zeros(cap, _lib.RAY)
+    f = oracle().oracle_pixel_rays
+    f.restype = ctypes.c_uint32
+    n = f(ctypes.byref(s), ptr(c), ctypes.c_uint32(x), ctypes.c_uint32(y), ptr(out), ctypes.c_uint32(cap))
+    return out[:min(n, cap)].copy()
+
+
 def counters_bytes(cnt):
     """Algorithmic bytes of the counted touches (the roofline's formula)."""
     t, o, i, b, tri, win = (int(x) for x in cnt)

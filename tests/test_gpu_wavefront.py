@@ -62,3 +62,43 @@ def test_wavefront_samples_per_frame():
     b = render(s, _lib.MODE_COMPUTE_ONLY, 2, samples=3)
     for k in range(2):
         assert same(a[k][1], b[k][1])
+
+
+def test_wavefront_equals_plain_full_size():
+    """The wavefront workload itself (10M triangles, 1024 instances, 16
+    lights, depth 12) at 1920x1080 over three frames.  On a mismatch, the
+    oracle's rays for the first differing pixel are replayed through the plain
+    and optimised closest-hit kernels to name the ray that diverges."""
+    s = scenes.wavefront_scene()
+    w, h = int(s.config["width"]), int(s.config["height"])
+    frames = 3
+    imgs = {}
+    with Context(w, h) as ctx:
+        ctx.upload(s)
+        for mode in (_lib.MODE_COMPUTE_ONLY, _lib.MODE_WAVEFRONT):
+            c = s.config.copy()
+            imgs[mode] = []
+            for b in range(frames):
+                c["batch"] = b
+                ctx.set_config(c)
+                ctx.render_frame(mode)
+                imgs[mode].append(ctx.read_image(_lib.IMAGE_FRAME))
+        bad = []
+        for b in range(frames):
+            d = np.any(imgs[_lib.MODE_COMPUTE_ONLY][b].view(np.uint32) != imgs[_lib.MODE_WAVEFRONT][b].view(np.uint32),
+                       axis=-1)
+            bad += [(b, int(y), int(x)) for y, x in np.argwhere(d)]
+        detail = []
+        if bad:
+            b, y, x = bad[0]
+            c = s.config.copy()
+            c["batch"] = b
+            rays = O.pixel_rays(s, c, x, y)
+            hp = ctx.closest_hit(rays, _lib.VARIANT_PLAIN)
+            hf = ctx.closest_hit(rays, _lib.VARIANT_FAST)
+            ho = O.closest_hit(s, rays)
+            for k in range(len(rays)):
+                if (hp[k]["object"], hp[k]["prim"], hp[k]["t"]) != (hf[k]["object"], hf[k]["prim"], hf[k]["t"]):
+                    detail.append({"ray": k, "r": rays[k].tolist(), "plain": hp[k].tolist(), "fast": hf[k].tolist(),
+                                   "oracle": ho[k].tolist()})
+    assert not bad, f"{len(bad)} pixels differ, first (frame, y, x) = {bad[0]}; diverging rays: {detail}"

@@ -73,24 +73,49 @@ def test_oversize_rejected():
     assert out[1]["admit_tick"] == 0
 
 
-def test_move_waits_for_earlier_requests_of_its_scene():
+def test_move_waits_for_earlier_requests_one_frame_set():
+    # With a single copy of the per-frame arrays a move waits for every
+    # earlier request of its scene.
     ev = [_req(0, 1 * MB, 5, scene=0), _req(0, 1 * MB, 2, scene=0), _move(1, scene=0),
           _req(1, 1 * MB, 1, scene=0), _req(1, 1 * MB, 1, scene=1), _req(2, 1 * MB, 1, scene=0)]
-    code, out = simulate_policy(ev, 100 * MB, 16, 2)
+    code, out = simulate_policy(ev, 100 * MB, 16, 2, frame_sets=1)
     assert code == 0
-    # the move applies only after both earlier scene-0 requests finished
     assert out[2]["admit_tick"] > max(out[0]["done_tick"], out[1]["done_tick"])
     assert out[2]["version"] == 1
-    # later scene-0 requests see the move; scene 1 is not held up
-    for i in (3, 5):
+    for i in (3, 5):  # later scene-0 requests see the move
         assert out[i]["version"] == 1 and out[i]["admit_tick"] >= out[2]["admit_tick"]
-    assert out[4]["version"] == 0 and out[4]["admit_tick"] == 1
+    assert out[4]["version"] == 0 and out[4]["admit_tick"] == 1  # scene 1 is not held up
     _check_invariants(ev, out, 100 * MB, 16)
+
+
+def test_two_frame_sets_overlap_versions():
+    # With two copies a move is applied while the previous version still
+    # renders; the next move waits for the version it overwrites.
+    ev = [_req(0, 1 * MB, 6), _move(1), _req(1, 1 * MB, 2), _move(2), _req(2, 1 * MB, 1)]
+    code, out = simulate_policy(ev, 100 * MB, 16, 1, frame_sets=2)
+    assert code == 0
+    assert out[1]["admit_tick"] == 1 and out[1]["version"] == 1  # applied at once
+    assert out[2]["version"] == 1 and out[2]["admit_tick"] == 1  # overlaps request 0
+    assert out[0]["done_tick"] > out[2]["admit_tick"]
+    assert out[3]["admit_tick"] > out[0]["done_tick"]             # version 2 overwrites version 0's copy
+    assert out[4]["version"] == 2 and out[4]["admit_tick"] >= out[3]["admit_tick"]
+    _check_invariants(ev, out, 100 * MB, 16)
+
+
+def test_pending_request_of_previous_version_still_admitted():
+    # A request queued for memory when the next move lands keeps its version
+    # and is admitted from the copy that still holds it.
+    ev = [_req(0, 80 * MB, 3), _req(0, 80 * MB, 1), _move(1), _req(1, 1 * MB, 1)]
+    code, out = simulate_policy(ev, 100 * MB, 16, 1, frame_sets=2)
+    assert code == 0
+    assert out[2]["admit_tick"] == 1               # move applied while request 1 waits for memory
+    assert out[1]["version"] == 0 and out[1]["admit_tick"] == 3
+    assert out[3]["version"] == 1
 
 
 def test_back_to_back_moves_apply_in_order():
     ev = [_move(0), _move(0), _req(0, 1 * MB, 1), _move(1), _req(1, 1 * MB, 1)]
-    code, out = simulate_policy(ev, 100 * MB, 16, 1)
+    code, out = simulate_policy(ev, 100 * MB, 16, 1, frame_sets=1)
     assert code == 0
     assert out[0]["version"] == 1 and out[1]["version"] == 2
     assert out[2]["version"] == 2 and out[4]["version"] == 3
@@ -98,8 +123,9 @@ def test_back_to_back_moves_apply_in_order():
     assert out[4]["admit_tick"] >= out[3]["admit_tick"]
 
 
+@pytest.mark.parametrize("frame_sets", [1, 2])
 @pytest.mark.parametrize("seed", [0, 1, 2, 3])
-def test_random_streams_keep_invariants(seed):
+def test_random_streams_keep_invariants(seed, frame_sets):
     rng = np.random.default_rng(seed)
     ev, t = [], 0
     for _ in range(300):
@@ -108,16 +134,24 @@ def test_random_streams_keep_invariants(seed):
             ev.append(_move(t, scene=int(rng.integers(0, 4))))
         else:
             ev.append(_req(t, int(rng.choice([1, 4, 16, 33]) * MB), int(rng.integers(1, 8)), scene=int(rng.integers(0, 4))))
-    code, out = simulate_policy(ev, 64 * MB, 8, 4)
+    code, out = simulate_policy(ev, 64 * MB, 8, 4, frame_sets=frame_sets)
     assert code == 0
     _check_invariants(ev, out, 64 * MB, 8)
-    # every request renders the version of its scene current at its arrival
     moves_before = {s: 0 for s in range(4)}
+    applied_at = {}
     for i, e in enumerate(ev):
+        s = e["scene"]
         if e["kind"] == _lib.POLICY_MOVE:
-            moves_before[e["scene"]] += 1
-            # applied after every earlier request of that scene finished
-            earlier = [j for j in range(i) if ev[j]["kind"] == _lib.POLICY_REQUEST and ev[j]["scene"] == e["scene"]]
-            assert all(out[j]["done_tick"] < out[i]["admit_tick"] for j in earlier)
+            moves_before[s] += 1
+            v = int(out[i]["version"])
+            assert v == moves_before[s]
+            applied_at[(s, v)] = int(out[i]["admit_tick"])
+            # the copy it overwrites held version v - frame_sets: all done
+            victims = [j for j in range(len(ev)) if ev[j]["kind"] == _lib.POLICY_REQUEST and ev[j]["scene"] == s
+                       and out[j]["status"] == 0 and out[j]["version"] == v - frame_sets]
+            assert all(out[j]["done_tick"] < out[i]["admit_tick"] for j in victims)
         else:
-            assert out[i]["version"] == moves_before[e["scene"]]
+            # every request renders the version of its scene current at its arrival
+            assert out[i]["version"] == moves_before[s]
+            if out[i]["version"] > 0 and out[i]["status"] == 0:
+                assert out[i]["admit_tick"] >= applied_at[(s, int(out[i]["version"]))]
