@@ -373,9 +373,12 @@ void destroy_fast(Ctx *c) {
     c->fast = nullptr;
 }
 
-// Closest hit over a ray batch; one thread per ray.
+// Closest hit over a ray batch; one thread per ray.  The occupancy bound
+// (8 blocks of 128 per SM, so at most 64 registers) was chosen by timing on
+// the B200: 12 % more rays/s than the unbounded 79-register build, whose
+// 6 resident blocks left the latency-bound walk short of warps.
 template <bool WT>
-__global__ void __launch_bounds__(128) k_closest_fast(DevScene S, FastView V, const ae_ray *__restrict__ rays,
+__global__ void __launch_bounds__(128, 8) k_closest_fast(DevScene S, FastView V, const ae_ray *__restrict__ rays,
                                                       uint32_t n, ae_hit *__restrict__ hits) {
     extern __shared__ uint2 stk[];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -153,8 +153,11 @@ def cpu_reference(scene, rays, budget_s=20.0):
 def measure_paths(local, width, height, frames=2):
     """Mpaths/s of compute-only frames (1 spp) on the wavefront workload:
     the plain megakernel against the wavefront form (4-wide 8-bit quantised
-    BVH, persistent stages, CUDA graph).  Frames are timed on the device
-    around the whole frame; the images of the two forms are compared."""
+    BVH, persistent stages, CUDA graph) and its precision form (watertight
+    test, FP16 shading normals, compensated accumulation).  Frames are timed
+    on the device around the whole frame; the plain and wavefront images are
+    compared, and primary-ray IDs of both optimised closest hits against the
+    plain kernel's."""
     from aviatorengine2_b200 import Context, _lib, scenes
     scene = scenes.wavefront_scene(width=width, height=height)
     out = {"workload": f"wavefront_scene {width}x{height}, 1 spp, depth {int(scene.config['depth'])}, "
@@ -163,7 +166,16 @@ def measure_paths(local, width, height, frames=2):
     imgs = {}
     with Context(width, height, device=local) as ctx:
         ctx.upload(scene)
-        for name, mode in (("plain", _lib.MODE_COMPUTE_ONLY), ("wavefront", _lib.MODE_WAVEFRONT)):
+        # Primary-ray instance and triangle IDs of the optimised closest hits
+        # against the reference-order kernel, on this frame's camera rays.
+        rays = ctx.camera_rays()
+        ref = ctx.closest_hit(rays, _lib.VARIANT_PLAIN)
+        for name, var in (("fast", _lib.VARIANT_FAST), ("precision", _lib.VARIANT_QUANT)):
+            h = ctx.closest_hit(rays, var)
+            out[f"primary_id_agreement_{name}"] = float(((h["object"] == ref["object"]) &
+                                                         (h["prim"] == ref["prim"])).mean())
+        for name, mode in (("plain", _lib.MODE_COMPUTE_ONLY), ("wavefront", _lib.MODE_WAVEFRONT),
+                           ("precision", _lib.MODE_WAVEFRONT_PRECISION)):
             c = scene.config.copy()
             ms = []
             for b in range(frames + 1):  # frame 0 warms up (and autotunes the wavefront)
@@ -179,6 +191,7 @@ def measure_paths(local, width, height, frames=2):
         info = ctx.wavefront_info()
         out["wavefront_extend"] = {"threads": info["threads"], "stack": info["stack"]}
     out["speedup"] = out["wavefront_mpaths"] / out["plain_mpaths"]
+    out["precision_speedup"] = out["precision_mpaths"] / out["plain_mpaths"]
     a, b = imgs["plain"], imgs["wavefront"]
     out["frames_bit_exact"] = bool(np.array_equal(a.view(np.uint32), b.view(np.uint32)))
     out["pixels_differing"] = int(np.any(a.view(np.uint32) != b.view(np.uint32), axis=-1).sum())
