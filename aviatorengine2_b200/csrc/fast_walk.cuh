@@ -1,0 +1,224 @@
+// fast_walk.cuh - the optimised closest hit (closest_fast, fast_trace.cuh)
+// re-expressed as a state machine that advances one step per call: one TLAS
+// node, one TLAS-leaf object, or one BLAS node (a leaf's triangles included).
+//
+// Why: the nested form runs a TLAS loop, a per-object loop and a BLAS loop
+// inside one another, and the lanes of a warp wait at the end of each inner
+// loop for the slowest lane.  On incoherent rays (bounces, shadow samples)
+// only a few lanes were active per instruction.  A kernel built on Walker
+// keeps every lane stepping its own ray and lets a lane that finishes start
+// its next ray at once, so warps stay full.
+//
+// Each ray takes exactly the steps of closest_fast in the same order with the
+// same arithmetic (same ToLocal, child order, stack discipline, ranking of
+// equal distances), so the Best it returns is bit-identical.
+#pragma once
+#include "fast_trace.cuh"
+
+namespace ae {
+
+enum : uint32_t { kWalkTlas = 0, kWalkObject = 1, kWalkBlas = 2, kWalkDone = 3 };
+
+// The walk's per-thread local stacks: the TLAS stack and the BLAS entries
+// beyond the shared-memory part.  Kept out of Walker so its scalar state can
+// live in registers.
+template <int SS = kSharedStack>
+struct WalkStacks {
+    int tstack[kTlasStack];
+    float tdist[kTlasStack];
+    uint2 spill[kFastStack - SS];
+};
+
+template <bool WT, int SS = kSharedStack>
+struct Walker {
+    // ray
+    f3 o, d, tinv, rinv;
+    float tn, time;
+    Best best;
+    uint32_t phase;
+    // TLAS
+    uint32_t tnode;
+    int tsp;
+    // objects of the current TLAS leaf
+    uint32_t ofirst, ocount, ok;
+    // current mesh instance
+    f3 lo, ld, linv;
+    WtRay W;
+    uint32_t tri_base, cur, slot;
+    uint64_t orank;
+    int bsp;
+
+    AE_DEV void start(const DevScene &S, f3 o_, f3 d_, float tn_, float time_) {
+        o = o_;
+        d = d_;
+        tn = tn_;
+        time = time_;
+        best.t = kFarStart; best.alpha = 0.0f; best.beta = 0.0f;
+        best.object = AE_MISS; best.prim = AE_MISS; best.orank = 0; best.lrank = 0;
+        tsp = 0;
+        phase = kWalkDone;
+        if (S.n_nodes == 0) return;
+        tinv = mk(slab_inv(d.x), slab_inv(d.y), slab_inv(d.z));
+        rinv = 1.0f / d;
+        const NodeBox nb = load_node(S.tlas, 0);
+        if (slab_ref(o, rinv, nb.lo, nb.hi, tn, kFarStart)) {
+            tnode = 0;
+            phase = kWalkTlas;
+        }
+    }
+
+    // Next TLAS stack entry no farther than the best hit, or done.
+    AE_DEV void tlas_pop(const WalkStacks<SS> &K) {
+        while (tsp > 0) {
+            tsp--;
+            if (K.tdist[tsp] <= best.t) {
+                tnode = uint32_t(K.tstack[tsp]);
+                phase = kWalkTlas;
+                return;
+            }
+        }
+        phase = kWalkDone;
+    }
+
+    // Next BLAS stack entry no farther than the best hit, or back to the
+    // leaf's remaining objects.
+    AE_DEV void blas_pop(const WalkStacks<SS> &K, const uint2 *stk, int tid, int nt) {
+        while (bsp > 0) {
+            bsp--;
+            const uint2 e = bsp < SS ? stk[bsp * nt + tid] : K.spill[bsp - SS];
+            if (__uint_as_float(e.y) <= best.t) {
+                cur = e.x;
+                return;
+            }
+        }
+        phase = kWalkObject;
+    }
+
+    // One step; returns true once the ray is finished (best is final).
+    AE_DEV bool step(const DevScene &S, const FastView &V, WalkStacks<SS> &K, uint2 *stk, int tid, int nt) {
+        if (phase == kWalkBlas) {
+            if (cur & kLeafBit) {
+                const uint32_t first = leaf_first(cur), cnt = leaf_count(cur);
+                const float4 *tris = V.tris + size_t(tri_base) * 3;
+                for (uint32_t k = 0; k < cnt; k++) {
+                    const uint32_t s = first + k;
+                    const float4 *r = tris + size_t(s) * 3;
+                    const float4 r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2);
+                    float t, a, b;
+                    const bool h = WT ? tri_test_wt(lo, W, tn, best.t, r0, r1, r2, t, a, b)
+                                      : tri_test_ref(lo, ld, tn, best.t, r0, r1, r2, t, a, b);
+                    if (h && takes(best, t, orank, ~first, s)) {
+                        best.t = t; best.alpha = a; best.beta = b;
+                        best.object = slot; best.prim = s;
+                        best.orank = orank; best.lrank = ~first;
+                    }
+                }
+                blas_pop(K, stk, tid, nt);
+            } else {
+                float tm[4];
+                uint32_t ch[4];
+                child_hits(V.nodes + cur, lo, linv, tn, best.t, tm, ch);
+#define AE_SWAP(i, j)                                            \
+    if (tm[j] < tm[i]) {                                         \
+        const float tt = tm[i]; tm[i] = tm[j]; tm[j] = tt;       \
+        const uint32_t cc = ch[i]; ch[i] = ch[j]; ch[j] = cc;    \
+    }
+                AE_SWAP(0, 1) AE_SWAP(2, 3) AE_SWAP(0, 2) AE_SWAP(1, 3) AE_SWAP(1, 2)
+#undef AE_SWAP
+                int nh = 0;
+#pragma unroll
+                for (int k = 0; k < 4; k++) nh += tm[k] != __int_as_float(0x7f800000) ? 1 : 0;
+                if (nh > 0) {
+                    for (int k = nh - 1; k >= 1; k--) {
+                        if (bsp < SS) stk[bsp * nt + tid] = make_uint2(ch[k], __float_as_uint(tm[k]));
+                        else if (bsp < kFastStack) K.spill[bsp - SS] = make_uint2(ch[k], __float_as_uint(tm[k]));
+                        bsp = bsp < kFastStack ? bsp + 1 : bsp;
+                    }
+                    cur = ch[0];
+                } else {
+                    blas_pop(K, stk, tid, nt);
+                }
+            }
+            return false;
+        }
+        if (phase == kWalkObject) {
+            if (ok >= ocount) {
+                tlas_pop(K);
+                return phase == kWalkDone;
+            }
+            slot = ofirst + ok;
+            ok++;
+            orank = (uint64_t(~ofirst) << 32) | slot;
+            const uint4 m = __ldg(V.meta + slot);
+            const uint32_t shape = m.x & 0xff;
+            if (shape == AE_SHAPE_MESH) {
+                // ToLocal (hybrid:534-543), as trace_mesh.
+                const float4 *ip = reinterpret_cast<const float4 *>(V.inst + m.y);
+                const float4 a = __ldg(ip), b = __ldg(ip + 1), c = __ldg(ip + 2);
+                lo = quat_rotate(-b.x, -b.y, -b.z, b.w, o - mk(a.x, a.y, a.z));
+                ld = quat_rotate(-b.x, -b.y, -b.z, b.w, d);
+                if (a.w != 0.0f && a.w != 1.0f) {
+                    const float inv = AE_DIV(1.0f, a.w);
+                    lo = lo * inv;
+                    ld = ld * inv;
+                }
+                linv = mk(slab_inv(ld.x), slab_inv(ld.y), slab_inv(ld.z));
+                if (WT) W = wt_setup(ld);
+                tri_base = __float_as_uint(c.y);
+                cur = __float_as_uint(c.x);
+                bsp = 0;
+                phase = kWalkBlas;
+            } else {
+                DHit h;
+                const ae_object *obj = S.objects + slot;
+                bool hit;
+                if (shape == AE_SHAPE_SPHERE) hit = hit_sphere_ref(obj, o, d, time, tn, best.t, h);
+                else if (shape == AE_SHAPE_QUAD) hit = hit_planar_ref(obj, false, o, d, tn, best.t, h);
+                else if (shape == AE_SHAPE_TRIANGLE) hit = hit_planar_ref(obj, true, o, d, tn, best.t, h);
+                else hit = hit_box_ref(obj, o, d, tn, best.t, h);
+                if (hit && takes(best, h.t, orank, 0u, 0u)) {
+                    best.t = h.t; best.alpha = h.alpha; best.beta = h.beta;
+                    best.object = slot; best.prim = AE_MISS; best.orank = orank; best.lrank = 0;
+                }
+            }
+            return false;
+        }
+        if (phase == kWalkTlas) {
+            const NodeBox nb = load_node(S.tlas, tnode);
+            if (nb.count > 0) {
+                ofirst = uint32_t(nb.left);
+                ocount = uint32_t(nb.count);
+                ok = 0;
+                phase = kWalkObject;
+                return false;
+            }
+            const NodeBox L = load_node(S.tlas, uint32_t(nb.left)), R = load_node(S.tlas, uint32_t(nb.right));
+            const f3 lt0 = (L.lo - o) * tinv, lt1 = (L.hi - o) * tinv;
+            const f3 rt0 = (R.lo - o) * tinv, rt1 = (R.hi - o) * tinv;
+            const float lmin = fmaxf(fmaxf(fminf(lt0.x, lt1.x), fminf(lt0.y, lt1.y)), fmaxf(fminf(lt0.z, lt1.z), tn));
+            const float lmax = fminf(fminf(fmaxf(lt0.x, lt1.x), fmaxf(lt0.y, lt1.y)), fmaxf(lt0.z, lt1.z));
+            const float rmin = fmaxf(fmaxf(fminf(rt0.x, rt1.x), fminf(rt0.y, rt1.y)), fmaxf(fminf(rt0.z, rt1.z), tn));
+            const float rmax = fminf(fminf(fmaxf(rt0.x, rt1.x), fmaxf(rt0.y, rt1.y)), fmaxf(rt0.z, rt1.z));
+            const float lmin_c = lmin * kEntryShrink, rmin_c = rmin * kEntryShrink;
+            const bool lh = lmin_c <= fminf(lmax * kExitGrow, best.t);
+            const bool rh = rmin_c <= fminf(rmax * kExitGrow, best.t);
+            if (lh && rh) {
+                const bool lfirst = lmin <= rmin;
+                if (tsp < kTlasStack) {
+                    K.tstack[tsp] = lfirst ? nb.right : nb.left;
+                    K.tdist[tsp] = lfirst ? rmin_c : lmin_c;
+                    tsp++;
+                }
+                tnode = uint32_t(lfirst ? nb.left : nb.right);
+                return false;
+            }
+            if (lh) { tnode = uint32_t(nb.left); return false; }
+            if (rh) { tnode = uint32_t(nb.right); return false; }
+            tlas_pop(K);
+            return phase == kWalkDone;
+        }
+        return true;
+    }
+};
+
+}  // namespace ae

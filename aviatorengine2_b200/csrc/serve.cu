@@ -53,6 +53,7 @@
 #include "context.h"
 #include "fast.h"
 #include "fast_trace.cuh"
+#include "fast_walk.cuh"
 #include "kernels.h"
 #include "serve_policy.h"
 #include "shade.cuh"
@@ -210,18 +211,54 @@ __global__ void __launch_bounds__(256) k_sv_shade(SvView W, int q) {
 
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS) k_sv_shadow(SvView W) {
+    // The reference's shadow loop per light sample on the step-wise Walker:
+    // a lane that finishes a sample starts its next one at once.  The
+    // sample's scene (its slot's) is read through the scene table.
     extern __shared__ uint2 stk[];
     const uint32_t count = W.cnt[SV_SH];
-    for (uint32_t k = blockIdx.x * THREADS + threadIdx.x; k < count; k += gridDim.x * THREADS) {
-        const uint32_t e = W.sq[k];
-        const uint32_t slot = e / W.max_lights;
-        const SceneRec &R = W.scenes[W.s_scene[slot]];
-        const DevScene S = R.S;
-        const FastView V = R.V;
+    const uint32_t stride = gridDim.x * THREADS;
+    uint32_t k = blockIdx.x * THREADS + threadIdx.x;
+    Walker<false> w;
+    WalkStacks<> K;
+    const SceneRec *R = nullptr;
+    uint32_t e = 0;
+    f3 so, sd, lp;
+    int step = 0;
+    bool active = k < count;
+    if (active) {
+        e = W.sq[k];
+        R = W.scenes + W.s_scene[e / W.max_lights];
         const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
-        const bool occluded = shadow_occluded(S, V, mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z), mk(l4.x, l4.y, l4.z),
-                                              d4.w, stk, threadIdx.x, THREADS);
-        W.sh.occ[e] = occluded ? 1 : 0;
+        so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
+        w.start(R->S, so, sd, 0.001f, d4.w);
+    }
+    while (active) {
+        if (!w.step(R->S, R->V, K, stk, threadIdx.x, THREADS)) continue;
+        const Best &b = w.best;
+        int verdict = 0;  // 0 unoccluded, 1 occluded, 2 through glass
+        if (b.object != AE_MISS && b.t < AE_SUB(distance(lp, so), 0.001f)) {
+            const uint32_t mt = load_head(R->S.objects + b.object).material;
+            verdict = mt == AE_MAT_DIFFUSE_LIGHT ? 0 : (mt != AE_MAT_DIELECTRIC ? 1 : 2);
+        }
+        if (verdict == 2) {
+            so = (so + sd * b.t) + sd * 0.001f;
+            if (++step < 4) {
+                w.start(R->S, so, sd, 0.001f, w.time);
+                continue;
+            }
+            verdict = 0;
+        }
+        W.sh.occ[e] = uint8_t(verdict);
+        k += stride;
+        active = k < count;
+        if (active) {
+            e = W.sq[k];
+            R = W.scenes + W.s_scene[e / W.max_lights];
+            const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
+            so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
+            step = 0;
+            w.start(R->S, so, sd, 0.001f, d4.w);
+        }
     }
 }
 
