@@ -112,6 +112,7 @@ SIGNATURES = {
     "ae_last_error": (ctypes.c_char_p, [_P]),
     "ae_upload_geometry": (_I, [_P, _P, _U32, _P, _U32, _P, _U32]),
     "ae_reserve_scene": (_I, [_P, _U32, _U32]),
+    "ae_upload_textures": (_I, [_P, _P, _U32, _U32, _U32]),
     "ae_upload_scene": (_I, [_P, _P, _U32, _P, _U32, _P, _U32, _P, _U32]),
     "ae_set_config": (_I, [_P, _P]),
     "ae_get_config": (_I, [_P, _P]),

@@ -287,6 +287,57 @@ AE_HD float rng_next(uint32_t &seed) {
     return AE_MUL(AE_U2F((x >> 22u) ^ x), 2.3283064365386963e-10f);  // / 2^32 (exact)
 }
 
+// ---------------------------------------------------------------------------
+// Texture sampling: GlobalTextureArray.SampleLevel(GlobalSampler,
+// float3(uv, layer), 0) (hybrid:919-925) on the reference's texture array and
+// sampler.  The array is RGBA8 sRGB, `layers` images of w x h texels of one
+// size (scene/texture.h:110-230, one level); the sampler filters linearly and
+// repeats on u and v (renderer/renderer.cpp:226-233).  Texels are decoded from
+// sRGB to linear before filtering, as the sRGB format requires, through a
+// 256-entry table of srgb_to_linear; the bilinear weights and blends are
+// binary32 operations (graphics hardware uses fixed-point sub-texel weights,
+// which no specification pins down).  A layer beyond the last is clamped to
+// it; non-finite coordinates sample at 0.
+// ---------------------------------------------------------------------------
+AE_HD float srgb_to_linear(uint32_t byte) {
+    const float c = AE_DIV(AE_U2F(byte), 255.0f);
+    return c <= 0.04045f ? AE_DIV(c, 12.92f) : powf_(AE_DIV(AE_ADD(c, 0.055f), 1.055f), 2.4f);
+}
+
+// Texel index of floor(x) (an integral float) under REPEAT addressing.
+AE_HD uint32_t repeat_index(float fl, uint32_t n) {
+    const float g = AE_FMIN(AE_FMAX(fl, -1073741824.0f), 1073741824.0f);
+    const int64_t i = (int64_t)g;
+    int64_t m = i % (int64_t)n;
+    if (m < 0) m += (int64_t)n;
+    return (uint32_t)m;
+}
+
+AE_HD f3 texel_linear(const uint32_t *layer, const float *lut, uint32_t w, uint32_t x, uint32_t y) {
+    const uint32_t t = layer[(size_t)y * w + x];
+    return mk(lut[t & 0xffu], lut[(t >> 8) & 0xffu], lut[(t >> 16) & 0xffu]);
+}
+
+// texels: layers * h * w RGBA8 words (r in the low byte), layer-major.
+AE_HD f3 texture_sample(const uint32_t *texels, const float *lut, uint32_t w, uint32_t h, uint32_t layers,
+                        uint32_t layer, float u, float v) {
+    if (layers == 0u || w == 0u || h == 0u) return splat(1.0f);  // BuildGPUArray's white layer
+    if (layer >= layers) layer = layers - 1u;
+    if (!(AE_FABS(u) <= 3.4028234e38f)) u = 0.0f;
+    if (!(AE_FABS(v) <= 3.4028234e38f)) v = 0.0f;
+    const float x = AE_SUB(AE_MUL(u, AE_U2F(w)), 0.5f), y = AE_SUB(AE_MUL(v, AE_U2F(h)), 0.5f);
+    const float fx = AE_FLOOR(x), fy = AE_FLOOR(y);
+    const float ax = AE_SUB(x, fx), ay = AE_SUB(y, fy);
+    const uint32_t x0 = repeat_index(fx, w), x1 = repeat_index(AE_ADD(fx, 1.0f), w);
+    const uint32_t y0 = repeat_index(fy, h), y1 = repeat_index(AE_ADD(fy, 1.0f), h);
+    const uint32_t *L = texels + (size_t)layer * w * h;
+    const f3 c00 = texel_linear(L, lut, w, x0, y0), c10 = texel_linear(L, lut, w, x1, y0);
+    const f3 c01 = texel_linear(L, lut, w, x0, y1), c11 = texel_linear(L, lut, w, x1, y1);
+    const f3 top = c00 + (c10 - c00) * ax;
+    const f3 bottom = c01 + (c11 - c01) * ax;
+    return top + (bottom - top) * ay;
+}
+
 // Quaternion rotate, math/quat.hpp:211-217 and hybrid:521-526:
 // v + w t + u x t with t = 2 (u x v).
 AE_HD f3 quat_rotate(float qx, float qy, float qz, float qw, f3 v) {

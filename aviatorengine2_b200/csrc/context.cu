@@ -52,6 +52,11 @@ DevScene Ctx::scene() const {
     S.n_nodes = n_nodes;
     S.n_lights = n_lights;
     S.n_instances = n_instances;
+    S.tex = tex.ptr;
+    S.srgb = srgb_lut.ptr;
+    S.tex_w = tex_w;
+    S.tex_h = tex_h;
+    S.tex_layers = tex_layers;
     return S;
 }
 
@@ -255,6 +260,37 @@ int ae_upload_geometry(ae_ctx *ctx, const ae_vertex *v, uint32_t nv, const uint3
     c->fast_ready = false;
     c->geometry_uploaded = true;
     return c->cuda(cudaStreamSynchronize(c->stream), "upload geometry");
+}
+
+// The material texture array: TextureLibrary::BuildGPUArray's result
+// (scene/texture.h:110-230) as plain bytes, plus the 256-entry sRGB decode
+// table every sample uses.
+int ae_upload_textures(ae_ctx *ctx, const uint8_t *texels, uint32_t width, uint32_t height, uint32_t layers) {
+    Ctx *c = reinterpret_cast<Ctx *>(ctx);
+    if (!c) return AE_ERR_INVALID;
+    if (layers && (!texels || !width || !height)) return c->fail(AE_ERR_INVALID, "bad texture array arguments");
+    if (layers && (width > 2048u || height > 2048u))
+        return c->fail(AE_ERR_OVERSIZE, "texture layers are at most 2048x2048 (kMaxTextureArrayDimension)");
+    if (layers > 2048u) return c->fail(AE_ERR_OVERSIZE, "at most 2048 texture layers");
+    cudaSetDevice(c->settings.device);
+    if (!c->srgb_lut.ptr) {
+        float lut[256];
+        for (uint32_t b = 0; b < 256; b++) lut[b] = srgb_to_linear(b);
+        int rc;
+        if (c->srgb_lut.reserve(256)) return c->fail(AE_ERR_OOM, "sRGB table");
+        if ((rc = c->cuda(cudaMemcpyAsync(c->srgb_lut.ptr, lut, sizeof(lut), cudaMemcpyHostToDevice, c->stream),
+                          "upload sRGB table")))
+            return rc;
+        if ((rc = c->cuda(cudaStreamSynchronize(c->stream), "upload sRGB table"))) return rc;
+    }
+    const size_t words = size_t(width) * height * layers;
+    int rc = upload(c, c->tex, reinterpret_cast<const uint32_t *>(texels), words, "textures");
+    if (rc) return rc;
+    c->tex_w = layers ? width : 0;
+    c->tex_h = layers ? height : 0;
+    c->tex_layers = layers;
+    c->scene_version++;
+    return c->cuda(cudaStreamSynchronize(c->stream), "upload textures");
 }
 
 int ae_reserve_scene(ae_ctx *ctx, uint32_t max_objects, uint32_t max_lights) {

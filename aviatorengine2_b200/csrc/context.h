@@ -83,6 +83,11 @@ struct Ctx {
     uint64_t scene_version_layout = 0;  // bumps when arrays are re-uploaded (topology may change)
     DevBuf<float> obj_box;              // world box per object (refit)
 
+    // Material texture array (ae_upload_textures) and its sRGB decode table.
+    DevBuf<uint32_t> tex;
+    DevBuf<float> srgb_lut;
+    uint32_t tex_w = 0, tex_h = 0, tex_layers = 0;
+
     // Images.
     DevBuf<float4> accum, frame;
     DevBuf<uchar4> display;

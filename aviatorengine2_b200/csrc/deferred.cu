@@ -25,6 +25,7 @@
 #include "context.h"
 #include "fast.h"
 #include "kernels.h"
+#include "shade.cuh"
 #include "trace_common.cuh"
 
 namespace ae {
@@ -266,18 +267,20 @@ struct SurfRec {  // the Hit of deferred.comp: geometry plus the material it sha
     f3 p, n;
     bool front;
     uint32_t slot;
-    f3 albedo;
+    f3 albedo;  // Object.Albedo (the G-buffer's albedo for raster surfaces)
+    f3 surf;    // SurfaceAlbedo (deferred:1194-1203): textured when the material has a layer
     float fuzz, emission, refraction;
     uint32_t type, shape;
 };
 
-AE_DEV SurfRec surf_from_hit(const DevScene &S, const DHit &h) {
+AE_DEV SurfRec surf_from_hit(const DevScene &S, const DHit &h, f3 o, f3 d) {
     const char *b = reinterpret_cast<const char *>(S.objects + h.slot);
     const float4 m0 = ld4(b + 80), m1 = ld4(b + 96), m2 = ld4(b + 112);
     SurfRec s;
     s.p = h.p; s.n = h.n; s.front = h.front; s.slot = h.slot;
     s.albedo = mk(m1.x, m1.y, m1.z); s.fuzz = m1.w; s.emission = m0.y; s.refraction = m2.x;
     s.shape = __float_as_uint(m2.y); s.type = __float_as_uint(m2.z);
+    s.surf = surface_albedo(S, h, load_mat(S.objects + h.slot), o, d);
     return s;
 }
 
@@ -379,7 +382,7 @@ AE_DEV f3 clamped_direct(const DevScene &S, const SurfRec &h, float time, uint32
             const char *lb = reinterpret_cast<const char *>(L);
             const float4 m0 = ld4(lb + 80), m1 = ld4(lb + 96);
             const f3 rad = m0.y * mk(m1.x, m1.y, m1.z);
-            acc = acc + h.albedo * rad * ct * omega;
+            acc = acc + h.surf * rad * ct * omega;
         }
     }
     const float luma = maxc(acc);
@@ -395,7 +398,7 @@ AE_DEV f3 trace_indirect(const DevScene &S, const DefParams &P, f3 pd, float tim
     f3 d = normalize(bd);
     const float s0 = dot(d, surf.n) < 0.0f ? -1.0f : 1.0f;
     f3 o = surf.p + surf.n * AE_MUL(0.001f, s0);
-    f3 thr = surf.type != AE_MAT_DIELECTRIC ? surf.albedo : splat(1.0f);
+    f3 thr = surf.type != AE_MAT_DIELECTRIC ? surf.surf : splat(1.0f);
     f3 acc = splat(0.0f);
     for (uint32_t b = 1; b < P.F.depth; b++) {
         DHit h;
@@ -403,7 +406,7 @@ AE_DEV f3 trace_indirect(const DevScene &S, const DefParams &P, f3 pd, float tim
             acc = acc + thr * P.F.sky;
             break;
         }
-        const SurfRec s = surf_from_hit(S, h);
+        const SurfRec s = surf_from_hit(S, h, o, d);
         if (s.type == AE_MAT_DIFFUSE_LIGHT) {
             acc = acc + thr * (s.emission * s.albedo);
             break;
@@ -414,7 +417,7 @@ AE_DEV f3 trace_indirect(const DevScene &S, const DefParams &P, f3 pd, float tim
         d = normalize(nx);
         const float sg = dot(d, s.n) < 0.0f ? -1.0f : 1.0f;
         o = s.p + s.n * AE_MUL(0.001f, sg);
-        if (s.type != AE_MAT_DIELECTRIC) thr = thr * s.albedo;
+        if (s.type != AE_MAT_DIELECTRIC) thr = thr * s.surf;
         const float p = clampf(maxc(thr), 0.1f, 1.0f);
         if (rng_next(seed) > p) break;
         thr = thr / p;
@@ -602,18 +605,20 @@ __global__ void __launch_bounds__(128) k_gbuffer(DevScene S, DefParams P, GBuf G
         (void)shade_n;
         if (found) {
             const ae_object *obj = S.objects + best.slot;
-            const char *b = reinterpret_cast<const char *>(obj);
-            const float4 m1 = ld4(b + 96), m2 = ld4(b + 112);
-            const uint32_t type = __float_as_uint(m2.z);
+            const MatRec mat = load_mat(obj);
+            const uint32_t type = mat.type;
+            // SurfaceBlock's albedo (gbuffer.frag:44-50): textured at the
+            // hit's UV when the material has a layer.
+            const f3 sa = surface_albedo(S, best, mat, o, d);
             // The raster normal is the surface's own (outward), not flipped
             // toward the viewer: undo the intersector's facing flip.
             const f3 nn = best.front ? best.n : -best.n;
             pos = make_float4(best.p.x, best.p.y, best.p.z, AE_U2F(best.slot));
             nrm = make_float4(nn.x, nn.y, nn.z, 1.0f);
             const bool vd = type == AE_MAT_METAL || type == AE_MAT_DIELECTRIC;
-            alb = make_uchar4((unsigned char)(int)AE_RINT(AE_MUL(saturate(m1.x), 255.0f)),
-                              (unsigned char)(int)AE_RINT(AE_MUL(saturate(m1.y), 255.0f)),
-                              (unsigned char)(int)AE_RINT(AE_MUL(saturate(m1.z), 255.0f)), vd ? 0 : 255);
+            alb = make_uchar4((unsigned char)(int)AE_RINT(AE_MUL(saturate(sa.x), 255.0f)),
+                              (unsigned char)(int)AE_RINT(AE_MUL(saturate(sa.y), 255.0f)),
+                              (unsigned char)(int)AE_RINT(AE_MUL(saturate(sa.z), 255.0f)), vd ? 0 : 255);
             // PerspectiveRH_ZO depth (math/mat4.h:84-95) of the view-space z.
             const float vz = dot(best.p - o, -P.F.cam_w);
             depth = AE_DIV(AE_MUL(P.zfar, AE_SUB(P.znear, vz)), AE_MUL(AE_SUB(P.znear, P.zfar), vz));
@@ -644,6 +649,7 @@ AE_DEV int resolve_primary(const DevScene &S, const GBuf &G, size_t px, f3 o, f3
             const float4 m0 = ld4(b + 80), m1 = ld4(b + 96), m2 = ld4(b + 112);
             const uchar4 a = G.alb[px];
             raster.albedo = mk(AE_DIV(AE_U2F(a.x), 255.0f), AE_DIV(AE_U2F(a.y), 255.0f), AE_DIV(AE_U2F(a.z), 255.0f));
+            raster.surf = raster.albedo;  // HitFromGBuffer clears TextureID (deferred:1477-1480)
             raster.fuzz = m1.w; raster.emission = m0.y; raster.refraction = m2.x;
             raster.shape = __float_as_uint(m2.y); raster.type = __float_as_uint(m2.z);
             raster.front = dot(d, raster.n) < 0.0f;
@@ -654,7 +660,7 @@ AE_DEV int resolve_primary(const DevScene &S, const GBuf &G, size_t px, f3 o, f3
     }
     DHit ah;
     if (traverse_bounded(S, o, d, time, 0.001f, far_limit, true, ah, seed)) {
-        hit = surf_from_hit(S, ah);
+        hit = surf_from_hit(S, ah, o, d);
         return 2;
     }
     if (has_raster) {
@@ -758,7 +764,7 @@ __global__ void __launch_bounds__(128) k_deferred(DevScene S, DefParams P, GBuf 
     if (P.reduced) {
         const bool demod = source == 1 && hit.type != AE_MAT_DIELECTRIC;
         f3 alb = splat(1.0f);
-        if (demod) alb = vmax(hit.albedo, splat(0.01f));
+        if (demod) alb = vmax(hit.surf, splat(0.01f));
         const f3 l = color / alb;
         I.reduced[size_t(cy) * P.ext_w + cx] = make_float4(l.x, l.y, l.z, demod ? 1.0f : 0.0f);
         return;

@@ -13,11 +13,13 @@ struct MatRec {
     f3 albedo;
     float fuzz, emission, refraction;
     uint32_t type;
+    uint32_t texture;  // layer in the texture array, or AE_NO_TEXTURE
+    float tint;        // TextureTint
 };
 AE_DEV MatRec load_mat(const ae_object *o) {
     const char *b = reinterpret_cast<const char *>(o);
     const float4 m0 = ld4(b + 80), m1 = ld4(b + 96), m2 = ld4(b + 112);
-    return MatRec{mk(m1.x, m1.y, m1.z), m1.w, m0.y, m2.x, __float_as_uint(m2.z)};
+    return MatRec{mk(m1.x, m1.y, m1.z), m1.w, m0.y, m2.x, __float_as_uint(m2.z), __float_as_uint(m2.w), m0.w};
 }
 
 AE_DEV f3 random_direction(uint32_t &seed) {
@@ -197,6 +199,71 @@ AE_DEV bool hit_normal(const DevScene &S, const ae_hit &h, f3 d, f3 &n) {
     n = normalize(quat_rotate(i1.x, i1.y, i1.z, i1.w, sh));
     if (!(dot(d, quat_rotate(i1.x, i1.y, i1.z, i1.w, geo)) < 0.0f)) n = -n;
     return true;
+}
+
+// Surface UV of a hit, recomputed from its record exactly as the intersector
+// that produced it sets hit.surface_uv: meshes interpolate the vertex UVs
+// (hybrid:702-704), quads and triangles take (alpha, beta) (467, 505),
+// spheres get_sphere_uv of the facing normal (264-271, 419), boxes BoxFaceUV
+// of the local hit point (711-727, 763), volumes (0, 0) (819).
+AE_DEV void hit_uv(const DevScene &S, const DHit &h, f3 o, f3 d, float &u, float &v) {
+    const ae_object *obj = S.objects + h.slot;
+    const ObjHead hd = load_head(obj);
+    const char *b = reinterpret_cast<const char *>(obj);
+    u = 0.0f;
+    v = 0.0f;
+    if (hd.material == AE_MAT_ISOTROPIC) return;
+    if (hd.shape == AE_SHAPE_MESH) {
+        const uint32_t ii = __float_as_uint(ld4(b + 80).z);
+        const float4 i2 = ld4(reinterpret_cast<const char *>(S.instances + ii) + 32);
+        const uint32_t vbase = __float_as_uint(i2.x), base = __float_as_uint(i2.y) + h.prim * 3u;
+        const float4 a1 = ld4(reinterpret_cast<const char *>(S.vertices + vbase + __ldg(S.indices + base)) + 16);
+        const float4 b1 = ld4(reinterpret_cast<const char *>(S.vertices + vbase + __ldg(S.indices + base + 1)) + 16);
+        const float4 c1 = ld4(reinterpret_cast<const char *>(S.vertices + vbase + __ldg(S.indices + base + 2)) + 16);
+        const float w0 = AE_SUB(AE_SUB(1.0f, h.alpha), h.beta);
+        u = AE_ADD(AE_ADD(AE_MUL(w0, a1.z), AE_MUL(h.alpha, b1.z)), AE_MUL(h.beta, c1.z));
+        v = AE_ADD(AE_ADD(AE_MUL(w0, a1.w), AE_MUL(h.alpha, b1.w)), AE_MUL(h.beta, c1.w));
+        return;
+    }
+    if (hd.shape == AE_SHAPE_QUAD || hd.shape == AE_SHAPE_TRIANGLE) {
+        u = h.alpha;
+        v = h.beta;
+        return;
+    }
+    if (hd.shape == AE_SHAPE_SPHERE) {
+        const float rot = ld4(b + 64).w;
+        const float theta = acosf_(-h.n.y);
+        const float phi = AE_ADD(atan2f_(-h.n.z, h.n.x), 3.14159265f);
+        u = fracf(AE_SUB(AE_DIV(phi, 6.2831853f), AE_DIV(rot, 6.2831853f)));
+        v = AE_DIV(theta, 3.14159265f);
+        return;
+    }
+    // Box: the local ray of BoxSpan, the face it was hit on.
+    const float4 q0 = ld4(b), q4 = ld4(b + 64);
+    const float sn = sinf_(q4.w), cs = cosf_(q4.w);
+    const f3 lo = yaw_rot(o - mk(q0.x, q0.y, q0.z), -sn, cs);
+    const f3 ld = yaw_rot(d, -sn, cs);
+    float tin, tout;
+    f3 nin, nout;
+    box_span_ref(obj, o, d, tin, tout, nin, nout);
+    const f3 ln = h.t == tin ? nin : nout;
+    const f3 lp = lo + ld * h.t;
+    float uu, vv;
+    if (AE_FABS(ln.x) > 0.5f) { uu = AE_DIV(lp.z, q4.z); vv = AE_DIV(lp.y, q4.y); }
+    else if (AE_FABS(ln.y) > 0.5f) { uu = AE_DIV(lp.x, q4.x); vv = AE_DIV(lp.z, q4.z); }
+    else { uu = AE_DIV(lp.x, q4.x); vv = AE_DIV(lp.y, q4.y); }
+    u = saturate(AE_ADD(AE_MUL(uu, 0.5f), 0.5f));
+    v = saturate(AE_ADD(AE_MUL(vv, 0.5f), 0.5f));
+}
+
+// SurfaceAlbedo, hybrid:940-949: the flat albedo, or the texel at the hit's
+// UV tinted by the albedo (texel * lerp(1, albedo, TextureTint)).
+AE_DEV f3 surface_albedo(const DevScene &S, const DHit &h, const MatRec &m, f3 o, f3 d) {
+    if (m.texture == AE_NO_TEXTURE) return m.albedo;
+    float u, v;
+    hit_uv(S, h, o, d, u, v);
+    const f3 texel = texture_sample(S.tex, S.srgb, S.tex_w, S.tex_h, S.tex_layers, m.texture, u, v);
+    return texel * lerp(splat(1.0f), m.albedo, m.tint);
 }
 
 // ToneMapACES + LinearToSRGB (hybrid:213-233) into 8-bit sRGB.

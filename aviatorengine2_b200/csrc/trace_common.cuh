@@ -39,6 +39,11 @@ struct DevScene {
     const ae_bvh_node *blas;
     const ae_instance *instances;
     uint32_t n_objects, n_nodes, n_lights, n_instances;
+    // material texture array (RGBA8 sRGB words, layer-major) and the sRGB
+    // decode table; tex_layers == 0: no array uploaded (samples white)
+    const uint32_t *tex;
+    const float *srgb;
+    uint32_t tex_w, tex_h, tex_layers;
 };
 
 AE_DEV float4 ld4(const void *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }

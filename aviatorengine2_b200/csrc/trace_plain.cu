@@ -65,8 +65,10 @@ AE_DEV f3 color_ray(const DevScene &S, const FrameParams &F, f3 o, f3 d, float t
             acc = acc + thr * (m.emission * m.albedo);
             break;
         }
+        // SurfaceAlbedo (textured when the material has a layer).
+        const f3 alb = m.type != AE_MAT_DIELECTRIC ? surface_albedo(S, h, m, o, d) : m.albedo;
         if (m.type == AE_MAT_LAMBERTIAN) {
-            f3 dl = direct_light(S, h, m.albedo, time, seed);
+            f3 dl = direct_light(S, h, alb, time, seed);
             const float luma = maxc(dl);
             if (luma > 8.0f) dl = dl * AE_DIV(8.0f, luma);
             acc = acc + thr * dl;
@@ -76,7 +78,7 @@ AE_DEV f3 color_ray(const DevScene &S, const FrameParams &F, f3 o, f3 d, float t
         d = normalize(sd);
         const float sgn = dot(d, h.n) < 0.0f ? -1.0f : 1.0f;
         o = h.p + h.n * AE_MUL(0.001f, sgn);
-        if (m.type != AE_MAT_DIELECTRIC) thr = thr * m.albedo;
+        if (m.type != AE_MAT_DIELECTRIC) thr = thr * alb;
         if (b > 0) {
             const float p = clampf(maxc(thr), 0.1f, 1.0f);
             if (rng_next(seed) > p) break;

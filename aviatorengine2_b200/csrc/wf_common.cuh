@@ -152,6 +152,8 @@ AE_DEV bool shade_vertex(const DevScene &S, const FastView &V, const PrecView &P
         acc = acc + thr * (m.emission * m.albedo);
         return false;
     }
+    // SurfaceAlbedo (textured when the material has a layer).
+    const f3 alb = m.type != AE_MAT_DIELECTRIC ? surface_albedo(S, h, m, o, d) : m.albedo;
     if (m.type == AE_MAT_LAMBERTIAN) {
         // Light samples in light order (CalculateDirectLight,
         // hybrid:1122-1212); occlusion is resolved by the shadow stage.
@@ -174,7 +176,7 @@ AE_DEV bool shade_vertex(const DevScene &S, const FastView &V, const PrecView &P
                     if (ct > 0.0f) {
                         const MatRec lm = load_mat(L);
                         const f3 rad = lm.emission * lm.albedo;
-                        const f3 c = m.albedo * rad * ct * omega;
+                        const f3 c = alb * rad * ct * omega;
                         const f3 so = h.p + h.n * 0.001f;
                         SH.o[e] = make_float4(so.x, so.y, so.z, 0.001f);
                         SH.d[e] = make_float4(sd.x, sd.y, sd.z, r.time);
@@ -194,7 +196,7 @@ AE_DEV bool shade_vertex(const DevScene &S, const FastView &V, const PrecView &P
     const f3 nd = normalize(sd);
     const float sgn = dot(nd, h.n) < 0.0f ? -1.0f : 1.0f;
     const f3 no = h.p + h.n * AE_MUL(0.001f, sgn);
-    if (m.type != AE_MAT_DIELECTRIC) thr = thr * m.albedo;
+    if (m.type != AE_MAT_DIELECTRIC) thr = thr * alb;
     if (bounce > 0) {
         const float p = clampf(maxc(thr), 0.1f, 1.0f);
         if (rng_next(seed) > p) return false;

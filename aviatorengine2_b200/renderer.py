@@ -72,8 +72,18 @@ class Context:
         lt, ins = np.ascontiguousarray(lights, np.uint32), np.ascontiguousarray(instances)
         self._chk(lib().ae_upload_scene(self._h, ptr(o), len(o), ptr(t), len(t), ptr(lt), len(lt), ptr(ins), len(ins)))
 
+    def upload_textures(self, textures):
+        """The material texture array: (layers, height, width, 4) RGBA8 sRGB."""
+        t = np.ascontiguousarray(textures, np.uint8)
+        self._keep_tex = t
+        layers, h, w, _ = t.shape
+        self._chk(lib().ae_upload_textures(self._h, ptr(t), w, h, layers))
+
     def upload(self, scene):
-        """Geometry once, then the per-frame arrays, then the scene's config."""
+        """Geometry once, then the per-frame arrays, then the scene's config
+        (and its texture array when it has one)."""
+        if getattr(scene, "textures", None) is not None:
+            self.upload_textures(scene.textures)
         self.upload_geometry(scene.vertices, scene.indices, scene.blas)
         self.upload_scene(scene.objects, scene.tlas, scene.lights, scene.instances)
         cfg = scene.config.copy()

@@ -235,12 +235,14 @@ class PackedScene:
     """The seven device arrays of RenderFrame's bind order
     (renderer/renderer.cpp:1456-1459) plus the config they were made for."""
 
-    def __init__(self, objects, tlas, lights, vertices, indices, blas, instances, config, order=None, name=""):
+    def __init__(self, objects, tlas, lights, vertices, indices, blas, instances, config, order=None, name="",
+                 textures=None):
         self.objects, self.tlas, self.lights = objects, tlas, lights
         self.vertices, self.indices, self.blas, self.instances = vertices, indices, blas, instances
         self.config = config
         self.order = order
         self.name = name
+        self.textures = textures  # (layers, height, width, 4) RGBA8 sRGB, or None
 
     @property
     def triangles(self):
@@ -320,6 +322,69 @@ def cornell_box(seed=1, width=320, height=240, depth=8):
         ents.append(entity(_lib.SHAPE_MESH, _lib.MAT_LAMBERTIAN, centre, rotation=yaw_quat(yaw), albedo=alb(), mesh=h))
     cfg = make_config(width, height, (5.0, 5.0, 24.0), (5.0, 5.0, 0.0), fov=40.0, depth=depth, sky=(0, 0, 0))
     return _finish(ents, meshes, cfg, "cornell_box")
+
+
+def procedural_textures(layers=4, width=64, height=48, seed=9):
+    """A texture array of RGBA8 sRGB layers (the shape BuildGPUArray makes):
+    checkers, stripes and value noise of seeded colours, so neighbouring
+    texels differ and bilinear blends are exercised."""
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:height, 0:width]
+    out = np.zeros((layers, height, width, 4), np.uint8)
+    for k in range(layers):
+        c0, c1 = rng.integers(0, 256, 3), rng.integers(0, 256, 3)
+        kind = k % 3
+        if kind == 0:
+            m = ((x // (4 + k)) + (y // (3 + k))) % 2
+        elif kind == 1:
+            m = ((x + 2 * y) // (5 + k)) % 2
+        else:
+            m = rng.random((height, width)) > 0.5
+        img = np.where(m[..., None] != 0, c0, c1).astype(np.int64)
+        img += rng.integers(-12, 13, img.shape)
+        out[k, ..., :3] = np.clip(img, 0, 255)
+        out[k, ..., 3] = 255
+    return out
+
+
+def textured_box(seed=6, width=160, height=120, depth=6):
+    """The Cornell box with textured materials on every shape the
+    intersectors give UVs for: mesh walls and a mesh icosphere (vertex UVs),
+    an analytic quad (alpha, beta), an analytic sphere with a UV rotation
+    (get_sphere_uv) and a yawed analytic box (BoxFaceUV); tints 0, 0.25 and
+    1, a textured metal, and a 4-layer procedural texture array."""
+    rng = np.random.default_rng(seed)
+    meshes = MeshLibrary()
+    ents = []
+    L = 10.0
+    ents.append(entity(_lib.SHAPE_QUAD, _lib.MAT_DIFFUSE_LIGHT, (3.5, L - 0.01, 3.5), albedo=(1, 1, 1),
+                       emission=15.0, u=(3.0, 0.0, 0.0), v=(0.0, 0.0, 3.0)))
+    walls = [((L / 2, 0.0, L / 2), (0, 0, L), (L, 0, 0)),
+             ((L / 2, L, L / 2), (L, 0, 0), (0, 0, L)),
+             ((L / 2, L / 2, 0.0), (L, 0, 0), (0, L, 0)),
+             ((0.0, L / 2, L / 2), (0, L, 0), (0, 0, L)),
+             ((L, L / 2, L / 2), (0, 0, L), (0, L, 0))]
+    tints = (0.0, 0.25, 1.0)
+    for k, (centre, u, v) in enumerate(walls):
+        h = meshes.add(*quad_mesh(u, v), double_sided=True)
+        ents.append(entity(_lib.SHAPE_MESH, _lib.MAT_LAMBERTIAN, centre, mesh=h,
+                           albedo=tuple(float(a) for a in rng.uniform(0.3, 0.9, 3)),
+                           texture_id=k % 4, texture_tint=tints[k % 3]))
+    ico = meshes.add(*icosphere(3, 1.4))
+    ents.append(entity(_lib.SHAPE_MESH, _lib.MAT_LAMBERTIAN, (7.0, 1.4, 3.0), mesh=ico, rotation=yaw_quat(0.7),
+                       albedo=(0.8, 0.6, 0.4), texture_id=2, texture_tint=0.25))
+    ents.append(entity(_lib.SHAPE_SPHERE, _lib.MAT_LAMBERTIAN, (3.0, 1.2, 6.5), radius=1.2,
+                       rotation=yaw_quat(1.1), albedo=(0.9, 0.9, 0.9), texture_id=1, texture_tint=0.0))
+    ents.append(entity(_lib.SHAPE_BOX, _lib.MAT_LAMBERTIAN, (6.5, 1.0, 7.0), half_extent=(1.0, 1.0, 0.8),
+                       rotation=yaw_quat(-0.4), albedo=(0.7, 0.8, 0.9), texture_id=3, texture_tint=1.0))
+    ents.append(entity(_lib.SHAPE_QUAD, _lib.MAT_LAMBERTIAN, (5.0, 6.0, 0.05), u=(3.0, 0.0, 0.0), v=(0.0, 2.0, 0.0),
+                       albedo=(1.0, 1.0, 1.0), texture_id=0, texture_tint=0.25))
+    ents.append(entity(_lib.SHAPE_SPHERE, _lib.MAT_METAL, (5.0, 3.5, 4.0), radius=0.9, fuzz=0.2,
+                       albedo=(0.9, 0.85, 0.8), texture_id=2, texture_tint=0.25))
+    cfg = make_config(width, height, (5.0, 5.0, 24.0), (5.0, 5.0, 0.0), fov=40.0, depth=depth, sky=(0, 0, 0))
+    s = _finish(ents, meshes, cfg, "textured_box")
+    s.textures = procedural_textures()
+    return s
 
 
 def instanced_meshes(seed=2, width=1920, height=1080, levels=(7, 6, 6, 5, 5), grid=512, n_instances=64,

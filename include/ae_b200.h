@@ -316,6 +316,15 @@ int ae_upload_geometry(ae_ctx *ctx, const ae_vertex *vertices, uint32_t nv,
  * on first use. */
 int ae_reserve_scene(ae_ctx *ctx, uint32_t max_objects, uint32_t max_lights);
 
+/* The material texture array GlobalTextureArray (TextureLibrary::BuildGPUArray,
+ * scene/texture.h:110-230): `layers` RGBA8 sRGB images of width x height
+ * texels (at most 2048 x 2048), row-major, one after another.  Objects name a
+ * layer with textureID; AE_NO_TEXTURE keeps the flat albedo.  Sampled as the
+ * shaders' SampleLevel(uv, layer, 0) with the renderer's linear REPEAT sampler
+ * (renderer/renderer.cpp:226-233).  With no array uploaded, textured
+ * materials sample white, as BuildGPUArray's 1x1 fallback layer. */
+int ae_upload_textures(ae_ctx *ctx, const uint8_t *texels, uint32_t width, uint32_t height, uint32_t layers);
+
 /* Renderer::UploadScene (renderer/renderer.cpp:931-1027): objects, TLAS,
  * light IDs and instances, in the storage-buffer order of RenderFrame
  * (renderer/renderer.cpp:1456-1459).  Fails with AE_ERR_OVERSIZE beyond the

@@ -216,10 +216,24 @@ struct Texture2D {
     T operator[](uint2 id) const { return data[size_t(id.y) * width + id.x]; }
 };
 struct SamplerState {};
+// The material texture array as the harness binds it (RGBA8 sRGB words,
+// layer-major).  SampleLevel uses the library's one definition of the
+// renderer's linear REPEAT sampler at level 0 (ae_math.h texture_sample); the
+// array layer is the coordinate rounded to nearest, clamped to the last.
 struct Texture2DArray {
-    // Textures are outside the measured configs: every material samples as
-    // white, which is what an untextured (kNoTexture) material never reaches.
-    float4 SampleLevel(const SamplerState &, const float3 &, float) const { return float4(1.0f); }
+    const uint32_t *texels = nullptr;
+    uint width = 0, height = 0, layers = 0;
+    float4 SampleLevel(const SamplerState &, const float3 &c, float) const {
+        static float lut[256];
+        static bool ready = false;
+        if (!ready) {
+            for (uint32_t b = 0; b < 256; b++) lut[b] = ae::srgb_to_linear(b);
+            ready = true;
+        }
+        const uint32_t layer = c.z <= 0.0f ? 0u : uint32_t(AE_FLOOR(c.z + 0.5f));
+        const ae::f3 t = ae::texture_sample(texels, lut, width, height, layers, layer, c.x, c.y);
+        return float4(t.x, t.y, t.z, 1.0f);
+    }
 };
 
 }  // namespace hlsl

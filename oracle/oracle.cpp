@@ -133,6 +133,9 @@ struct Scene {
     const uint32_t *indices;
     const ae_bvh_node *blas;
     const ae_instance *instances;
+    // material texture array: RGBA8 sRGB words, layer-major (0 layers: none)
+    const uint32_t *tex;
+    uint32_t tex_w, tex_h, tex_layers;
 };
 
 template <class T> struct Ray {
@@ -492,8 +495,58 @@ template <class T> bool traverse(const Scene &S, const Ray<T> &r, T tn, Hit<T> &
 // Shading
 // ---------------------------------------------------------------------------
 
-// SurfaceAlbedo without textures, hybrid:940-949.
-template <class T> V<T> surface_albedo(const Hit<T> &h) { return albedo<T>(*h.obj); }
+// textureColor, hybrid:919-925: SampleLevel(uv, layer, 0) with the
+// renderer's linear REPEAT sampler on the RGBA8 sRGB array (decode, then
+// bilinear).  Float: the shared definition in ae_math.h.  Double: the same
+// steps in double (sRGB decode with libm pow).
+inline const float *srgb_table() {
+    static float lut[256];
+    static bool ready = false;
+    if (!ready) {
+        for (uint32_t b = 0; b < 256; b++) lut[b] = ae::srgb_to_linear(b);
+        ready = true;
+    }
+    return lut;
+}
+inline V<float> texture_color(const Scene &S, uint32_t layer, float u, float v) {
+    const ae::f3 c = ae::texture_sample(S.tex, srgb_table(), S.tex_w, S.tex_h, S.tex_layers, layer, u, v);
+    return v3<float>(c.x, c.y, c.z);
+}
+inline V<double> texture_color(const Scene &S, uint32_t layer, double u, double v) {
+    if (S.tex_layers == 0 || S.tex_w == 0 || S.tex_h == 0) return v3<double>(1, 1, 1);
+    if (layer >= S.tex_layers) layer = S.tex_layers - 1;
+    if (!(std::fabs(u) <= 1.7e308)) u = 0;
+    if (!(std::fabs(v) <= 1.7e308)) v = 0;
+    auto dec = [](uint32_t b) {
+        const double c = double(b) / 255.0;
+        return c <= 0.04045 ? c / 12.92 : std::pow((c + 0.055) / 1.055, 2.4);
+    };
+    auto wrap = [](double f, uint32_t n) {
+        const double g = std::fmin(std::fmax(f, -1073741824.0), 1073741824.0);
+        int64_t m = int64_t(g) % int64_t(n);
+        return uint32_t(m < 0 ? m + int64_t(n) : m);
+    };
+    const double x = u * S.tex_w - 0.5, y = v * S.tex_h - 0.5;
+    const double fx = std::floor(x), fy = std::floor(y), ax = x - fx, ay = y - fy;
+    const uint32_t x0 = wrap(fx, S.tex_w), x1 = wrap(fx + 1, S.tex_w), y0 = wrap(fy, S.tex_h), y1 = wrap(fy + 1, S.tex_h);
+    const uint32_t *L = S.tex + size_t(layer) * S.tex_w * S.tex_h;
+    auto tx = [&](uint32_t xx, uint32_t yy) {
+        const uint32_t t = L[size_t(yy) * S.tex_w + xx];
+        return v3<double>(dec(t & 0xff), dec((t >> 8) & 0xff), dec((t >> 16) & 0xff));
+    };
+    const V<double> top = tx(x0, y0) + (tx(x1, y0) - tx(x0, y0)) * ax;
+    const V<double> bot = tx(x0, y1) + (tx(x1, y1) - tx(x0, y1)) * ax;
+    return top + (bot - top) * ay;
+}
+
+// SurfaceAlbedo, hybrid:940-949: the flat albedo, or the texel at the hit's
+// UV tinted by it (texel * lerp(1, albedo, TextureTint)).
+template <class T> V<T> surface_albedo(const Scene &S, const Hit<T> &h) {
+    if (h.obj->textureID == AE_NO_TEXTURE) return albedo<T>(*h.obj);
+    const V<T> texel = texture_color(S, h.obj->textureID, h.u, h.v);
+    const V<T> one = v3<T>(1, 1, 1);
+    return texel * (one + T(h.obj->textureTint) * (albedo<T>(*h.obj) - one));
+}
 
 template <class T> V<T> random_direction(Rng &rng) {
     // hybrid:245-251
@@ -601,7 +654,7 @@ template <class T> V<T> direct_light(const Scene &S, const Hit<T> &h, const Ray<
         }
         if (!occluded) {
             const V<T> rad = T(L.emission) * albedo<T>(L);
-            const V<T> brdf = surface_albedo(h);
+            const V<T> brdf = surface_albedo(S, h);
             acc = acc + brdf * rad * ct * omega;
         }
     }
@@ -633,7 +686,7 @@ template <class T> V<T> color_ray(const Scene &S, const ae_config &cfg, Ray<T> r
         ray.d = nrm(sd);
         const T sign = dot(ray.d, h.n) < 0 ? T(-1) : T(1);
         ray.o = h.p + h.n * (T(0.001f) * sign);
-        if (h.obj->colorType != AE_MAT_DIELECTRIC) thr = thr * surface_albedo(h);
+        if (h.obj->colorType != AE_MAT_DIELECTRIC) thr = thr * surface_albedo(S, h);
         if (b > 0) {
             T p = maxc(thr);
             p = M<T>::fmin(M<T>::fmax(p, T(0.1f)), T(1));
@@ -1042,6 +1095,8 @@ inline bool hit_mesh_ordered(const Scene &S, const ae_object &obj, const Ray<flo
     h.n = nrm(qrot<float>(I.qx, I.qy, I.qz, I.qw, sh));
     h.front = dot(r.d, qrot<float>(I.qx, I.qy, I.qz, I.qw, geo)) < 0;
     if (!h.front) h.n = -h.n;
+    h.u = w0 * A.u + ba * B.u + bb * C.u;  // deferred:801-803
+    h.v = w0 * A.v + ba * B.v + bb * C.v;
     h.prim = (best - I.indexBase) / 3u;
     h.alpha = ba;
     h.beta = bb;
@@ -1167,7 +1222,8 @@ inline bool occluded(const Scene &S, const Ray<float> &r, float tn, float tf, Rn
 // The deferred Hit: geometry plus the (possibly G-buffer) albedo it shades with.
 struct DSurf {
     Hit<float> h;
-    Vf albedo;
+    Vf albedo;  // Object.Albedo (the G-buffer's for raster surfaces)
+    Vf surf;    // SurfaceAlbedo (deferred:1194-1203)
     const ae_object *obj = nullptr;
 };
 
@@ -1192,7 +1248,7 @@ inline Vf clamped_direct(const Scene &S, const DSurf &s, float time, Rng &rng) {
         sr.time = time;
         if (!occluded(S, sr, 0.001f, dist - 0.001f, rng)) {
             const Vf rad = float(L.emission) * albedo<float>(L);
-            acc = acc + s.albedo * rad * ct * omega;
+            acc = acc + s.surf * rad * ct * omega;
         }
     }
     const float luma = maxc(acc);
@@ -1200,11 +1256,12 @@ inline Vf clamped_direct(const Scene &S, const DSurf &s, float time, Rng &rng) {
     return acc;
 }
 
-inline DSurf surf_of(const Hit<float> &h) {
+inline DSurf surf_of(const Scene &S, const Hit<float> &h) {
     DSurf s;
     s.h = h;
     s.obj = h.obj;
     s.albedo = albedo<float>(*h.obj);
+    s.surf = surface_albedo(S, h);
     return s;
 }
 
@@ -1220,7 +1277,7 @@ inline Vf trace_indirect(const Scene &S, const ae_config &c, const Ray<float> &p
     const float s0 = dot(ray.d, surf.h.n) < 0 ? -1.0f : 1.0f;
     ray.o = surf.h.p + surf.h.n * (0.001f * s0);
     ray.time = primary.time;
-    Vf thr = surf.obj->colorType != AE_MAT_DIELECTRIC ? surf.albedo : v3<float>(1, 1, 1);
+    Vf thr = surf.obj->colorType != AE_MAT_DIELECTRIC ? surf.surf : v3<float>(1, 1, 1);
     Vf acc = v3<float>(0, 0, 0);
     const Vf sky = v3<float>(c.sky_r, c.sky_g, c.sky_b);
     for (uint32_t b = 1; b < c.depth; b++) {
@@ -1233,14 +1290,14 @@ inline Vf trace_indirect(const Scene &S, const ae_config &c, const Ray<float> &p
             acc = acc + thr * (float(h.obj->emission) * albedo<float>(*h.obj));
             break;
         }
-        const DSurf s = surf_of(h);
+        const DSurf s = surf_of(S, h);
         if (h.obj->colorType == AE_MAT_LAMBERTIAN) acc = acc + thr * clamped_direct(S, s, ray.time, rng);
         Vf nx;
         if (!bounce(ray, h, nx, rng)) break;
         ray.d = nrm(nx);
         const float sg = dot(ray.d, h.n) < 0 ? -1.0f : 1.0f;
         ray.o = h.p + h.n * (0.001f * sg);
-        if (h.obj->colorType != AE_MAT_DIELECTRIC) thr = thr * albedo<float>(*h.obj);
+        if (h.obj->colorType != AE_MAT_DIELECTRIC) thr = thr * s.surf;
         float p = maxc(thr);
         p = M<float>::fmin(M<float>::fmax(p, 0.1f), 1.0f);
         if (rng.next<float>() > p) break;
@@ -1358,6 +1415,7 @@ inline int resolve_primary(const Scene &S, const ae_config &c, const Planes &P, 
             raster.h.n = nrm(v3<float>(pn[0], pn[1], pn[2]));
             const float *pa = at4(P.galb, W, x, y);
             raster.albedo = v3<float>(pa[0], pa[1], pa[2]);
+            raster.surf = raster.albedo;  // HitFromGBuffer clears TextureID (deferred:1477-1480)
             raster.h.front = dot(primary.d, raster.h.n) < 0;
             if (!raster.h.front) raster.h.n = -raster.h.n;
             raster.h.t = len(raster.h.p - primary.o);
@@ -1367,7 +1425,7 @@ inline int resolve_primary(const Scene &S, const ae_config &c, const Planes &P, 
     }
     Hit<float> ah;
     if (traverse_bounded(S, primary, 0.001f, far_limit, true, ah, rng)) {
-        hit = surf_of(ah);
+        hit = surf_of(S, ah);
         return 2;
     }
     if (has_raster) {
@@ -1468,6 +1526,7 @@ inline void deferred_cell(const Scene &S, const ae_config &c, const Planes &P, u
             raster.h.n = nrm(v3<float>(pn[0], pn[1], pn[2]));
             const float *pa = at4(P.galb, W, x, y);
             raster.albedo = v3<float>(pa[0], pa[1], pa[2]);
+            raster.surf = raster.albedo;  // HitFromGBuffer clears TextureID (deferred:1477-1480)
             raster.h.front = dot(primary.d, raster.h.n) < 0;
             if (!raster.h.front) raster.h.n = -raster.h.n;
             raster.h.t = len(raster.h.p - K.src);
@@ -1479,7 +1538,7 @@ inline void deferred_cell(const Scene &S, const ae_config &c, const Planes &P, u
     int source = 0;
     Hit<float> ah;
     if (traverse_bounded(S, primary, 0.001f, far_limit, true, ah, rng)) {
-        hit = surf_of(ah);
+        hit = surf_of(S, ah);
         source = 2;
     } else if (has_raster) {
         hit = raster;
@@ -1502,7 +1561,7 @@ inline void deferred_cell(const Scene &S, const ae_config &c, const Planes &P, u
     if (reduced) {
         const bool demod = source == 1 && hit.obj->colorType != AE_MAT_DIELECTRIC;
         Vf alb = v3<float>(1, 1, 1);
-        if (demod) alb = vmax(hit.albedo, v3<float>(0.01f, 0.01f, 0.01f));
+        if (demod) alb = vmax(hit.surf, v3<float>(0.01f, 0.01f, 0.01f));
         put4(P.reduced, P.red_w, cx, cy, color / alb, demod ? 1.0f : 0.0f);
         return;
     }
@@ -1671,7 +1730,9 @@ extern "C" int oracle_gbuffer(const oracle::Scene *S, const ae_config *c, float 
             P[0] = best.p.x; P[1] = best.p.y; P[2] = best.p.z; P[3] = float(best.slot);
             N[0] = nn.x; N[1] = nn.y; N[2] = nn.z; N[3] = 1.0f;
             const ae_object &o = *best.obj;
-            const float al[3] = {o.r, o.g, o.b};
+            // SurfaceBlock's albedo (gbuffer.frag:44-50), textured at the hit's UV.
+            const Vf sa = surface_albedo(*S, best);
+            const float al[3] = {sa.x, sa.y, sa.z};
             for (int k = 0; k < 3; k++) A[k] = uint8_t(int(std::rint(std::fmin(std::fmax(al[k], 0.0f), 1.0f) * 255.0f)));
             A[3] = (o.colorType == AE_MAT_METAL || o.colorType == AE_MAT_DIELECTRIC) ? 0 : 255;
             const float vz = dot(best.p - r.o, fwd);

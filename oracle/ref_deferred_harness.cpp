@@ -88,6 +88,14 @@ void aeref_d_bind(const ae_object *objects, uint32_t n_objects, const ae_bvh_nod
     (void)n_objects; (void)n_nodes; (void)n_lights; (void)nv; (void)ni; (void)nb; (void)n_instances;
 }
 
+// The material texture array (GlobalTextureArray): RGBA8 sRGB words.
+void aeref_d_bind_textures(const uint32_t *texels, uint32_t width, uint32_t height, uint32_t layers) {
+    hlsl::d::GlobalTextureArray.texels = texels;
+    hlsl::d::GlobalTextureArray.width = width;
+    hlsl::d::GlobalTextureArray.height = height;
+    hlsl::d::GlobalTextureArray.layers = layers;
+}
+
 void aeref_d_set_config(const ae_config *c) {
     using namespace hlsl;
     AE_SET_CONFIG(d)

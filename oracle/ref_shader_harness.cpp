@@ -42,6 +42,20 @@ void aeref_bind(const ae_object *objects, uint32_t n_objects, const ae_bvh_node 
     hlsl::instances.count = n_instances;
 }
 
+// The material texture array (GlobalTextureArray): RGBA8 sRGB words.
+void aeref_bind_textures(const uint32_t *texels, uint32_t width, uint32_t height, uint32_t layers) {
+    hlsl::GlobalTextureArray.texels = texels;
+    hlsl::GlobalTextureArray.width = width;
+    hlsl::GlobalTextureArray.height = height;
+    hlsl::GlobalTextureArray.layers = layers;
+}
+
+// One texture sample through the shader's own binding (test of the sampler).
+void aeref_sample_texture(float u, float v, uint32_t layer, float *rgb) {
+    const hlsl::float4 t = hlsl::GlobalTextureArray.SampleLevel(hlsl::GlobalSampler, hlsl::float3(u, v, float(layer)), 0.0f);
+    rgb[0] = t.x; rgb[1] = t.y; rgb[2] = t.z;
+}
+
 void aeref_set_config(const ae_config *c) {
     using namespace hlsl;
     Source = float3(c->source_x, c->source_y, c->source_z);

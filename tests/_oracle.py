@@ -21,7 +21,19 @@ _P = ctypes.c_void_p
 class OScene(ctypes.Structure):
     _fields_ = [("objects", _P), ("n_objects", ctypes.c_uint32), ("tlas", _P), ("n_nodes", ctypes.c_uint32),
                 ("lights", _P), ("n_lights", ctypes.c_uint32), ("vertices", _P), ("indices", _P), ("blas", _P),
-                ("instances", _P)]
+                ("instances", _P), ("tex", _P), ("tex_w", ctypes.c_uint32), ("tex_h", ctypes.c_uint32),
+                ("tex_layers", ctypes.c_uint32)]
+
+
+def texture_words(scene):
+    """(words, width, height, layers) of a scene's texture array: RGBA8 as
+    little-endian uint32 words, layer-major; (None, 0, 0, 0) without one."""
+    t = getattr(scene, "textures", None)
+    if t is None or len(t) == 0:
+        return None, 0, 0, 0
+    t = np.ascontiguousarray(t, np.uint8)
+    layers, h, w, _ = t.shape
+    return t.view(np.uint32).reshape(-1), w, h, layers
 
 
 def ptr(a):
@@ -60,8 +72,9 @@ def oscene(scene):
     keep = [np.ascontiguousarray(a) for a in (scene.objects, scene.tlas, scene.lights, scene.vertices, scene.indices,
                                               scene.blas, scene.instances)]
     o, t, l, v, i, b, ins = keep
-    s = OScene(ptr(o), len(o), ptr(t), len(t), ptr(l), len(l), ptr(v), ptr(i), ptr(b), ptr(ins))
-    s._keep = keep
+    tw, w, h, layers = texture_words(scene)
+    s = OScene(ptr(o), len(o), ptr(t), len(t), ptr(l), len(l), ptr(v), ptr(i), ptr(b), ptr(ins), ptr(tw), w, h, layers)
+    s._keep = keep + [tw]
     return s
 
 
@@ -126,7 +139,9 @@ def ref_bind(scene):
     u32 = ctypes.c_uint32
     L.aeref_bind(ptr(o), u32(len(o)), ptr(t), u32(len(t)), ptr(l), u32(len(l)), ptr(v), u32(len(v)), ptr(i),
                  u32(len(i)), ptr(b), u32(len(b)), ptr(ins), u32(len(ins)))
-    _cache["_ref_keep"] = keep
+    tw, w, h, layers = texture_words(scene)
+    L.aeref_bind_textures(ptr(tw), u32(w), u32(h), u32(layers))
+    _cache["_ref_keep"] = keep + [tw]
 
 
 def ref_set_config(config):
@@ -278,6 +293,9 @@ def hybrid_frame(scene, config, gb, state, impl="oracle", threads=0):
         u32 = ctypes.c_uint32
         L.aeref_d_bind(ptr(o), u32(len(o)), ptr(t), u32(len(t)), ptr(l), u32(len(l)), ptr(v), u32(len(v)), ptr(i),
                        u32(len(i)), ptr(b), u32(len(b)), ptr(ins), u32(len(ins)))
+        tw, tw_w, tw_h, tw_l = texture_words(scene)
+        L.aeref_d_bind_textures(ptr(tw), u32(tw_w), u32(tw_h), u32(tw_l))
+        keep.append(tw)
         L.aeref_d_set_config(ptr(c))
         if not (red and int(c["displayOnly"][0])):
             L.aeref_deferred(ptr(pos), ptr(nrm), ptr(albf), ptr(dep), ptr(state.img[rs]), ptr(state.geo[rs]),
