@@ -21,6 +21,9 @@ Workloads (all inputs seeded; no dataset is involved):
                    emissive quads above the field.
   hybrid_box       the Cornell box plus analytic spheres and boxes, for the
                    hybrid renderer's raster/analytic split.
+  textured_box     the Cornell box with textured materials on every shape.
+  media_box        the Cornell box with isotropic volumes (a box and a
+                   sphere), an analytic triangle and a moving sphere.
   serving_scenes   8 scenes built like wavefront_scene with 50k to 5M unique
                    triangles and 512 instances each (4096 in all), whose
                    instances move along seeded random walks (random_walk).
@@ -439,6 +442,40 @@ def hybrid_box(seed=3, width=160, height=120, depth=4):
                        albedo=(0.7, 0.7, 0.2), mesh=h))
     cfg = s.config.copy()
     return _finish(ents, meshes, cfg, "hybrid_box")
+
+
+def media_box(seed=7, width=128, height=96, depth=6):
+    """The Cornell box with participating media and the remaining analytic
+    shapes: an isotropic fog box and an isotropic smoke sphere (HitVolume,
+    hybrid:779-822: one RNG draw per volume the walk tests; ISOTROPIC
+    scattering, 1020-1025), an analytic triangle, a sphere moving over the
+    shutter (Position2, the ray's time draw), and a glass box."""
+    rng = np.random.default_rng(seed)
+    meshes = MeshLibrary()
+    ents = []
+    L = 10.0
+    ents.append(entity(_lib.SHAPE_QUAD, _lib.MAT_DIFFUSE_LIGHT, (3.5, L - 0.01, 3.5), emission=15.0,
+                       u=(3.0, 0.0, 0.0), v=(0.0, 0.0, 3.0)))
+    ents.append(entity(_lib.SHAPE_BOX, _lib.MAT_ISOTROPIC, (6.5, 2.0, 5.5), half_extent=(1.5, 2.0, 1.5),
+                       rotation=yaw_quat(0.3), albedo=(0.8, 0.8, 0.9), density=0.35))
+    ents.append(entity(_lib.SHAPE_SPHERE, _lib.MAT_ISOTROPIC, (3.0, 5.5, 4.5), radius=1.3, albedo=(0.9, 0.6, 0.4),
+                       density=0.8))
+    ents.append(entity(_lib.SHAPE_TRIANGLE, _lib.MAT_LAMBERTIAN, (1.0, 0.5, 8.0), u=(3.0, 0.0, 0.0),
+                       v=(0.0, 3.0, -1.0), albedo=(0.3, 0.7, 0.4)))
+    mover = entity(_lib.SHAPE_SPHERE, _lib.MAT_METAL, (2.5, 1.0, 2.5), radius=0.9, albedo=(0.8, 0.8, 0.8), fuzz=0.05)
+    mover["prev_position"] = (3.3, 1.2, 2.8)  # Position2: where the shutter closes
+    ents.append(mover)
+    ents.append(entity(_lib.SHAPE_BOX, _lib.MAT_DIELECTRIC, (7.5, 6.5, 7.0), half_extent=(0.7, 0.7, 0.7),
+                       rotation=yaw_quat(-0.6), ior=1.5))
+    walls = [((L / 2, 0.0, L / 2), (0, 0, L), (L, 0, 0)), ((L / 2, L, L / 2), (L, 0, 0), (0, 0, L)),
+             ((L / 2, L / 2, 0.0), (L, 0, 0), (0, L, 0)), ((0.0, L / 2, L / 2), (0, L, 0), (0, 0, L)),
+             ((L, L / 2, L / 2), (0, 0, L), (0, L, 0))]
+    for centre, u, v in walls:
+        h = meshes.add(*quad_mesh(u, v), double_sided=True)
+        ents.append(entity(_lib.SHAPE_MESH, _lib.MAT_LAMBERTIAN, centre,
+                           albedo=tuple(float(x) for x in rng.uniform(0.2, 0.8, 3)), mesh=h))
+    cfg = make_config(width, height, (5.0, 5.0, 24.0), (5.0, 5.0, 0.0), fov=40.0, depth=depth, sky=(0, 0, 0))
+    return _finish(ents, meshes, cfg, "media_box")
 
 
 def wavefront_scene(seed=4, width=1920, height=1080, depth=12, n_meshes=32, n_instances=1024, n_lights=16,

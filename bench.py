@@ -124,9 +124,11 @@ def make_workload(ctx, scene):
     return prim, bounce[valid].copy()
 
 
-def cpu_reference(scene, rays, budget_s=20.0):
+def cpu_reference(scene, rays, budget_s=12.0):
     """The reference's own traversal (its shader, compiled for the CPU under
-    oracle/_ref) on a bounded sample of the ray set, all host cores."""
+    oracle/_ref) on a bounded sample of the ray set, all host cores: a random
+    subset when the whole set would take longer than the budget, otherwise
+    the whole set traced repeatedly until about `budget_s` of CPU time."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import _oracle as O
     kind = "reference" if O.ref_available() else "port"
@@ -134,20 +136,26 @@ def cpu_reference(scene, rays, budget_s=20.0):
     fn = O.ref_closest_hit if kind == "reference" else O.closest_hit
     rng = np.random.default_rng(0)
     n = min(len(rays), 65536)
-    sample = rays[np.sort(rng.choice(len(rays), n, replace=False))]
+    probe = rays[np.sort(rng.choice(len(rays), n, replace=False))]
     t0 = time.perf_counter()
-    fn(scene, sample, threads=cores)
-    dt = time.perf_counter() - t0
-    # Grow the sample to fill about `budget_s` of CPU time (bounded).
-    n2 = int(min(len(rays), max(n, n * budget_s / max(dt, 1e-3) * 0.5)))
-    if n2 > n:
-        sample = rays[np.sort(rng.choice(len(rays), n2, replace=False))]
-        t0 = time.perf_counter()
+    fn(scene, probe, threads=cores)
+    rate = n / max(time.perf_counter() - t0, 1e-6)
+    want = int(rate * budget_s)
+    if want < len(rays):
+        sample = rays[np.sort(rng.choice(len(rays), max(want, n), replace=False))]
+        passes = 1
+    else:
+        sample = rays
+        passes = max(1, int(round(want / len(rays))))
+    t0 = time.perf_counter()
+    for _ in range(passes):
         fn(scene, sample, threads=cores)
-        dt = time.perf_counter() - t0
-        n = n2
-    return {"value": n / dt / 1e6, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"{n} rays drawn uniformly from the step's {len(rays)} (primary + bounce), {dt:.2f} s"}
+    dt = time.perf_counter() - t0
+    total = len(sample) * passes
+    what = (f"{len(sample)} rays drawn uniformly from the step's {len(rays)}" if passes == 1 else
+            f"the step's {len(rays)} rays (primary + bounce) traced {passes} times")
+    return {"value": total / dt / 1e6, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{what}, {dt:.2f} s"}
 
 
 def measure_paths(local, width, height, frames=2):
@@ -276,7 +284,8 @@ def run_reference_arm(args):
         cpu_reference(scene, rays[:20000], budget_s=0.0)
     base = None
     for _ in range(args.steps):
-        base = cpu_reference(scene, rays, budget_s=8.0)
+        # about 90 s of CPU work over all steps
+        base = cpu_reference(scene, rays, budget_s=max(1.0, min(6.0, 90.0 / max(args.steps, 1))))
         steps.append(base["value"])
     v = float(np.median(steps))
     base["value"] = v

@@ -1,10 +1,12 @@
-"""Textured materials (SurfaceAlbedo with textureColor, hybrid:919-949,
-deferred:1173-1203): the oracle against the reference's own shaders run on
-the CPU, over a scene where every intersector supplies UVs (mesh vertex UVs,
-quad alpha/beta, sphere get_sphere_uv, box BoxFaceUV) and tints 0, 0.25, 1.
-The texture sampler itself (one definition shared by the kernels, the oracle
-and the reference harness) is checked against an independent numpy
-restatement of bilinear, REPEAT, sRGB-decoded sampling."""
+"""Materials beyond flat albedo, pinned against the reference's own shaders
+run on the CPU.  Textures (SurfaceAlbedo with textureColor, hybrid:919-949,
+deferred:1173-1203) over a scene where every intersector supplies UVs (mesh
+vertex UVs, quad alpha/beta, sphere get_sphere_uv, box BoxFaceUV) with tints
+0, 0.25, 1; the texture sampler itself (one definition shared by the kernels,
+the oracle and the reference harness) against an independent numpy
+restatement of bilinear, REPEAT, sRGB-decoded sampling; and participating
+media with the remaining analytic shapes (HitVolume, ISOTROPIC, analytic
+triangle, a sphere moving over the shutter)."""
 import ctypes
 
 import numpy as np
@@ -94,3 +96,36 @@ def test_textured_hybrid_frames_equal_reference():
         for a, b, what in ((so.img[so.history], sr.img[sr.history], "image"),
                            (so.display, sr.display, "display")):
             assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), f"frame {f}: {what} differs"
+
+
+@needs_ref
+def test_media_and_analytic_frames_equal_reference():
+    """Participating media (HitVolume and ISOTROPIC scattering, with their RNG
+    draws inside the walk), an analytic triangle, a moving sphere and a glass
+    box: oracle equals the reference's compute-only shader bit for bit."""
+    s = scenes.media_box()
+    cfg = s.config.copy()
+    acc_o = acc_r = None
+    for b in range(3):
+        cfg["batch"] = b
+        acc_o, disp_o, _ = O.render_frame(s, cfg, acc_o)
+        acc_r, disp_r = O.ref_render(s, cfg, acc_r)
+        assert np.array_equal(acc_o.view(np.uint32), acc_r.view(np.uint32)), f"frame {b}"
+        assert np.array_equal(disp_o, disp_r)
+
+
+@needs_ref
+def test_media_hybrid_frames_equal_reference():
+    s = scenes.media_box(width=96, height=72, depth=4)
+    c = s.config.copy()
+    c["traceScale"], c["historyCap"] = 1.0, 32.0
+    w, h = int(c["width"]), int(c["height"])
+    so, sr = O.HybridState(w, h), O.HybridState(w, h)
+    for f in range(2):
+        c["frameIndex"] = f
+        c["historyReset"] = 1 if f == 0 else 0
+        gb = O.gbuffer(s, c)
+        O.hybrid_frame(s, c, gb, so, "oracle")
+        O.hybrid_frame(s, c, gb, sr, "reference")
+        assert np.array_equal(so.img[so.history].view(np.uint32), sr.img[sr.history].view(np.uint32)), f"frame {f}"
+        assert np.array_equal(so.display.view(np.uint32), sr.display.view(np.uint32))
