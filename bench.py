@@ -314,6 +314,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-rate", type=float, default=0.5, help="Poisson arrivals per second")
+    ap.add_argument("--serve-sweep", default="", help="comma-separated arrival rates: also run the serving "
+                    "leg at each (reported as serving_sweep)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -453,6 +455,9 @@ def main():
     serving = None
     if not args.no_serve and rank == 0:
         serving = measure_serving(local, args.serve_requests, args.serve_rate)
+    sweep = None
+    if args.serve_sweep and rank == 0:
+        sweep = [measure_serving(local, args.serve_requests, float(r)) for r in args.serve_sweep.split(",")]
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -465,6 +470,8 @@ def main():
             "clocks": clk.summary(),
             "per_step_ms": [round(t, 4) for t in times],
             "paths": paths, "serving": serving}
+    if sweep is not None:
+        line["serving_sweep"] = sweep
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

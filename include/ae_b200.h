@@ -492,7 +492,7 @@ typedef struct ae_serve_settings {
     uint32_t max_requests;     /* requests resident at once; 0 = 64, at most 1024 */
     uint64_t arena_bytes;      /* device memory for request images; 0 = 1 GiB */
     uint32_t ticks_per_launch; /* queue ticks per graph replay (even); 0 = 4 */
-    uint32_t extend_threads;   /* 64, 128 or 256; 0 = 64 */
+    uint32_t extend_threads;   /* 0 = step-wise walker (default); 64, 128 or 256 = tile-staged extend */
     uint32_t max_scenes;       /* resident scenes; 0 = 16 */
     uint32_t claim_policy;     /* AE_CLAIM_OLDEST_FIRST (0) or AE_CLAIM_SHARED (1) */
     uint32_t reserved[4];
