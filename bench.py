@@ -107,8 +107,8 @@ def load_peaks():
 
 def load_traffic():
     """DRAM bytes per ray of the closest-hit kernel from a committed ncu
-    summary (profiles/closest_hit_traffic.json), or None."""
-    p = os.path.join(ROOT, "profiles", "closest_hit_traffic.json")
+    summary (profiles/k_closest_fast_instanced_meshes_traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "k_closest_fast_instanced_meshes_traffic.json")
     if os.path.exists(p):
         with open(p) as f:
             return json.load(f)
