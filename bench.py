@@ -96,6 +96,23 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(x, pg, device=None):
+    """The largest of x over all ranks (x itself with no process group): the
+    step time every replica's throughput is divided by."""
+    if pg is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_rank, world, seconds):
+    """Whole-job throughput of `world` independent replicas that each process
+    `units_per_rank` in `seconds` (the max over ranks), in millions per second."""
+    return units_per_rank * world / seconds / 1e6
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -392,13 +409,9 @@ def main():
         if pg:
             pg.barrier()
     launches = ctx.launch_count - launches0
-    ms = float(np.sum(times)) / args.steps
-    if pg:
-        t = torch.tensor([ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(float(np.sum(times)) / args.steps, pg, dev)
     rays_step = n1 + n2
-    value = rays_step * world / (ms / 1e3) / 1e6
+    value = replica_value(rays_step, world, ms / 1e3)
 
     e2e = None
     if not args.no_e2e:
@@ -423,12 +436,8 @@ def main():
             t0 = time.perf_counter()
             e2e_step()
             et.append(time.perf_counter() - t0)
-        e2e_s = float(np.mean(et))
-        if pg:
-            t = torch.tensor([e2e_s], device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e = {"value": rays_step * world / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": int((n1 + n2) * 32),
+        e2e_s = max_over_ranks(float(np.mean(et)), pg, dev)
+        e2e = {"value": replica_value(rays_step, world, e2e_s), "unit": UNIT, "h2d_bytes_per_step": int((n1 + n2) * 32),
                "d2h_bytes_per_step": int((n1 + n2) * 20)}
 
     peak, peak_kind = load_peaks()
