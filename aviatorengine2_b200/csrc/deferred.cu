@@ -571,8 +571,6 @@ __global__ void __launch_bounds__(128) k_gbuffer(DevScene S, DefParams P, GBuf G
         float tf = kFarStart;
         bool found = false;
         DHit best;
-        f3 shade_n = splat(0.0f);
-        uint32_t seed = 1u;
         while (sp > 0) {
             const NodeBox n = load_node(S.tlas, uint32_t(stack[--sp]));
             if (!slab_ref(o, inv, n.lo, n.hi, 0.001f, tf)) continue;
@@ -601,8 +599,6 @@ __global__ void __launch_bounds__(128) k_gbuffer(DevScene S, DefParams P, GBuf G
                 stack[sp++] = n.right;
             }
         }
-        (void)seed;
-        (void)shade_n;
         if (found) {
             const ae_object *obj = S.objects + best.slot;
             const MatRec mat = load_mat(obj);
