@@ -42,7 +42,13 @@ class Context:
         if h:
             lib().ae_destroy(h)
 
-    __del__ = close
+    def __del__(self):
+        # At interpreter exit the ctypes module state may already be gone;
+        # the process is ending and the driver releases the device anyway.
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def __enter__(self):
         return self

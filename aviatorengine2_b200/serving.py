@@ -37,7 +37,13 @@ class Server:
             lib().ae_serve_destroy(h)
         self._outputs = {}
 
-    __del__ = close
+    def __del__(self):
+        # At interpreter exit the ctypes module state may already be gone;
+        # the process is ending and the driver releases the device anyway.
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def __enter__(self):
         return self
