@@ -19,6 +19,14 @@ namespace ae {
 
 enum : uint32_t { kWalkTlas = 0, kWalkObject = 1, kWalkBlas = 2, kWalkDone = 3 };
 
+// Minimum resident 128-thread blocks per SM asked of the compiler for every
+// kernel built on Walker (extend and shadow, wavefront and serving): caps them
+// at 72 registers.  Measured at 1920x1080 on the 10M-triangle wavefront scene:
+// 7 blocks (28-108 bytes of spills) beat both the unbounded build (79-87
+// registers, 6 blocks) and 8 blocks (64 registers, 110-280 bytes of spills) -
+// wavefront frame 177 ms against 192 ms and 179 ms.
+constexpr int kWalkBlocksPerSm = 7;
+
 // The walk's per-thread local stacks: the TLAS stack and the BLAS entries
 // beyond the shared-memory part.  Kept out of Walker so its scalar state can
 // live in registers.

@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(THREADS) k_sv_extend(SvView W, int q) {
 
 // Extend on the step-wise Walker: each thread steps its own queued ray (its
 // own scene's) and takes the next (k + grid size) as soon as one finishes.
-__global__ void __launch_bounds__(128) k_sv_extend_walk(SvView W, int q) {
+__global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_sv_extend_walk(SvView W, int q) {
     extern __shared__ uint2 stk[];
     const uint32_t count = W.cnt[q];
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(256) k_sv_shade(SvView W, int q) {
 }
 
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) k_sv_shadow(SvView W) {
+__global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_sv_shadow(SvView W) {
     // The reference's shadow loop per light sample on the step-wise Walker:
     // a lane that finishes a sample starts its next one at once.  The
     // sample's scene (its slot's) is read through the scene table.

@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(THREADS) k_wf_extend(DevScene S, FastView V, W
 // its own queued ray and taking the next (k + grid size) when one finishes.
 // For incoherent queues (bounces past the camera rays).
 template <bool WT>
-__global__ void __launch_bounds__(128) k_wf_extend_walk(DevScene S, FastView V, WfView W, int bounce) {
+__global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_wf_extend_walk(DevScene S, FastView V, WfView W, int bounce) {
     extern __shared__ uint2 stk[];
     const int q = bounce & 1;
     const uint32_t count = W.cnt[q];
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(256) k_wf_shade(DevScene S, FastView V, WfView
 // lane that finishes an entry starts its next one at once instead of waiting
 // for the warp's longest traversal.
 template <int THREADS, bool WT>
-__global__ void __launch_bounds__(THREADS) k_wf_shadow(DevScene S, FastView V, WfView W) {
+__global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_wf_shadow(DevScene S, FastView V, WfView W) {
     extern __shared__ uint2 stk[];
     const uint32_t count = W.cnt[C_SH];
     const uint32_t stride = gridDim.x * THREADS;
