@@ -1,0 +1,984 @@
+// bvh_build.cu - the binned-SAH BVH build (BuildBVH, scene/bvh.h:120-295) on
+// the GPU.  It produces the host builder's tree node for node and slot for
+// slot (host_scene.cpp SahBuilder, itself pinned to the reference).
+//
+// The reference recursion is sequential, but what it does at a node depends
+// only on that node's primitive range as the ancestors' partitions left it.
+// The device builds the same tree in two phases:
+//
+//   * nodes of more than kWarpTask primitives, one tree level per round:
+//     blocks of kChunk positions reduce the node box and centroid bounds,
+//     bin the 3 x 12 SAH buckets in shared memory and partition;
+//   * every node of at most kWarpTask primitives: one warp builds its whole
+//     subtree with the reference's pre-order work list, each per-node loop
+//     spread over the 32 lanes.
+//
+// Node indices are the recursion's pre-order; they are assigned at the end
+// from the subtree sizes.  Leaf slots are positions in the permuted index
+// array, which is the reference's outOrder.
+//
+// Exactness:
+//   * Every float operation is the reference's, with _rn intrinsics (no
+//     contraction): the centroid (min + max) * 0.5, the bucket
+//     (c - cmin) * (12 / extent) truncated, HalfArea, the costs.
+//   * The node box folds with std::min / std::max, which keep the FIRST of
+//     equal values.  Equal floats differ in bits only as +0 / -0, so the box
+//     reductions carry (value, position) keys and the smallest position among
+//     equal values wins.  Centroid bounds and bucket boxes only reach
+//     differences, products and comparisons, where +0 and -0 act alike, and
+//     reduce by value.
+//   * std::partition (libstdc++, the bidirectional form random-access
+//     iterators use) scans from the left for an element failing the predicate
+//     and from the right for one passing it, swaps them and repeats until the
+//     scans meet.  The result: with T passing elements in the range, the k-th
+//     failing element of [start, start + T) counted from the left trades
+//     places with the k-th passing element of [start + T, end) counted from
+//     the right, and every other element stays.  The device finds those ranks
+//     with scans and moves the pairs through a stash.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cstring>
+#include <vector>
+
+#include "../../include/ae_b200.h"
+#include "ae_math.h"
+
+namespace ae {
+namespace {
+
+// scene/bvh.h:13, 93, 101 and scene/aabb.h:12
+constexpr int kLeafSize = 4;
+constexpr int kBins = 12;
+constexpr int kMaxDepth = 20;
+constexpr float kBoundsMinimum = 0.0001f;
+constexpr float kHalfMinimum = kBoundsMinimum * 0.5f;
+
+// Subtrees of at most this many primitives are built by one warp (the
+// default; any threshold gives the same tree).
+constexpr uint32_t kWarpTask = 1024;
+constexpr int kWarpsPerBlock = 8;
+// Positions per block in the level-by-level phase: 256 threads x 8.
+constexpr int kThreads = 256;
+constexpr int kPer = 8;
+constexpr uint32_t kChunk = kThreads * kPer;
+// Bucket record: ordered min x,y,z, ordered max x,y,z, count.
+constexpr int kBinWords = 7;
+constexpr int kBinTable = 3 * kBins * kBinWords;
+// Pre-order work list of one warp: at most one pending right child per depth
+// plus the current left child.
+constexpr int kWarpStack = kMaxDepth + 4;
+
+struct Chunk { uint32_t task, begin, end; };
+struct BigTask { uint32_t start, end, depth; };
+struct SmallTask { uint32_t start, end, depth; };
+
+// Per large task, reset every round.
+struct TaskAcc {
+    unsigned long long bmin[3], bmax[3];  // (ordered value, position) keys
+    uint32_t cmin[3], cmax[3];            // ordered centroid bounds
+    uint32_t bins[kBinTable];
+};
+
+struct Decision {
+    ae_aabb box;       // union of the node's primitive boxes (not yet widened)
+    int32_t leaf;      // 1: the node is a leaf
+    int32_t axis;      // winning axis, -1 = no plane separates (median split)
+    int32_t split;     // first bucket on the right
+    float cmin, scale; // bucket mapping on the winning axis
+};
+
+// Order-preserving map of floats onto unsigned integers (-0 below +0).
+__device__ __forceinline__ uint32_t ord(float f) {
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float unord(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+// Keys for the first-occurrence box fold.  Position 0 stands for the fold's
+// starting value (AABB::Empty), which comes before every primitive.
+__device__ __forceinline__ unsigned long long min_key(float v, uint32_t pos) {
+    const float z = v == 0.0f ? 0.0f : v;
+    return (static_cast<unsigned long long>(ord(z)) << 32) | (pos + 1u);
+}
+__device__ __forceinline__ unsigned long long max_key(float v, uint32_t pos) {
+    const float z = v == 0.0f ? 0.0f : v;
+    return (static_cast<unsigned long long>(ord(z)) << 32) | (0xffffffffu - (pos + 1u));
+}
+__device__ __forceinline__ unsigned long long min_key_empty() {
+    return static_cast<unsigned long long>(ord(FLT_MAX)) << 32;
+}
+__device__ __forceinline__ unsigned long long max_key_empty() {
+    return (static_cast<unsigned long long>(ord(-FLT_MAX)) << 32) | 0xffffffffu;
+}
+__device__ __forceinline__ float min_from_key(unsigned long long k, const ae_aabb *pb, int axis) {
+    const uint32_t lo = static_cast<uint32_t>(k);
+    return lo == 0u ? FLT_MAX : (&pb[lo - 1u].min_x)[axis];
+}
+__device__ __forceinline__ float max_from_key(unsigned long long k, const ae_aabb *pb, int axis) {
+    const uint32_t lo = 0xffffffffu - static_cast<uint32_t>(k);
+    return lo == 0u ? -FLT_MAX : (&pb[lo - 1u].min_x)[axis + 3];
+}
+
+__device__ __forceinline__ float centre(const ae_aabb &b, int axis) {
+    const float *f = &b.min_x;
+    return AE_MUL(AE_ADD(f[axis], f[axis + 3]), 0.5f);
+}
+__device__ __forceinline__ int bucket(float c, float cmin, float scale) {
+    // c >= cmin, so the product is >= 0 (or NaN -> 0); max() only keeps an
+    // overflowing extent inside the table.
+    return max(0, min(kBins - 1, __float2int_rz(AE_MUL(AE_SUB(c, cmin), scale))));
+}
+__device__ __forceinline__ float half_area(const float lo[3], const float hi[3]) {
+    const float dx = AE_SUB(hi[0], lo[0]), dy = AE_SUB(hi[1], lo[1]), dz = AE_SUB(hi[2], lo[2]);
+    return AE_ADD(AE_ADD(AE_MUL(dx, dy), AE_MUL(dy, dz)), AE_MUL(dz, dx));
+}
+
+// MakeNode, scene/bvh.h:58-89.
+__device__ __forceinline__ ae_bvh_node make_node(const ae_aabb &b, int left, int right, int count) {
+    ae_bvh_node n;
+    n.min_x = b.min_x; n.min_y = b.min_y; n.min_z = b.min_z; n.pad0 = 0.0f;
+    n.max_x = b.max_x; n.max_y = b.max_y; n.max_z = b.max_z;
+    if (AE_SUB(n.max_x, n.min_x) < kBoundsMinimum) { n.min_x = AE_SUB(n.min_x, kHalfMinimum); n.max_x = AE_ADD(n.max_x, kHalfMinimum); }
+    if (AE_SUB(n.max_y, n.min_y) < kBoundsMinimum) { n.min_y = AE_SUB(n.min_y, kHalfMinimum); n.max_y = AE_ADD(n.max_y, kHalfMinimum); }
+    if (AE_SUB(n.max_z, n.min_z) < kBoundsMinimum) { n.min_z = AE_SUB(n.min_z, kHalfMinimum); n.max_z = AE_ADD(n.max_z, kHalfMinimum); }
+    n.left = left; n.right = right; n.count = count; n.padding = 0; n.pad_trailing = 0;
+    return n;
+}
+
+// The bucket sweep of one axis (scene/bvh.h:203-236) over a bucket table of
+// ordered bounds and counts.  Returns the axis's cheapest plane in the
+// reference's visiting order (right to left, strict <), cost FLT_MAX if none.
+__device__ void sweep_axis(const uint32_t *bins, float &best_cost, int &best_split) {
+    float left_cost[kBins - 1];
+    int left_count[kBins - 1];
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    int acc = 0;
+    for (int s = 0; s < kBins - 1; s++) {
+        const uint32_t *b = bins + s * kBinWords;
+        for (int a = 0; a < 3; a++) {
+            lo[a] = fminf(lo[a], unord(b[a]));
+            hi[a] = fmaxf(hi[a], unord(b[3 + a]));
+        }
+        acc += int(b[6]);
+        left_count[s] = acc;
+        left_cost[s] = acc > 0 ? AE_MUL(half_area(lo, hi), float(acc)) : 0.0f;
+    }
+    for (int a = 0; a < 3; a++) { lo[a] = FLT_MAX; hi[a] = -FLT_MAX; }
+    acc = 0;
+    best_cost = FLT_MAX;
+    best_split = 0;
+    for (int s = kBins - 1; s > 0; s--) {
+        const uint32_t *b = bins + s * kBinWords;
+        for (int a = 0; a < 3; a++) {
+            lo[a] = fminf(lo[a], unord(b[a]));
+            hi[a] = fmaxf(hi[a], unord(b[3 + a]));
+        }
+        acc += int(b[6]);
+        if (left_count[s - 1] == 0 || acc == 0) continue;
+        const float cost = AE_ADD(left_cost[s - 1], AE_MUL(half_area(lo, hi), float(acc)));
+        if (cost < best_cost) { best_cost = cost; best_split = s; }
+    }
+}
+
+__device__ __forceinline__ void bins_reset(uint32_t *bins, int i) {
+    const int w = i % kBinWords;
+    bins[i] = w < 3 ? ord(FLT_MAX) : (w < 6 ? ord(-FLT_MAX) : 0u);
+}
+
+// Centroid extent of one axis -> bucket mapping; false when the reference
+// skips the axis (extent <= 0).
+__device__ __forceinline__ bool axis_mapping(uint32_t ocmin, uint32_t ocmax, float &cmin, float &scale) {
+    cmin = unord(ocmin);
+    const float extent = AE_SUB(unord(ocmax), cmin);
+    if (extent <= 0.0f) return false;
+    scale = AE_DIV(float(kBins), extent);
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Setup: copy the boxes into the permuted array, identity order, and flag a
+// coordinate that is not finite.
+// ---------------------------------------------------------------------------
+__global__ void k_setup(const ae_aabb *bounds, uint32_t n, uint32_t *idx, ae_aabb *pb, int *bad) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const ae_aabb b = bounds[i];
+    const float *f = &b.min_x;
+    bool finite = true;
+    for (int a = 0; a < 6; a++) finite &= isfinite(f[a]);
+    if (!finite) atomicExch(bad, 1);
+    idx[i] = i;
+    pb[i] = b;
+}
+
+// ---------------------------------------------------------------------------
+// Level-by-level phase (nodes larger than kWarpTask).
+// ---------------------------------------------------------------------------
+__global__ void k_acc_reset(TaskAcc *acc, uint32_t ntasks) {
+    const uint32_t t = blockIdx.x;
+    if (t >= ntasks) return;
+    TaskAcc &A = acc[t];
+    if (threadIdx.x < 3) {
+        A.bmin[threadIdx.x] = min_key_empty();
+        A.bmax[threadIdx.x] = max_key_empty();
+        A.cmin[threadIdx.x] = ord(FLT_MAX);
+        A.cmax[threadIdx.x] = ord(-FLT_MAX);
+    }
+    for (int i = threadIdx.x; i < kBinTable; i += blockDim.x) bins_reset(A.bins, i);
+}
+
+template <class T, class Op>
+__device__ __forceinline__ T warp_all(T v, Op op) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+struct MinOp { template <class T> __device__ T operator()(T a, T b) const { return b < a ? b : a; } };
+struct MaxOp { template <class T> __device__ T operator()(T a, T b) const { return a < b ? b : a; } };
+
+// Box keys and centroid bounds of one chunk, folded into its task.
+__global__ void __launch_bounds__(kThreads) k_big_reduce(const Chunk *chunks, const ae_aabb *pb, TaskAcc *acc) {
+    const Chunk C = chunks[blockIdx.x];
+    unsigned long long kmin[3], kmax[3];
+    uint32_t cmin[3], cmax[3];
+    for (int a = 0; a < 3; a++) {
+        kmin[a] = min_key_empty(); kmax[a] = max_key_empty();
+        cmin[a] = ord(FLT_MAX); cmax[a] = ord(-FLT_MAX);
+    }
+    for (uint32_t p = C.begin + threadIdx.x; p < C.end; p += kThreads) {
+        const ae_aabb b = pb[p];
+        const float *f = &b.min_x;
+        for (int a = 0; a < 3; a++) {
+            kmin[a] = MinOp()(kmin[a], min_key(f[a], p));
+            kmax[a] = MaxOp()(kmax[a], max_key(f[a + 3], p));
+            const uint32_t c = ord(centre(b, a));
+            cmin[a] = min(cmin[a], c);
+            cmax[a] = max(cmax[a], c);
+        }
+    }
+    __shared__ unsigned long long skmin[kThreads / 32][3], skmax[kThreads / 32][3];
+    __shared__ uint32_t scmin[kThreads / 32][3], scmax[kThreads / 32][3];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int a = 0; a < 3; a++) {
+        kmin[a] = warp_all(kmin[a], MinOp());
+        kmax[a] = warp_all(kmax[a], MaxOp());
+        cmin[a] = __reduce_min_sync(0xffffffffu, cmin[a]);
+        cmax[a] = __reduce_max_sync(0xffffffffu, cmax[a]);
+        if (lane == 0) { skmin[w][a] = kmin[a]; skmax[w][a] = kmax[a]; scmin[w][a] = cmin[a]; scmax[w][a] = cmax[a]; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        const int a = threadIdx.x;
+        unsigned long long m0 = skmin[0][a], m1 = skmax[0][a];
+        uint32_t c0 = scmin[0][a], c1 = scmax[0][a];
+        for (int i = 1; i < kThreads / 32; i++) {
+            m0 = MinOp()(m0, skmin[i][a]); m1 = MaxOp()(m1, skmax[i][a]);
+            c0 = min(c0, scmin[i][a]); c1 = max(c1, scmax[i][a]);
+        }
+        TaskAcc &A = acc[C.task];
+        atomicMin(&A.bmin[a], m0);
+        atomicMax(&A.bmax[a], m1);
+        atomicMin(&A.cmin[a], c0);
+        atomicMax(&A.cmax[a], c1);
+    }
+}
+
+// The 3 x 12 buckets of one chunk, in shared memory, folded into its task.
+__global__ void __launch_bounds__(kThreads) k_big_bin(const Chunk *chunks, const BigTask *tasks, const ae_aabb *pb,
+                                                      TaskAcc *acc) {
+    const Chunk C = chunks[blockIdx.x];
+    const BigTask T = tasks[C.task];
+    if (T.depth >= uint32_t(kMaxDepth)) return;  // a leaf: no buckets
+    TaskAcc &A = acc[C.task];
+    __shared__ uint32_t sb[kBinTable];
+    for (int i = threadIdx.x; i < kBinTable; i += kThreads) bins_reset(sb, i);
+    float cmin[3], scale[3];
+    bool ok[3];
+    for (int a = 0; a < 3; a++) ok[a] = axis_mapping(A.cmin[a], A.cmax[a], cmin[a], scale[a]);
+    __syncthreads();
+    for (uint32_t p = C.begin + threadIdx.x; p < C.end; p += kThreads) {
+        const ae_aabb b = pb[p];
+        const float *f = &b.min_x;
+        for (int a = 0; a < 3; a++) {
+            if (!ok[a]) continue;
+            uint32_t *r = sb + (a * kBins + bucket(centre(b, a), cmin[a], scale[a])) * kBinWords;
+            for (int k = 0; k < 3; k++) {
+                atomicMin(r + k, ord(f[k]));
+                atomicMax(r + 3 + k, ord(f[k + 3]));
+            }
+            atomicAdd(r + 6, 1u);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kBinTable; i += kThreads) {
+        const int rec = i / kBinWords, wd = i % kBinWords;
+        if (sb[rec * kBinWords + 6] == 0u) continue;
+        if (wd < 3) atomicMin(&A.bins[i], sb[i]);
+        else if (wd < 6) atomicMax(&A.bins[i], sb[i]);
+        else atomicAdd(&A.bins[i], sb[i]);
+    }
+}
+
+// One thread per task: the node box, leaf or not, the SAH plane.
+__global__ void k_big_decide(const BigTask *tasks, uint32_t ntasks, const TaskAcc *acc, const ae_aabb *pb,
+                             Decision *dec) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntasks) return;
+    const BigTask T = tasks[t];
+    const TaskAcc &A = acc[t];
+    Decision D;
+    float *bx = &D.box.min_x;
+    for (int a = 0; a < 3; a++) {
+        bx[a] = min_from_key(A.bmin[a], pb, a);
+        bx[a + 3] = max_from_key(A.bmax[a], pb, a);
+    }
+    const uint32_t count = T.end - T.start;
+    D.leaf = (count <= uint32_t(kLeafSize) || T.depth >= uint32_t(kMaxDepth)) ? 1 : 0;
+    D.axis = -1; D.split = 0; D.cmin = 0.0f; D.scale = 0.0f;
+    if (!D.leaf) {
+        float best = FLT_MAX;
+        for (int a = 0; a < 3; a++) {
+            float cm, sc;
+            if (!axis_mapping(A.cmin[a], A.cmax[a], cm, sc)) continue;
+            float c; int s;
+            sweep_axis(A.bins + a * kBins * kBinWords, c, s);
+            if (c < best) { best = c; D.axis = a; D.split = s; D.cmin = cm; D.scale = sc; }
+        }
+    }
+    dec[t] = D;
+}
+
+__device__ __forceinline__ bool goes_left(const ae_aabb &b, const Decision &D) {
+    return bucket(centre(b, D.axis), D.cmin, D.scale) < D.split;
+}
+
+// Passing elements per chunk (positions [begin, end) of a splitting task).
+__global__ void __launch_bounds__(kThreads) k_big_count(const Chunk *chunks, const Decision *dec, const ae_aabb *pb,
+                                                        uint32_t *chunk_true) {
+    const Chunk C = chunks[blockIdx.x];
+    const Decision D = dec[C.task];
+    if (D.leaf || D.axis < 0) {
+        if (threadIdx.x == 0) chunk_true[blockIdx.x] = 0;
+        return;
+    }
+    uint32_t n = 0;
+    for (uint32_t p = C.begin + threadIdx.x; p < C.end; p += kThreads) n += goes_left(pb[p], D) ? 1u : 0u;
+    n = __reduce_add_sync(0xffffffffu, n);
+    __shared__ uint32_t s[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = n;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int i = 0; i < kThreads / 32; i++) t += s[i];
+        chunk_true[blockIdx.x] = t;
+    }
+}
+
+// Misplaced elements of a splitting task go to the stash: the k-th failing
+// element left of the boundary to start + k, the k-th passing element right
+// of it (counted from the right) to end - 1 - k.  kinfo[p] = k + 1, bit 31
+// set for the passing kind, 0 for an element that stays.
+__global__ void __launch_bounds__(kThreads) k_big_stash(const Chunk *chunks, const BigTask *tasks, const Decision *dec,
+                                                        const uint32_t *task_true, const uint32_t *chunk_base,
+                                                        const uint32_t *idx, const ae_aabb *pb, uint32_t *stash_idx,
+                                                        ae_aabb *stash_pb, uint32_t *kinfo) {
+    const Chunk C = chunks[blockIdx.x];
+    const Decision D = dec[C.task];
+    if (D.leaf || D.axis < 0) return;
+    const BigTask T = tasks[C.task];
+    const uint32_t ntrue = task_true[C.task];
+    const uint32_t boundary = T.start + ntrue;
+    // Each thread takes kPer consecutive positions.
+    const uint32_t p0 = C.begin + threadIdx.x * kPer;
+    bool pass[kPer];
+    uint32_t mine = 0;
+    for (int j = 0; j < kPer; j++) {
+        const uint32_t p = p0 + j;
+        pass[j] = p < C.end && goes_left(pb[p], D);
+        mine += pass[j] ? 1u : 0u;
+    }
+    // Block exclusive scan of the per-thread counts.
+    __shared__ uint32_t s[kThreads / 32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) s[w] = incl;
+    __syncthreads();
+    uint32_t before = chunk_base[blockIdx.x] + incl - mine;
+    for (int i = 0; i < w; i++) before += s[i];
+    for (int j = 0; j < kPer; j++) {
+        const uint32_t p = p0 + j;
+        if (p >= C.end) break;
+        uint32_t info = 0;
+        if (p < boundary && !pass[j]) {
+            const uint32_t k = (p - T.start) - before;
+            stash_idx[T.start + k] = idx[p];
+            stash_pb[T.start + k] = pb[p];
+            info = k + 1u;
+        } else if (p >= boundary && pass[j]) {
+            const uint32_t k = ntrue - before - 1u;
+            stash_idx[T.end - 1u - k] = idx[p];
+            stash_pb[T.end - 1u - k] = pb[p];
+            info = (k + 1u) | 0x80000000u;
+        }
+        kinfo[p] = info;
+        before += pass[j] ? 1u : 0u;
+    }
+}
+
+// Each misplaced element takes its partner's record from the stash.
+__global__ void __launch_bounds__(kThreads) k_big_unstash(const Chunk *chunks, const BigTask *tasks, const Decision *dec,
+                                                          const uint32_t *kinfo, const uint32_t *stash_idx,
+                                                          const ae_aabb *stash_pb, uint32_t *idx, ae_aabb *pb) {
+    const Chunk C = chunks[blockIdx.x];
+    const Decision D = dec[C.task];
+    if (D.leaf || D.axis < 0) return;
+    const BigTask T = tasks[C.task];
+    for (uint32_t p = C.begin + threadIdx.x; p < C.end; p += kThreads) {
+        const uint32_t info = kinfo[p];
+        if (info == 0u) continue;
+        const uint32_t k = (info & 0x7fffffffu) - 1u;
+        const uint32_t from = (info & 0x80000000u) ? T.start + k : T.end - 1u - k;
+        idx[p] = stash_idx[from];
+        pb[p] = stash_pb[from];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One warp per subtree of at most kWarpTask primitives.
+// ---------------------------------------------------------------------------
+struct WarpWork { uint32_t start, end, depth; int32_t parent, right; };
+
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_warp_build(const SmallTask *tasks, uint32_t ntasks,
+                                                                   uint32_t *idx, ae_aabb *pb, uint32_t *stash_idx,
+                                                                   ae_aabb *stash_pb, uint32_t *kinfo,
+                                                                   ae_bvh_node *tmp, uint32_t *sub_count) {
+    __shared__ uint32_t sbins[kWarpsPerBlock][kBinTable];
+    __shared__ WarpWork sstack[kWarpsPerBlock][kWarpStack];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t t = blockIdx.x * kWarpsPerBlock + w;
+    if (t >= ntasks) return;
+    uint32_t *bins = sbins[w];
+    WarpWork *stack = sstack[w];
+    const SmallTask task = tasks[t];
+    ae_bvh_node *out = tmp + 2ull * task.start;
+    if (lane == 0) stack[0] = WarpWork{task.start, task.end, task.depth, -1, 0};
+    int sp = 1;
+    int li = 0;
+    __syncwarp();
+    while (sp > 0) {
+        const WarpWork wk = stack[--sp];
+        __syncwarp();
+        const int self = li++;
+        if (lane == 0 && wk.parent >= 0) {
+            if (wk.right) out[wk.parent].right = self;
+            else out[wk.parent].left = self;
+        }
+        // Box and centroid bounds.
+        unsigned long long kmin[3], kmax[3];
+        uint32_t cmn[3], cmx[3];
+        for (int a = 0; a < 3; a++) {
+            kmin[a] = min_key_empty(); kmax[a] = max_key_empty();
+            cmn[a] = ord(FLT_MAX); cmx[a] = ord(-FLT_MAX);
+        }
+        for (uint32_t p = wk.start + lane; p < wk.end; p += 32) {
+            const ae_aabb b = pb[p];
+            const float *f = &b.min_x;
+            for (int a = 0; a < 3; a++) {
+                kmin[a] = MinOp()(kmin[a], min_key(f[a], p));
+                kmax[a] = MaxOp()(kmax[a], max_key(f[a + 3], p));
+                const uint32_t c = ord(centre(b, a));
+                cmn[a] = min(cmn[a], c);
+                cmx[a] = max(cmx[a], c);
+            }
+        }
+        ae_aabb box;
+        float *bx = &box.min_x;
+        for (int a = 0; a < 3; a++) {
+            bx[a] = min_from_key(warp_all(kmin[a], MinOp()), pb, a);
+            bx[a + 3] = max_from_key(warp_all(kmax[a], MaxOp()), pb, a);
+            cmn[a] = __reduce_min_sync(0xffffffffu, cmn[a]);
+            cmx[a] = __reduce_max_sync(0xffffffffu, cmx[a]);
+        }
+        const uint32_t count = wk.end - wk.start;
+        if (count <= uint32_t(kLeafSize) || wk.depth >= uint32_t(kMaxDepth)) {
+            if (lane == 0) out[self] = make_node(box, int(wk.start), -1, int(count));
+            __syncwarp();
+            continue;
+        }
+        // Buckets.
+        float cmin[3], scale[3];
+        bool ok[3];
+        for (int a = 0; a < 3; a++) ok[a] = axis_mapping(cmn[a], cmx[a], cmin[a], scale[a]);
+        for (int i = lane; i < kBinTable; i += 32) bins_reset(bins, i);
+        __syncwarp();
+        if (ok[0] || ok[1] || ok[2]) {
+            for (uint32_t p = wk.start + lane; p < wk.end; p += 32) {
+                const ae_aabb b = pb[p];
+                const float *f = &b.min_x;
+                for (int a = 0; a < 3; a++) {
+                    if (!ok[a]) continue;
+                    uint32_t *r = bins + (a * kBins + bucket(centre(b, a), cmin[a], scale[a])) * kBinWords;
+                    for (int k = 0; k < 3; k++) {
+                        atomicMin(r + k, ord(f[k]));
+                        atomicMax(r + 3 + k, ord(f[k + 3]));
+                    }
+                    atomicAdd(r + 6, 1u);
+                }
+            }
+        }
+        __syncwarp();
+        // Lanes 0-2 sweep one axis each; axes are then taken in order with
+        // strict <, as the reference's single loop over axes does.
+        float c = FLT_MAX;
+        int s = 0;
+        if (lane < 3 && ok[lane]) sweep_axis(bins + lane * kBins * kBinWords, c, s);
+        const float c0 = __shfl_sync(0xffffffffu, c, 0), c1 = __shfl_sync(0xffffffffu, c, 1),
+                    c2 = __shfl_sync(0xffffffffu, c, 2);
+        const int s0 = __shfl_sync(0xffffffffu, s, 0), s1 = __shfl_sync(0xffffffffu, s, 1),
+                  s2 = __shfl_sync(0xffffffffu, s, 2);
+        float best = FLT_MAX;
+        int axis = -1, split = 0;
+        if (c0 < best) { best = c0; axis = 0; split = s0; }
+        if (c1 < best) { best = c1; axis = 1; split = s1; }
+        if (c2 < best) { best = c2; axis = 2; split = s2; }
+        uint32_t mid = wk.start + count / 2;
+        if (axis >= 0) {
+            Decision D;
+            D.axis = axis; D.split = split; D.cmin = cmin[axis]; D.scale = scale[axis];
+            uint32_t ntrue = 0;
+            for (uint32_t base = wk.start; base < wk.end; base += 32) {
+                const uint32_t p = base + lane;
+                ntrue += __popc(__ballot_sync(0xffffffffu, p < wk.end && goes_left(pb[p], D)));
+            }
+            const uint32_t boundary = wk.start + ntrue;
+            uint32_t before = 0;
+            for (uint32_t base = wk.start; base < wk.end; base += 32) {
+                const uint32_t p = base + lane;
+                const bool pass = p < wk.end && goes_left(pb[p], D);
+                const uint32_t m = __ballot_sync(0xffffffffu, pass);
+                const uint32_t b = before + __popc(m & ((1u << lane) - 1u));
+                if (p < wk.end) {
+                    uint32_t info = 0;
+                    if (p < boundary && !pass) {
+                        const uint32_t k = (p - wk.start) - b;
+                        stash_idx[wk.start + k] = idx[p];
+                        stash_pb[wk.start + k] = pb[p];
+                        info = k + 1u;
+                    } else if (p >= boundary && pass) {
+                        const uint32_t k = ntrue - b - 1u;
+                        stash_idx[wk.end - 1u - k] = idx[p];
+                        stash_pb[wk.end - 1u - k] = pb[p];
+                        info = (k + 1u) | 0x80000000u;
+                    }
+                    kinfo[p] = info;
+                }
+                before += __popc(m);
+            }
+            __syncwarp();
+            for (uint32_t p = wk.start + lane; p < wk.end; p += 32) {
+                const uint32_t info = kinfo[p];
+                if (info == 0u) continue;
+                const uint32_t k = (info & 0x7fffffffu) - 1u;
+                const uint32_t from = (info & 0x80000000u) ? wk.start + k : wk.end - 1u - k;
+                idx[p] = stash_idx[from];
+                pb[p] = stash_pb[from];
+            }
+            __syncwarp();
+            mid = boundary;
+        }
+        if (mid <= wk.start || mid >= wk.end) mid = wk.start + count / 2;
+        if (lane == 0) {
+            out[self] = make_node(box, -1, -1, 0);
+            stack[sp] = WarpWork{mid, wk.end, wk.depth + 1, self, 1};
+            stack[sp + 1] = WarpWork{wk.start, mid, wk.depth + 1, self, 0};
+        }
+        sp += 2;
+        __syncwarp();
+    }
+    if (lane == 0) sub_count[t] = uint32_t(li);
+}
+
+// ---------------------------------------------------------------------------
+// Final numbering.
+// ---------------------------------------------------------------------------
+// One block per warp-built subtree: local node indices -> global.
+__global__ void k_place_subtrees(const SmallTask *tasks, const uint32_t *sub_count, const uint32_t *sub_base,
+                                 const ae_bvh_node *tmp, ae_bvh_node *out) {
+    const uint32_t t = blockIdx.x;
+    const ae_bvh_node *src = tmp + 2ull * tasks[t].start;
+    const uint32_t base = sub_base[t], n = sub_count[t];
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        ae_bvh_node nd = src[i];
+        if (nd.count == 0) {
+            nd.left += int(base);
+            nd.right += int(base);
+        }
+        out[base + i] = nd;
+    }
+}
+
+struct TopPlace { uint32_t at; int32_t left, right; uint32_t start, count; int32_t leaf; };
+
+__global__ void k_place_top(const TopPlace *place, const Decision *dec_all, uint32_t ntop, ae_bvh_node *out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntop) return;
+    const TopPlace P = place[t];
+    const ae_aabb box = dec_all[t].box;
+    out[P.at] = P.leaf ? make_node(box, int(P.start), -1, int(P.count)) : make_node(box, P.left, P.right, 0);
+}
+
+// Triangle boxes: Surround2Points(a, b) then SurroundPoint(c),
+// scene/aabb.h:96-103, with std::min / std::max (first of equal values).
+__device__ __forceinline__ float smin(float a, float b) { return b < a ? b : a; }
+__device__ __forceinline__ float smax(float a, float b) { return a < b ? b : a; }
+
+__global__ void k_triangle_boxes(const ae_vertex *v, const uint32_t *idx, uint32_t tris, ae_aabb *out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tris) return;
+    const ae_vertex a = v[idx[3 * t]], b = v[idx[3 * t + 1]], c = v[idx[3 * t + 2]];
+    ae_aabb e;
+    e.min_x = smin(smin(a.px, b.px), c.px);
+    e.min_y = smin(smin(a.py, b.py), c.py);
+    e.min_z = smin(smin(a.pz, b.pz), c.pz);
+    e.max_x = smax(smax(a.px, b.px), c.px);
+    e.max_y = smax(smax(a.py, b.py), c.py);
+    e.max_z = smax(smax(a.pz, b.pz), c.pz);
+    out[t] = e;
+}
+
+// Indices in leaf-slot order (scene/mesh_library.h:147-153).
+__global__ void k_reorder_indices(const uint32_t *idx, const uint32_t *order, uint32_t tris, uint32_t *out) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= tris) return;
+    const uint32_t t = order[s];
+    out[3 * s] = idx[3 * t];
+    out[3 * s + 1] = idx[3 * t + 1];
+    out[3 * s + 2] = idx[3 * t + 2];
+}
+
+// ---------------------------------------------------------------------------
+// Host driver.
+// ---------------------------------------------------------------------------
+template <class T> struct Buf {
+    T *p = nullptr;
+    ~Buf() { reset(); }
+    void reset() {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    cudaError_t alloc(size_t n) { return cudaMalloc(&p, (n ? n : 1) * sizeof(T)); }
+};
+
+#define AE_CK(x)                                  \
+    do {                                          \
+        if ((x) != cudaSuccess) {                 \
+            cudaGetLastError();                   \
+            return AE_ERR_CUDA;                   \
+        }                                         \
+    } while (0)
+
+struct TopNode {
+    BigTask task;
+    int32_t left = 0, right = 0;  // >= 0: top node; < 0: warp subtree -1 - id
+    bool leaf = false;
+};
+
+}  // namespace
+
+// Builds the tree over `d_bounds` (device, n boxes) on `st`.  On success
+// d_nodes (2n capacity) holds the nodes, d_order the leaf-slot permutation,
+// *node_count their number.
+int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uint32_t *d_order,
+                  uint32_t *node_count, cudaStream_t st, uint32_t warp_subtree = kWarpTask) {
+    *node_count = 0;
+    if (n == 0) return AE_OK;
+    Buf<ae_aabb> pb, stash_pb;
+    Buf<uint32_t> stash_idx, kinfo;
+    Buf<ae_bvh_node> tmp;
+    Buf<int> bad;
+    AE_CK(pb.alloc(n));
+    AE_CK(stash_pb.alloc(n));
+    AE_CK(stash_idx.alloc(n));
+    AE_CK(kinfo.alloc(n));
+    AE_CK(tmp.alloc(2ull * n));
+    AE_CK(bad.alloc(1));
+    AE_CK(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
+    uint32_t *idx = d_order;
+    k_setup<<<(n + 255) / 256, 256, 0, st>>>(d_bounds, n, idx, pb.p, bad.p);
+    int h_bad = 0;
+    AE_CK(cudaMemcpyAsync(&h_bad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    AE_CK(cudaStreamSynchronize(st));
+    if (h_bad) return AE_ERR_INVALID;
+
+    std::vector<TopNode> top;
+    std::vector<SmallTask> small;
+    std::vector<Decision> top_dec;
+    std::vector<BigTask> level;
+    std::vector<uint32_t> level_top;  // top node of each task of the level
+    if (n > warp_subtree) {
+        level.push_back(BigTask{0, n, 0});
+        level_top.push_back(0);
+        top.push_back(TopNode{});
+        top[0].task = level[0];
+    } else {
+        small.push_back(SmallTask{0, n, 0});
+    }
+    Buf<TaskAcc> acc;
+    Buf<BigTask> d_tasks;
+    Buf<Chunk> d_chunks;
+    Buf<Decision> d_dec;
+    Buf<uint32_t> d_chunk_true, d_chunk_base, d_task_true;
+    size_t cap_tasks = 0, cap_chunks = 0;
+    std::vector<Chunk> chunks;
+    std::vector<Decision> dec;
+    std::vector<uint32_t> chunk_true, chunk_base, task_true;
+    while (!level.empty()) {
+        const uint32_t nt = uint32_t(level.size());
+        chunks.clear();
+        for (uint32_t t = 0; t < nt; t++)
+            for (uint32_t b = level[t].start; b < level[t].end; b += kChunk)
+                chunks.push_back(Chunk{t, b, b + kChunk < level[t].end ? b + kChunk : level[t].end});
+        const uint32_t nc = uint32_t(chunks.size());
+        if (nt > cap_tasks) {
+            cap_tasks = nt * 2;
+            acc.reset();
+            d_tasks.reset();
+            d_dec.reset();
+            d_task_true.reset();
+            AE_CK(acc.alloc(cap_tasks));
+            AE_CK(d_tasks.alloc(cap_tasks));
+            AE_CK(d_dec.alloc(cap_tasks));
+            AE_CK(d_task_true.alloc(cap_tasks));
+        }
+        if (nc > cap_chunks) {
+            cap_chunks = nc * 2;
+            d_chunks.reset();
+            d_chunk_true.reset();
+            d_chunk_base.reset();
+            AE_CK(d_chunks.alloc(cap_chunks));
+            AE_CK(d_chunk_true.alloc(cap_chunks));
+            AE_CK(d_chunk_base.alloc(cap_chunks));
+        }
+        AE_CK(cudaMemcpyAsync(d_tasks.p, level.data(), nt * sizeof(BigTask), cudaMemcpyHostToDevice, st));
+        AE_CK(cudaMemcpyAsync(d_chunks.p, chunks.data(), nc * sizeof(Chunk), cudaMemcpyHostToDevice, st));
+        k_acc_reset<<<nt, 128, 0, st>>>(acc.p, nt);
+        k_big_reduce<<<nc, kThreads, 0, st>>>(d_chunks.p, pb.p, acc.p);
+        k_big_bin<<<nc, kThreads, 0, st>>>(d_chunks.p, d_tasks.p, pb.p, acc.p);
+        k_big_decide<<<(nt + 127) / 128, 128, 0, st>>>(d_tasks.p, nt, acc.p, pb.p, d_dec.p);
+        k_big_count<<<nc, kThreads, 0, st>>>(d_chunks.p, d_dec.p, pb.p, d_chunk_true.p);
+        dec.resize(nt);
+        chunk_true.resize(nc);
+        AE_CK(cudaMemcpyAsync(dec.data(), d_dec.p, nt * sizeof(Decision), cudaMemcpyDeviceToHost, st));
+        AE_CK(cudaMemcpyAsync(chunk_true.data(), d_chunk_true.p, nc * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        AE_CK(cudaStreamSynchronize(st));
+        task_true.assign(nt, 0);
+        chunk_base.resize(nc);
+        for (uint32_t c = 0; c < nc; c++) {
+            chunk_base[c] = task_true[chunks[c].task];
+            task_true[chunks[c].task] += chunk_true[c];
+        }
+        AE_CK(cudaMemcpyAsync(d_chunk_base.p, chunk_base.data(), nc * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        AE_CK(cudaMemcpyAsync(d_task_true.p, task_true.data(), nt * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        k_big_stash<<<nc, kThreads, 0, st>>>(d_chunks.p, d_tasks.p, d_dec.p, d_task_true.p, d_chunk_base.p, idx, pb.p,
+                                             stash_idx.p, stash_pb.p, kinfo.p);
+        k_big_unstash<<<nc, kThreads, 0, st>>>(d_chunks.p, d_tasks.p, d_dec.p, kinfo.p, stash_idx.p, stash_pb.p, idx,
+                                               pb.p);
+        AE_CK(cudaGetLastError());
+        // Children of this level.  The copies above were staged from pageable
+        // memory, so the host arrays may be reused at once.
+        std::vector<BigTask> next;
+        std::vector<uint32_t> next_top;
+        if (top_dec.size() < top.size()) top_dec.resize(top.size());
+        for (uint32_t t = 0; t < nt; t++) {
+            const BigTask T = level[t];
+            const uint32_t id = level_top[t];
+            top_dec[id] = dec[t];
+            if (dec[t].leaf) {
+                top[id].leaf = true;
+                continue;
+            }
+            const uint32_t count = T.end - T.start;
+            uint32_t mid = dec[t].axis >= 0 ? T.start + task_true[t] : T.start + count / 2;
+            if (mid <= T.start || mid >= T.end) mid = T.start + count / 2;
+            const BigTask kids[2] = {BigTask{T.start, mid, T.depth + 1}, BigTask{mid, T.end, T.depth + 1}};
+            for (int side = 0; side < 2; side++) {
+                const BigTask &K = kids[side];
+                int32_t ref;
+                if (K.end - K.start > warp_subtree) {
+                    ref = int32_t(top.size());
+                    top.push_back(TopNode{});
+                    top.back().task = K;
+                    next.push_back(K);
+                    next_top.push_back(uint32_t(ref));
+                } else {
+                    ref = -1 - int32_t(small.size());
+                    small.push_back(SmallTask{K.start, K.end, K.depth});
+                }
+                if (side == 0) top[id].left = ref;
+                else top[id].right = ref;
+            }
+        }
+        AE_CK(cudaStreamSynchronize(st));
+        level.swap(next);
+        level_top.swap(next_top);
+    }
+
+    // Warp-built subtrees.
+    const uint32_t ns = uint32_t(small.size());
+    Buf<SmallTask> d_small;
+    Buf<uint32_t> d_sub_count, d_sub_base;
+    AE_CK(d_small.alloc(ns));
+    AE_CK(d_sub_count.alloc(ns));
+    AE_CK(d_sub_base.alloc(ns));
+    std::vector<uint32_t> sub_count(ns), sub_base(ns);
+    if (ns) {
+        AE_CK(cudaMemcpyAsync(d_small.p, small.data(), ns * sizeof(SmallTask), cudaMemcpyHostToDevice, st));
+        k_warp_build<<<(ns + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, st>>>(
+            d_small.p, ns, idx, pb.p, stash_idx.p, stash_pb.p, kinfo.p, tmp.p, d_sub_count.p);
+        AE_CK(cudaGetLastError());
+        AE_CK(cudaMemcpyAsync(sub_count.data(), d_sub_count.p, ns * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        AE_CK(cudaStreamSynchronize(st));
+    }
+    // Pre-order numbering: a node, then its left subtree, then its right.
+    std::vector<TopPlace> place(top.size());
+    uint32_t next_index = 0;
+    std::vector<int32_t> work;
+    work.push_back(top.empty() ? -1 : 0);
+    std::vector<uint32_t> root_of_top(top.size());
+    while (!work.empty()) {
+        const int32_t ref = work.back();
+        work.pop_back();
+        if (ref >= 0) {
+            root_of_top[ref] = next_index++;
+            if (!top[ref].leaf) {
+                work.push_back(top[ref].right);
+                work.push_back(top[ref].left);
+            }
+        } else {
+            const uint32_t s = uint32_t(-1 - ref);
+            sub_base[s] = next_index;
+            next_index += sub_count[s];
+        }
+    }
+    for (size_t i = 0; i < top.size(); i++) {
+        TopPlace &P = place[i];
+        P.at = root_of_top[i];
+        P.leaf = top[i].leaf ? 1 : 0;
+        P.start = top[i].task.start;
+        P.count = top[i].task.end - top[i].task.start;
+        auto root = [&](int32_t r) { return r >= 0 ? int32_t(root_of_top[r]) : int32_t(sub_base[-1 - r]); };
+        P.left = P.leaf ? 0 : root(top[i].left);
+        P.right = P.leaf ? 0 : root(top[i].right);
+    }
+    if (ns) {
+        AE_CK(cudaMemcpyAsync(d_sub_base.p, sub_base.data(), ns * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        k_place_subtrees<<<ns, 256, 0, st>>>(d_small.p, d_sub_count.p, d_sub_base.p, tmp.p, d_nodes);
+    }
+    if (!top.empty()) {
+        Buf<TopPlace> d_place;
+        Buf<Decision> d_top_dec;
+        AE_CK(d_place.alloc(top.size()));
+        AE_CK(d_top_dec.alloc(top.size()));
+        AE_CK(cudaMemcpyAsync(d_place.p, place.data(), top.size() * sizeof(TopPlace), cudaMemcpyHostToDevice, st));
+        AE_CK(cudaMemcpyAsync(d_top_dec.p, top_dec.data(), top.size() * sizeof(Decision), cudaMemcpyHostToDevice, st));
+        k_place_top<<<uint32_t((top.size() + 127) / 128), 128, 0, st>>>(d_place.p, d_top_dec.p, uint32_t(top.size()),
+                                                                         d_nodes);
+        AE_CK(cudaGetLastError());
+        AE_CK(cudaStreamSynchronize(st));
+    }
+    AE_CK(cudaGetLastError());
+    AE_CK(cudaStreamSynchronize(st));
+    *node_count = next_index;
+    return AE_OK;
+}
+
+// MeshLibrary::Add's device part: the triangle boxes, the BLAS and the
+// indices in leaf-slot order.  Host arrays in and out.
+int gpu_mesh_blas(const ae_vertex *v, uint32_t nv, const uint32_t *idx, uint32_t ni, ae_bvh_node *out_nodes,
+                  uint32_t *out_count, uint32_t *out_indices) {
+    *out_count = 0;
+    const uint32_t tris = ni / 3;
+    if (tris == 0) return AE_OK;
+    cudaStream_t st;
+    AE_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamDestroy(s); } } guard{st};
+    Buf<ae_vertex> dv;
+    Buf<uint32_t> di, dorder, dout;
+    Buf<ae_aabb> dbox;
+    Buf<ae_bvh_node> dnodes;
+    AE_CK(dv.alloc(nv));
+    AE_CK(di.alloc(ni));
+    AE_CK(dorder.alloc(tris));
+    AE_CK(dout.alloc(ni));
+    AE_CK(dbox.alloc(tris));
+    AE_CK(dnodes.alloc(2ull * tris));
+    AE_CK(cudaMemcpyAsync(dv.p, v, size_t(nv) * sizeof(ae_vertex), cudaMemcpyHostToDevice, st));
+    AE_CK(cudaMemcpyAsync(di.p, idx, size_t(ni) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    k_triangle_boxes<<<(tris + 255) / 256, 256, 0, st>>>(dv.p, di.p, tris, dbox.p);
+    uint32_t count = 0;
+    const int rc = gpu_build_bvh(dbox.p, tris, dnodes.p, dorder.p, &count, st);
+    if (rc != AE_OK) return rc;
+    k_reorder_indices<<<(tris + 255) / 256, 256, 0, st>>>(di.p, dorder.p, tris, dout.p);
+    AE_CK(cudaMemcpyAsync(out_nodes, dnodes.p, size_t(count) * sizeof(ae_bvh_node), cudaMemcpyDeviceToHost, st));
+    AE_CK(cudaMemcpyAsync(out_indices, dout.p, size_t(ni) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    AE_CK(cudaStreamSynchronize(st));
+    *out_count = count;
+    return AE_OK;
+}
+
+}  // namespace ae
+
+extern "C" int ae_build_bvh_gpu_ex(const ae_aabb *bounds, uint32_t n, uint32_t warp_subtree, ae_bvh_node *out_nodes,
+                                   uint32_t *out_node_count, uint32_t *out_order) {
+    if (!out_node_count) return AE_ERR_INVALID;
+    *out_node_count = 0;
+    if (n == 0) return AE_OK;
+    if (!bounds || !out_nodes || !out_order) return AE_ERR_INVALID;
+    cudaStream_t st;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return AE_ERR_CUDA;
+    }
+    int rc = AE_OK;
+    {
+        ae::Buf<ae_aabb> db;
+        ae::Buf<uint32_t> dorder;
+        ae::Buf<ae_bvh_node> dnodes;
+        uint32_t count = 0;
+        if (db.alloc(n) != cudaSuccess || dorder.alloc(n) != cudaSuccess || dnodes.alloc(2ull * n) != cudaSuccess) {
+            cudaGetLastError();
+            rc = AE_ERR_OOM;
+        } else if (cudaMemcpyAsync(db.p, bounds, size_t(n) * sizeof(ae_aabb), cudaMemcpyHostToDevice, st) !=
+                   cudaSuccess) {
+            rc = AE_ERR_CUDA;
+        } else {
+            rc = ae::gpu_build_bvh(db.p, n, dnodes.p, dorder.p, &count, st, warp_subtree);
+            if (rc == AE_OK) {
+                if (cudaMemcpyAsync(out_nodes, dnodes.p, size_t(count) * sizeof(ae_bvh_node), cudaMemcpyDeviceToHost,
+                                    st) != cudaSuccess ||
+                    cudaMemcpyAsync(out_order, dorder.p, size_t(n) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st) !=
+                        cudaSuccess ||
+                    cudaStreamSynchronize(st) != cudaSuccess) {
+                    rc = AE_ERR_CUDA;
+                } else {
+                    *out_node_count = count;
+                }
+            }
+        }
+        if (rc == AE_ERR_CUDA) cudaGetLastError();
+    }
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+extern "C" int ae_build_bvh_gpu(const ae_aabb *bounds, uint32_t n, ae_bvh_node *out_nodes, uint32_t *out_node_count,
+                                uint32_t *out_order) {
+    return ae_build_bvh_gpu_ex(bounds, n, ae::kWarpTask, out_nodes, out_node_count, out_order);
+}

@@ -232,6 +232,12 @@ bool HasScale(float s) { return s != 0.0f && s != 1.0f; }
 
 }  // namespace
 
+namespace ae {
+// The device part of MeshLibrary::Add (bvh_build.cu).
+int gpu_mesh_blas(const ae_vertex *v, uint32_t nv, const uint32_t *idx, uint32_t ni, ae_bvh_node *out_nodes,
+                  uint32_t *out_count, uint32_t *out_indices);
+}  // namespace ae
+
 // ---------------------------------------------------------------------------
 // Mesh library
 // ---------------------------------------------------------------------------
@@ -263,9 +269,11 @@ int ae_build_bvh(const ae_aabb *bounds, uint32_t n, ae_bvh_node *out_nodes, uint
 ae_mesh_library *ae_mesh_library_create(void) { return new (std::nothrow) ae_mesh_library(); }
 void ae_mesh_library_destroy(ae_mesh_library *lib) { delete lib; }
 
-// MeshLibrary::Add, scene/mesh_library.h:91-159.
-int ae_mesh_library_add(ae_mesh_library *lib, const ae_vertex *v, uint32_t nv, const uint32_t *idx, uint32_t ni,
-                        int double_sided) {
+// MeshLibrary::Add, scene/mesh_library.h:91-159.  With on_gpu the triangle
+// boxes, the BLAS and the leaf-order indices come from the device builder
+// (bvh_build.cu), which produces the same bytes.
+static int mesh_library_add(ae_mesh_library *lib, const ae_vertex *v, uint32_t nv, const uint32_t *idx, uint32_t ni,
+                            int double_sided, bool on_gpu) {
     if (!lib || (nv && !v) || (ni && !idx) || ni % 3 != 0) return AE_ERR_INVALID;
     for (uint32_t i = 0; i < ni; i++)
         if (idx[i] >= nv) return AE_ERR_LAYOUT;
@@ -284,6 +292,17 @@ int ae_mesh_library_add(ae_mesh_library *lib, const ae_vertex *v, uint32_t nv, c
         range.localBounds = local;
         const uint32_t tris = ni / 3;
         range.triangleCount = tris;
+        if (on_gpu) {
+            std::vector<ae_bvh_node> nodes(size_t(tris) * 2);
+            std::vector<uint32_t> leaf_order_indices(ni);
+            uint32_t count = 0;
+            const int rc = ae::gpu_mesh_blas(v, nv, idx, ni, nodes.data(), &count, leaf_order_indices.data());
+            if (rc != AE_OK) return rc;
+            lib->indices.insert(lib->indices.end(), leaf_order_indices.begin(), leaf_order_indices.end());
+            lib->blas.insert(lib->blas.end(), nodes.begin(), nodes.begin() + count);
+            lib->ranges.push_back(range);
+            return int(lib->ranges.size() - 1);
+        }
         std::vector<ae_aabb> triBounds(tris);
         for (uint32_t t = 0; t < tris; t++) {
             const ae_vertex &a = v[idx[3 * t]], &b = v[idx[3 * t + 1]], &c = v[idx[3 * t + 2]];
@@ -308,6 +327,15 @@ int ae_mesh_library_add(ae_mesh_library *lib, const ae_vertex *v, uint32_t nv, c
         return AE_ERR_OOM;
     }
     return int(lib->ranges.size() - 1);
+}
+
+int ae_mesh_library_add(ae_mesh_library *lib, const ae_vertex *v, uint32_t nv, const uint32_t *idx, uint32_t ni,
+                        int double_sided) {
+    return mesh_library_add(lib, v, nv, idx, ni, double_sided, false);
+}
+int ae_mesh_library_add_gpu(ae_mesh_library *lib, const ae_vertex *v, uint32_t nv, const uint32_t *idx, uint32_t ni,
+                            int double_sided) {
+    return mesh_library_add(lib, v, nv, idx, ni, double_sided, true);
 }
 
 int ae_mesh_library_range(const ae_mesh_library *lib, uint32_t handle, ae_mesh_range *out) {

@@ -40,9 +40,12 @@ from ._lib import check, lib, ptr
 # Mesh library
 # ---------------------------------------------------------------------------
 class MeshLibrary:
-    """MeshLibrary of scene/mesh_library.h over the C ABI."""
+    """MeshLibrary of scene/mesh_library.h over the C ABI.  With gpu=True each
+    add() builds its BLAS on the GPU (ae_mesh_library_add_gpu: the same
+    bytes as the host build)."""
 
-    def __init__(self):
+    def __init__(self, gpu=False):
+        self.gpu = bool(gpu)
         self._h = lib().ae_mesh_library_create()
         if not self._h:
             raise MemoryError("ae_mesh_library_create")
@@ -55,9 +58,10 @@ class MeshLibrary:
     def add(self, vertices, indices, double_sided=False):
         v = np.ascontiguousarray(vertices, dtype=_lib.VERTEX)
         i = np.ascontiguousarray(indices, dtype=np.uint32).ravel()
-        handle = lib().ae_mesh_library_add(self._h, ptr(v), len(v), ptr(i), len(i), int(double_sided))
+        fn = "ae_mesh_library_add_gpu" if self.gpu else "ae_mesh_library_add"
+        handle = getattr(lib(), fn)(self._h, ptr(v), len(v), ptr(i), len(i), int(double_sided))
         if handle < 0:
-            raise _lib.AeError(handle, "ae_mesh_library_add")
+            raise _lib.AeError(handle, fn)
         return handle
 
     def range(self, handle):
@@ -85,14 +89,22 @@ class MeshLibrary:
         return self._h
 
 
-def build_bvh(bounds):
-    """BuildBVH (scene/bvh.h:275-295) over an (n, 6) float32 array of boxes."""
+def build_bvh(bounds, gpu=False, warp_subtree=None):
+    """BuildBVH (scene/bvh.h:275-295) over an (n, 6) float32 array of boxes;
+    gpu=True runs the device builder (ae_build_bvh_gpu, same output), with
+    `warp_subtree` as its phase threshold when given."""
     b = np.ascontiguousarray(bounds, dtype=np.float32).reshape(-1, 6)
     n = len(b)
     nodes = np.zeros(max(2 * n, 1), _lib.NODE)
     order = np.zeros(max(n, 1), np.uint32)
     count = ctypes.c_uint32()
-    check(lib().ae_build_bvh(ptr(b), n, ptr(nodes), ctypes.byref(count), ptr(order)), what="ae_build_bvh")
+    if gpu and warp_subtree is not None:
+        fn = "ae_build_bvh_gpu_ex"
+        rc = lib().ae_build_bvh_gpu_ex(ptr(b), n, int(warp_subtree), ptr(nodes), ctypes.byref(count), ptr(order))
+    else:
+        fn = "ae_build_bvh_gpu" if gpu else "ae_build_bvh"
+        rc = getattr(lib(), fn)(ptr(b), n, ptr(nodes), ctypes.byref(count), ptr(order))
+    check(rc, what=fn)
     return nodes[:count.value].copy(), order[:n].copy()
 
 
@@ -391,10 +403,11 @@ def textured_box(seed=6, width=160, height=120, depth=6):
 
 
 def instanced_meshes(seed=2, width=1920, height=1080, levels=(7, 6, 6, 5, 5), grid=512, n_instances=64,
-                     n_heightfields=3):
-    """64 instances over 8 unique meshes; 2,099,206 triangles at the defaults."""
+                     n_heightfields=3, gpu_build=False):
+    """64 instances over 8 unique meshes; 2,099,206 triangles at the defaults.
+    gpu_build: BLAS builds on the GPU (identical bytes)."""
     rng = np.random.default_rng(seed)
-    meshes = MeshLibrary()
+    meshes = MeshLibrary(gpu=gpu_build)
     handles = []
     for _ in range(n_heightfields):
         handles.append(meshes.add(*heightfield(grid, 20.0, 2.5, rng)))
@@ -479,12 +492,12 @@ def media_box(seed=7, width=128, height=96, depth=6):
 
 
 def wavefront_scene(seed=4, width=1920, height=1080, depth=12, n_meshes=32, n_instances=1024, n_lights=16,
-                    target_tris=10_000_000):
+                    target_tris=10_000_000, gpu_build=False):
     """The wavefront workload: meshes drawn from the heightfield and icosphere
     generators until about `target_tris` unique triangles, instanced 1024
-    times, lit by 16 emissive quads."""
+    times, lit by 16 emissive quads.  gpu_build: BLAS builds on the GPU."""
     rng = np.random.default_rng(seed)
-    meshes = MeshLibrary()
+    meshes = MeshLibrary(gpu=gpu_build)
     handles, kinds = [], []
     budget = target_tris
     for k in range(n_meshes):
@@ -522,12 +535,13 @@ def wavefront_scene(seed=4, width=1920, height=1080, depth=12, n_meshes=32, n_in
 SERVING_TRIANGLES = (50_000, 120_000, 250_000, 500_000, 1_000_000, 2_000_000, 3_500_000, 5_000_000)
 
 
-def serving_scenes(seed=5, tri_targets=SERVING_TRIANGLES, instances_per_scene=512, depth=8, n_meshes=8):
+def serving_scenes(seed=5, tri_targets=SERVING_TRIANGLES, instances_per_scene=512, depth=8, n_meshes=8,
+                   gpu_build=False):
     """The serving workload's resident scenes: wavefront_scene's generators
     and material mix at each triangle budget, `instances_per_scene` instances
     each, 16 emissive quads."""
     return [wavefront_scene(seed=seed + k, width=640, height=480, depth=depth, n_meshes=n_meshes,
-                            n_instances=instances_per_scene, n_lights=16, target_tris=t)
+                            n_instances=instances_per_scene, n_lights=16, target_tris=t, gpu_build=gpu_build)
             for k, t in enumerate(tri_targets)]
 
 

@@ -197,6 +197,21 @@ int ae_build_bvh(const ae_aabb *bounds, uint32_t n,
                  ae_bvh_node *out_nodes, uint32_t *out_node_count,
                  uint32_t *out_order);
 
+/* ae_build_bvh on the GPU (the current device): the same nodes and the same
+ * leaf-slot order, bit for bit.  Host arrays in and out with the capacities
+ * of ae_build_bvh.  AE_ERR_INVALID for a NaN or infinite coordinate (the
+ * reference's bucket index is undefined for those). */
+int ae_build_bvh_gpu(const ae_aabb *bounds, uint32_t n,
+                     ae_bvh_node *out_nodes, uint32_t *out_node_count,
+                     uint32_t *out_order);
+/* ae_build_bvh_gpu with the subtree size at or below which one warp builds a
+ * whole subtree (ae_build_bvh_gpu uses 1024).  Nodes above it are built one
+ * tree level per round by blocks of 2048 boxes.  Every value gives the same
+ * tree; it only moves work between the two phases. */
+int ae_build_bvh_gpu_ex(const ae_aabb *bounds, uint32_t n, uint32_t warp_subtree,
+                        ae_bvh_node *out_nodes, uint32_t *out_node_count,
+                        uint32_t *out_order);
+
 /* Mesh library: MeshLibrary, scene/mesh_library.h:64-159, with 32-bit input
  * indices (the reference's Mesh is uint16, scene/mesh.h:24, too small for a
  * 512x512 grid).  Add() appends local vertices, builds the BLAS over the
@@ -213,6 +228,10 @@ void ae_mesh_library_destroy(ae_mesh_library *lib);
 /* Returns the mesh handle (>= 0) or a negative ae_status. */
 int ae_mesh_library_add(ae_mesh_library *lib, const ae_vertex *vertices, uint32_t nv,
                         const uint32_t *indices, uint32_t ni, int double_sided);
+/* ae_mesh_library_add with the triangle boxes, the BLAS build and the
+ * leaf-order index rewrite on the GPU; appends the same bytes. */
+int ae_mesh_library_add_gpu(ae_mesh_library *lib, const ae_vertex *vertices, uint32_t nv,
+                            const uint32_t *indices, uint32_t ni, int double_sided);
 int ae_mesh_library_range(const ae_mesh_library *lib, uint32_t handle, ae_mesh_range *out);
 /* Sizes of the flattened arrays (elements). */
 void ae_mesh_library_sizes(const ae_mesh_library *lib, uint64_t *nv, uint64_t *ni, uint64_t *nb);
