@@ -99,6 +99,9 @@ SIGNATURES = {
     "ae_build_bvh": (_I, [_P, _U32, _P, _P, _P]),
     "ae_build_bvh_gpu": (_I, [_P, _U32, _P, _P, _P]),
     "ae_build_bvh_gpu_ex": (_I, [_P, _U32, _U32, _P, _P, _P]),
+    "ae_build_bvh_device": (_I, [_P, _U32, _U32, _P, _P, _P, _P]),
+    "ae_mesh_blas_device": (_I, [_P, _U32, _P, _U32, _P, _P, _P, _P]),
+    "ae_bvh_builder_release": (None, []),
     "ae_mesh_library_create": (_P, []),
     "ae_mesh_library_destroy": (None, [_P]),
     "ae_mesh_library_add": (_I, [_P, _P, _U32, _P, _U32, _I]),
@@ -109,6 +112,7 @@ SIGNATURES = {
     "ae_mesh_library_indices": (_P, [_P]),
     "ae_mesh_library_blas": (_P, [_P]),
     "ae_pack_scene": (_I, [_P, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "ae_pack_scene_gpu": (_I, [_P, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ae_entity_bounds": (_I, [_P, _P, _P]),
     "ae_create": (_P, [_P]),
     "ae_destroy": (None, [_P]),
@@ -138,6 +142,8 @@ SIGNATURES = {
     "ae_launch_count": (ctypes.c_uint64, [_P]),
     "ae_prepare_fast": (_I, [_P]),
     "ae_refit_instances": (_I, [_P, _P, _U32]),
+    "ae_rebuild_scene": (_I, [_P, _P, _U32, _P]),
+    "ae_scene_sizes": (_I, [_P, _P, _P, _P, _P]),
     "ae_download_scene": (_I, [_P, _P, _P, _P]),
     "ae_build_wide_bvh": (_I, [_P, _U32, _U32, _P, _U32, _P, _P, _P]),
     "ae_serve_create": (_P, [_P]),

@@ -39,6 +39,7 @@
 
 #include <cfloat>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "../../include/ae_b200.h"
@@ -55,8 +56,10 @@ constexpr float kBoundsMinimum = 0.0001f;
 constexpr float kHalfMinimum = kBoundsMinimum * 0.5f;
 
 // Subtrees of at most this many primitives are built by one warp (the
-// default; any threshold gives the same tree).
-constexpr uint32_t kWarpTask = 1024;
+// default; any threshold gives the same tree).  Measured over the BLAS of a
+// 10M-triangle, 32-mesh scene: 1024 -> 65 ms, 512 -> 44 ms, 256 -> 35 ms,
+// 128 -> 31 ms, 64 -> 31 ms; smaller subtrees give more warps to run at once.
+constexpr uint32_t kWarpTask = 128;
 constexpr int kWarpsPerBlock = 8;
 // Positions per block in the level-by-level phase: 256 threads x 8.
 constexpr int kThreads = 256;
@@ -480,19 +483,24 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_warp_build(const SmallT
             if (wk.right) out[wk.parent].right = self;
             else out[wk.parent].left = self;
         }
-        // Box and centroid bounds.
-        unsigned long long kmin[3], kmax[3];
-        uint32_t cmn[3], cmx[3];
+        // Box and centroid bounds.  Each lane folds its positions (ascending,
+        // strict comparisons: the first of equal values stays); across lanes
+        // the extreme value wins, then the smallest position holding it.
+        // Position 0 is the fold's starting value (AABB::Empty).
+        uint32_t vmin[3], pmin[3], vmax[3], pmax[3], cmn[3], cmx[3];
         for (int a = 0; a < 3; a++) {
-            kmin[a] = min_key_empty(); kmax[a] = max_key_empty();
+            vmin[a] = ord(FLT_MAX); pmin[a] = 0u;
+            vmax[a] = ord(-FLT_MAX); pmax[a] = 0u;
             cmn[a] = ord(FLT_MAX); cmx[a] = ord(-FLT_MAX);
         }
         for (uint32_t p = wk.start + lane; p < wk.end; p += 32) {
             const ae_aabb b = pb[p];
             const float *f = &b.min_x;
             for (int a = 0; a < 3; a++) {
-                kmin[a] = MinOp()(kmin[a], min_key(f[a], p));
-                kmax[a] = MaxOp()(kmax[a], max_key(f[a + 3], p));
+                const uint32_t lo = ord(f[a] == 0.0f ? 0.0f : f[a]);
+                const uint32_t hi = ord(f[a + 3] == 0.0f ? 0.0f : f[a + 3]);
+                if (lo < vmin[a]) { vmin[a] = lo; pmin[a] = p + 1u; }
+                if (hi > vmax[a]) { vmax[a] = hi; pmax[a] = p + 1u; }
                 const uint32_t c = ord(centre(b, a));
                 cmn[a] = min(cmn[a], c);
                 cmx[a] = max(cmx[a], c);
@@ -501,8 +509,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_warp_build(const SmallT
         ae_aabb box;
         float *bx = &box.min_x;
         for (int a = 0; a < 3; a++) {
-            bx[a] = min_from_key(warp_all(kmin[a], MinOp()), pb, a);
-            bx[a + 3] = max_from_key(warp_all(kmax[a], MaxOp()), pb, a);
+            const uint32_t wmin = __reduce_min_sync(0xffffffffu, vmin[a]);
+            const uint32_t wmax = __reduce_max_sync(0xffffffffu, vmax[a]);
+            const uint32_t fmin = __reduce_min_sync(0xffffffffu, vmin[a] == wmin ? pmin[a] : 0xffffffffu);
+            const uint32_t fmax = __reduce_min_sync(0xffffffffu, vmax[a] == wmax ? pmax[a] : 0xffffffffu);
+            bx[a] = fmin == 0u ? FLT_MAX : (&pb[fmin - 1u].min_x)[a];
+            bx[a + 3] = fmax == 0u ? -FLT_MAX : (&pb[fmax - 1u].min_x)[a + 3];
             cmn[a] = __reduce_min_sync(0xffffffffu, cmn[a]);
             cmx[a] = __reduce_max_sync(0xffffffffu, cmx[a]);
         }
@@ -639,10 +651,16 @@ __global__ void k_place_top(const TopPlace *place, const Decision *dec_all, uint
 __device__ __forceinline__ float smin(float a, float b) { return b < a ? b : a; }
 __device__ __forceinline__ float smax(float a, float b) { return a < b ? b : a; }
 
-__global__ void k_triangle_boxes(const ae_vertex *v, const uint32_t *idx, uint32_t tris, ae_aabb *out) {
+__global__ void k_triangle_boxes(const ae_vertex *v, uint32_t nv, const uint32_t *idx, uint32_t tris, ae_aabb *out,
+                                 int *bad) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= tris) return;
-    const ae_vertex a = v[idx[3 * t]], b = v[idx[3 * t + 1]], c = v[idx[3 * t + 2]];
+    const uint32_t i0 = idx[3 * t], i1 = idx[3 * t + 1], i2 = idx[3 * t + 2];
+    if (i0 >= nv || i1 >= nv || i2 >= nv) {
+        atomicExch(bad, 1);
+        return;
+    }
+    const ae_vertex a = v[i0], b = v[i1], c = v[i2];
     ae_aabb e;
     e.min_x = smin(smin(a.px, b.px), c.px);
     e.min_y = smin(smin(a.py, b.py), c.py);
@@ -663,17 +681,75 @@ __global__ void k_reorder_indices(const uint32_t *idx, const uint32_t *order, ui
     out[3 * s + 2] = idx[3 * t + 2];
 }
 
+// RebuildAcceleration's packing after the build (renderer/renderer.cpp:
+// 1096-1121): objects in slot order, each mesh numbered by its rank among the
+// meshes in slot order (PackObjects), lights as the slots of emissive objects
+// in slot order (LightIndices).  One block walks the slots in order with
+// block-wide scans.  flags: bit 0 mesh, bit 1 light.
+__global__ void __launch_bounds__(1024) k_assemble(uint32_t n, const uint32_t *order, const uint32_t *flags,
+                                                   const ae_object *obj_t, const ae_instance *inst_t,
+                                                   ae_object *objects, ae_instance *instances, uint32_t *lights,
+                                                   uint32_t *counts) {
+    __shared__ uint32_t wm[32], wl[32];
+    __shared__ uint32_t base_m, base_l;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) { base_m = 0; base_l = 0; }
+    __syncthreads();
+    for (uint32_t b = 0; b < n; b += blockDim.x) {
+        const uint32_t slot = b + threadIdx.x;
+        const uint32_t e = slot < n ? order[slot] : 0u;
+        const uint32_t f = slot < n ? flags[e] : 0u;
+        const uint32_t mesh = f & 1u, light = (f >> 1) & 1u;
+        const uint32_t mm = __ballot_sync(0xffffffffu, mesh), ml = __ballot_sync(0xffffffffu, light);
+        const uint32_t below = (1u << lane) - 1u;
+        if (lane == 0) { wm[w] = __popc(mm); wl[w] = __popc(ml); }
+        __syncthreads();
+        uint32_t rm = base_m + __popc(mm & below), rl = base_l + __popc(ml & below);
+        for (int i = 0; i < w; i++) { rm += wm[i]; rl += wl[i]; }
+        if (slot < n) {
+            ae_object o = obj_t[e];
+            if (mesh) {
+                o.instanceIndex = rm;
+                instances[rm] = inst_t[e];
+            }
+            objects[slot] = o;
+            if (light) lights[rl] = slot;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t tm = 0, tl = 0;
+            for (int i = 0; i < int(blockDim.x >> 5); i++) { tm += wm[i]; tl += wl[i]; }
+            base_m += tm;
+            base_l += tl;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { counts[0] = base_m; counts[1] = base_l; }
+}
+
 // ---------------------------------------------------------------------------
 // Host driver.
 // ---------------------------------------------------------------------------
-template <class T> struct Buf {
+// Device scratch that only grows, kept between builds (cudaMalloc and
+// cudaFree synchronise the device and cost more than a small build).
+template <class T> struct Grow {
     T *p = nullptr;
-    ~Buf() { reset(); }
-    void reset() {
+    size_t cap = 0;
+    cudaError_t need(size_t n) {
+        if (n <= cap && p) return cudaSuccess;
         if (p) cudaFree(p);
         p = nullptr;
+        cap = 0;
+        const size_t want = n + n / 4 + 16;
+        const cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+        if (e == cudaSuccess) cap = want;
+        return e;
     }
-    cudaError_t alloc(size_t n) { return cudaMalloc(&p, (n ? n : 1) * sizeof(T)); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
 };
 
 #define AE_CK(x)                                  \
@@ -683,6 +759,40 @@ template <class T> struct Buf {
             return AE_ERR_CUDA;                   \
         }                                         \
     } while (0)
+
+struct Scratch {
+    Grow<ae_aabb> pb, stash_pb;
+    Grow<uint32_t> stash_idx, kinfo;
+    Grow<ae_bvh_node> tmp;
+    Grow<int> bad;
+    Grow<TaskAcc> acc;
+    Grow<BigTask> tasks;
+    Grow<Chunk> chunks;
+    Grow<Decision> dec, top_dec;
+    Grow<uint32_t> chunk_true, chunk_base, task_true, sub_count, sub_base;
+    Grow<SmallTask> small;
+    Grow<TopPlace> place;
+    // mesh builds
+    Grow<ae_vertex> v;
+    Grow<uint32_t> idx, order, out_idx;
+    Grow<ae_aabb> box;
+    Grow<ae_bvh_node> nodes;
+    // scene packing
+    Grow<ae_object> obj_t, objects;
+    Grow<ae_instance> inst_t, instances;
+    Grow<uint32_t> flags, lights, counts;
+    void release() {
+        obj_t.release(); objects.release(); inst_t.release(); instances.release(); flags.release();
+        lights.release(); counts.release();
+        pb.release(); stash_pb.release(); stash_idx.release(); kinfo.release(); tmp.release(); bad.release();
+        acc.release(); tasks.release(); chunks.release(); dec.release(); top_dec.release(); chunk_true.release();
+        chunk_base.release(); task_true.release(); sub_count.release(); sub_base.release(); small.release();
+        place.release(); v.release(); idx.release(); order.release(); out_idx.release(); box.release();
+        nodes.release();
+    }
+};
+Scratch g_scratch;
+std::mutex g_mutex;  // one build at a time per process: they share g_scratch
 
 struct TopNode {
     BigTask task;
@@ -699,16 +809,17 @@ int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uin
                   uint32_t *node_count, cudaStream_t st, uint32_t warp_subtree = kWarpTask) {
     *node_count = 0;
     if (n == 0) return AE_OK;
-    Buf<ae_aabb> pb, stash_pb;
-    Buf<uint32_t> stash_idx, kinfo;
-    Buf<ae_bvh_node> tmp;
-    Buf<int> bad;
-    AE_CK(pb.alloc(n));
-    AE_CK(stash_pb.alloc(n));
-    AE_CK(stash_idx.alloc(n));
-    AE_CK(kinfo.alloc(n));
-    AE_CK(tmp.alloc(2ull * n));
-    AE_CK(bad.alloc(1));
+    Scratch &S = g_scratch;
+    auto &pb = S.pb, &stash_pb = S.stash_pb;
+    auto &stash_idx = S.stash_idx, &kinfo = S.kinfo;
+    auto &tmp = S.tmp;
+    auto &bad = S.bad;
+    AE_CK(pb.need(n));
+    AE_CK(stash_pb.need(n));
+    AE_CK(stash_idx.need(n));
+    AE_CK(kinfo.need(n));
+    AE_CK(tmp.need(2ull * n));
+    AE_CK(bad.need(1));
     AE_CK(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
     uint32_t *idx = d_order;
     k_setup<<<(n + 255) / 256, 256, 0, st>>>(d_bounds, n, idx, pb.p, bad.p);
@@ -730,12 +841,11 @@ int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uin
     } else {
         small.push_back(SmallTask{0, n, 0});
     }
-    Buf<TaskAcc> acc;
-    Buf<BigTask> d_tasks;
-    Buf<Chunk> d_chunks;
-    Buf<Decision> d_dec;
-    Buf<uint32_t> d_chunk_true, d_chunk_base, d_task_true;
-    size_t cap_tasks = 0, cap_chunks = 0;
+    auto &acc = S.acc;
+    auto &d_tasks = S.tasks;
+    auto &d_chunks = S.chunks;
+    auto &d_dec = S.dec;
+    auto &d_chunk_true = S.chunk_true, &d_chunk_base = S.chunk_base, &d_task_true = S.task_true;
     std::vector<Chunk> chunks;
     std::vector<Decision> dec;
     std::vector<uint32_t> chunk_true, chunk_base, task_true;
@@ -746,26 +856,13 @@ int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uin
             for (uint32_t b = level[t].start; b < level[t].end; b += kChunk)
                 chunks.push_back(Chunk{t, b, b + kChunk < level[t].end ? b + kChunk : level[t].end});
         const uint32_t nc = uint32_t(chunks.size());
-        if (nt > cap_tasks) {
-            cap_tasks = nt * 2;
-            acc.reset();
-            d_tasks.reset();
-            d_dec.reset();
-            d_task_true.reset();
-            AE_CK(acc.alloc(cap_tasks));
-            AE_CK(d_tasks.alloc(cap_tasks));
-            AE_CK(d_dec.alloc(cap_tasks));
-            AE_CK(d_task_true.alloc(cap_tasks));
-        }
-        if (nc > cap_chunks) {
-            cap_chunks = nc * 2;
-            d_chunks.reset();
-            d_chunk_true.reset();
-            d_chunk_base.reset();
-            AE_CK(d_chunks.alloc(cap_chunks));
-            AE_CK(d_chunk_true.alloc(cap_chunks));
-            AE_CK(d_chunk_base.alloc(cap_chunks));
-        }
+        AE_CK(acc.need(nt));
+        AE_CK(d_tasks.need(nt));
+        AE_CK(d_dec.need(nt));
+        AE_CK(d_task_true.need(nt));
+        AE_CK(d_chunks.need(nc));
+        AE_CK(d_chunk_true.need(nc));
+        AE_CK(d_chunk_base.need(nc));
         AE_CK(cudaMemcpyAsync(d_tasks.p, level.data(), nt * sizeof(BigTask), cudaMemcpyHostToDevice, st));
         AE_CK(cudaMemcpyAsync(d_chunks.p, chunks.data(), nc * sizeof(Chunk), cudaMemcpyHostToDevice, st));
         k_acc_reset<<<nt, 128, 0, st>>>(acc.p, nt);
@@ -825,18 +922,17 @@ int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uin
                 else top[id].right = ref;
             }
         }
-        AE_CK(cudaStreamSynchronize(st));
         level.swap(next);
         level_top.swap(next_top);
     }
 
     // Warp-built subtrees.
     const uint32_t ns = uint32_t(small.size());
-    Buf<SmallTask> d_small;
-    Buf<uint32_t> d_sub_count, d_sub_base;
-    AE_CK(d_small.alloc(ns));
-    AE_CK(d_sub_count.alloc(ns));
-    AE_CK(d_sub_base.alloc(ns));
+    auto &d_small = S.small;
+    auto &d_sub_count = S.sub_count, &d_sub_base = S.sub_base;
+    AE_CK(d_small.need(ns));
+    AE_CK(d_sub_count.need(ns));
+    AE_CK(d_sub_base.need(ns));
     std::vector<uint32_t> sub_count(ns), sub_base(ns);
     if (ns) {
         AE_CK(cudaMemcpyAsync(d_small.p, small.data(), ns * sizeof(SmallTask), cudaMemcpyHostToDevice, st));
@@ -882,10 +978,10 @@ int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uin
         k_place_subtrees<<<ns, 256, 0, st>>>(d_small.p, d_sub_count.p, d_sub_base.p, tmp.p, d_nodes);
     }
     if (!top.empty()) {
-        Buf<TopPlace> d_place;
-        Buf<Decision> d_top_dec;
-        AE_CK(d_place.alloc(top.size()));
-        AE_CK(d_top_dec.alloc(top.size()));
+        auto &d_place = S.place;
+        auto &d_top_dec = S.top_dec;
+        AE_CK(d_place.need(top.size()));
+        AE_CK(d_top_dec.need(top.size()));
         AE_CK(cudaMemcpyAsync(d_place.p, place.data(), top.size() * sizeof(TopPlace), cudaMemcpyHostToDevice, st));
         AE_CK(cudaMemcpyAsync(d_top_dec.p, top_dec.data(), top.size() * sizeof(Decision), cudaMemcpyHostToDevice, st));
         k_place_top<<<uint32_t((top.size() + 127) / 128), 128, 0, st>>>(d_place.p, d_top_dec.p, uint32_t(top.size()),
@@ -899,41 +995,124 @@ int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uin
     return AE_OK;
 }
 
-// MeshLibrary::Add's device part: the triangle boxes, the BLAS and the
-// indices in leaf-slot order.  Host arrays in and out.
+// MeshLibrary::Add's device part on device arrays: the triangle boxes, the
+// BLAS and the indices in leaf-slot order.
+int gpu_mesh_blas_device(const ae_vertex *d_v, uint32_t nv, const uint32_t *d_idx, uint32_t ni, ae_bvh_node *d_nodes,
+                         uint32_t *out_count, uint32_t *d_out_idx, cudaStream_t st) {
+    *out_count = 0;
+    const uint32_t tris = ni / 3;
+    if (tris == 0) return AE_OK;
+    Scratch &S = g_scratch;
+    AE_CK(S.box.need(tris));
+    AE_CK(S.order.need(tris));
+    AE_CK(S.bad.need(1));
+    AE_CK(cudaMemsetAsync(S.bad.p, 0, sizeof(int), st));
+    k_triangle_boxes<<<(tris + 255) / 256, 256, 0, st>>>(d_v, nv, d_idx, tris, S.box.p, S.bad.p);
+    int h_bad = 0;
+    AE_CK(cudaMemcpyAsync(&h_bad, S.bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    AE_CK(cudaStreamSynchronize(st));
+    if (h_bad) return AE_ERR_LAYOUT;
+    const int rc = gpu_build_bvh(S.box.p, tris, d_nodes, S.order.p, out_count, st);
+    if (rc != AE_OK) return rc;
+    k_reorder_indices<<<(tris + 255) / 256, 256, 0, st>>>(d_idx, S.order.p, tris, d_out_idx);
+    AE_CK(cudaGetLastError());
+    AE_CK(cudaStreamSynchronize(st));
+    return AE_OK;
+}
+
+namespace {
+struct OwnStream {
+    cudaStream_t s = nullptr;
+    cudaError_t make() { return cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking); }
+    ~OwnStream() { if (s) cudaStreamDestroy(s); }
+};
+}  // namespace
+
+// The same with host arrays (indices already checked against nv).
 int gpu_mesh_blas(const ae_vertex *v, uint32_t nv, const uint32_t *idx, uint32_t ni, ae_bvh_node *out_nodes,
                   uint32_t *out_count, uint32_t *out_indices) {
     *out_count = 0;
     const uint32_t tris = ni / 3;
     if (tris == 0) return AE_OK;
-    cudaStream_t st;
-    AE_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamDestroy(s); } } guard{st};
-    Buf<ae_vertex> dv;
-    Buf<uint32_t> di, dorder, dout;
-    Buf<ae_aabb> dbox;
-    Buf<ae_bvh_node> dnodes;
-    AE_CK(dv.alloc(nv));
-    AE_CK(di.alloc(ni));
-    AE_CK(dorder.alloc(tris));
-    AE_CK(dout.alloc(ni));
-    AE_CK(dbox.alloc(tris));
-    AE_CK(dnodes.alloc(2ull * tris));
-    AE_CK(cudaMemcpyAsync(dv.p, v, size_t(nv) * sizeof(ae_vertex), cudaMemcpyHostToDevice, st));
-    AE_CK(cudaMemcpyAsync(di.p, idx, size_t(ni) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-    k_triangle_boxes<<<(tris + 255) / 256, 256, 0, st>>>(dv.p, di.p, tris, dbox.p);
+    std::lock_guard<std::mutex> lock(g_mutex);
+    OwnStream st;
+    AE_CK(st.make());
+    Scratch &S = g_scratch;
+    AE_CK(S.v.need(nv));
+    AE_CK(S.idx.need(ni));
+    AE_CK(S.out_idx.need(ni));
+    AE_CK(S.nodes.need(2ull * tris));
+    AE_CK(cudaMemcpyAsync(S.v.p, v, size_t(nv) * sizeof(ae_vertex), cudaMemcpyHostToDevice, st.s));
+    AE_CK(cudaMemcpyAsync(S.idx.p, idx, size_t(ni) * sizeof(uint32_t), cudaMemcpyHostToDevice, st.s));
     uint32_t count = 0;
-    const int rc = gpu_build_bvh(dbox.p, tris, dnodes.p, dorder.p, &count, st);
+    const int rc = gpu_mesh_blas_device(S.v.p, nv, S.idx.p, ni, S.nodes.p, &count, S.out_idx.p, st.s);
     if (rc != AE_OK) return rc;
-    k_reorder_indices<<<(tris + 255) / 256, 256, 0, st>>>(di.p, dorder.p, tris, dout.p);
-    AE_CK(cudaMemcpyAsync(out_nodes, dnodes.p, size_t(count) * sizeof(ae_bvh_node), cudaMemcpyDeviceToHost, st));
-    AE_CK(cudaMemcpyAsync(out_indices, dout.p, size_t(ni) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    AE_CK(cudaStreamSynchronize(st));
+    AE_CK(cudaMemcpyAsync(out_nodes, S.nodes.p, size_t(count) * sizeof(ae_bvh_node), cudaMemcpyDeviceToHost, st.s));
+    AE_CK(cudaMemcpyAsync(out_indices, S.out_idx.p, size_t(ni) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st.s));
+    AE_CK(cudaStreamSynchronize(st.s));
     *out_count = count;
     return AE_OK;
 }
 
+// ae_pack_scene's per-entity part (host_scene.cpp).
+int pack_templates(const ae_entity *ents, uint32_t n, const ae_mesh_library *lib, ae_aabb *bounds,
+                   ae_object *objects, ae_instance *instances, uint32_t *flags);
+
 }  // namespace ae
+
+extern "C" int ae_pack_scene_gpu(const ae_entity *ents, uint32_t n, const ae_mesh_library *lib,
+                                 ae_object *out_objects, ae_bvh_node *out_nodes, uint32_t *out_node_count,
+                                 uint32_t *out_lights, uint32_t *out_light_count, ae_instance *out_instances,
+                                 uint32_t *out_instance_count, uint32_t *out_order) {
+    if (!out_node_count || !out_light_count || !out_instance_count) return AE_ERR_INVALID;
+    *out_node_count = *out_light_count = *out_instance_count = 0;
+    if (n == 0) return AE_OK;
+    if (!ents || !out_objects || !out_nodes || !out_lights || !out_instances || !out_order) return AE_ERR_INVALID;
+    std::vector<ae_aabb> bounds(n);
+    std::vector<ae_object> obj_t(n);
+    std::vector<ae_instance> inst_t(n);
+    std::vector<uint32_t> flags(n);
+    int rc = ae::pack_templates(ents, n, lib, bounds.data(), obj_t.data(), inst_t.data(), flags.data());
+    if (rc != AE_OK) return rc;
+    std::lock_guard<std::mutex> lock(ae::g_mutex);
+    ae::OwnStream st;
+    AE_CK(st.make());
+    ae::Scratch &S = ae::g_scratch;
+    if (S.box.need(n) != cudaSuccess || S.order.need(n) != cudaSuccess || S.nodes.need(2ull * n) != cudaSuccess ||
+        S.obj_t.need(n) != cudaSuccess || S.objects.need(n) != cudaSuccess || S.inst_t.need(n) != cudaSuccess ||
+        S.instances.need(n) != cudaSuccess || S.flags.need(n) != cudaSuccess || S.lights.need(n) != cudaSuccess ||
+        S.counts.need(2) != cudaSuccess) {
+        cudaGetLastError();
+        return AE_ERR_OOM;
+    }
+    AE_CK(cudaMemcpyAsync(S.box.p, bounds.data(), size_t(n) * sizeof(ae_aabb), cudaMemcpyHostToDevice, st.s));
+    AE_CK(cudaMemcpyAsync(S.obj_t.p, obj_t.data(), size_t(n) * sizeof(ae_object), cudaMemcpyHostToDevice, st.s));
+    AE_CK(cudaMemcpyAsync(S.inst_t.p, inst_t.data(), size_t(n) * sizeof(ae_instance), cudaMemcpyHostToDevice, st.s));
+    AE_CK(cudaMemcpyAsync(S.flags.p, flags.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice, st.s));
+    uint32_t nodes = 0;
+    rc = ae::gpu_build_bvh(S.box.p, n, S.nodes.p, S.order.p, &nodes, st.s);
+    if (rc != AE_OK) return rc;
+    ae::k_assemble<<<1, 1024, 0, st.s>>>(n, S.order.p, S.flags.p, S.obj_t.p, S.inst_t.p, S.objects.p, S.instances.p,
+                                         S.lights.p, S.counts.p);
+    AE_CK(cudaGetLastError());
+    uint32_t counts[2] = {0, 0};
+    AE_CK(cudaMemcpyAsync(counts, S.counts.p, sizeof(counts), cudaMemcpyDeviceToHost, st.s));
+    AE_CK(cudaStreamSynchronize(st.s));
+    AE_CK(cudaMemcpyAsync(out_objects, S.objects.p, size_t(n) * sizeof(ae_object), cudaMemcpyDeviceToHost, st.s));
+    AE_CK(cudaMemcpyAsync(out_nodes, S.nodes.p, size_t(nodes) * sizeof(ae_bvh_node), cudaMemcpyDeviceToHost, st.s));
+    AE_CK(cudaMemcpyAsync(out_order, S.order.p, size_t(n) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st.s));
+    if (counts[0])
+        AE_CK(cudaMemcpyAsync(out_instances, S.instances.p, size_t(counts[0]) * sizeof(ae_instance),
+                              cudaMemcpyDeviceToHost, st.s));
+    if (counts[1])
+        AE_CK(cudaMemcpyAsync(out_lights, S.lights.p, size_t(counts[1]) * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                              st.s));
+    AE_CK(cudaStreamSynchronize(st.s));
+    *out_node_count = nodes;
+    *out_instance_count = counts[0];
+    *out_light_count = counts[1];
+    return AE_OK;
+}
 
 extern "C" int ae_build_bvh_gpu_ex(const ae_aabb *bounds, uint32_t n, uint32_t warp_subtree, ae_bvh_node *out_nodes,
                                    uint32_t *out_node_count, uint32_t *out_order) {
@@ -941,44 +1120,55 @@ extern "C" int ae_build_bvh_gpu_ex(const ae_aabb *bounds, uint32_t n, uint32_t w
     *out_node_count = 0;
     if (n == 0) return AE_OK;
     if (!bounds || !out_nodes || !out_order) return AE_ERR_INVALID;
-    cudaStream_t st;
-    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    std::lock_guard<std::mutex> lock(ae::g_mutex);
+    ae::OwnStream st;
+    AE_CK(st.make());
+    ae::Scratch &S = ae::g_scratch;
+    if (S.box.need(n) != cudaSuccess || S.order.need(n) != cudaSuccess || S.nodes.need(2ull * n) != cudaSuccess) {
         cudaGetLastError();
-        return AE_ERR_CUDA;
+        return AE_ERR_OOM;
     }
-    int rc = AE_OK;
-    {
-        ae::Buf<ae_aabb> db;
-        ae::Buf<uint32_t> dorder;
-        ae::Buf<ae_bvh_node> dnodes;
-        uint32_t count = 0;
-        if (db.alloc(n) != cudaSuccess || dorder.alloc(n) != cudaSuccess || dnodes.alloc(2ull * n) != cudaSuccess) {
-            cudaGetLastError();
-            rc = AE_ERR_OOM;
-        } else if (cudaMemcpyAsync(db.p, bounds, size_t(n) * sizeof(ae_aabb), cudaMemcpyHostToDevice, st) !=
-                   cudaSuccess) {
-            rc = AE_ERR_CUDA;
-        } else {
-            rc = ae::gpu_build_bvh(db.p, n, dnodes.p, dorder.p, &count, st, warp_subtree);
-            if (rc == AE_OK) {
-                if (cudaMemcpyAsync(out_nodes, dnodes.p, size_t(count) * sizeof(ae_bvh_node), cudaMemcpyDeviceToHost,
-                                    st) != cudaSuccess ||
-                    cudaMemcpyAsync(out_order, dorder.p, size_t(n) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st) !=
-                        cudaSuccess ||
-                    cudaStreamSynchronize(st) != cudaSuccess) {
-                    rc = AE_ERR_CUDA;
-                } else {
-                    *out_node_count = count;
-                }
-            }
-        }
-        if (rc == AE_ERR_CUDA) cudaGetLastError();
-    }
-    cudaStreamDestroy(st);
-    return rc;
+    AE_CK(cudaMemcpyAsync(S.box.p, bounds, size_t(n) * sizeof(ae_aabb), cudaMemcpyHostToDevice, st.s));
+    uint32_t count = 0;
+    const int rc = ae::gpu_build_bvh(S.box.p, n, S.nodes.p, S.order.p, &count, st.s, warp_subtree);
+    if (rc != AE_OK) return rc;
+    AE_CK(cudaMemcpyAsync(out_nodes, S.nodes.p, size_t(count) * sizeof(ae_bvh_node), cudaMemcpyDeviceToHost, st.s));
+    AE_CK(cudaMemcpyAsync(out_order, S.order.p, size_t(n) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st.s));
+    AE_CK(cudaStreamSynchronize(st.s));
+    *out_node_count = count;
+    return AE_OK;
 }
 
 extern "C" int ae_build_bvh_gpu(const ae_aabb *bounds, uint32_t n, ae_bvh_node *out_nodes, uint32_t *out_node_count,
                                 uint32_t *out_order) {
     return ae_build_bvh_gpu_ex(bounds, n, ae::kWarpTask, out_nodes, out_node_count, out_order);
+}
+
+extern "C" int ae_build_bvh_device(const ae_aabb *d_bounds, uint32_t n, uint32_t warp_subtree, ae_bvh_node *d_nodes,
+                                   uint32_t *out_node_count, uint32_t *d_order, void *stream) {
+    if (!out_node_count) return AE_ERR_INVALID;
+    *out_node_count = 0;
+    if (n == 0) return AE_OK;
+    if (!d_bounds || !d_nodes || !d_order) return AE_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(ae::g_mutex);
+    return ae::gpu_build_bvh(d_bounds, n, d_nodes, d_order, out_node_count, static_cast<cudaStream_t>(stream),
+                             warp_subtree);
+}
+
+extern "C" int ae_mesh_blas_device(const ae_vertex *d_vertices, uint32_t nv, const uint32_t *d_indices, uint32_t ni,
+                                   ae_bvh_node *d_nodes, uint32_t *out_node_count, uint32_t *d_out_indices,
+                                   void *stream) {
+    if (!out_node_count) return AE_ERR_INVALID;
+    *out_node_count = 0;
+    if (ni % 3 != 0) return AE_ERR_INVALID;
+    if (ni == 0) return AE_OK;
+    if (!d_vertices || !d_indices || !d_nodes || !d_out_indices) return AE_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(ae::g_mutex);
+    return ae::gpu_mesh_blas_device(d_vertices, nv, d_indices, ni, d_nodes, out_node_count, d_out_indices,
+                                    static_cast<cudaStream_t>(stream));
+}
+
+extern "C" void ae_bvh_builder_release(void) {
+    std::lock_guard<std::mutex> lock(ae::g_mutex);
+    ae::g_scratch.release();
 }

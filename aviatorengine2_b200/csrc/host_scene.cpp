@@ -232,6 +232,10 @@ bool HasScale(float s) { return s != 0.0f && s != 1.0f; }
 
 }  // namespace
 
+extern "C" {
+static int pack_entity(const ae_entity &e, const ae_mesh_library *lib, ae_object &o, ae_instance &inst);
+}
+
 namespace ae {
 // The device part of MeshLibrary::Add (bvh_build.cu).
 int gpu_mesh_blas(const ae_vertex *v, uint32_t nv, const uint32_t *idx, uint32_t ni, ae_bvh_node *out_nodes,
@@ -413,6 +417,54 @@ int ae_entity_bounds(const ae_entity *e, const ae_mesh_library *lib, ae_aabb *ou
 
 // RebuildAcceleration minus the upload (renderer/renderer.cpp:1087-1130):
 // bounds -> BuildBVH -> slot order -> LightIndices -> PackObjects.
+// One entity's object record (BaseGPU and the shape's fields, scene/shapes.h:
+// 182-214, 286-291) and, for a mesh, its instance record (PackObjects,
+// renderer/renderer.cpp:833-858).  instanceIndex is left 0: it is the
+// mesh's rank among meshes in slot order, known only after the build.
+static int pack_entity(const ae_entity &e, const ae_mesh_library *lib, ae_object &o, ae_instance &inst) {
+    std::memset(&o, 0, sizeof(o));
+    std::memset(&inst, 0, sizeof(inst));
+    o.x = e.position[0]; o.y = e.position[1]; o.z = e.position[2];
+    o.x2 = e.prev_position[0]; o.y2 = e.prev_position[1]; o.z2 = e.prev_position[2];
+    StorePreviousRotation(o, ShaderRotation(e.shape, ToQ(e.prev_rotation)));
+    o.r = e.albedo[0]; o.g = e.albedo[1]; o.b = e.albedo[2];
+    o.fuzz = e.fuzz; o.refraction = e.ior; o.emission = e.emission; o.density = e.density;
+    o.shapeType = e.shape; o.colorType = e.material;
+    o.textureID = e.texture_id; o.textureTint = e.texture_tint;
+    const Q q = ToQ(e.rotation);
+    switch (e.shape) {
+    case AE_SHAPE_SPHERE:
+        o.radius = e.radius;
+        o.rotation = YawOf(q);
+        break;
+    case AE_SHAPE_QUAD:
+    case AE_SHAPE_TRIANGLE: {
+        const V3 u = Rotate(q, V3{e.u[0], e.u[1], e.u[2]});
+        const V3 v = Rotate(q, V3{e.v[0], e.v[1], e.v[2]});
+        o.u_x = u.x; o.u_y = u.y; o.u_z = u.z;
+        o.v_x = v.x; o.v_y = v.y; o.v_z = v.z;
+        break;
+    }
+    case AE_SHAPE_BOX:
+        o.half_x = e.half_extent[0]; o.half_y = e.half_extent[1]; o.half_z = e.half_extent[2];
+        o.rotation = YawOf(q);
+        break;
+    case AE_SHAPE_MESH: {
+        if (!lib || e.mesh >= lib->ranges.size()) return AE_ERR_LAYOUT;
+        const ae_mesh_range &r = lib->ranges[e.mesh];
+        inst.px = e.position[0]; inst.py = e.position[1]; inst.pz = e.position[2];
+        inst.scale = HasScale(e.scale) ? e.scale : 0.0f;
+        inst.qx = q.x; inst.qy = q.y; inst.qz = q.z; inst.qw = q.w;
+        inst.vertexBase = r.vertexBase; inst.indexBase = r.indexBase;
+        inst.triangleCount = r.triangleCount; inst.blasBase = r.blasBase;
+        break;
+    }
+    default:
+        return AE_ERR_INVALID;
+    }
+    return AE_OK;
+}
+
 int ae_pack_scene(const ae_entity *ents, uint32_t n, const ae_mesh_library *lib, ae_object *out_objects,
                   ae_bvh_node *out_nodes, uint32_t *out_node_count, uint32_t *out_lights,
                   uint32_t *out_light_count, ae_instance *out_instances, uint32_t *out_instance_count,
@@ -437,49 +489,12 @@ int ae_pack_scene(const ae_entity *ents, uint32_t n, const ae_mesh_library *lib,
             out_order[slot] = order[slot];
             if (e.material == AE_MAT_DIFFUSE_LIGHT) out_lights[lights++] = slot;
             ae_object o;
-            std::memset(&o, 0, sizeof(o));
-            // BaseGPU, scene/shapes.h:185-214
-            o.x = e.position[0]; o.y = e.position[1]; o.z = e.position[2];
-            o.x2 = e.prev_position[0]; o.y2 = e.prev_position[1]; o.z2 = e.prev_position[2];
-            StorePreviousRotation(o, ShaderRotation(e.shape, ToQ(e.prev_rotation)));
-            o.r = e.albedo[0]; o.g = e.albedo[1]; o.b = e.albedo[2];
-            o.fuzz = e.fuzz; o.refraction = e.ior; o.emission = e.emission; o.density = e.density;
-            o.shapeType = e.shape; o.colorType = e.material;
-            o.textureID = e.texture_id; o.textureTint = e.texture_tint;
-            const Q q = ToQ(e.rotation);
-            switch (e.shape) {
-            case AE_SHAPE_SPHERE:
-                o.radius = e.radius;
-                o.rotation = YawOf(q);
-                break;
-            case AE_SHAPE_QUAD:
-            case AE_SHAPE_TRIANGLE: {
-                const V3 u = Rotate(q, V3{e.u[0], e.u[1], e.u[2]});
-                const V3 v = Rotate(q, V3{e.v[0], e.v[1], e.v[2]});
-                o.u_x = u.x; o.u_y = u.y; o.u_z = u.z;
-                o.v_x = v.x; o.v_y = v.y; o.v_z = v.z;
-                break;
-            }
-            case AE_SHAPE_BOX:
-                o.half_x = e.half_extent[0]; o.half_y = e.half_extent[1]; o.half_z = e.half_extent[2];
-                o.rotation = YawOf(q);
-                break;
-            case AE_SHAPE_MESH: {
-                if (!lib || e.mesh >= lib->ranges.size()) return AE_ERR_LAYOUT;
-                const ae_mesh_range &r = lib->ranges[e.mesh];
-                ae_instance inst;
-                std::memset(&inst, 0, sizeof(inst));
-                inst.px = e.position[0]; inst.py = e.position[1]; inst.pz = e.position[2];
-                inst.scale = HasScale(e.scale) ? e.scale : 0.0f;
-                inst.qx = q.x; inst.qy = q.y; inst.qz = q.z; inst.qw = q.w;
-                inst.vertexBase = r.vertexBase; inst.indexBase = r.indexBase;
-                inst.triangleCount = r.triangleCount; inst.blasBase = r.blasBase;
+            ae_instance inst;
+            const int rc = pack_entity(e, lib, o, inst);
+            if (rc != AE_OK) return rc;
+            if (e.shape == AE_SHAPE_MESH) {
                 o.instanceIndex = instances;
                 out_instances[instances++] = inst;
-                break;
-            }
-            default:
-                return AE_ERR_INVALID;
             }
             out_objects[slot] = o;
         }
@@ -492,3 +507,39 @@ int ae_pack_scene(const ae_entity *ents, uint32_t n, const ae_mesh_library *lib,
 }
 
 }  // extern "C"
+
+namespace ae {
+// Per entity, in entity order: its world box, object and instance records
+// (instanceIndex 0) and flags (bit 0 mesh, bit 1 light) - everything of
+// RebuildAcceleration that does not depend on the slot order, for the device
+// rebuild (ae_rebuild_scene).
+int pack_templates(const ae_entity *ents, uint32_t n, const ae_mesh_library *lib, ae_aabb *bounds,
+                   ae_object *objects, ae_instance *instances, uint32_t *flags) {
+    for (uint32_t i = 0; i < n; i++) {
+        int rc = ae_entity_bounds(&ents[i], lib, &bounds[i]);
+        if (rc == AE_OK) rc = pack_entity(ents[i], lib, objects[i], instances[i]);
+        if (rc != AE_OK) return rc;
+        flags[i] = (ents[i].shape == AE_SHAPE_MESH ? 1u : 0u) | (ents[i].material == AE_MAT_DIFFUSE_LIGHT ? 2u : 0u);
+    }
+    return AE_OK;
+}
+}  // namespace ae
+
+// RebuildAcceleration + UploadScene (renderer/renderer.cpp:1087-1130,
+// 931-1027) with the build and the packing on the GPU.
+extern "C" int ae_rebuild_scene(ae_ctx *ctx, const ae_entity *ents, uint32_t n, const ae_mesh_library *lib) {
+    if (!ctx || (n && !ents)) return AE_ERR_INVALID;
+    try {
+        std::vector<ae_object> objects(std::max(n, 1u));
+        std::vector<ae_bvh_node> nodes(2 * size_t(n) + 1);
+        std::vector<uint32_t> lights(std::max(n, 1u)), order(std::max(n, 1u));
+        std::vector<ae_instance> instances(std::max(n, 1u));
+        uint32_t nn = 0, nl = 0, ni = 0;
+        const int rc = ae_pack_scene_gpu(ents, n, lib, objects.data(), nodes.data(), &nn, lights.data(), &nl,
+                                         instances.data(), &ni, order.data());
+        if (rc != AE_OK) return rc;
+        return ae_upload_scene(ctx, objects.data(), n, nodes.data(), nn, lights.data(), nl, instances.data(), ni);
+    } catch (const std::bad_alloc &) {
+        return AE_ERR_OOM;
+    }
+}

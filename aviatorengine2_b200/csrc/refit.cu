@@ -274,3 +274,14 @@ extern "C" int ae_download_scene(ae_ctx *ctx, ae_object *objects, ae_bvh_node *t
     if (!rc) rc = c->cuda(cudaStreamSynchronize(c->stream), "download");
     return rc;
 }
+
+extern "C" int ae_scene_sizes(const ae_ctx *ctx, uint32_t *n_objects, uint32_t *n_nodes, uint32_t *n_lights,
+                              uint32_t *n_instances) {
+    const Ctx *c = reinterpret_cast<const Ctx *>(ctx);
+    if (!c) return AE_ERR_INVALID;
+    if (n_objects) *n_objects = c->n_objects;
+    if (n_nodes) *n_nodes = c->n_nodes;
+    if (n_lights) *n_lights = c->n_lights;
+    if (n_instances) *n_instances = c->n_instances;
+    return AE_OK;
+}

@@ -172,15 +172,27 @@ class Context:
         self._chk(lib().ae_bounce_rays(self._h, ptr(p), ptr(h), len(p), ptr(out), ptr(valid)))
         return out, valid.astype(bool)
 
+    def rebuild_scene(self, entities, meshes):
+        """RebuildAcceleration + UploadScene on the GPU (ae_rebuild_scene): the
+        scene becomes exactly what scenes.pack(entities, meshes) uploads."""
+        ents = np.ascontiguousarray(np.array(entities, dtype=_lib.ENTITY))
+        self._chk(lib().ae_rebuild_scene(self._h, ptr(ents), len(ents), meshes.handle if meshes else None))
+
     def refit_instances(self, instances):
         ins = np.ascontiguousarray(instances, dtype=_lib.INSTANCE)
         self._chk(lib().ae_refit_instances(self._h, ptr(ins), len(ins)))
 
+    def scene_sizes(self):
+        """(objects, TLAS nodes, lights, instances) of the scene on the device."""
+        v = [ctypes.c_uint32() for _ in range(4)]
+        self._chk(lib().ae_scene_sizes(self._h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
     def download_scene(self):
-        sc = self.scene
-        o = np.zeros(len(sc.objects), _lib.OBJECT)
-        t = np.zeros(len(sc.tlas), _lib.NODE)
-        i = np.zeros(len(sc.instances), _lib.INSTANCE)
+        n_obj, n_nodes, _, n_inst = self.scene_sizes()
+        o = np.zeros(n_obj, _lib.OBJECT)
+        t = np.zeros(n_nodes, _lib.NODE)
+        i = np.zeros(n_inst, _lib.INSTANCE)
         self._chk(lib().ae_download_scene(self._h, ptr(o), ptr(t), ptr(i)))
         return o, t, i
 

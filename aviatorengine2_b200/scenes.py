@@ -268,9 +268,10 @@ class PackedScene:
                                       self.instances))
 
 
-def pack(entities, meshes):
+def pack(entities, meshes, gpu=False):
     """RebuildAcceleration minus the upload: TLAS over the entities, objects in
-    slot order, light IDs, instances (renderer/renderer.cpp:1087-1130)."""
+    slot order, light IDs, instances (renderer/renderer.cpp:1087-1130).
+    gpu=True builds and packs on the GPU (ae_pack_scene_gpu, same bytes)."""
     ents = np.ascontiguousarray(np.array(entities, dtype=_lib.ENTITY))
     n = len(ents)
     objects = np.zeros(max(n, 1), _lib.OBJECT)
@@ -279,9 +280,10 @@ def pack(entities, meshes):
     insts = np.zeros(max(n, 1), _lib.INSTANCE)
     order = np.zeros(max(n, 1), np.uint32)
     nn, nl, ni = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
-    check(lib().ae_pack_scene(ptr(ents), n, meshes.handle if meshes else None, ptr(objects), ptr(nodes),
-                              ctypes.byref(nn), ptr(lights), ctypes.byref(nl), ptr(insts), ctypes.byref(ni),
-                              ptr(order)), what="ae_pack_scene")
+    fn = "ae_pack_scene_gpu" if gpu else "ae_pack_scene"
+    check(getattr(lib(), fn)(ptr(ents), n, meshes.handle if meshes else None, ptr(objects), ptr(nodes),
+                             ctypes.byref(nn), ptr(lights), ctypes.byref(nl), ptr(insts), ctypes.byref(ni),
+                             ptr(order)), what=fn)
     return objects[:n].copy(), nodes[:nn.value].copy(), lights[:nl.value].copy(), insts[:ni.value].copy(), order[:n]
 
 
@@ -491,14 +493,11 @@ def media_box(seed=7, width=128, height=96, depth=6):
     return _finish(ents, meshes, cfg, "media_box")
 
 
-def wavefront_scene(seed=4, width=1920, height=1080, depth=12, n_meshes=32, n_instances=1024, n_lights=16,
-                    target_tris=10_000_000, gpu_build=False):
-    """The wavefront workload: meshes drawn from the heightfield and icosphere
-    generators until about `target_tris` unique triangles, instanced 1024
-    times, lit by 16 emissive quads.  gpu_build: BLAS builds on the GPU."""
-    rng = np.random.default_rng(seed)
-    meshes = MeshLibrary(gpu=gpu_build)
-    handles, kinds = [], []
+def wavefront_meshes(rng, n_meshes=32, target_tris=10_000_000):
+    """wavefront_scene's unique meshes, alternating heightfields and
+    icospheres sized to share `target_tris` triangles, and a material kind
+    per mesh (60 % Lambertian, 25 % metal, 15 % dielectric)."""
+    geometry, kinds = [], []
     budget = target_tris
     for k in range(n_meshes):
         remaining = n_meshes - k
@@ -510,9 +509,21 @@ def wavefront_scene(seed=4, width=1920, height=1080, depth=12, n_meshes=32, n_in
             lv = int(max(2, min(8, round(np.log(max(want, 80) / 20) / np.log(4)))))
             v, i = icosphere(lv, 5.0)
         budget -= len(i) // 3
-        handles.append(meshes.add(v, i))
+        geometry.append((v, i))
         r = rng.random()
         kinds.append(_lib.MAT_LAMBERTIAN if r < 0.6 else (_lib.MAT_METAL if r < 0.85 else _lib.MAT_DIELECTRIC))
+    return geometry, kinds
+
+
+def wavefront_scene(seed=4, width=1920, height=1080, depth=12, n_meshes=32, n_instances=1024, n_lights=16,
+                    target_tris=10_000_000, gpu_build=False):
+    """The wavefront workload: meshes drawn from the heightfield and icosphere
+    generators until about `target_tris` unique triangles, instanced 1024
+    times, lit by 16 emissive quads.  gpu_build: BLAS builds on the GPU."""
+    rng = np.random.default_rng(seed)
+    meshes = MeshLibrary(gpu=gpu_build)
+    geometry, kinds = wavefront_meshes(rng, n_meshes, target_tris)
+    handles = [meshes.add(v, i) for v, i in geometry]
     mat = []
     for k in range(n_meshes):
         mat.append(dict(albedo=tuple(float(x) for x in rng.uniform(0.2, 0.8, 3)),

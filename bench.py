@@ -223,6 +223,64 @@ def measure_paths(local, width, height, frames=2):
     return out
 
 
+def measure_build(local, reps=3):
+    """BLAS builds of the wavefront workload's 32 meshes (10,067,490
+    triangles): MeshLibrary::Add's triangle boxes, binned-SAH build and
+    leaf-order index rewrite, on the GPU from device-resident vertex and index
+    arrays (ae_mesh_blas_device, timed with CUDA events around all 32 builds;
+    the builder synchronises the stream between tree levels, and that host
+    time is inside the events) against the host builder (ae_mesh_library_add,
+    one thread, wall clock).  The device output is compared with the host's
+    byte for byte."""
+    import ctypes
+    import torch
+    from aviatorengine2_b200 import _lib, scenes
+    from aviatorengine2_b200._lib import lib
+    geometry, _ = scenes.wavefront_meshes(np.random.default_rng(4))
+    tris = sum(len(i) // 3 for _, i in geometry)
+    dev = torch.device("cuda", local)
+    d_v = [torch.from_numpy(np.ascontiguousarray(v, _lib.VERTEX).view(np.uint8)).to(dev) for v, _ in geometry]
+    d_i = [torch.from_numpy(np.ascontiguousarray(i, np.uint32).view(np.int32)).to(dev) for _, i in geometry]
+    d_n = [torch.empty(2 * (len(i) // 3) * 48, dtype=torch.uint8, device=dev) for _, i in geometry]
+    d_o = [torch.empty(len(i), dtype=torch.int32, device=dev) for _, i in geometry]
+    counts = [ctypes.c_uint32() for _ in geometry]
+    stream = torch.cuda.current_stream(dev)
+    L = lib()
+
+    def build_all():
+        for k, (v, i) in enumerate(geometry):
+            rc = L.ae_mesh_blas_device(d_v[k].data_ptr(), len(v), d_i[k].data_ptr(), len(i), d_n[k].data_ptr(),
+                                       ctypes.byref(counts[k]), d_o[k].data_ptr(), ctypes.c_void_p(stream.cuda_stream))
+            if rc:
+                raise _lib.AeError(rc, "ae_mesh_blas_device")
+
+    ms = []
+    for r in range(reps + 1):  # the first pass grows the builder's scratch
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        build_all()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if r:
+            ms.append(e0.elapsed_time(e1))
+    host = scenes.MeshLibrary()
+    t0 = time.perf_counter()
+    for v, i in geometry:
+        host.add(v, i)
+    host_s = time.perf_counter() - t0
+    _, h_idx, h_blas = host.arrays()
+    g_blas = np.concatenate([d_n[k][: counts[k].value * 48].cpu().numpy() for k in range(len(geometry))])
+    g_idx = np.concatenate([d_o[k].cpu().numpy().view(np.uint32) for k in range(len(geometry))])
+    # The library's BLAS links are mesh-relative: the concatenation is the same bytes.
+    exact = bool(np.array_equal(g_blas, h_blas.view(np.uint8).ravel()) and np.array_equal(g_idx, h_idx))
+    gpu_ms = float(np.mean(ms))
+    return {"workload": f"BLAS of wavefront_scene's {len(geometry)} meshes, {tris} triangles",
+            "triangles": int(tris), "gpu_ms": gpu_ms, "gpu_mtris_per_s": tris / (gpu_ms / 1e3) / 1e6,
+            "host_s": host_s, "host_mtris_per_s": tris / host_s / 1e6, "host_threads": 1,
+            "speedup": host_s * 1e3 / gpu_ms, "bit_exact": exact, "reps": reps}
+
+
 def measure_serving(local, n_requests=16, rate=0.5, seed=7, claim_policy=1):
     """The serving loop under a Poisson stream of requests over the 8 resident
     serving scenes: resolution uniform over {256^2, 640x480, 960x540,
@@ -329,6 +387,7 @@ def main():
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--no-paths", action="store_true", help="skip the Mpaths/s leg (plain vs wavefront frames)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--no-build", action="store_true", help="skip the BVH build leg")
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-rate", type=float, default=0.5, help="Poisson arrivals per second")
     ap.add_argument("--serve-sweep", default="", help="comma-separated arrival rates: also run the serving "
@@ -461,6 +520,9 @@ def main():
     paths = None
     if not args.no_paths and rank == 0:
         paths = measure_paths(local, args.width, args.height)
+    build = None
+    if not args.no_build and rank == 0:
+        build = measure_build(local)
     serving = None
     if not args.no_serve and rank == 0:
         serving = measure_serving(local, args.serve_requests, args.serve_rate)
@@ -478,7 +540,7 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "per_step_ms": [round(t, 4) for t in times],
-            "paths": paths, "serving": serving}
+            "paths": paths, "serving": serving, "bvh_build": build}
     if sweep is not None:
         line["serving_sweep"] = sweep
     if rank == 0:

@@ -205,12 +205,33 @@ int ae_build_bvh_gpu(const ae_aabb *bounds, uint32_t n,
                      ae_bvh_node *out_nodes, uint32_t *out_node_count,
                      uint32_t *out_order);
 /* ae_build_bvh_gpu with the subtree size at or below which one warp builds a
- * whole subtree (ae_build_bvh_gpu uses 1024).  Nodes above it are built one
+ * whole subtree (ae_build_bvh_gpu uses 128).  Nodes above it are built one
  * tree level per round by blocks of 2048 boxes.  Every value gives the same
  * tree; it only moves work between the two phases. */
 int ae_build_bvh_gpu_ex(const ae_aabb *bounds, uint32_t n, uint32_t warp_subtree,
                         ae_bvh_node *out_nodes, uint32_t *out_node_count,
                         uint32_t *out_order);
+
+/* The device builder on device arrays (all pointers device memory except
+ * out_node_count), enqueued on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream).  d_nodes holds 2n nodes, d_order n.  Returns once the
+ * build has finished; it synchronises `stream` between tree levels. */
+int ae_build_bvh_device(const ae_aabb *d_bounds, uint32_t n, uint32_t warp_subtree,
+                        ae_bvh_node *d_nodes, uint32_t *out_node_count,
+                        uint32_t *d_order, void *stream);
+
+/* MeshLibrary::Add's device part on device arrays: triangle boxes (as
+ * Surround2Points + SurroundPoint), the BLAS over them and the indices in
+ * leaf-slot order (scene/mesh_library.h:130-153).  d_nodes holds 2*(ni/3)
+ * nodes, d_out_indices ni.  AE_ERR_LAYOUT for an index >= nv. */
+int ae_mesh_blas_device(const ae_vertex *d_vertices, uint32_t nv,
+                        const uint32_t *d_indices, uint32_t ni,
+                        ae_bvh_node *d_nodes, uint32_t *out_node_count,
+                        uint32_t *d_out_indices, void *stream);
+
+/* The device builder keeps its scratch (about 150 bytes per box of the
+ * largest build so far) between calls; this frees it. */
+void ae_bvh_builder_release(void);
 
 /* Mesh library: MeshLibrary, scene/mesh_library.h:64-159, with 32-bit input
  * indices (the reference's Mesh is uint16, scene/mesh.h:24, too small for a
@@ -272,6 +293,16 @@ int ae_pack_scene(const ae_entity *entities, uint32_t n, const ae_mesh_library *
                   uint32_t *out_lights, uint32_t *out_light_count,
                   ae_instance *out_instances, uint32_t *out_instance_count,
                   uint32_t *out_order);
+
+/* ae_pack_scene with the TLAS build and the slot-order packing (objects,
+ * instance numbering, light list) on the GPU: the same arrays, bit for bit.
+ * World boxes and per-entity records are made on the host as in
+ * ae_pack_scene. */
+int ae_pack_scene_gpu(const ae_entity *entities, uint32_t n, const ae_mesh_library *lib,
+                      ae_object *out_objects, ae_bvh_node *out_nodes, uint32_t *out_node_count,
+                      uint32_t *out_lights, uint32_t *out_light_count,
+                      ae_instance *out_instances, uint32_t *out_instance_count,
+                      uint32_t *out_order);
 
 /* World bounds of one entity (SphereBounds/QuadBounds/BoxBounds/
  * TriangleBounds/MeshBounds, scene/shapes.h:70-145). */
@@ -472,6 +503,12 @@ int ae_prepare_fast(ae_ctx *ctx);
 int ae_build_wide_bvh(const ae_bvh_node *blas, uint32_t n_nodes, uint32_t tri_count, void *out_nodes,
                       uint32_t capacity, uint32_t *out_count, uint32_t *out_root, int32_t *out_stack);
 
+/* RebuildAcceleration + UploadScene (renderer/renderer.cpp:1087-1130):
+ * ae_pack_scene_gpu of the entities, then ae_upload_scene.  The context's
+ * scene is then exactly the reference's after a rebuild (SAH TLAS, objects
+ * in slot order), unlike ae_refit_instances, which keeps the tree. */
+int ae_rebuild_scene(ae_ctx *ctx, const ae_entity *entities, uint32_t n, const ae_mesh_library *lib);
+
 /* GPU TLAS refit: new instance transforms on the device; recompute world
  * bounds of every mesh object bottom-up without rebuilding topology
  * (replaces the per-frame CPU rebuild of renderer/renderer.cpp:1087-1130
@@ -482,6 +519,9 @@ int ae_refit_instances(ae_ctx *ctx, const ae_instance *instances, uint32_t n);
  * refit): objects, TLAS nodes, instances, each sized as last uploaded.  Null
  * pointers are skipped. */
 int ae_download_scene(ae_ctx *ctx, ae_object *objects, ae_bvh_node *tlas, ae_instance *instances);
+/* Element counts of the current scene arrays (null pointers skipped). */
+int ae_scene_sizes(const ae_ctx *ctx, uint32_t *n_objects, uint32_t *n_nodes, uint32_t *n_lights,
+                   uint32_t *n_instances);
 
 /* ------------------------------------------------------------------------ */
 /* Render serving (no counterpart in the reference, which renders one scene  */

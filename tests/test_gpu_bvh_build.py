@@ -12,9 +12,9 @@ from aviatorengine2_b200 import AeError, scenes
 
 pytestmark = pytest.mark.gpu
 
-# warp_subtree: None = the default (1024); 0 = every node in the level
+# warp_subtree: None = the default (128); 0 = every node in the level
 # rounds; 1 << 30 = the whole tree in one warp.
-PHASES = [None, 0, 4, 37, 1 << 30]
+PHASES = [None, 0, 4, 37, 1024, 1 << 30]
 
 
 def boxes(n, seed, flat=0.0, dup=0.0, zeros=0.0, spread=50.0):
@@ -126,3 +126,111 @@ def test_scene_built_on_gpu_equals_host():
     b = scenes.wavefront_scene(gpu_build=False, **kw)
     for name in ("objects", "tlas", "lights", "vertices", "indices", "blas", "instances"):
         assert np.array_equal(getattr(a, name).view(np.uint8), getattr(b, name).view(np.uint8)), name
+
+
+def test_device_pointer_entry_points():
+    import ctypes
+
+    import torch
+    from aviatorengine2_b200 import _lib
+    from aviatorengine2_b200._lib import lib
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    b = boxes(20000, 16, flat=0.2, zeros=0.05)
+    d_b = torch.from_numpy(b.view(np.uint8)).to(dev)
+    d_n = torch.empty(2 * len(b) * 48, dtype=torch.uint8, device=dev)
+    d_o = torch.empty(len(b), dtype=torch.int32, device=dev)
+    cnt = ctypes.c_uint32()
+    assert lib().ae_build_bvh_device(d_b.data_ptr(), len(b), 64, d_n.data_ptr(), ctypes.byref(cnt), d_o.data_ptr(),
+                                     ctypes.c_void_p(stream.cuda_stream)) == 0
+    h_nodes, h_order = scenes.build_bvh(b)
+    assert cnt.value == len(h_nodes)
+    assert np.array_equal(d_n[: cnt.value * 48].cpu().numpy(), h_nodes.view(np.uint8).ravel())
+    assert np.array_equal(d_o.cpu().numpy().view(np.uint32), h_order)
+
+    v, i = scenes.icosphere(5, 2.0)
+    d_v = torch.from_numpy(np.ascontiguousarray(v, _lib.VERTEX).view(np.uint8)).to(dev)
+    d_i = torch.from_numpy(np.ascontiguousarray(i, np.uint32).view(np.int32)).to(dev)
+    d_n = torch.empty(2 * (len(i) // 3) * 48, dtype=torch.uint8, device=dev)
+    d_o = torch.empty(len(i), dtype=torch.int32, device=dev)
+    assert lib().ae_mesh_blas_device(d_v.data_ptr(), len(v), d_i.data_ptr(), len(i), d_n.data_ptr(),
+                                     ctypes.byref(cnt), d_o.data_ptr(), ctypes.c_void_p(stream.cuda_stream)) == 0
+    host = scenes.MeshLibrary()
+    host.add(v, i)
+    _, h_idx, h_blas = host.arrays()
+    assert np.array_equal(d_n[: cnt.value * 48].cpu().numpy(), h_blas.view(np.uint8).ravel())
+    assert np.array_equal(d_o.cpu().numpy().view(np.uint32), h_idx)
+    # An index past the vertex count is refused before any vertex is read.
+    d_i[7] = len(v)
+    assert lib().ae_mesh_blas_device(d_v.data_ptr(), len(v), d_i.data_ptr(), len(i), d_n.data_ptr(),
+                                     ctypes.byref(cnt), d_o.data_ptr(), ctypes.c_void_p(stream.cuda_stream)) == -4
+    lib().ae_bvh_builder_release()
+
+
+def _entities(n, seed, meshes, handles):
+    """n entities of every shape and material, meshes instanced from
+    `handles`, about 2 % emissive."""
+    from aviatorengine2_b200 import _lib
+    rng = np.random.default_rng(seed)
+    shapes = [_lib.SHAPE_SPHERE, _lib.SHAPE_QUAD, _lib.SHAPE_TRIANGLE, _lib.SHAPE_BOX, _lib.SHAPE_MESH]
+    mats = [_lib.MAT_LAMBERTIAN, _lib.MAT_METAL, _lib.MAT_DIELECTRIC]
+    out = []
+    for k in range(n):
+        shape = shapes[int(rng.integers(0, 5))]
+        mat = _lib.MAT_DIFFUSE_LIGHT if rng.random() < 0.02 else mats[int(rng.integers(0, 3))]
+        pos = tuple(float(x) for x in rng.uniform(-200, 200, 3))
+        kw = dict(albedo=tuple(float(x) for x in rng.uniform(0.2, 0.8, 3)), emission=4.0, fuzz=0.1)
+        if shape == _lib.SHAPE_SPHERE:
+            kw["radius"] = float(rng.uniform(0.2, 3))
+        elif shape in (_lib.SHAPE_QUAD, _lib.SHAPE_TRIANGLE):
+            kw["u"], kw["v"] = (float(rng.uniform(0.5, 4)), 0.0, 0.0), (0.0, 0.0, float(rng.uniform(0.5, 4)))
+        elif shape == _lib.SHAPE_BOX:
+            kw["half_extent"] = tuple(float(x) for x in rng.uniform(0.2, 2, 3))
+        else:
+            kw["mesh"] = handles[int(rng.integers(0, len(handles)))]
+            kw["scale"] = float(rng.uniform(0.5, 2.0))
+        rot = scenes.random_quat(rng) if shape != _lib.SHAPE_SPHERE else scenes.yaw_quat(float(rng.uniform(0, 6)))
+        out.append(scenes.entity(shape, mat, pos, rotation=rot, **kw))
+    return out
+
+
+@pytest.mark.parametrize("n", [1, 7, 900, 5000, 70000])
+def test_pack_scene_gpu_equals_host(n):
+    meshes, handles = _library(False)
+    ents = _entities(n, 17 + n, meshes, handles)
+    g = scenes.pack(ents, meshes, gpu=True)
+    h = scenes.pack(ents, meshes)
+    for a, b in zip(g, h):
+        assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+def test_rebuild_scene_equals_reference_rebuild():
+    # A moved scene rebuilt on the device renders the frames of the same scene
+    # packed on the host and uploaded: the reference's rebuild, exactly.
+    from aviatorengine2_b200 import Context, _lib
+    meshes, handles = _library(False)
+    ents = _entities(600, 18, meshes, handles)
+    cfg = scenes.make_config(64, 48, (0.0, 60.0, 420.0), (0.0, 0.0, 0.0), fov=60.0, depth=4, sky=(0.3, 0.4, 0.5))
+    first = scenes._finish(ents, meshes, cfg, "entities")
+    rng = np.random.default_rng(19)
+    moved = []
+    for e in ents:
+        m = e.copy()
+        m["prev_position"], m["prev_rotation"] = e["position"], e["rotation"]
+        m["position"] = e["position"] + rng.normal(0, 3.0, 3).astype(np.float32)
+        moved.append(m)
+    twin_scene = scenes._finish(moved, meshes, cfg, "entities moved")
+    with Context(64, 48) as ctx, Context(64, 48) as twin:
+        ctx.upload(first)
+        ctx.rebuild_scene(moved, meshes)
+        twin.upload(twin_scene)
+        for a, b in zip(ctx.download_scene(), twin.download_scene()):
+            assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+        c = twin_scene.config.copy()
+        for b in range(2):
+            c["batch"] = b
+            for x in (ctx, twin):
+                x.set_config(c)
+                x.render_frame(_lib.MODE_COMPUTE_ONLY)
+        assert np.array_equal(ctx.read_image(_lib.IMAGE_ACCUM).view(np.uint32),
+                              twin.read_image(_lib.IMAGE_ACCUM).view(np.uint32))
