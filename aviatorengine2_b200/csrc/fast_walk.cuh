@@ -56,12 +56,15 @@ struct Walker {
     uint64_t orank;
     int bsp;
 
-    AE_DEV void start(const DevScene &S, f3 o_, f3 d_, float tn_, float time_) {
+    // tmax below kFarStart starts the walk as if a hit at tmax were already
+    // found: every hit nearer than tmax is still found, with the same tie
+    // ranking, and nothing at or beyond it is reported as nearer.
+    AE_DEV void start(const DevScene &S, f3 o_, f3 d_, float tn_, float time_, float tmax = kFarStart) {
         o = o_;
         d = d_;
         tn = tn_;
         time = time_;
-        best.t = kFarStart; best.alpha = 0.0f; best.beta = 0.0f;
+        best.t = tmax; best.alpha = 0.0f; best.beta = 0.0f;
         best.object = AE_MISS; best.prim = AE_MISS; best.orank = 0; best.lrank = 0;
         tsp = 0;
         phase = kWalkDone;

@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_s
         R = W.scenes + W.s_scene[e / W.max_lights];
         const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
         so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
-        w.start(R->S, so, sd, 0.001f, d4.w);
+        w.start(R->S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
     }
     while (active) {
         if (!w.step(R->S, R->V, K, stk, threadIdx.x, THREADS)) continue;
@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_s
         if (verdict == 2) {
             so = (so + sd * b.t) + sd * 0.001f;
             if (++step < 4) {
-                w.start(R->S, so, sd, 0.001f, w.time);
+                w.start(R->S, so, sd, 0.001f, w.time, AE_SUB(distance(lp, so), 0.001f));
                 continue;
             }
             verdict = 0;
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_s
             const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
             so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
             step = 0;
-            w.start(R->S, so, sd, 0.001f, d4.w);
+            w.start(R->S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
         }
     }
 }

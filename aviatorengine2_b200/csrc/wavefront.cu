@@ -267,7 +267,10 @@ __global__ void __launch_bounds__(256) k_wf_shade(DevScene S, FastView V, WfView
 // Shadow: the reference's occlusion loop per entry (hybrid:1167-1191: up to
 // four closest hits, stepping through glass), run on a step-wise Walker so a
 // lane that finishes an entry starts its next one at once instead of waiting
-// for the warp's longest traversal.
+// for the warp's longest traversal.  The loop only asks whether the closest
+// hit lies before |lp - so| - 0.001 (a hit at or beyond it, or none, leaves
+// the sample unoccluded), so each walk starts with that distance as its
+// bound: the verdict and the glass step are those of the unbounded walk.
 template <int THREADS, bool WT>
 __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_wf_shadow(DevScene S, FastView V, WfView W) {
     extern __shared__ uint2 stk[];
@@ -284,7 +287,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_w
         e = W.sq[k];
         const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
         so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
-        w.start(S, so, sd, 0.001f, d4.w);
+        w.start(S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
     }
     while (active) {
         if (!w.step(S, V, K, stk, threadIdx.x, THREADS)) continue;
@@ -297,7 +300,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_w
         if (verdict == 2) {
             so = (so + sd * b.t) + sd * 0.001f;
             if (++step < 4) {
-                w.start(S, so, sd, 0.001f, w.time);
+                w.start(S, so, sd, 0.001f, w.time, AE_SUB(distance(lp, so), 0.001f));
                 continue;
             }
             verdict = 0;
@@ -310,7 +313,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_w
             const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
             so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
             step = 0;
-            w.start(S, so, sd, 0.001f, d4.w);
+            w.start(S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
         }
     }
 }
