@@ -429,19 +429,42 @@ int ae_closest_hit(ae_ctx *ctx, const ae_ray *rays, uint32_t n, ae_hit *hits, in
     cudaSetDevice(c->settings.device);
     int rc = prepare_variant(c, variant);
     if (rc) return rc;
-    // Host -> device -> host in chunks over two streams, so the copies of one
-    // chunk overlap the tracing of the other.
-    const uint32_t chunk = std::min<uint32_t>(n, 1u << 19);
+    // Host -> device -> host in chunks over three streams, each with its own
+    // staging slot, so the copies of one chunk overlap the tracing of the
+    // others.  Chunks ramp 64K -> 512K rays at the start and back down at the
+    // end, so the first kernel starts after a short copy and the last copy
+    // back is short.
+    constexpr uint32_t kBig = 1u << 19;
+    static const uint32_t kRamp[3] = {1u << 16, 1u << 17, 1u << 18};
+    std::vector<uint32_t> plan;
+    const uint32_t ramp_total = 2 * (kRamp[0] + kRamp[1] + kRamp[2]);
+    if (n <= ramp_total) {
+        const uint32_t parts = std::max(1u, (n + kRamp[1] - 1) / kRamp[1]);
+        for (uint32_t i = 0; i < parts; i++) plan.push_back(n / parts + (i < n % parts ? 1u : 0u));
+    } else {
+        for (uint32_t r : kRamp) plan.push_back(r);
+        for (uint32_t mid = n - ramp_total; mid > 0;) {
+            const uint32_t m = std::min(kBig, mid);
+            plan.push_back(m);
+            mid -= m;
+        }
+        for (int i = 2; i >= 0; i--) plan.push_back(kRamp[i]);
+    }
+    const uint32_t chunk = *std::max_element(plan.begin(), plan.end());
     if (!c->side_stream) {
         if ((rc = c->cuda(cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking), "stream"))) return rc;
     }
-    if (c->io_rays[0].reserve(chunk) || c->io_rays[1].reserve(chunk) || c->io_hits[0].reserve(chunk) ||
-        c->io_hits[1].reserve(chunk))
-        return c->fail(AE_ERR_OOM, "staging allocation failed");
-    cudaStream_t st[2] = {c->stream, c->side_stream};
-    uint32_t k = 0;
-    for (uint32_t off = 0; off < n; off += chunk, k ^= 1) {
-        const uint32_t m = std::min(chunk, n - off);
+    if (!c->side_stream2) {
+        if ((rc = c->cuda(cudaStreamCreateWithFlags(&c->side_stream2, cudaStreamNonBlocking), "stream"))) return rc;
+    }
+    for (int k = 0; k < Ctx::kIoSlots; k++)
+        if (c->io_rays[k].reserve(chunk) || c->io_hits[k].reserve(chunk))
+            return c->fail(AE_ERR_OOM, "staging allocation failed");
+    cudaStream_t st[Ctx::kIoSlots] = {c->stream, c->side_stream, c->side_stream2};
+    uint32_t off = 0;
+    for (size_t i = 0; i < plan.size(); i++) {
+        const int k = int(i % Ctx::kIoSlots);
+        const uint32_t m = plan[i];
         if ((rc = c->cuda(cudaMemcpyAsync(c->io_rays[k].ptr, rays + off, size_t(m) * sizeof(ae_ray),
                                           cudaMemcpyHostToDevice, st[k]), "copy rays")))
             return rc;
@@ -449,7 +472,9 @@ int ae_closest_hit(ae_ctx *ctx, const ae_ray *rays, uint32_t n, ae_hit *hits, in
         if ((rc = c->cuda(cudaMemcpyAsync(hits + off, c->io_hits[k].ptr, size_t(m) * sizeof(ae_hit),
                                           cudaMemcpyDeviceToHost, st[k]), "copy hits")))
             return rc;
+        off += m;
     }
+    if ((rc = c->cuda(cudaStreamSynchronize(c->side_stream2), "closest hit"))) return rc;
     if ((rc = c->cuda(cudaStreamSynchronize(c->side_stream), "closest hit"))) return rc;
     return c->cuda(cudaStreamSynchronize(c->stream), "closest hit");
 }

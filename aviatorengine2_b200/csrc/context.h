@@ -50,6 +50,7 @@ struct Ctx {
     ae_config config{};
     cudaStream_t stream = nullptr;
     cudaStream_t side_stream = nullptr;
+    cudaStream_t side_stream2 = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string err;
     uint64_t launches = 0;
@@ -93,8 +94,10 @@ struct Ctx {
     DevBuf<uchar4> display;
 
     // Host-buffer tracing staging.
-    DevBuf<ae_ray> io_rays[2];
-    DevBuf<ae_hit> io_hits[2];
+    // Staging slots of the host-buffer closest hit (ae_closest_hit).
+    static constexpr int kIoSlots = 3;
+    DevBuf<ae_ray> io_rays[kIoSlots];
+    DevBuf<ae_hit> io_hits[kIoSlots];
 
     // Optimised forms.
     FastScene *fast = nullptr;

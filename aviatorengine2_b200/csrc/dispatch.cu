@@ -12,6 +12,7 @@ Ctx::~Ctx() {
     destroy_deferred(this);
     destroy_refit(this);
     if (side_stream) cudaStreamDestroy(side_stream);
+    if (side_stream2) cudaStreamDestroy(side_stream2);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
