@@ -56,10 +56,11 @@ constexpr float kBoundsMinimum = 0.0001f;
 constexpr float kHalfMinimum = kBoundsMinimum * 0.5f;
 
 // Subtrees of at most this many primitives are built by one warp (the
-// default; any threshold gives the same tree).  Measured over the BLAS of a
-// 10M-triangle, 32-mesh scene: 1024 -> 65 ms, 512 -> 44 ms, 256 -> 35 ms,
-// 128 -> 31 ms, 64 -> 31 ms; smaller subtrees give more warps to run at once.
-constexpr uint32_t kWarpTask = 128;
+// default; any threshold gives the same tree).  Measured over the BLAS builds
+// of a 10M-triangle, 32-mesh scene: 32 -> 86 ms, 64 -> 71 ms, 128 -> 64 ms,
+// 256 -> 61 ms, 512 -> 65 ms, 1024 -> 87 ms.  Smaller subtrees give more
+// warps to run at once but more tree levels to run as rounds.
+constexpr uint32_t kWarpTask = 256;
 constexpr int kWarpsPerBlock = 8;
 // Positions per block in the level-by-level phase: 256 threads x 8.
 constexpr int kThreads = 256;
@@ -325,13 +326,9 @@ __global__ void __launch_bounds__(kThreads) k_big_bin(const Chunk *chunks, const
     }
 }
 
-// One thread per task: the node box, leaf or not, the SAH plane.
-__global__ void k_big_decide(const BigTask *tasks, uint32_t ntasks, const TaskAcc *acc, const ae_aabb *pb,
-                             Decision *dec) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ntasks) return;
-    const BigTask T = tasks[t];
-    const TaskAcc &A = acc[t];
+// The node box, leaf or not, the SAH plane (scene/bvh.h:148-247), from the
+// task's accumulated keys and buckets.
+__device__ Decision decide(const BigTask &T, const TaskAcc &A, const ae_aabb *pb) {
     Decision D;
     float *bx = &D.box.min_x;
     for (int a = 0; a < 3; a++) {
@@ -351,18 +348,27 @@ __global__ void k_big_decide(const BigTask *tasks, uint32_t ntasks, const TaskAc
             if (c < best) { best = c; D.axis = a; D.split = s; D.cmin = cm; D.scale = sc; }
         }
     }
-    dec[t] = D;
+    return D;
 }
 
 __device__ __forceinline__ bool goes_left(const ae_aabb &b, const Decision &D) {
     return bucket(centre(b, D.axis), D.cmin, D.scale) < D.split;
 }
 
-// Passing elements per chunk (positions [begin, end) of a splitting task).
-__global__ void __launch_bounds__(kThreads) k_big_count(const Chunk *chunks, const Decision *dec, const ae_aabb *pb,
-                                                        uint32_t *chunk_true) {
+// Each block decides its task (the task's first chunk publishes the
+// decision) and counts the chunk's elements that go left.
+__global__ void __launch_bounds__(kThreads) k_big_count(const Chunk *chunks, const BigTask *tasks, const TaskAcc *acc,
+                                                        const ae_aabb *pb, Decision *dec, uint32_t *chunk_true) {
     const Chunk C = chunks[blockIdx.x];
-    const Decision D = dec[C.task];
+    __shared__ Decision sD;
+    __shared__ uint32_t s[kThreads / 32];
+    if (threadIdx.x == 0) {
+        const BigTask T = tasks[C.task];
+        sD = decide(T, acc[C.task], pb);
+        if (C.begin == T.start) dec[C.task] = sD;
+    }
+    __syncthreads();
+    const Decision D = sD;
     if (D.leaf || D.axis < 0) {
         if (threadIdx.x == 0) chunk_true[blockIdx.x] = 0;
         return;
@@ -370,7 +376,6 @@ __global__ void __launch_bounds__(kThreads) k_big_count(const Chunk *chunks, con
     uint32_t n = 0;
     for (uint32_t p = C.begin + threadIdx.x; p < C.end; p += kThreads) n += goes_left(pb[p], D) ? 1u : 0u;
     n = __reduce_add_sync(0xffffffffu, n);
-    __shared__ uint32_t s[kThreads / 32];
     if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = n;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -868,8 +873,7 @@ int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uin
         k_acc_reset<<<nt, 128, 0, st>>>(acc.p, nt);
         k_big_reduce<<<nc, kThreads, 0, st>>>(d_chunks.p, pb.p, acc.p);
         k_big_bin<<<nc, kThreads, 0, st>>>(d_chunks.p, d_tasks.p, pb.p, acc.p);
-        k_big_decide<<<(nt + 127) / 128, 128, 0, st>>>(d_tasks.p, nt, acc.p, pb.p, d_dec.p);
-        k_big_count<<<nc, kThreads, 0, st>>>(d_chunks.p, d_dec.p, pb.p, d_chunk_true.p);
+        k_big_count<<<nc, kThreads, 0, st>>>(d_chunks.p, d_tasks.p, acc.p, pb.p, d_dec.p, d_chunk_true.p);
         dec.resize(nt);
         chunk_true.resize(nc);
         AE_CK(cudaMemcpyAsync(dec.data(), d_dec.p, nt * sizeof(Decision), cudaMemcpyDeviceToHost, st));

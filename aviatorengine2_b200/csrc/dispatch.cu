@@ -22,7 +22,8 @@ int prepare_variant(Ctx *c, int variant) {
     switch (variant) {
     case AE_VARIANT_PLAIN: return AE_OK;
     case AE_VARIANT_FAST:
-    case AE_VARIANT_QUANT: return prepare_fast(c);
+    case AE_VARIANT_QUANT:
+    case AE_VARIANT_FAST_WALK: return prepare_fast(c);
     default: return c->fail(AE_ERR_INVALID, "unknown kernel variant %d", variant);
     }
 }
@@ -35,6 +36,7 @@ int closest_hit_dispatch(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, i
     if (timed && (rc = c->cuda(cudaEventRecord(c->ev0, st), "event"))) return rc;
     cudaError_t e;
     if (variant == AE_VARIANT_PLAIN) e = launch_closest_plain(c->scene(), rays, n, hits, st);
+    else if (variant == AE_VARIANT_FAST_WALK) e = launch_closest_walk(c, rays, n, hits, st);
     else e = launch_closest_fast(c, rays, n, hits, variant == AE_VARIANT_QUANT, st);
     if ((rc = c->cuda(e, "closest hit launch"))) return rc;
     c->launches++;

@@ -45,6 +45,7 @@
 #include "context.h"
 #include "fast.h"
 #include "fast_trace.cuh"
+#include "fast_walk.cuh"
 #include "kernels.h"
 #include "trace_common.cuh"
 
@@ -395,6 +396,62 @@ __global__ void __launch_bounds__(128, 8) k_closest_fast(DevScene S, FastView V,
     out.object = best.object;
     out.prim = best.prim;
     hits[i] = out;
+}
+
+// The same closest hit on the step-wise Walker, for incoherent ray sets
+// (bounce rays): a persistent grid where each thread takes its next ray as
+// soon as one finishes.  Bit-identical hits.
+__global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_closest_walk(DevScene S, FastView V,
+                                                                     const ae_ray *__restrict__ rays, uint32_t n,
+                                                                     ae_hit *__restrict__ hits) {
+    extern __shared__ uint2 stk[];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    Walker<false> w;
+    WalkStacks<> K;
+    bool active = k < n;
+    if (active) {
+        const ae_ray r = rays[k];
+        w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+    }
+    while (active) {
+        if (!w.step(S, V, K, stk, threadIdx.x, blockDim.x)) continue;
+        const Best &b = w.best;
+        const bool any = b.object != AE_MISS;
+        ae_hit h;
+        h.t = any ? b.t : 0.0f;
+        h.alpha = any ? b.alpha : 0.0f;
+        h.beta = any ? b.beta : 0.0f;
+        h.object = b.object;
+        h.prim = b.prim;
+        hits[k] = h;
+        k += stride;
+        active = k < n;
+        if (active) {
+            const ae_ray r = rays[k];
+            w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+        }
+    }
+}
+
+cudaError_t launch_closest_walk(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    FastScene &F = *c->fast;
+    FastView V{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr};
+    const int threads = 128;
+    const size_t smem = size_t(kSharedStack) * threads * sizeof(uint2);
+    static int per_sm = 0, sms = 0;
+    if (!per_sm) {
+        cudaFuncSetAttribute(k_closest_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_closest_walk, threads, smem);
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        per_sm = std::max(per_sm, 1);
+    }
+    const uint32_t grid = std::min<uint32_t>(uint32_t(per_sm) * uint32_t(sms), (n + threads - 1) / threads);
+    k_closest_walk<<<grid, threads, smem, st>>>(c->scene(), V, rays, n, hits);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_closest_fast(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, bool quant, cudaStream_t st) {

@@ -32,7 +32,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "closest-hit Mrays/s (1080p primary + diffuse bounce rays, 2.1M-triangle instanced scene)"
 UNIT = "Mrays/s"
-VARIANTS = {"plain": 0, "fast": 1, "quant": 2}
+VARIANTS = {"plain": 0, "fast": 1, "quant": 2, "walk": 3}
 
 
 def dist_env():
@@ -381,6 +381,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--variant", default=os.environ.get("AE_BENCH_VARIANT", "best"))
+    ap.add_argument("--bounce-variant", default="same",
+                    help="kernel family for the bounce rays ('same' = --variant's, or plain/fast/quant/walk)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--width", type=int, default=1920)
@@ -422,6 +424,8 @@ def main():
         except Exception:
             variant = "plain"
     vid = VARIANTS[variant]
+    bounce_variant = variant if args.bounce_variant == "same" else args.bounce_variant
+    vid2 = VARIANTS[bounce_variant]
 
     dev = torch.device("cuda", local)
     d_prim = torch.from_numpy(prim.view(np.uint8)).to(dev)
@@ -434,7 +438,7 @@ def main():
 
     def step():
         ctx.closest_hit_device(d_prim.data_ptr(), n1, d_hits1.data_ptr(), vid)
-        ctx.closest_hit_device(d_bounce.data_ptr(), n2, d_hits2.data_ptr(), vid)
+        ctx.closest_hit_device(d_bounce.data_ptr(), n2, d_hits2.data_ptr(), vid2)
 
     for _ in range(args.warmup):
         step()
@@ -484,7 +488,7 @@ def main():
 
         def e2e_step():
             _lib.check(L.ae_closest_hit(ctx.handle, h_prim.data_ptr(), n1, h_h1.data_ptr(), vid), ctx.handle)
-            _lib.check(L.ae_closest_hit(ctx.handle, h_bounce.data_ptr(), n2, h_h2.data_ptr(), vid), ctx.handle)
+            _lib.check(L.ae_closest_hit(ctx.handle, h_bounce.data_ptr(), n2, h_h2.data_ptr(), vid2), ctx.handle)
 
         for _ in range(2):
             e2e_step()
@@ -534,6 +538,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene and camera)",
             "config": {"workload": f"instanced_meshes {W}x{H} primary+bounce closest hit", "variant": variant,
+                       "bounce_variant": bounce_variant,
                        "rays_per_step": rays_step, "primary_rays": n1, "bounce_rays": n2,
                        "triangles": int(scene.triangles), "instances": int(len(scene.instances)),
                        "l2": "flushed before every step (512 MB write)", "parallelism": f"replicas x{world}"},

@@ -205,7 +205,7 @@ int ae_build_bvh_gpu(const ae_aabb *bounds, uint32_t n,
                      ae_bvh_node *out_nodes, uint32_t *out_node_count,
                      uint32_t *out_order);
 /* ae_build_bvh_gpu with the subtree size at or below which one warp builds a
- * whole subtree (ae_build_bvh_gpu uses 128).  Nodes above it are built one
+ * whole subtree (ae_build_bvh_gpu uses 256).  Nodes above it are built one
  * tree level per round by blocks of 2048 boxes.  Every value gives the same
  * tree; it only moves work between the two phases. */
 int ae_build_bvh_gpu_ex(const ae_aabb *bounds, uint32_t n, uint32_t warp_subtree,
@@ -330,8 +330,10 @@ typedef struct ae_settings {
 
 /* Kernel families.  PLAIN reproduces the reference order of operations;
  * FAST is the optimised closest-hit (ordered traversal, packed triangles);
- * QUANT adds 8-bit child bounds and the watertight triangle test. */
-enum { AE_VARIANT_PLAIN = 0, AE_VARIANT_FAST = 1, AE_VARIANT_QUANT = 2 };
+ * QUANT adds 8-bit child bounds and the watertight triangle test; FAST_WALK
+ * is FAST's walk run one step at a time per thread on a persistent grid (the
+ * same hits; faster on incoherent sets such as bounce rays). */
+enum { AE_VARIANT_PLAIN = 0, AE_VARIANT_FAST = 1, AE_VARIANT_QUANT = 2, AE_VARIANT_FAST_WALK = 3 };
 
 /* Render modes for ae_render_frame.  AE_MODE_WAVEFRONT_PRECISION is the
  * wavefront tracer in the precision form: watertight triangle test, FP16

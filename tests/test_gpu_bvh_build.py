@@ -12,7 +12,7 @@ from aviatorengine2_b200 import AeError, scenes
 
 pytestmark = pytest.mark.gpu
 
-# warp_subtree: None = the default (128); 0 = every node in the level
+# warp_subtree: None = the default (256); 0 = every node in the level
 # rounds; 1 << 30 = the whole tree in one warp.
 PHASES = [None, 0, 4, 37, 1024, 1 << 30]
 

@@ -83,6 +83,24 @@ def test_fast_instanced_primary_and_bounce_bit_exact(instanced):
         assert same(c.closest_hit(b, _lib.VARIANT_FAST), O.closest_hit(s, b))
 
 
+def test_walk_variant_equals_fast(instanced):
+    """FAST_WALK (the same walk one step at a time per thread, persistent
+    grid) returns FAST's hits byte for byte, through the device and the
+    host-buffer entry points."""
+    s = instanced
+    with ctx_for(s) as c:
+        prim = c.camera_rays()
+        fast = c.closest_hit(prim, _lib.VARIANT_FAST)
+        assert same(c.closest_hit(prim, _lib.VARIANT_FAST_WALK), fast)
+        bounce, valid = c.bounce_rays(prim, fast)
+        b = bounce[valid]
+        assert same(c.closest_hit(b, _lib.VARIANT_FAST_WALK), O.closest_hit(s, b))
+        r = random_rays(300000, 0, 100, 6)
+        assert same(c.closest_hit(r, _lib.VARIANT_FAST_WALK), c.closest_hit(r, _lib.VARIANT_FAST))
+        for n in (1, 31, 1000):
+            assert same(c.closest_hit(r[:n], _lib.VARIANT_FAST_WALK), c.closest_hit(r[:n], _lib.VARIANT_FAST))
+
+
 def test_fast_random_rays_inside_scene(instanced):
     s = instanced
     with ctx_for(s) as c:
