@@ -381,8 +381,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--variant", default=os.environ.get("AE_BENCH_VARIANT", "best"))
-    ap.add_argument("--bounce-variant", default="same",
-                    help="kernel family for the bounce rays ('same' = --variant's, or plain/fast/quant/walk)")
+    ap.add_argument("--bounce-variant", default="walk",
+                    help="kernel family for the bounce rays ('same' = --variant's, or plain/fast/quant/walk); "
+                         "walk: FAST's walk one step at a time per thread, the same hits, for incoherent rays")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--width", type=int, default=1920)
@@ -424,7 +425,7 @@ def main():
         except Exception:
             variant = "plain"
     vid = VARIANTS[variant]
-    bounce_variant = variant if args.bounce_variant == "same" else args.bounce_variant
+    bounce_variant = variant if args.bounce_variant == "same" or variant != "fast" else args.bounce_variant
     vid2 = VARIANTS[bounce_variant]
 
     dev = torch.device("cuda", local)

@@ -332,7 +332,7 @@ typedef struct ae_settings {
  * FAST is the optimised closest-hit (ordered traversal, packed triangles);
  * QUANT adds 8-bit child bounds and the watertight triangle test; FAST_WALK
  * is FAST's walk run one step at a time per thread on a persistent grid (the
- * same hits; faster on incoherent sets such as bounce rays). */
+ * same hits; for incoherent sets such as bounce rays). */
 enum { AE_VARIANT_PLAIN = 0, AE_VARIANT_FAST = 1, AE_VARIANT_QUANT = 2, AE_VARIANT_FAST_WALK = 3 };
 
 /* Render modes for ae_render_frame.  AE_MODE_WAVEFRONT_PRECISION is the

@@ -83,22 +83,33 @@ def test_fast_instanced_primary_and_bounce_bit_exact(instanced):
         assert same(c.closest_hit(b, _lib.VARIANT_FAST), O.closest_hit(s, b))
 
 
-def test_walk_variant_equals_fast(instanced):
+@pytest.mark.parametrize("variant", [_lib.VARIANT_FAST_WALK])
+def test_walk_variant_equals_fast(instanced, variant):
     """FAST_WALK (the same walk one step at a time per thread, persistent
-    grid) returns FAST's hits byte for byte, through the device and the
-    host-buffer entry points."""
+    grid) returns FAST's hits byte for byte - coherent camera rays, bounce
+    rays, random rays, ragged sizes."""
     s = instanced
     with ctx_for(s) as c:
         prim = c.camera_rays()
         fast = c.closest_hit(prim, _lib.VARIANT_FAST)
-        assert same(c.closest_hit(prim, _lib.VARIANT_FAST_WALK), fast)
+        assert same(c.closest_hit(prim, variant), fast)
         bounce, valid = c.bounce_rays(prim, fast)
         b = bounce[valid]
-        assert same(c.closest_hit(b, _lib.VARIANT_FAST_WALK), O.closest_hit(s, b))
+        assert same(c.closest_hit(b, variant), O.closest_hit(s, b))
         r = random_rays(300000, 0, 100, 6)
-        assert same(c.closest_hit(r, _lib.VARIANT_FAST_WALK), c.closest_hit(r, _lib.VARIANT_FAST))
-        for n in (1, 31, 1000):
-            assert same(c.closest_hit(r[:n], _lib.VARIANT_FAST_WALK), c.closest_hit(r[:n], _lib.VARIANT_FAST))
+        assert same(c.closest_hit(r, variant), c.closest_hit(r, _lib.VARIANT_FAST))
+        for n in (1, 31, 33, 1000):
+            assert same(c.closest_hit(r[:n], variant), c.closest_hit(r[:n], _lib.VARIANT_FAST))
+
+
+@pytest.mark.parametrize("variant", [_lib.VARIANT_FAST_WALK])
+def test_walk_variant_cornell(variant):
+    s = scenes.cornell_box()
+    with ctx_for(s) as c:
+        rays = c.camera_rays()
+        assert same(c.closest_hit(rays, variant), O.closest_hit(s, rays))
+        r = random_rays(100000, -2, 12, 7)
+        assert same(c.closest_hit(r, variant), c.closest_hit(r, _lib.VARIANT_FAST))
 
 
 def test_fast_random_rays_inside_scene(instanced):
@@ -136,9 +147,12 @@ def test_fast_ties_between_coincident_objects():
         c.upload(s)
         c.prepare_fast()
         got = c.closest_hit(r, _lib.VARIANT_FAST)
+        others = [c.closest_hit(r, _lib.VARIANT_FAST_WALK)]
     want = O.closest_hit(s, r)
     assert (want["object"] != _lib.MISS).mean() > 0.5
     assert same(got, want)
+    for o in others:
+        assert same(o, want)
 
 
 def test_quant_primary_ids_and_values(instanced):
