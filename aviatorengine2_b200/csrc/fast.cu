@@ -399,37 +399,101 @@ __global__ void __launch_bounds__(128, 8) k_closest_fast(DevScene S, FastView V,
 }
 
 // The same closest hit on the step-wise Walker, for incoherent ray sets
-// (bounce rays): a persistent grid where each thread takes its next ray as
-// soon as one finishes.  Bit-identical hits.
+// (bounce rays): a persistent grid where each lane starts its next ray as soon
+// as one finishes.  Bit-identical hits.
+//
+// DYN: rays are handed out in chunks of kWalkChunk consecutive rays per warp
+// from a global counter, and the lanes of a warp take theirs from the warp's
+// current chunk, so the rays a warp has in flight stay close in the input
+// order (neighbouring pixels: neighbouring origins and nodes).  On a
+// 1.3M-ray bounce set this took 3.70 -> 3.31 ms.  It keeps every block busy
+// to the end of the launch, which suits a launch that has the GPU to itself;
+// the smaller launches of the pipelined host-buffer call, which overlap on
+// three streams, use the static assignment (lane i: rays i, i + grid size,
+// ...), whose blocks retire early and make room for the next launch.
+constexpr uint32_t kWalkChunk = 64;
+constexpr uint32_t kWalkDynamicMin = (1u << 19) + 1;  // above the host pipeline's largest chunk
+
+template <bool DYN>
 __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_closest_walk(DevScene S, FastView V,
                                                                      const ae_ray *__restrict__ rays, uint32_t n,
-                                                                     ae_hit *__restrict__ hits) {
+                                                                     ae_hit *__restrict__ hits, uint32_t *next) {
     extern __shared__ uint2 stk[];
-    const uint32_t stride = gridDim.x * blockDim.x;
-    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    Walker<false> w;
-    WalkStacks<> K;
-    bool active = k < n;
-    if (active) {
-        const ae_ray r = rays[k];
-        w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
-    }
-    while (active) {
-        if (!w.step(S, V, K, stk, threadIdx.x, blockDim.x)) continue;
-        const Best &b = w.best;
-        const bool any = b.object != AE_MISS;
-        ae_hit h;
-        h.t = any ? b.t : 0.0f;
-        h.alpha = any ? b.alpha : 0.0f;
-        h.beta = any ? b.beta : 0.0f;
-        h.object = b.object;
-        h.prim = b.prim;
-        hits[k] = h;
-        k += stride;
-        active = k < n;
+    if (!DYN) {
+        const uint32_t stride = gridDim.x * blockDim.x;
+        uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+        Walker<false> w;
+        WalkStacks<> K;
+        bool active = k < n;
         if (active) {
             const ae_ray r = rays[k];
             w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+        }
+        while (active) {
+            if (!w.step(S, V, K, stk, threadIdx.x, blockDim.x)) continue;
+            const Best &b = w.best;
+            const bool any = b.object != AE_MISS;
+            ae_hit h;
+            h.t = any ? b.t : 0.0f;
+            h.alpha = any ? b.alpha : 0.0f;
+            h.beta = any ? b.beta : 0.0f;
+            h.object = b.object;
+            h.prim = b.prim;
+            hits[k] = h;
+            k += stride;
+            active = k < n;
+            if (active) {
+                const ae_ray r = rays[k];
+                w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+            }
+        }
+        return;
+    }
+    const uint32_t lane = threadIdx.x & 31, below = (1u << lane) - 1u;
+    Walker<false> w;
+    WalkStacks<> K;
+    uint32_t k = 0, cbase = 0, cend = 0;  // cbase/cend: the warp's chunk, the same in every lane
+    bool active = false, need = true, exhausted = false;
+    for (;;) {
+        // Lanes without a ray take the next ones of the warp's chunk, in lane
+        // order; a new chunk is fetched when it runs out.
+        uint32_t m = __ballot_sync(0xffffffffu, need);
+        while (m && !exhausted) {
+            if (cbase >= cend) {
+                uint32_t b = 0;
+                if (lane == 0) b = atomicAdd(next, kWalkChunk);
+                b = __shfl_sync(0xffffffffu, b, 0);
+                if (b >= n) {
+                    exhausted = true;
+                    break;
+                }
+                cbase = b;
+                cend = min(b + kWalkChunk, n);
+            }
+            const uint32_t take = min(cend - cbase, uint32_t(__popc(m)));
+            if (need && uint32_t(__popc(m & below)) < take) {
+                k = cbase + __popc(m & below);
+                need = false;
+                active = true;
+                const ae_ray r = rays[k];
+                w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+            }
+            cbase += take;
+            m = __ballot_sync(0xffffffffu, need);
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (active && w.step(S, V, K, stk, threadIdx.x, blockDim.x)) {
+            const Best &b = w.best;
+            const bool any = b.object != AE_MISS;
+            ae_hit h;
+            h.t = any ? b.t : 0.0f;
+            h.alpha = any ? b.alpha : 0.0f;
+            h.beta = any ? b.beta : 0.0f;
+            h.object = b.object;
+            h.prim = b.prim;
+            hits[k] = h;
+            active = false;
+            need = true;
         }
     }
 }
@@ -442,15 +506,24 @@ cudaError_t launch_closest_walk(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *
     const size_t smem = size_t(kSharedStack) * threads * sizeof(uint2);
     static int per_sm = 0, sms = 0;
     if (!per_sm) {
-        cudaFuncSetAttribute(k_closest_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_closest_walk, threads, smem);
+        cudaFuncSetAttribute(k_closest_walk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaFuncSetAttribute(k_closest_walk<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_closest_walk<true>, threads, smem);
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         per_sm = std::max(per_sm, 1);
     }
     const uint32_t grid = std::min<uint32_t>(uint32_t(per_sm) * uint32_t(sms), (n + threads - 1) / threads);
-    k_closest_walk<<<grid, threads, smem, st>>>(c->scene(), V, rays, n, hits);
+    if (n < kWalkDynamicMin) {
+        k_closest_walk<false><<<grid, threads, smem, st>>>(c->scene(), V, rays, n, hits, nullptr);
+        return cudaGetLastError();
+    }
+    if (F.walk_next.reserve(FastScene::kWalkCounters)) return cudaErrorMemoryAllocation;
+    uint32_t *next = F.walk_next.ptr + (F.walk_pos++ % FastScene::kWalkCounters);
+    cudaError_t e = cudaMemsetAsync(next, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    k_closest_walk<true><<<grid, threads, smem, st>>>(c->scene(), V, rays, n, hits, next);
     return cudaGetLastError();
 }
 

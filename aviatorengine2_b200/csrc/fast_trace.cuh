@@ -51,6 +51,11 @@ struct FastScene {
     DevBuf<uint4> obj_meta;  // per object slot: shape | material << 8, instance
     DevBuf<uint4> shade16;   // precision form: FP16 normals and UVs, 2 per triangle
     uint32_t shade16_tris = 0;
+    // Ray counters of the batch walker (k_closest_walk), one per launch in
+    // flight: a ring, so launches on different streams never share one.
+    static constexpr uint32_t kWalkCounters = 64;
+    DevBuf<uint32_t> walk_next;
+    uint32_t walk_pos = 0;
     uint32_t n_nodes = 0, n_tris = 0;
     int max_stack = 0;
     uint64_t geometry_key = 0, scene_key = ~0ull;

@@ -102,6 +102,30 @@ def test_walk_variant_equals_fast(instanced, variant):
             assert same(c.closest_hit(r[:n], variant), c.closest_hit(r[:n], _lib.VARIANT_FAST))
 
 
+def test_walk_variant_large_device_batch(instanced):
+    """A device-resident batch above 512K rays takes the walker's chunked
+    assignment (warps claim runs of consecutive rays); its hits equal FAST's
+    byte for byte, twice in a row (fresh and reused counters)."""
+    import torch
+    s = instanced
+    with ctx_for(s) as c:
+        prim = c.camera_rays()
+        fast = c.closest_hit(prim, _lib.VARIANT_FAST)
+        bounce, valid = c.bounce_rays(prim, fast)
+        r = np.concatenate([bounce[valid], random_rays(600000, 0, 100, 9)])
+        assert len(r) > (1 << 19)
+        want = c.closest_hit(r, _lib.VARIANT_FAST)
+        dev = torch.device("cuda", 0)
+        d_r = torch.from_numpy(r.view(np.uint8)).to(dev)
+        for _ in range(2):
+            d_h = torch.zeros(len(r) * 20, dtype=torch.uint8, device=dev)
+            torch.cuda.synchronize(dev)  # the library works on its own stream
+            c.closest_hit_device(d_r.data_ptr(), len(r), d_h.data_ptr(), _lib.VARIANT_FAST_WALK)
+            c.synchronize()
+            got = d_h.cpu().numpy().view(_lib.HIT)
+            assert same(got, want)
+
+
 @pytest.mark.parametrize("variant", [_lib.VARIANT_FAST_WALK])
 def test_walk_variant_cornell(variant):
     s = scenes.cornell_box()
