@@ -101,11 +101,13 @@ SIGNATURES = {
     "ae_build_bvh_gpu_ex": (_I, [_P, _U32, _U32, _P, _P, _P]),
     "ae_build_bvh_device": (_I, [_P, _U32, _U32, _P, _P, _P, _P]),
     "ae_mesh_blas_device": (_I, [_P, _U32, _P, _U32, _P, _P, _P, _P]),
+    "ae_mesh_blas_device_many": (_I, [_U32, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ae_bvh_builder_release": (None, []),
     "ae_mesh_library_create": (_P, []),
     "ae_mesh_library_destroy": (None, [_P]),
     "ae_mesh_library_add": (_I, [_P, _P, _U32, _P, _U32, _I]),
     "ae_mesh_library_add_gpu": (_I, [_P, _P, _U32, _P, _U32, _I]),
+    "ae_mesh_library_add_many_gpu": (_I, [_P, _U32, _P, _P, _P, _P, _P, _P]),
     "ae_mesh_library_range": (_I, [_P, _U32, _P]),
     "ae_mesh_library_sizes": (None, [_P, _P, _P, _P]),
     "ae_mesh_library_vertices": (_P, [_P]),

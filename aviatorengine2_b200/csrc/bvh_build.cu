@@ -75,7 +75,10 @@ constexpr int kWarpStack = kMaxDepth + 4;
 
 struct Chunk { uint32_t task, begin, end; };
 struct BigTask { uint32_t start, end, depth; };
-struct SmallTask { uint32_t start, end, depth; };
+// A subtree for one warp.  root: the first position of its tree's range
+// (leaf slots are relative to it); out: where its tree's nodes start in the
+// output array.
+struct SmallTask { uint32_t start, end, depth, root, out; };
 
 // Per large task, reset every round.
 struct TaskAcc {
@@ -525,7 +528,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_warp_build(const SmallT
         }
         const uint32_t count = wk.end - wk.start;
         if (count <= uint32_t(kLeafSize) || wk.depth >= uint32_t(kMaxDepth)) {
-            if (lane == 0) out[self] = make_node(box, int(wk.start), -1, int(count));
+            if (lane == 0) out[self] = make_node(box, int(wk.start - task.root), -1, int(count));
             __syncwarp();
             continue;
         }
@@ -626,18 +629,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_warp_build(const SmallT
 // Final numbering.
 // ---------------------------------------------------------------------------
 // One block per warp-built subtree: local node indices -> global.
+// sub_base: the subtree's first node index within its tree (links are
+// relative to the tree); the nodes land at the tree's offset in `out`.
 __global__ void k_place_subtrees(const SmallTask *tasks, const uint32_t *sub_count, const uint32_t *sub_base,
                                  const ae_bvh_node *tmp, ae_bvh_node *out) {
     const uint32_t t = blockIdx.x;
     const ae_bvh_node *src = tmp + 2ull * tasks[t].start;
     const uint32_t base = sub_base[t], n = sub_count[t];
+    ae_bvh_node *dst = out + tasks[t].out;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         ae_bvh_node nd = src[i];
         if (nd.count == 0) {
             nd.left += int(base);
             nd.right += int(base);
         }
-        out[base + i] = nd;
+        dst[base + i] = nd;
     }
 }
 
@@ -676,11 +682,13 @@ __global__ void k_triangle_boxes(const ae_vertex *v, uint32_t nv, const uint32_t
     out[t] = e;
 }
 
-// Indices in leaf-slot order (scene/mesh_library.h:147-153).
-__global__ void k_reorder_indices(const uint32_t *idx, const uint32_t *order, uint32_t tris, uint32_t *out) {
+// Indices in leaf-slot order (scene/mesh_library.h:147-153); `order` holds
+// triangle numbers offset by `first` (a mesh's range in a forest build).
+__global__ void k_reorder_indices(const uint32_t *idx, const uint32_t *order, uint32_t first, uint32_t tris,
+                                  uint32_t *out) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= tris) return;
-    const uint32_t t = order[s];
+    const uint32_t t = order[s] - first;
     out[3 * s] = idx[3 * t];
     out[3 * s + 1] = idx[3 * t + 1];
     out[3 * s + 2] = idx[3 * t + 2];
@@ -781,7 +789,7 @@ struct Scratch {
     Grow<ae_vertex> v;
     Grow<uint32_t> idx, order, out_idx;
     Grow<ae_aabb> box;
-    Grow<ae_bvh_node> nodes;
+    Grow<ae_bvh_node> nodes, mesh_nodes;
     // scene packing
     Grow<ae_object> obj_t, objects;
     Grow<ae_instance> inst_t, instances;
@@ -793,7 +801,7 @@ struct Scratch {
         acc.release(); tasks.release(); chunks.release(); dec.release(); top_dec.release(); chunk_true.release();
         chunk_base.release(); task_true.release(); sub_count.release(); sub_base.release(); small.release();
         place.release(); v.release(); idx.release(); order.release(); out_idx.release(); box.release();
-        nodes.release();
+        nodes.release(); mesh_nodes.release();
     }
 };
 Scratch g_scratch;
@@ -801,6 +809,7 @@ std::mutex g_mutex;  // one build at a time per process: they share g_scratch
 
 struct TopNode {
     BigTask task;
+    uint32_t tree = 0;            // index of the tree (root range) it belongs to
     int32_t left = 0, right = 0;  // >= 0: top node; < 0: warp subtree -1 - id
     bool leaf = false;
 };
@@ -810,9 +819,17 @@ struct TopNode {
 // Builds the tree over `d_bounds` (device, n boxes) on `st`.  On success
 // d_nodes (2n capacity) holds the nodes, d_order the leaf-slot permutation,
 // *node_count their number.
-int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uint32_t *d_order,
-                  uint32_t *node_count, cudaStream_t st, uint32_t warp_subtree = kWarpTask) {
-    *node_count = 0;
+// A forest: one tree per range [first[r], first[r + 1]) of the n boxes
+// (first[0] = 0, first[n_trees] = n), all built in the same level rounds and
+// warp launch.  Tree r's nodes go to d_nodes + 2 * first[r] (room for its
+// 2 * count - 1), with links and leaf slots relative to its own range, so
+// each tree is exactly the one built over its range alone;
+// node_counts[r] = its node count.  d_order: per position, the index of the
+// box there (positions of a range hold that range's boxes).
+int gpu_build_forest(const ae_aabb *d_bounds, const uint32_t *first, uint32_t n_trees, ae_bvh_node *d_nodes,
+                     uint32_t *d_order, uint32_t *node_counts, cudaStream_t st, uint32_t warp_subtree) {
+    for (uint32_t r = 0; r < n_trees; r++) node_counts[r] = 0;
+    const uint32_t n = first[n_trees];
     if (n == 0) return AE_OK;
     Scratch &S = g_scratch;
     auto &pb = S.pb, &stash_pb = S.stash_pb;
@@ -838,13 +855,25 @@ int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uin
     std::vector<Decision> top_dec;
     std::vector<BigTask> level;
     std::vector<uint32_t> level_top;  // top node of each task of the level
-    if (n > warp_subtree) {
-        level.push_back(BigTask{0, n, 0});
-        level_top.push_back(0);
-        top.push_back(TopNode{});
-        top[0].task = level[0];
-    } else {
-        small.push_back(SmallTask{0, n, 0});
+    std::vector<int32_t> tree_root(n_trees, 0);  // ref of each tree's root (see TopNode::left)
+    std::vector<char> tree_empty(n_trees, 0);
+    for (uint32_t r = 0; r < n_trees; r++) {
+        const uint32_t a = first[r], b = first[r + 1];
+        if (b <= a) {
+            tree_empty[r] = 1;
+            continue;
+        }
+        if (b - a > warp_subtree) {
+            tree_root[r] = int32_t(top.size());
+            level.push_back(BigTask{a, b, 0});
+            level_top.push_back(uint32_t(top.size()));
+            top.push_back(TopNode{});
+            top.back().task = level.back();
+            top.back().tree = r;
+        } else {
+            tree_root[r] = -1 - int32_t(small.size());
+            small.push_back(SmallTask{a, b, 0, a, 2 * a});
+        }
     }
     auto &acc = S.acc;
     auto &d_tasks = S.tasks;
@@ -912,15 +941,17 @@ int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uin
             for (int side = 0; side < 2; side++) {
                 const BigTask &K = kids[side];
                 int32_t ref;
+                const uint32_t tree = top[id].tree;
                 if (K.end - K.start > warp_subtree) {
                     ref = int32_t(top.size());
                     top.push_back(TopNode{});
                     top.back().task = K;
+                    top.back().tree = tree;
                     next.push_back(K);
                     next_top.push_back(uint32_t(ref));
                 } else {
                     ref = -1 - int32_t(small.size());
-                    small.push_back(SmallTask{K.start, K.end, K.depth});
+                    small.push_back(SmallTask{K.start, K.end, K.depth, first[tree], 2 * first[tree]});
                 }
                 if (side == 0) top[id].left = ref;
                 else top[id].right = ref;
@@ -946,32 +977,38 @@ int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uin
         AE_CK(cudaMemcpyAsync(sub_count.data(), d_sub_count.p, ns * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         AE_CK(cudaStreamSynchronize(st));
     }
-    // Pre-order numbering: a node, then its left subtree, then its right.
+    // Pre-order numbering per tree: a node, then its left subtree, then its
+    // right.
     std::vector<TopPlace> place(top.size());
-    uint32_t next_index = 0;
     std::vector<int32_t> work;
-    work.push_back(top.empty() ? -1 : 0);
     std::vector<uint32_t> root_of_top(top.size());
-    while (!work.empty()) {
-        const int32_t ref = work.back();
-        work.pop_back();
-        if (ref >= 0) {
-            root_of_top[ref] = next_index++;
-            if (!top[ref].leaf) {
-                work.push_back(top[ref].right);
-                work.push_back(top[ref].left);
+    for (uint32_t r = 0; r < n_trees; r++) {
+        if (tree_empty[r]) continue;
+        uint32_t next_index = 0;
+        work.push_back(tree_root[r]);
+        while (!work.empty()) {
+            const int32_t ref = work.back();
+            work.pop_back();
+            if (ref >= 0) {
+                root_of_top[ref] = next_index++;
+                if (!top[ref].leaf) {
+                    work.push_back(top[ref].right);
+                    work.push_back(top[ref].left);
+                }
+            } else {
+                const uint32_t s = uint32_t(-1 - ref);
+                sub_base[s] = next_index;
+                next_index += sub_count[s];
             }
-        } else {
-            const uint32_t s = uint32_t(-1 - ref);
-            sub_base[s] = next_index;
-            next_index += sub_count[s];
         }
+        node_counts[r] = next_index;
     }
     for (size_t i = 0; i < top.size(); i++) {
         TopPlace &P = place[i];
-        P.at = root_of_top[i];
+        const uint32_t tree_first = first[top[i].tree];
+        P.at = 2 * tree_first + root_of_top[i];
         P.leaf = top[i].leaf ? 1 : 0;
-        P.start = top[i].task.start;
+        P.start = top[i].task.start - tree_first;
         P.count = top[i].task.end - top[i].task.start;
         auto root = [&](int32_t r) { return r >= 0 ? int32_t(root_of_top[r]) : int32_t(sub_base[-1 - r]); };
         P.left = P.leaf ? 0 : root(top[i].left);
@@ -995,8 +1032,14 @@ int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uin
     }
     AE_CK(cudaGetLastError());
     AE_CK(cudaStreamSynchronize(st));
-    *node_count = next_index;
     return AE_OK;
+}
+
+// One tree over all n boxes.
+int gpu_build_bvh(const ae_aabb *d_bounds, uint32_t n, ae_bvh_node *d_nodes, uint32_t *d_order,
+                  uint32_t *node_count, cudaStream_t st, uint32_t warp_subtree = kWarpTask) {
+    const uint32_t first[2] = {0, n};
+    return gpu_build_forest(d_bounds, first, 1, d_nodes, d_order, node_count, st, warp_subtree);
 }
 
 // MeshLibrary::Add's device part on device arrays: the triangle boxes, the
@@ -1018,7 +1061,54 @@ int gpu_mesh_blas_device(const ae_vertex *d_v, uint32_t nv, const uint32_t *d_id
     if (h_bad) return AE_ERR_LAYOUT;
     const int rc = gpu_build_bvh(S.box.p, tris, d_nodes, S.order.p, out_count, st);
     if (rc != AE_OK) return rc;
-    k_reorder_indices<<<(tris + 255) / 256, 256, 0, st>>>(d_idx, S.order.p, tris, d_out_idx);
+    k_reorder_indices<<<(tris + 255) / 256, 256, 0, st>>>(d_idx, S.order.p, 0u, tris, d_out_idx);
+    AE_CK(cudaGetLastError());
+    AE_CK(cudaStreamSynchronize(st));
+    return AE_OK;
+}
+
+// The BLAS of k meshes at once: one forest build over all their triangles,
+// so the meshes share the level rounds and the warp launch.  Arrays of device
+// pointers, one entry per mesh; each mesh's output equals
+// gpu_mesh_blas_device's.
+int gpu_mesh_blas_many(uint32_t k, const ae_vertex *const *d_v, const uint32_t *nv, const uint32_t *const *d_idx,
+                       const uint32_t *ni, ae_bvh_node *const *d_nodes, uint32_t *out_counts,
+                       uint32_t *const *d_out_idx, cudaStream_t st) {
+    std::vector<uint32_t> first(size_t(k) + 1, 0);
+    for (uint32_t m = 0; m < k; m++) {
+        out_counts[m] = 0;
+        if (ni[m] % 3 != 0) return AE_ERR_INVALID;
+        if (ni[m] && (!d_v[m] || !d_idx[m] || !d_nodes[m] || !d_out_idx[m])) return AE_ERR_INVALID;
+        first[m + 1] = first[m] + ni[m] / 3;
+    }
+    const uint32_t total = first[k];
+    if (total == 0) return AE_OK;
+    Scratch &S = g_scratch;
+    AE_CK(S.box.need(total));
+    AE_CK(S.order.need(total));
+    AE_CK(S.nodes.need(2ull * total));
+    AE_CK(S.bad.need(1));
+    AE_CK(cudaMemsetAsync(S.bad.p, 0, sizeof(int), st));
+    for (uint32_t m = 0; m < k; m++) {
+        const uint32_t tris = first[m + 1] - first[m];
+        if (tris)
+            k_triangle_boxes<<<(tris + 255) / 256, 256, 0, st>>>(d_v[m], nv[m], d_idx[m], tris, S.box.p + first[m],
+                                                                  S.bad.p);
+    }
+    int h_bad = 0;
+    AE_CK(cudaMemcpyAsync(&h_bad, S.bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    AE_CK(cudaStreamSynchronize(st));
+    if (h_bad) return AE_ERR_LAYOUT;
+    const int rc = gpu_build_forest(S.box.p, first.data(), k, S.nodes.p, S.order.p, out_counts, st, kWarpTask);
+    if (rc != AE_OK) return rc;
+    for (uint32_t m = 0; m < k; m++) {
+        const uint32_t tris = first[m + 1] - first[m];
+        if (!tris) continue;
+        k_reorder_indices<<<(tris + 255) / 256, 256, 0, st>>>(d_idx[m], S.order.p + first[m], first[m], tris,
+                                                               d_out_idx[m]);
+        AE_CK(cudaMemcpyAsync(d_nodes[m], S.nodes.p + 2ull * first[m], size_t(out_counts[m]) * sizeof(ae_bvh_node),
+                              cudaMemcpyDeviceToDevice, st));
+    }
     AE_CK(cudaGetLastError());
     AE_CK(cudaStreamSynchronize(st));
     return AE_OK;
@@ -1031,6 +1121,51 @@ struct OwnStream {
     ~OwnStream() { if (s) cudaStreamDestroy(s); }
 };
 }  // namespace
+
+// k meshes with host arrays (indices already checked against nv): staged
+// into device buffers, built as one forest, copied back.  out_nodes[m] holds
+// 2 * ni[m] / 3 nodes, out_indices[m] ni[m] indices.
+int gpu_mesh_blas_many_host(uint32_t k, const ae_vertex *const *v, const uint32_t *nv, const uint32_t *const *idx,
+                            const uint32_t *ni, ae_bvh_node *const *out_nodes, uint32_t *out_counts,
+                            uint32_t *const *out_indices) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    OwnStream st;
+    AE_CK(st.make());
+    Scratch &S = g_scratch;
+    std::vector<size_t> vo(size_t(k) + 1, 0), io(size_t(k) + 1, 0);
+    for (uint32_t m = 0; m < k; m++) {
+        vo[m + 1] = vo[m] + nv[m];
+        io[m + 1] = io[m] + ni[m];
+        if (ni[m] % 3 != 0) return AE_ERR_INVALID;
+    }
+    AE_CK(S.v.need(vo[k]));
+    AE_CK(S.idx.need(io[k]));
+    AE_CK(S.out_idx.need(io[k]));
+    // Node room per mesh: 2 * tris, laid out like the forest's own array.
+    Grow<ae_bvh_node> &staged = S.mesh_nodes;
+    AE_CK(staged.need(2 * (io[k] / 3) + 1));
+    std::vector<const ae_vertex *> dv(k);
+    std::vector<const uint32_t *> di(k);
+    std::vector<ae_bvh_node *> dn(k);
+    std::vector<uint32_t *> dout(k);
+    for (uint32_t m = 0; m < k; m++) {
+        if (nv[m]) AE_CK(cudaMemcpyAsync(S.v.p + vo[m], v[m], size_t(nv[m]) * sizeof(ae_vertex), cudaMemcpyHostToDevice, st.s));
+        if (ni[m]) AE_CK(cudaMemcpyAsync(S.idx.p + io[m], idx[m], size_t(ni[m]) * sizeof(uint32_t), cudaMemcpyHostToDevice, st.s));
+        dv[m] = S.v.p + vo[m];
+        di[m] = S.idx.p + io[m];
+        dn[m] = staged.p + 2 * (io[m] / 3);
+        dout[m] = S.out_idx.p + io[m];
+    }
+    const int rc = gpu_mesh_blas_many(k, dv.data(), nv, di.data(), ni, dn.data(), out_counts, dout.data(), st.s);
+    if (rc != AE_OK) return rc;
+    for (uint32_t m = 0; m < k; m++) {
+        if (!ni[m]) continue;
+        AE_CK(cudaMemcpyAsync(out_nodes[m], dn[m], size_t(out_counts[m]) * sizeof(ae_bvh_node), cudaMemcpyDeviceToHost, st.s));
+        AE_CK(cudaMemcpyAsync(out_indices[m], dout[m], size_t(ni[m]) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st.s));
+    }
+    AE_CK(cudaStreamSynchronize(st.s));
+    return AE_OK;
+}
 
 // The same with host arrays (indices already checked against nv).
 int gpu_mesh_blas(const ae_vertex *v, uint32_t nv, const uint32_t *idx, uint32_t ni, ae_bvh_node *out_nodes,
@@ -1170,6 +1305,17 @@ extern "C" int ae_mesh_blas_device(const ae_vertex *d_vertices, uint32_t nv, con
     std::lock_guard<std::mutex> lock(ae::g_mutex);
     return ae::gpu_mesh_blas_device(d_vertices, nv, d_indices, ni, d_nodes, out_node_count, d_out_indices,
                                     static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int ae_mesh_blas_device_many(uint32_t k, const ae_vertex *const *d_vertices, const uint32_t *nv,
+                                        const uint32_t *const *d_indices, const uint32_t *ni,
+                                        ae_bvh_node *const *d_nodes, uint32_t *out_node_counts,
+                                        uint32_t *const *d_out_indices, void *stream) {
+    if (k && (!d_vertices || !nv || !d_indices || !ni || !d_nodes || !out_node_counts || !d_out_indices))
+        return AE_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(ae::g_mutex);
+    return ae::gpu_mesh_blas_many(k, d_vertices, nv, d_indices, ni, d_nodes, out_node_counts, d_out_indices,
+                                  static_cast<cudaStream_t>(stream));
 }
 
 extern "C" void ae_bvh_builder_release(void) {

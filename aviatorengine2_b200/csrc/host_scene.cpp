@@ -240,6 +240,9 @@ namespace ae {
 // The device part of MeshLibrary::Add (bvh_build.cu).
 int gpu_mesh_blas(const ae_vertex *v, uint32_t nv, const uint32_t *idx, uint32_t ni, ae_bvh_node *out_nodes,
                   uint32_t *out_count, uint32_t *out_indices);
+int gpu_mesh_blas_many_host(uint32_t k, const ae_vertex *const *v, const uint32_t *nv, const uint32_t *const *idx,
+                            const uint32_t *ni, ae_bvh_node *const *out_nodes, uint32_t *out_counts,
+                            uint32_t *const *out_indices);
 }  // namespace ae
 
 // ---------------------------------------------------------------------------
@@ -340,6 +343,60 @@ int ae_mesh_library_add(ae_mesh_library *lib, const ae_vertex *v, uint32_t nv, c
 int ae_mesh_library_add_gpu(ae_mesh_library *lib, const ae_vertex *v, uint32_t nv, const uint32_t *idx, uint32_t ni,
                             int double_sided) {
     return mesh_library_add(lib, v, nv, idx, ni, double_sided, true);
+}
+
+// k calls of ae_mesh_library_add_gpu in one: the k BLAS are built together
+// on the GPU (one forest build, bvh_build.cu) and appended in order, each
+// exactly as its own call would append it.  out_handles[m] receives mesh m's
+// handle; nothing is appended when any mesh is refused.
+int ae_mesh_library_add_many_gpu(ae_mesh_library *lib, uint32_t k, const ae_vertex *const *v, const uint32_t *nv,
+                                 const uint32_t *const *idx, const uint32_t *ni, const int *double_sided,
+                                 int *out_handles) {
+    if (!lib || (k && (!v || !nv || !idx || !ni || !out_handles))) return AE_ERR_INVALID;
+    for (uint32_t m = 0; m < k; m++) {
+        if ((nv[m] && !v[m]) || (ni[m] && !idx[m]) || ni[m] % 3 != 0) return AE_ERR_INVALID;
+        for (uint32_t i = 0; i < ni[m]; i++)
+            if (idx[m][i] >= nv[m]) return AE_ERR_LAYOUT;
+    }
+    try {
+        std::vector<std::vector<ae_bvh_node>> nodes(k);
+        std::vector<std::vector<uint32_t>> leaf_order(k);
+        std::vector<ae_bvh_node *> np(k);
+        std::vector<uint32_t *> ip(k);
+        std::vector<uint32_t> counts(k, 0);
+        for (uint32_t m = 0; m < k; m++) {
+            nodes[m].resize(std::max<size_t>(size_t(ni[m] / 3) * 2, 1));
+            leaf_order[m].resize(std::max<size_t>(ni[m], 1));
+            np[m] = nodes[m].data();
+            ip[m] = leaf_order[m].data();
+        }
+        if (k) {
+            const int rc = ae::gpu_mesh_blas_many_host(k, v, nv, idx, ni, np.data(), counts.data(), ip.data());
+            if (rc != AE_OK) return rc;
+        }
+        for (uint32_t m = 0; m < k; m++) {
+            ae_mesh_range range{};
+            range.vertexBase = uint32_t(lib->vertices.size());
+            range.indexBase = uint32_t(lib->indices.size());
+            range.blasBase = uint32_t(lib->blas.size());
+            range.doubleSided = double_sided && double_sided[m] ? 1u : 0u;
+            ae_aabb local = EmptyBox();
+            lib->vertices.reserve(lib->vertices.size() + nv[m]);
+            for (uint32_t i = 0; i < nv[m]; i++) {
+                lib->vertices.push_back(v[m][i]);
+                local = GrowToPoint(local, v[m][i].px, v[m][i].py, v[m][i].pz);
+            }
+            range.localBounds = local;
+            range.triangleCount = ni[m] / 3;
+            lib->indices.insert(lib->indices.end(), leaf_order[m].begin(), leaf_order[m].begin() + ni[m]);
+            lib->blas.insert(lib->blas.end(), nodes[m].begin(), nodes[m].begin() + counts[m]);
+            lib->ranges.push_back(range);
+            out_handles[m] = int(lib->ranges.size() - 1);
+        }
+    } catch (const std::bad_alloc &) {
+        return AE_ERR_OOM;
+    }
+    return AE_OK;
 }
 
 int ae_mesh_library_range(const ae_mesh_library *lib, uint32_t handle, ae_mesh_range *out) {

@@ -64,6 +64,26 @@ class MeshLibrary:
             raise _lib.AeError(handle, fn)
         return handle
 
+    def add_many(self, meshes, double_sided=None):
+        """add() for a list of (vertices, indices); with gpu=True the BLAS are
+        built together (ae_mesh_library_add_many_gpu: the same bytes as k
+        add() calls).  Returns the handles."""
+        if not self.gpu:
+            ds = double_sided or [False] * len(meshes)
+            return [self.add(v, i, d) for (v, i), d in zip(meshes, ds)]
+        vs = [np.ascontiguousarray(v, dtype=_lib.VERTEX) for v, _ in meshes]
+        ix = [np.ascontiguousarray(i, dtype=np.uint32).ravel() for _, i in meshes]
+        k = len(meshes)
+        vp = (ctypes.c_void_p * k)(*[a.ctypes.data for a in vs])
+        ip = (ctypes.c_void_p * k)(*[a.ctypes.data for a in ix])
+        nv = np.array([len(a) for a in vs], np.uint32)
+        ni = np.array([len(a) for a in ix], np.uint32)
+        ds = np.array([int(bool(d)) for d in (double_sided or [False] * k)], np.int32)
+        out = np.zeros(max(k, 1), np.int32)
+        check(lib().ae_mesh_library_add_many_gpu(self._h, k, vp, ptr(nv), ip, ptr(ni), ptr(ds), ptr(out)),
+              what="ae_mesh_library_add_many_gpu")
+        return [int(h) for h in out[:k]]
+
     def range(self, handle):
         r = np.zeros(1, _lib.MESH_RANGE)
         check(lib().ae_mesh_library_range(self._h, handle, ptr(r)), what="ae_mesh_library_range")
@@ -523,7 +543,7 @@ def wavefront_scene(seed=4, width=1920, height=1080, depth=12, n_meshes=32, n_in
     rng = np.random.default_rng(seed)
     meshes = MeshLibrary(gpu=gpu_build)
     geometry, kinds = wavefront_meshes(rng, n_meshes, target_tris)
-    handles = [meshes.add(v, i) for v, i in geometry]
+    handles = meshes.add_many(geometry)
     mat = []
     for k in range(n_meshes):
         mat.append(dict(albedo=tuple(float(x) for x in rng.uniform(0.2, 0.8, 3)),

@@ -229,6 +229,15 @@ int ae_mesh_blas_device(const ae_vertex *d_vertices, uint32_t nv,
                         ae_bvh_node *d_nodes, uint32_t *out_node_count,
                         uint32_t *d_out_indices, void *stream);
 
+/* ae_mesh_blas_device for k meshes at once (arrays of k device pointers and
+ * sizes, held in host memory): the k trees are built together - they share
+ * the builder's level rounds and its warp launch - and each mesh's nodes,
+ * count and indices equal its own ae_mesh_blas_device call's. */
+int ae_mesh_blas_device_many(uint32_t k, const ae_vertex *const *d_vertices, const uint32_t *nv,
+                             const uint32_t *const *d_indices, const uint32_t *ni,
+                             ae_bvh_node *const *d_nodes, uint32_t *out_node_counts,
+                             uint32_t *const *d_out_indices, void *stream);
+
 /* The device builder keeps its scratch (about 150 bytes per box of the
  * largest build so far) between calls; this frees it. */
 void ae_bvh_builder_release(void);
@@ -253,6 +262,13 @@ int ae_mesh_library_add(ae_mesh_library *lib, const ae_vertex *vertices, uint32_
  * leaf-order index rewrite on the GPU; appends the same bytes. */
 int ae_mesh_library_add_gpu(ae_mesh_library *lib, const ae_vertex *vertices, uint32_t nv,
                             const uint32_t *indices, uint32_t ni, int double_sided);
+/* k calls of ae_mesh_library_add_gpu in one (host arrays of k pointers and
+ * sizes; double_sided may be NULL): the k BLAS are built together on the GPU
+ * and appended in order, each exactly as its own call would append it.
+ * out_handles[m] receives mesh m's handle; nothing is appended on failure. */
+int ae_mesh_library_add_many_gpu(ae_mesh_library *lib, uint32_t k, const ae_vertex *const *vertices,
+                                 const uint32_t *nv, const uint32_t *const *indices, const uint32_t *ni,
+                                 const int *double_sided, int *out_handles);
 int ae_mesh_library_range(const ae_mesh_library *lib, uint32_t handle, ae_mesh_range *out);
 /* Sizes of the flattened arrays (elements). */
 void ae_mesh_library_sizes(const ae_mesh_library *lib, uint64_t *nv, uint64_t *ni, uint64_t *nb);

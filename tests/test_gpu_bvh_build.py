@@ -234,3 +234,58 @@ def test_rebuild_scene_equals_reference_rebuild():
                 x.render_frame(_lib.MODE_COMPUTE_ONLY)
         assert np.array_equal(ctx.read_image(_lib.IMAGE_ACCUM).view(np.uint32),
                               twin.read_image(_lib.IMAGE_ACCUM).view(np.uint32))
+
+
+def _forest_meshes():
+    rng = np.random.default_rng(21)
+    return [scenes.heightfield(200, 20.0, 2.5, rng), scenes.box_mesh((1.0, 2.0, 0.5)),
+            (np.zeros(0, dtype=scenes._lib.VERTEX), np.zeros(0, np.uint32)), scenes.icosphere(5, 3.0),
+            scenes.quad_mesh((2.0, 0.0, 0.0), (0.0, 0.0, 3.0)), scenes.icosphere(1, 1.0),
+            scenes.heightfield(64, 10.0, 1.0, rng)]
+
+
+def test_library_add_many_equals_separate_adds():
+    meshes = _forest_meshes()
+    ds = [False, False, False, False, True, False, False]
+    g = scenes.MeshLibrary(gpu=True)
+    gh = g.add_many(meshes, ds)
+    h = scenes.MeshLibrary()
+    hh = [h.add(v, i, d) for (v, i), d in zip(meshes, ds)]
+    assert gh == hh
+    for a, b in zip(g.arrays(), h.arrays()):
+        assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+    for x, y in zip(gh, hh):
+        assert g.range(x).tobytes() == h.range(y).tobytes()
+
+
+def test_device_many_equals_per_mesh():
+    import ctypes
+
+    import torch
+    from aviatorengine2_b200 import _lib
+    from aviatorengine2_b200._lib import lib
+    meshes = [m for m in _forest_meshes() if len(m[1])]
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    k = len(meshes)
+    d_v = [torch.from_numpy(np.ascontiguousarray(v, _lib.VERTEX).view(np.uint8)).to(dev) for v, _ in meshes]
+    d_i = [torch.from_numpy(np.ascontiguousarray(i, np.uint32).view(np.int32)).to(dev) for _, i in meshes]
+    d_n = [torch.empty(2 * (len(i) // 3) * 48, dtype=torch.uint8, device=dev) for _, i in meshes]
+    d_o = [torch.empty(len(i), dtype=torch.int32, device=dev) for _, i in meshes]
+    P = ctypes.c_void_p
+    nv = np.array([len(v) for v, _ in meshes], np.uint32)
+    ni = np.array([len(i) for _, i in meshes], np.uint32)
+    counts = np.zeros(k, np.uint32)
+    for _ in range(2):  # twice: the builder's scratch is reused
+        rc = lib().ae_mesh_blas_device_many(k, (P * k)(*[t.data_ptr() for t in d_v]), _lib.ptr(nv),
+                                            (P * k)(*[t.data_ptr() for t in d_i]), _lib.ptr(ni),
+                                            (P * k)(*[t.data_ptr() for t in d_n]), _lib.ptr(counts),
+                                            (P * k)(*[t.data_ptr() for t in d_o]), P(stream.cuda_stream))
+        assert rc == 0
+        for m, (v, i) in enumerate(meshes):
+            host = scenes.MeshLibrary()
+            host.add(v, i)
+            _, h_idx, h_blas = host.arrays()
+            assert counts[m] == len(h_blas)
+            assert np.array_equal(d_n[m][: int(counts[m]) * 48].cpu().numpy(), h_blas.view(np.uint8).ravel())
+            assert np.array_equal(d_o[m].cpu().numpy().view(np.uint32), h_idx)
