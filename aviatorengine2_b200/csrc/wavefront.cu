@@ -54,12 +54,7 @@ struct WfParams {
 // Device counters: [0],[1] ray queue sizes (ping-pong), [2] shadow queue,
 // [3] error flags, [4..4+kMaxBounce) extend tile counters, then shadow tiles.
 constexpr int kMaxBounce = 64;
-enum {
-    C_Q0 = 0, C_Q1 = 1, C_SH = 2, C_ERR = 3, C_TILE = 4, C_SHTILE = 4 + kMaxBounce,
-    C_EXWALK = 4 + 2 * kMaxBounce,  // per bounce: rays handed out by k_wf_extend_walk
-    C_SHWALK = 4 + 3 * kMaxBounce,  // per bounce: entries handed out by k_wf_shadow
-    C_COUNT = 4 + 4 * kMaxBounce
-};
+enum { C_Q0 = 0, C_Q1 = 1, C_SH = 2, C_ERR = 3, C_TILE = 4, C_SHTILE = 4 + kMaxBounce, C_COUNT = 4 + 2 * kMaxBounce };
 
 struct WfView {
     ae_ray *qray[2];
@@ -111,9 +106,6 @@ void destroy_wavefront(Ctx *c) {
     c->wave = nullptr;
 }
 
-// Queue entries a warp of a walker kernel claims at a time.
-constexpr uint32_t kWalkChunk = 64;
-
 // ---------------------------------------------------------------------------
 // Stages
 // ---------------------------------------------------------------------------
@@ -123,7 +115,7 @@ __global__ void __launch_bounds__(256) k_wf_generate(WfView W) {
         W.cnt[C_Q0] = P.n_paths;
         W.cnt[C_Q1] = 0;
         W.cnt[C_SH] = 0;
-        for (int k = 0; k < 4 * kMaxBounce; k++) W.cnt[C_TILE + k] = 0;
+        for (int k = 0; k < 2 * kMaxBounce; k++) W.cnt[C_TILE + k] = 0;
     }
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P.n_paths; p += gridDim.x * blockDim.x) {
         const uint32_t x = p % P.F.width, y = p / P.F.width;
@@ -203,97 +195,39 @@ __global__ void __launch_bounds__(THREADS) k_wf_extend(DevScene S, FastView V, W
     }
 }
 
-// Extend on the step-wise Walker: a persistent grid, each lane stepping its
-// own queued ray and starting the next as soon as one finishes.  Warps claim
-// runs of kWalkChunk consecutive queue entries from a per-bounce counter and
-// their lanes take entries from the warp's run, so the rays a warp has in
-// flight stay close in queue order.  For incoherent queues (bounces past the
-// camera rays).
+// Extend on the step-wise Walker: a persistent grid, each thread stepping
+// its own queued ray and taking the next (k + grid size) when one finishes.
+// For incoherent queues (bounces past the camera rays).
 template <bool WT>
 __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_wf_extend_walk(DevScene S, FastView V, WfView W, int bounce) {
     extern __shared__ uint2 stk[];
-    // The precision form (watertight walk, more live state) keeps the static
-    // assignment - lane i: entries i, i + grid size, ...: there the run logic
-    // cost more in spills than it gained (1080p frame 186 -> 191 ms).
-    constexpr bool DYN = !WT;
-    if (!DYN) {
-        const int q = bounce & 1;
-        const uint32_t count = W.cnt[q];
-        const uint32_t stride = gridDim.x * blockDim.x;
-        uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-        Walker<WT> w;
-        WalkStacks<> K;
-        bool active = k < count;
+    const int q = bounce & 1;
+    const uint32_t count = W.cnt[q];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    Walker<WT> w;
+    WalkStacks<> K;
+    bool active = k < count;
+    if (active) {
+        const ae_ray r = W.qray[q][k];
+        w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+    }
+    while (active) {
+        if (!w.step(S, V, K, stk, threadIdx.x, blockDim.x)) continue;
+        const Best &b = w.best;
+        const bool any = b.object != AE_MISS;
+        ae_hit h;
+        h.t = any ? b.t : 0.0f;
+        h.alpha = any ? b.alpha : 0.0f;
+        h.beta = any ? b.beta : 0.0f;
+        h.object = b.object;
+        h.prim = b.prim;
+        W.qhit[k] = h;
+        k += stride;
+        active = k < count;
         if (active) {
             const ae_ray r = W.qray[q][k];
             w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
-        }
-        while (active) {
-            if (!w.step(S, V, K, stk, threadIdx.x, blockDim.x)) continue;
-            const Best &b = w.best;
-            const bool any = b.object != AE_MISS;
-            ae_hit h;
-            h.t = any ? b.t : 0.0f;
-            h.alpha = any ? b.alpha : 0.0f;
-            h.beta = any ? b.beta : 0.0f;
-            h.object = b.object;
-            h.prim = b.prim;
-            W.qhit[k] = h;
-            k += stride;
-            active = k < count;
-            if (active) {
-                const ae_ray r = W.qray[q][k];
-                w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
-            }
-        }
-        return;
-    }
-    const int q = bounce & 1;
-    const uint32_t count = W.cnt[q];
-    uint32_t *next = &W.cnt[C_EXWALK + bounce];
-    const uint32_t lane = threadIdx.x & 31, below = (1u << lane) - 1u;
-    Walker<WT> w;
-    WalkStacks<> K;
-    uint32_t k = 0, cbase = 0, cend = 0;
-    bool active = false, need = true, exhausted = false;
-    for (;;) {
-        uint32_t m = __ballot_sync(0xffffffffu, need);
-        while (m && !exhausted) {
-            if (cbase >= cend) {
-                uint32_t b = 0;
-                if (lane == 0) b = atomicAdd(next, kWalkChunk);
-                b = __shfl_sync(0xffffffffu, b, 0);
-                if (b >= count) {
-                    exhausted = true;
-                    break;
-                }
-                cbase = b;
-                cend = min(b + kWalkChunk, count);
-            }
-            const uint32_t take = min(cend - cbase, uint32_t(__popc(m)));
-            if (need && uint32_t(__popc(m & below)) < take) {
-                k = cbase + __popc(m & below);
-                need = false;
-                active = true;
-                const ae_ray r = W.qray[q][k];
-                w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
-            }
-            cbase += take;
-            m = __ballot_sync(0xffffffffu, need);
-        }
-        if (!__any_sync(0xffffffffu, active)) break;
-        if (active && w.step(S, V, K, stk, threadIdx.x, blockDim.x)) {
-            const Best &b = w.best;
-            const bool any = b.object != AE_MISS;
-            ae_hit h;
-            h.t = any ? b.t : 0.0f;
-            h.alpha = any ? b.alpha : 0.0f;
-            h.beta = any ? b.beta : 0.0f;
-            h.object = b.object;
-            h.prim = b.prim;
-            W.qhit[k] = h;
-            active = false;
-            need = true;
         }
     }
 }
@@ -338,118 +272,48 @@ __global__ void __launch_bounds__(256) k_wf_shade(DevScene S, FastView V, WfView
 // the sample unoccluded), so each walk starts with that distance as its
 // bound: the verdict and the glass step are those of the unbounded walk.
 template <int THREADS, bool WT>
-__global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_wf_shadow(DevScene S, FastView V,
-                                                                                       WfView W, int bounce) {
+__global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_wf_shadow(DevScene S, FastView V, WfView W) {
     extern __shared__ uint2 stk[];
-    constexpr bool DYN = !WT;  // as k_wf_extend_walk
-    if (!DYN) {
-        const uint32_t count = W.cnt[C_SH];
-        const uint32_t stride = gridDim.x * THREADS;
-        uint32_t k = blockIdx.x * THREADS + threadIdx.x;
-        Walker<WT> w;
-        WalkStacks<> K;
-        uint32_t e = 0;
-        f3 so, sd, lp;
-        int step = 0;
-        bool active = k < count;
+    const uint32_t count = W.cnt[C_SH];
+    const uint32_t stride = gridDim.x * THREADS;
+    uint32_t k = blockIdx.x * THREADS + threadIdx.x;
+    Walker<WT> w;
+    WalkStacks<> K;
+    uint32_t e = 0;
+    f3 so, sd, lp;
+    int step = 0;
+    bool active = k < count;
+    if (active) {
+        e = W.sq[k];
+        const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
+        so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
+        w.start(S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
+    }
+    while (active) {
+        if (!w.step(S, V, K, stk, threadIdx.x, THREADS)) continue;
+        const Best &b = w.best;
+        int verdict = 0;  // 0 unoccluded, 1 occluded, 2 through glass
+        if (b.object != AE_MISS && b.t < AE_SUB(distance(lp, so), 0.001f)) {
+            const uint32_t mt = load_head(S.objects + b.object).material;
+            verdict = mt == AE_MAT_DIFFUSE_LIGHT ? 0 : (mt != AE_MAT_DIELECTRIC ? 1 : 2);
+        }
+        if (verdict == 2) {
+            so = (so + sd * b.t) + sd * 0.001f;
+            if (++step < 4) {
+                w.start(S, so, sd, 0.001f, w.time, AE_SUB(distance(lp, so), 0.001f));
+                continue;
+            }
+            verdict = 0;
+        }
+        W.sh.occ[e] = uint8_t(verdict);
+        k += stride;
+        active = k < count;
         if (active) {
             e = W.sq[k];
             const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
             so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
+            step = 0;
             w.start(S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
-        }
-        while (active) {
-            if (!w.step(S, V, K, stk, threadIdx.x, THREADS)) continue;
-            const Best &b = w.best;
-            int verdict = 0;  // 0 unoccluded, 1 occluded, 2 through glass
-            if (b.object != AE_MISS && b.t < AE_SUB(distance(lp, so), 0.001f)) {
-                const uint32_t mt = load_head(S.objects + b.object).material;
-                verdict = mt == AE_MAT_DIFFUSE_LIGHT ? 0 : (mt != AE_MAT_DIELECTRIC ? 1 : 2);
-            }
-            if (verdict == 2) {
-                so = (so + sd * b.t) + sd * 0.001f;
-                if (++step < 4) {
-                    w.start(S, so, sd, 0.001f, w.time, AE_SUB(distance(lp, so), 0.001f));
-                    continue;
-                }
-                verdict = 0;
-            }
-            W.sh.occ[e] = uint8_t(verdict);
-            k += stride;
-            active = k < count;
-            if (active) {
-                e = W.sq[k];
-                const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
-                so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
-                step = 0;
-                w.start(S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
-            }
-        }
-        return;
-    }
-    const uint32_t count = W.cnt[C_SH];
-    uint32_t *next = &W.cnt[C_SHWALK + bounce];
-    const uint32_t lane = threadIdx.x & 31, below = (1u << lane) - 1u;
-    Walker<WT> w;
-    WalkStacks<> K;
-    uint32_t k = 0, e = 0, cbase = 0, cend = 0;
-    f3 so, sd, lp;
-    int step = 0;
-    bool active = false, need = true, exhausted = false;
-    for (;;) {
-        // Lanes without an entry take the next ones of the warp's run of
-        // consecutive queue entries (the light samples of neighbouring
-        // vertices), claiming a new run when it is used up.
-        uint32_t m = __ballot_sync(0xffffffffu, need);
-        while (m && !exhausted) {
-            if (cbase >= cend) {
-                uint32_t b = 0;
-                if (lane == 0) b = atomicAdd(next, kWalkChunk);
-                b = __shfl_sync(0xffffffffu, b, 0);
-                if (b >= count) {
-                    exhausted = true;
-                    break;
-                }
-                cbase = b;
-                cend = min(b + kWalkChunk, count);
-            }
-            const uint32_t take = min(cend - cbase, uint32_t(__popc(m)));
-            if (need && uint32_t(__popc(m & below)) < take) {
-                k = cbase + __popc(m & below);
-                need = false;
-                active = true;
-                e = W.sq[k];
-                const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
-                so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
-                step = 0;
-                w.start(S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
-            }
-            cbase += take;
-            m = __ballot_sync(0xffffffffu, need);
-        }
-        if (!__any_sync(0xffffffffu, active)) break;
-        if (active && w.step(S, V, K, stk, threadIdx.x, THREADS)) {
-            const Best &b = w.best;
-            int verdict = 0;  // 0 unoccluded, 1 occluded, 2 through glass
-            if (b.object != AE_MISS && b.t < AE_SUB(distance(lp, so), 0.001f)) {
-                const uint32_t mt = load_head(S.objects + b.object).material;
-                verdict = mt == AE_MAT_DIFFUSE_LIGHT ? 0 : (mt != AE_MAT_DIELECTRIC ? 1 : 2);
-            }
-            bool done = true;
-            if (verdict == 2) {
-                so = (so + sd * b.t) + sd * 0.001f;
-                if (++step < 4) {
-                    w.start(S, so, sd, 0.001f, w.time, AE_SUB(distance(lp, so), 0.001f));
-                    done = false;
-                } else {
-                    verdict = 0;
-                }
-            }
-            if (done) {
-                W.sh.occ[e] = uint8_t(verdict);
-                active = false;
-                need = true;
-            }
         }
     }
 }
@@ -655,10 +519,10 @@ static int record_sample(Ctx *c, cudaStream_t st, int cfg_index, const Grids &G,
         else k_wf_extend_walk<false><<<G.wgrid, 128, shsmem, st>>>(S, V, W, int(b));
         if (prec) {
             k_wf_shade<true><<<grid256, 256, 0, st>>>(S, V, W, int(b));
-            k_wf_shadow<128, true><<<shgrid, 128, shsmem, st>>>(S, V, W, int(b));
+            k_wf_shadow<128, true><<<shgrid, 128, shsmem, st>>>(S, V, W);
         } else {
             k_wf_shade<false><<<grid256, 256, 0, st>>>(S, V, W, int(b));
-            k_wf_shadow<128, false><<<shgrid, 128, shsmem, st>>>(S, V, W, int(b));
+            k_wf_shadow<128, false><<<shgrid, 128, shsmem, st>>>(S, V, W);
         }
         k_wf_connect<<<grid256, 256, 0, st>>>(W, int(b));
     }
