@@ -430,11 +430,9 @@ def instanced_meshes(seed=2, width=1920, height=1080, levels=(7, 6, 6, 5, 5), gr
     gpu_build: BLAS builds on the GPU (identical bytes)."""
     rng = np.random.default_rng(seed)
     meshes = MeshLibrary(gpu=gpu_build)
-    handles = []
-    for _ in range(n_heightfields):
-        handles.append(meshes.add(*heightfield(grid, 20.0, 2.5, rng)))
-    for lv in levels:
-        handles.append(meshes.add(*icosphere(lv, 5.0)))
+    geometry = [heightfield(grid, 20.0, 2.5, rng) for _ in range(n_heightfields)]
+    geometry += [icosphere(lv, 5.0) for lv in levels]
+    handles = meshes.add_many(geometry)
     ents = []
     for k in range(n_instances):
         pos = tuple(float(x) for x in rng.uniform(0.0, 100.0, 3))
