@@ -429,8 +429,12 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_closest_walk(DevScene
             const ae_ray r = rays[k];
             w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
         }
-        while (active) {
-            if (!w.step(S, V, K, stk, threadIdx.x, blockDim.x)) continue;
+        uint32_t iter = 0;
+        for (;;) {
+            if (!__any_sync(0xffffffffu, active)) break;
+            // Only the warp's largest phase group steps (warp_pick_group).
+            const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, iter);
+            if (!active || w.group() != pick || !w.step(S, V, K, stk, threadIdx.x, blockDim.x)) continue;
             const Best &b = w.best;
             const bool any = b.object != AE_MISS;
             ae_hit h;
@@ -453,6 +457,7 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_closest_walk(DevScene
     Walker<false> w;
     WalkStacks<> K;
     uint32_t k = 0, cbase = 0, cend = 0;  // cbase/cend: the warp's chunk, the same in every lane
+    uint32_t iter = 0;
     bool active = false, need = true, exhausted = false;
     for (;;) {
         // Lanes without a ray take the next ones of the warp's chunk, in lane
@@ -482,7 +487,10 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_closest_walk(DevScene
             m = __ballot_sync(0xffffffffu, need);
         }
         if (!__any_sync(0xffffffffu, active)) break;
-        if (active && w.step(S, V, K, stk, threadIdx.x, blockDim.x)) {
+        // Only the warp's largest phase group steps (warp_pick_group): on the
+        // 1080p bounce set 3.31 -> 2.70 ms.
+        const uint32_t pick = warp_pick_group(w.group(), active, iter);
+        if (active && w.group() == pick && w.step(S, V, K, stk, threadIdx.x, blockDim.x)) {
             const Best &b = w.best;
             const bool any = b.object != AE_MISS;
             ae_hit h;

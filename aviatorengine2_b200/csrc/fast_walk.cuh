@@ -105,6 +105,12 @@ struct Walker {
         phase = kWalkObject;
     }
 
+    // The walk's phase group for warp-level step scheduling: 0 TLAS node,
+    // 1 object of a TLAS leaf, 2 BLAS interior node, 3 BLAS leaf.
+    AE_DEV uint32_t group() const {
+        return phase == kWalkBlas ? ((cur & kLeafBit) ? 3u : 2u) : (phase == kWalkTlas ? 0u : 1u);
+    }
+
     // One step; returns true once the ray is finished (best is final).
     AE_DEV bool step(const DevScene &S, const FastView &V, WalkStacks<SS> &K, uint2 *stk, int tid, int nt) {
         if (phase == kWalkBlas) {
@@ -231,5 +237,34 @@ struct Walker {
         return true;
     }
 };
+
+// Which phase group a warp steps this iteration: the largest group among its
+// active lanes, so the lanes that step run the same code; every fourth
+// iteration the group of the next active lane at or after a rotating
+// position, so every lane steps at least once every 128 iterations.  `group`
+// of an inactive lane is ignored.  All 32 lanes must call this together.
+// Scheduling only: each lane's own sequence of steps, and so its result, is
+// unchanged.
+AE_DEV uint32_t warp_pick_group(uint32_t group, bool active, uint32_t &iter) {
+    const uint32_t g = active ? group : 4u;
+    uint32_t pick;
+    if ((iter & 3u) == 3u) {
+        const uint32_t am = __ballot_sync(0xffffffffu, active);
+        const uint32_t r = (iter >> 2) & 31u;
+        const uint32_t rot = (am >> r) | (r ? (am << (32u - r)) : 0u);
+        const uint32_t src = (r + uint32_t(__ffs(rot)) - 1u) & 31u;
+        pick = __shfl_sync(0xffffffffu, g, int(src));
+    } else {
+        uint32_t best = 0, bc = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < 4; k++) {
+            const uint32_t c = uint32_t(__popc(__ballot_sync(0xffffffffu, g == k)));
+            if (c > bc) { bc = c; best = k; }
+        }
+        pick = best;
+    }
+    iter++;
+    return pick;
+}
 
 }  // namespace ae

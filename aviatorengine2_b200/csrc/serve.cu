@@ -193,8 +193,12 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_sv_extend_walk(SvView
         R = W.scenes + W.s_scene[W.qslot[q][k]];
         w.start(R->S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
     }
-    while (active) {
-        if (!w.step(R->S, R->V, K, stk, threadIdx.x, blockDim.x)) continue;
+    uint32_t iter = 0;
+    for (;;) {
+        if (!__any_sync(0xffffffffu, active)) break;
+        // Only the warp's largest phase group steps (warp_pick_group).
+        const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, iter);
+        if (!active || w.group() != pick || !w.step(R->S, R->V, K, stk, threadIdx.x, blockDim.x)) continue;
         const Best &b = w.best;
         const bool any = b.object != AE_MISS;
         ae_hit h;
@@ -270,8 +274,12 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_s
         so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
         w.start(R->S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
     }
-    while (active) {
-        if (!w.step(R->S, R->V, K, stk, threadIdx.x, THREADS)) continue;
+    uint32_t iter = 0;
+    for (;;) {
+        if (!__any_sync(0xffffffffu, active)) break;
+        // Only the warp's largest phase group steps (warp_pick_group).
+        const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, iter);
+        if (!active || w.group() != pick || !w.step(R->S, R->V, K, stk, threadIdx.x, THREADS)) continue;
         const Best &b = w.best;
         int verdict = 0;  // 0 unoccluded, 1 occluded, 2 through glass
         if (b.object != AE_MISS && b.t < AE_SUB(distance(lp, so), 0.001f)) {

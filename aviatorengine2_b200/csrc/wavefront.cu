@@ -212,8 +212,12 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_wf_extend_walk(DevSce
         const ae_ray r = W.qray[q][k];
         w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
     }
-    while (active) {
-        if (!w.step(S, V, K, stk, threadIdx.x, blockDim.x)) continue;
+    uint32_t iter = 0;
+    for (;;) {
+        if (!__any_sync(0xffffffffu, active)) break;
+        // Only the warp's largest phase group steps (warp_pick_group).
+        const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, iter);
+        if (!active || w.group() != pick || !w.step(S, V, K, stk, threadIdx.x, blockDim.x)) continue;
         const Best &b = w.best;
         const bool any = b.object != AE_MISS;
         ae_hit h;
@@ -289,8 +293,12 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_w
         so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
         w.start(S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
     }
-    while (active) {
-        if (!w.step(S, V, K, stk, threadIdx.x, THREADS)) continue;
+    uint32_t iter = 0;
+    for (;;) {
+        if (!__any_sync(0xffffffffu, active)) break;
+        // Only the warp's largest phase group steps (warp_pick_group).
+        const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, iter);
+        if (!active || w.group() != pick || !w.step(S, V, K, stk, threadIdx.x, THREADS)) continue;
         const Best &b = w.best;
         int verdict = 0;  // 0 unoccluded, 1 occluded, 2 through glass
         if (b.object != AE_MISS && b.t < AE_SUB(distance(lp, so), 0.001f)) {
