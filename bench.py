@@ -18,6 +18,7 @@ sum over ranks, timed as the max over ranks.
 """
 import argparse
 import ctypes
+import hashlib
 import json
 import os
 import subprocess
@@ -141,16 +142,55 @@ def make_workload(ctx, scene):
     return prim, bounce[valid].copy()
 
 
-def cpu_reference(scene, rays, budget_s=12.0):
-    """The reference's own traversal (its shader, compiled for the CPU under
-    oracle/_ref) on a bounded sample of the ray set, all host cores: a random
-    subset when the whole set would take longer than the budget, otherwise
-    the whole set traced repeatedly until about `budget_s` of CPU time."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
+def _oracle_modules():
+    """The oracle bindings (tests/_oracle.py) and the reference-scene packer
+    (oracle/ref_scene.py).  Neither imports the library under test."""
+    for d in (os.path.join(ROOT, "tests"), os.path.join(ROOT, "oracle")):
+        if d not in sys.path:
+            sys.path.insert(0, d)
     import _oracle as O
-    kind = "reference" if O.ref_available() else "port"
+    import ref_scene as R
+    return O, R
+
+
+def digest(*arrays):
+    """First 16 hex digits of SHA-256 over the arrays' bytes, in order."""
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).view(np.uint8).tobytes())
+    return h.hexdigest()[:16]
+
+
+def scene_digest(scene):
+    """Digest of the seven device arrays (RenderFrame's bind order) and the config."""
+    return digest(scene.objects, scene.tlas, scene.lights, scene.vertices, scene.indices, scene.blas,
+                  scene.instances, np.array(scene.config).reshape(1))
+
+
+def workload_config(W, H, n_prim, n_bounce, triangles, instances, scene_dig, rays_dig, world):
+    """The `config` object both arms print: the workload and nothing about
+    the implementation, so equal dicts mean equal work."""
+    return {"workload": f"instanced_meshes {W}x{H} primary+bounce closest hit",
+            "rays_per_step": int(n_prim + n_bounce), "primary_rays": int(n_prim), "bounce_rays": int(n_bounce),
+            "triangles": int(triangles), "instances": int(instances), "instance_scale": "uniform in [0.5, 2]",
+            "scene_sha256_16": scene_dig, "rays_sha256_16": rays_dig,
+            "l2": "GPU arm: flushed before every step (512 MB write)", "parallelism": f"replicas x{world}"}
+
+
+def cpu_reference(scene, rays, budget_s=12.0, impl="port"):
+    """The reference's closest hit on the CPU over a bounded sample of the ray
+    set, all host cores: a random subset when the whole set would take longer
+    than the budget, otherwise the whole set traced repeatedly until about
+    `budget_s`.  impl "port": the oracle's restatement of the reference's
+    traversal (TraverseBVH/HitMesh, hybrid:600-917) with the instance-scale
+    extension, which traces this workload's scaled instances; impl
+    "reference": the reference's own shader compiled for the CPU
+    (oracle/_ref), which has rigid instances only."""
+    O, _ = _oracle_modules()
     cores = os.cpu_count() or 1
-    fn = O.ref_closest_hit if kind == "reference" else O.closest_hit
+    if impl == "reference" and not O.ref_available():
+        raise RuntimeError("oracle/_ref is not built")
+    fn = O.ref_closest_hit if impl == "reference" else O.closest_hit
     rng = np.random.default_rng(0)
     n = min(len(rays), 65536)
     probe = rays[np.sort(rng.choice(len(rays), n, replace=False))]
@@ -171,12 +211,8 @@ def cpu_reference(scene, rays, budget_s=12.0):
     total = len(sample) * passes
     what = (f"{len(sample)} rays drawn uniformly from the step's {len(rays)}" if passes == 1 else
             f"the step's {len(rays)} rays (primary + bounce) traced {passes} times")
-    out = {"value": total / dt / 1e6, "unit": UNIT, "cores": cores, "kind": kind,
-           "sample": f"{what}, {dt:.2f} s"}
-    if kind == "reference" and np.any((scene.instances["scale"] != 0) & (scene.instances["scale"] != 1)):
-        out["note"] = ("the reference's traversal has rigid instances (no per-instance scale): it traces the same "
-                       "rays against the instances at scale 1")
-    return out
+    return {"value": total / dt / 1e6, "unit": UNIT, "cores": cores, "kind": impl,
+            "sample": f"{what}, {dt:.2f} s"}
 
 
 def measure_paths(local, width, height, frames=2):
@@ -368,40 +404,70 @@ def measure_serving(local, n_requests=16, rate=0.5, seed=7, claim_policy=1):
 
 
 def run_reference_arm(args):
+    """The reference's CPU implementation of the path on this box's host
+    cores, over the same scene bytes and the same rays as our arm, with none
+    of the library's code: the scene is packed by the reference's own scene
+    code (oracle/ref_scene.py over oracle/_ref), the rays are made by the
+    oracle, and the timed closest hit is the oracle's restatement of the
+    reference traversal (kind "port"), because the reference's own traversal
+    has rigid instances and this workload scales them.  The reference's own
+    compiled traversal is timed beside it on the rigid twin of the scene
+    (the same rays, every instance at scale 1): that figure and the port's on
+    the same rigid scene show the port runs at the reference's speed."""
     rank, world, local = dist_env()
     if rank != 0:
         return 0
-    # No library kernel on this path: the ray set is generated on the CPU by
-    # the oracle with the rules of our arm (camera rays of frame 0, closest
-    # hits with the instances' scale, one diffuse bounce per hit), so both arms
-    # trace the same 3.39M rays.  The reference's own traversal then times
-    # them; its instance transform is rigid (it has no per-instance scale), so
-    # it meets the 64 instances at scale 1.
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import _oracle as O
-    from aviatorengine2_b200 import scenes
-    scene = scenes.instanced_meshes()
+    O, R = _oracle_modules()
+    import importlib.util
+    spec_mod = importlib.util.spec_from_file_location("ae_synth", os.path.join(ROOT, "aviatorengine2_b200", "synth.py"))
+    synth = importlib.util.module_from_spec(spec_mod)
+    spec_mod.loader.exec_module(synth)
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's scene code compiled "
+                                                              "for the CPU) is not built"}), flush=True)
+        return 0
     cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    scene = R.build_instanced(synth.instanced_meshes_spec(width=args.width, height=args.height))
+    build_s = time.perf_counter() - t0
     prim = O.camera_rays(scene.config)
     hits = O.closest_hit(scene, prim, threads=cores)
     bounce, valid = O.bounce_rays(scene, scene.config, prim, hits)
-    rays = np.concatenate([prim, bounce[valid]])
-    steps = []
+    bounce = bounce[valid]
+    rays = np.concatenate([prim, bounce])
+    W, H = int(scene.config["width"]), int(scene.config["height"])
+    config = workload_config(W, H, len(prim), len(bounce), scene.triangles, len(scene.instances),
+                             scene_digest(scene), digest(prim, bounce), world)
     for _ in range(args.warmup):
         cpu_reference(scene, rays[:20000], budget_s=0.0)
+    steps = []
     base = None
     for _ in range(args.steps):
-        # about 90 s of CPU work over all steps
-        base = cpu_reference(scene, rays, budget_s=max(1.0, min(6.0, 90.0 / max(args.steps, 1))))
+        # about 60 s of CPU work over all steps
+        base = cpu_reference(scene, rays, budget_s=max(1.0, min(6.0, 60.0 / max(args.steps, 1))))
         steps.append(base["value"])
     v = float(np.median(steps))
     base["value"] = v
+    base["sample"] += f"; median of {args.steps} steps"
+    rigid = None
+    if O.ref_available():
+        twin = R.Scene(scene.objects, scene.tlas, scene.lights, scene.vertices, scene.indices, scene.blas,
+                       scene.instances.copy(), scene.config, "instanced_meshes (rigid twin)")
+        twin.instances["scale"] = 0.0
+        own = cpu_reference(twin, rays, budget_s=8.0, impl="reference")
+        port = cpu_reference(twin, rays, budget_s=8.0, impl="port")
+        rigid = {"workload": "the same rays against the rigid twin of the scene (every instance at scale 1)",
+                 "reference_own_traversal": own, "port": port, "port_over_reference": port["value"] / own["value"]}
+    native = sorted({ln.split()[-1] for ln in open("/proc/self/maps") if ln.rstrip().endswith(".so")
+                     and ROOT in ln})
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": len(rays) / (v * 1e6) * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": "instanced_meshes 1920x1080 primary+bounce closest hit",
-                       "rays_per_step": int(len(rays)), "triangles": int(scene.triangles)},
-            "cpu_baseline": base, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene and camera)",
+            "config": config, "cpu_baseline": base,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "scene_build": {"by": "the reference's MeshLibrary::Add steps, MeshBounds, BuildBVH and MeshToGPU "
+                                  "(oracle/_ref/libaeref_scene.so)", "seconds": build_s},
+            "reference_rigid_twin": rigid, "repo_native_libraries_loaded": native}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -578,6 +644,8 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu:
         cpu = cpu_reference(scene, np.concatenate([prim, bounce]))
+        cpu["note"] = ("the oracle's restatement of the reference traversal, which traces the scaled instances; "
+                       "--impl reference prints the reference's own compiled traversal on the rigid twin beside it")
 
     # Frame-level legs: rank 0 only (the other replicas would repeat them).
     paths = None
@@ -596,11 +664,9 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene and camera)",
-            "config": {"workload": f"instanced_meshes {W}x{H} primary+bounce closest hit", "variant": variant,
-                       "bounce_variant": bounce_variant,
-                       "rays_per_step": rays_step, "primary_rays": n1, "bounce_rays": n2,
-                       "triangles": int(scene.triangles), "instances": int(len(scene.instances)),
-                       "l2": "flushed before every step (512 MB write)", "parallelism": f"replicas x{world}"},
+            "config": workload_config(W, H, n1, n2, scene.triangles, len(scene.instances), scene_digest(scene),
+                                      digest(prim, bounce), world),
+            "kernels": {"camera_rays": variant, "bounce_rays": bounce_variant},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "per_step_ms": [round(t, 4) for t in times],

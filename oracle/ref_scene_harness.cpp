@@ -83,4 +83,55 @@ void aeref_box_bounds(const float *pos, const float *rot, const float *half, flo
     out[3] = b.max_x; out[4] = b.max_y; out[5] = b.max_z;
 }
 
+// MeshLibrary::Add (scene/mesh_library.h:91-159) over uint32 indices.  The
+// reference's Add reads the uint16 index list of its Mesh class, which cannot
+// address the 262,144 vertices of a 512x512 grid; its four steps are run here
+// through the reference's own helpers (AABB::Empty, SurroundPoint,
+// Surround2Points, BuildBVH) with only the index type widened.  Outputs: the
+// BLAS (capacity 2 * ni / 3 nodes, mesh-relative), the indices in leaf-slot
+// order and the local bounds (6 floats).  The vertices are appended verbatim
+// (step 1), so the caller keeps its own copy.
+int aeref_mesh_add_u32(const Vertex_GPU *v, uint32_t nv, const uint32_t *indices, uint32_t ni,
+                       BVHNode_GPU *out_blas, uint32_t *out_blas_count, uint32_t *out_indices, float *out_local) {
+    AABB local = AABB::Empty();
+    for (uint32_t i = 0; i < nv; i++) local = SurroundPoint(local, v[i].px, v[i].py, v[i].pz);
+    out_local[0] = local.min_x; out_local[1] = local.min_y; out_local[2] = local.min_z;
+    out_local[3] = local.max_x; out_local[4] = local.max_y; out_local[5] = local.max_z;
+    const uint32_t tris = ni / 3;
+    std::vector<AABB> tb;
+    tb.reserve(tris);
+    for (uint32_t t = 0; t < tris; t++) {
+        const Vertex_GPU &a = v[indices[3 * t]], &b = v[indices[3 * t + 1]], &c = v[indices[3 * t + 2]];
+        const AABB edge = Surround2Points(Point3(a.px, a.py, a.pz), Point3(b.px, b.py, b.pz));
+        tb.push_back(SurroundPoint(edge, c.px, c.py, c.pz));
+    }
+    std::vector<BVHNode_GPU> nodes;
+    std::vector<uint32_t> order;
+    BuildBVH(tb, nodes, order);
+    for (uint32_t k = 0; k < uint32_t(order.size()); k++)
+        for (int j = 0; j < 3; j++) out_indices[3 * k + j] = indices[order[k] * 3 + j];
+    std::memcpy(out_blas, nodes.data(), nodes.size() * sizeof(BVHNode_GPU));
+    *out_blas_count = uint32_t(nodes.size());
+    return 0;
+}
+
+// One mesh entity's object record through the reference's MeshToGPU
+// (scene/shapes.h:286-291 over BaseGPU, 182-214): transform (position xyz,
+// rotation xyzw) and material fields.
+int aeref_mesh_object(const float *pos, const float *rot, const float *albedo, uint32_t type, float fuzz, float ior,
+                      float emission, float density, uint32_t instance_index, Object_GPU *out) {
+    TransformComponent t;
+    t.position = Point3(pos[0], pos[1], pos[2]);
+    t.rotation = Quat<float>(rot[3], rot[0], rot[1], rot[2]);
+    Material m;
+    m.type = static_cast<MaterialType>(type);
+    m.albedo = Color(albedo[0], albedo[1], albedo[2]);
+    m.fuzz = fuzz;
+    m.ior = ior;
+    m.emission = emission;
+    m.density = density;
+    *out = MeshToGPU(t, m, instance_index);
+    return 0;
+}
+
 }  // extern "C"

@@ -1,16 +1,27 @@
 """Test-side bindings of the oracle (oracle/liboracle.so) and of the
 reference's own code compiled for the CPU pin (oracle/_ref/*.so).
 
-Only tests/, bench.py's CPU baseline and __graft_entry__.smoke() use this.
+Only tests/, bench.py's CPU baseline and reference arm, and
+__graft_entry__.smoke() use this.  It imports nothing from the library under
+test: the byte layouts come from oracle/layouts.py.
 """
 import ctypes
+import importlib.util
 import os
 
 import numpy as np
 
-from aviatorengine2_b200 import _lib
-
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _load_module(name, path):
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+_lib = _load_module("ae_oracle_layouts", os.path.join(ROOT, "oracle", "layouts.py"))
 ORACLE = os.path.join(ROOT, "oracle", "liboracle.so")
 REF_SCENE = os.path.join(ROOT, "oracle", "_ref", "libaeref_scene.so")
 REF_SHADER = os.path.join(ROOT, "oracle", "_ref", "libaeref_shader.so")
