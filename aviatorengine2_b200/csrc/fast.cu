@@ -239,6 +239,9 @@ bool build_qbvh(const ae_bvh_node *bin, uint32_t n_bin, uint32_t tri_count, std:
 }
 
 int prepare_fast(Ctx *c) {
+    // Not ready until this call accepts the current scene: every early
+    // return below leaves the optimised structures unusable.
+    c->fast_ready = false;
     if (!c->geometry_uploaded || !c->scene_uploaded) return c->fail(AE_ERR_STATE, "prepare before uploads");
     if (!c->fast) c->fast = new (std::nothrow) FastScene();
     if (!c->fast) return c->fail(AE_ERR_OOM, "fast scene");

@@ -19,7 +19,12 @@
 //   * every call on a device reuses the same array and it keeps the last
 //     call's contents.  Nothing in it needs to start at zero: each call
 //     writes every ray and every hit it reads back.  Calls that overlap on
-//     the GPU (two threads, or two contexts on one device) race on it.
+//     the GPU (two threads, or two contexts on one device) race on it;
+//   * the cached address belongs to the device's primary context: after a
+//     cudaDeviceReset (or anything else that destroys that context) it is
+//     stale, so the entry point must not be used across a reset;
+//   * the call makes the context's device current while it runs and gives
+//     the calling thread back its previous current device on return.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -54,14 +59,35 @@ extern "C" int ae_closest_hit_noalloc(ae_ctx *ctx, const ae_ray *rays, uint32_t 
         return c->fail(AE_ERR_OVERSIZE, "ae_closest_hit_noalloc takes at most %u rays per call (got %u); split the batch",
                        kMaxRays, n);
     if (!c->scene_uploaded) return c->fail(AE_ERR_STATE, "trace before ae_upload_scene");
+    if (variant == AE_VARIANT_FAST_WALK)
+        return c->fail(AE_ERR_INVALID, "AE_VARIANT_FAST_WALK reserves per-launch counters in device memory the "
+                                       "library allocates; use AE_VARIANT_FAST or AE_VARIANT_QUANT here");
     if (variant != AE_VARIANT_PLAIN && variant != AE_VARIANT_FAST && variant != AE_VARIANT_QUANT)
         return c->fail(AE_ERR_INVALID, "unknown kernel variant %d", variant);
     // The optimised structures are built (allocated) by ae_prepare_fast; this
-    // entry point only uses them when they are current.
-    if (variant != AE_VARIANT_PLAIN && !(c->fast_ready && c->fast && c->fast->scene_key == c->scene_version))
-        return c->fail(AE_ERR_STATE, "call ae_prepare_fast (which allocates) before the no-allocation entry point");
+    // entry point only uses them when they are current and were accepted for
+    // this scene (the optimised kernels have no participating media).
+    if (variant != AE_VARIANT_PLAIN) {
+        if (!(c->fast_ready && c->fast && c->fast->scene_key == c->scene_version))
+            return c->fail(AE_ERR_STATE, "call ae_prepare_fast (which allocates) before the no-allocation entry point");
+        if (c->fast->has_volumes)
+            return c->fail(AE_ERR_STATE, "participating media consume RNG in the reference's visit order; use the "
+                                         "plain kernel");
+    }
     const int dev = c->settings.device;
     if (dev < 0 || dev >= kMaxDevices) return c->fail(AE_ERR_INVALID, "device ordinal %d out of range", dev);
+    int prev_dev = -1;
+    if (cudaGetDevice(&prev_dev) != cudaSuccess) {
+        cudaGetLastError();
+        prev_dev = -1;
+    }
+    // Gives the calling thread its current device back on every return path.
+    struct RestoreDevice {
+        int dev;
+        ~RestoreDevice() {
+            if (dev >= 0) cudaSetDevice(dev);
+        }
+    } restore{prev_dev == dev ? -1 : prev_dev};
     int rc = c->cuda(cudaSetDevice(dev), "cudaSetDevice");
     if (rc) return rc;
     void *base;

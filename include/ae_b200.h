@@ -459,9 +459,15 @@ int ae_closest_hit_device(ae_ctx *ctx, const ae_ray *d_rays, uint32_t n, ae_hit 
  * through one fixed array compiled into the library, AE_NOALLOC_MAX_RAYS rays
  * (3.25 MiB, held by every GPU that loads the library until exit); larger
  * batches are refused with AE_ERR_OVERSIZE.  The first call on a device looks
- * up the array's device address and should come before any stream capture.
- * All calls on a device share the array: calls that overlap on the GPU race.
- * FAST/QUANT need ae_prepare_fast (which allocates) to have run first. */
+ * up the array's device address and should come before any stream capture;
+ * that cached address is stale after cudaDeviceReset, so do not use this
+ * entry point across a device reset.  All calls on a device share the array:
+ * calls that overlap on the GPU race.  Variants: AE_VARIANT_PLAIN, and
+ * AE_VARIANT_FAST / AE_VARIANT_QUANT once ae_prepare_fast (which allocates)
+ * has accepted the current scene (AE_ERR_STATE otherwise, also for scenes
+ * with participating media); AE_VARIANT_FAST_WALK is refused because its
+ * launch reserves counters in memory the library allocates.  The calling
+ * thread's current device is restored on return. */
 #define AE_NOALLOC_MAX_RAYS 65536u
 int ae_closest_hit_noalloc(ae_ctx *ctx, const ae_ray *rays, uint32_t n, ae_hit *hits, int variant);
 

@@ -37,7 +37,7 @@ def random_rays(n, seed):
     return r
 
 
-@pytest.mark.parametrize("variant", [_lib.VARIANT_PLAIN, _lib.VARIANT_FAST])
+@pytest.mark.parametrize("variant", [_lib.VARIANT_PLAIN, _lib.VARIANT_FAST, _lib.VARIANT_QUANT])
 def test_noalloc_matches_closest_hit_twice(variant):
     s = scenes.instanced_meshes(width=256, height=256, levels=(4, 3, 3, 2, 2), grid=64)
     with Context(256, 256) as ctx:
@@ -61,3 +61,40 @@ def test_noalloc_refuses_oversize_batches():
         rc, _ = noalloc(ctx, np.zeros(MAX_RAYS + 1, _lib.RAY), _lib.VARIANT_PLAIN)
         assert rc == -3
         assert b"at most 65536" in _lib.lib().ae_last_error(ctx.handle)
+
+
+def test_noalloc_refuses_stale_or_unprepared_structures():
+    """The optimised variants need ae_prepare_fast to have accepted the scene
+    now uploaded: before it, after a new scene upload, and after a prepare that
+    refused a scene with participating media, the call returns AE_ERR_STATE
+    (as ae_closest_hit refuses the media scene) instead of tracing with
+    structures of another scene."""
+    box = scenes.cornell_box(width=64, height=48)
+    rays = random_rays(512, 3)
+    with Context(64, 48) as ctx:
+        ctx.reserve_scene(64, 16)  # room for the media scene uploaded later
+        ctx.upload(box)
+        for v in (_lib.VARIANT_FAST, _lib.VARIANT_QUANT):
+            assert noalloc(ctx, rays, v)[0] == -7          # before ae_prepare_fast
+        ctx.prepare_fast()
+        rc, got = noalloc(ctx, rays, _lib.VARIANT_FAST)
+        assert rc == 0 and np.array_equal(got.view(np.uint8), ctx.closest_hit(rays, _lib.VARIANT_FAST).view(np.uint8))
+        ctx.upload_scene(box.objects, box.tlas, box.lights, box.instances)
+        assert noalloc(ctx, rays, _lib.VARIANT_FAST)[0] == -7  # a new scene version, not prepared yet
+        media = scenes.media_box(width=64, height=48)
+        ctx.upload(media)
+        with pytest.raises(_lib.AeError):
+            ctx.prepare_fast()                               # media are refused by the optimised forms
+        for v in (_lib.VARIANT_FAST, _lib.VARIANT_QUANT):
+            assert noalloc(ctx, rays, v)[0] == -7
+        assert noalloc(ctx, rays, _lib.VARIANT_PLAIN)[0] == 0
+
+
+def test_noalloc_refuses_walk_variant_with_its_reason():
+    s = scenes.cornell_box(width=64, height=48)
+    with Context(64, 48) as ctx:
+        ctx.upload(s)
+        ctx.prepare_fast()
+        rc, _ = noalloc(ctx, random_rays(64, 4), _lib.VARIANT_FAST_WALK)
+        assert rc == -1
+        assert b"FAST_WALK" in _lib.lib().ae_last_error(ctx.handle)
