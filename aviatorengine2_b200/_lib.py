@@ -83,7 +83,7 @@ SHAPE_SPHERE, SHAPE_QUAD, SHAPE_BOX, SHAPE_TRIANGLE, SHAPE_MESH = range(5)
 MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_DIFFUSE_LIGHT, MAT_ISOTROPIC = range(5)
 NO_TEXTURE = 0xFFFFFFFF
 MISS = 0xFFFFFFFF
-VARIANT_PLAIN, VARIANT_FAST, VARIANT_QUANT, VARIANT_FAST_WALK = 0, 1, 2, 3
+VARIANT_PLAIN, VARIANT_FAST, VARIANT_QUANT, VARIANT_FAST_WALK, VARIANT_PLAIN_WT = 0, 1, 2, 3, 4
 MODE_COMPUTE_ONLY, MODE_DEFERRED, MODE_WAVEFRONT, MODE_WAVEFRONT_PRECISION = 0, 1, 2, 3
 IMAGE_ACCUM, IMAGE_DISPLAY, IMAGE_FRAME, IMAGE_REDUCED, IMAGE_HISTORY_GEOMETRY = range(5)
 POLICY_REQUEST, POLICY_MOVE = 0, 1

@@ -20,7 +20,8 @@ Ctx::~Ctx() {
 
 int prepare_variant(Ctx *c, int variant) {
     switch (variant) {
-    case AE_VARIANT_PLAIN: return AE_OK;
+    case AE_VARIANT_PLAIN:
+    case AE_VARIANT_PLAIN_WT: return AE_OK;
     case AE_VARIANT_FAST:
     case AE_VARIANT_QUANT:
     case AE_VARIANT_FAST_WALK: return prepare_fast(c);
@@ -35,7 +36,8 @@ int closest_hit_dispatch(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, i
     if (n == 0) return AE_OK;
     if (timed && (rc = c->cuda(cudaEventRecord(c->ev0, st), "event"))) return rc;
     cudaError_t e;
-    if (variant == AE_VARIANT_PLAIN) e = launch_closest_plain(c->scene(), rays, n, hits, st);
+    if (variant == AE_VARIANT_PLAIN || variant == AE_VARIANT_PLAIN_WT)
+        e = launch_closest_plain(c->scene(), rays, n, hits, st, variant == AE_VARIANT_PLAIN_WT);
     else if (variant == AE_VARIANT_FAST_WALK) e = launch_closest_walk(c, rays, n, hits, st);
     else e = launch_closest_fast(c, rays, n, hits, variant == AE_VARIANT_QUANT, st);
     if ((rc = c->cuda(e, "closest hit launch"))) return rc;

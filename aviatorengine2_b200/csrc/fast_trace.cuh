@@ -123,53 +123,10 @@ AE_DEV bool tri_test_ref(f3 o, f3 d, float tn, float tf, const float4 &r0, const
     return !(a < 0.0f || b < 0.0f || AE_ADD(a, b) > 1.0f);
 }
 
-// Watertight test: shear the triangle into the ray's frame and decide inside
-// by the signs of the three 2D edge functions, falling back to double when an
-// edge function is exactly zero (Woop, Benthin and Wald 2013, sections 3-4).
-struct WtRay {
-    int kx, ky, kz;
-    float sx, sy, sz;
-};
-AE_DEV WtRay wt_setup(f3 d) {
-    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
-    int kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
-    int kx = kz == 2 ? 0 : kz + 1;
-    int ky = kx == 2 ? 0 : kx + 1;
-    const float dk[3] = {d.x, d.y, d.z};
-    if (dk[kz] < 0.0f) { const int tmp = kx; kx = ky; ky = tmp; }
-    WtRay w;
-    w.kx = kx; w.ky = ky; w.kz = kz;
-    w.sx = __fdiv_rn(dk[kx], dk[kz]);
-    w.sy = __fdiv_rn(dk[ky], dk[kz]);
-    w.sz = __fdiv_rn(1.0f, dk[kz]);
-    return w;
-}
-AE_DEV float comp(f3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+// The watertight test (trace_common.cuh) over a 48-byte triangle record.
 AE_DEV bool tri_test_wt(f3 o, const WtRay &W, float tn, float tf, const float4 &r0, const float4 &r1,
                         const float4 &r2, float &t, float &a, float &b) {
-    const f3 A = mk(r0.x, r0.y, r0.z) - o, B = mk(r0.w, r1.x, r1.y) - o, C = mk(r1.z, r1.w, r2.x) - o;
-    const float Az = comp(A, W.kz), Bz = comp(B, W.kz), Cz = comp(C, W.kz);
-    const float Ax = __fsub_rn(comp(A, W.kx), __fmul_rn(W.sx, Az)), Ay = __fsub_rn(comp(A, W.ky), __fmul_rn(W.sy, Az));
-    const float Bx = __fsub_rn(comp(B, W.kx), __fmul_rn(W.sx, Bz)), By = __fsub_rn(comp(B, W.ky), __fmul_rn(W.sy, Bz));
-    const float Cx = __fsub_rn(comp(C, W.kx), __fmul_rn(W.sx, Cz)), Cy = __fsub_rn(comp(C, W.ky), __fmul_rn(W.sy, Cz));
-    float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
-    float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
-    float Wv = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
-    if (U == 0.0f || V == 0.0f || Wv == 0.0f) {
-        U = float(double(Cx) * double(By) - double(Cy) * double(Bx));
-        V = float(double(Ax) * double(Cy) - double(Ay) * double(Cx));
-        Wv = float(double(Bx) * double(Ay) - double(By) * double(Ax));
-    }
-    if ((U < 0.0f || V < 0.0f || Wv < 0.0f) && (U > 0.0f || V > 0.0f || Wv > 0.0f)) return false;
-    const float det = __fadd_rn(__fadd_rn(U, V), Wv);
-    if (det == 0.0f) return false;
-    const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, __fmul_rn(W.sz, Az)), __fmul_rn(V, __fmul_rn(W.sz, Bz))),
-                              __fmul_rn(Wv, __fmul_rn(W.sz, Cz)));
-    t = __fdiv_rn(T, det);
-    if (!(t >= tn) || t > tf) return false;
-    a = __fdiv_rn(V, det);
-    b = __fdiv_rn(Wv, det);
-    return true;
+    return tri_wt(o, W, tn, tf, mk(r0.x, r0.y, r0.z), mk(r0.w, r1.x, r1.y), mk(r1.z, r1.w, r2.x), t, a, b);
 }
 
 // Relative widening of slab intervals in the optimised walk (entry scaled

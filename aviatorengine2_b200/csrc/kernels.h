@@ -22,7 +22,9 @@ struct FrameParams {
 
 FrameParams make_frame_params(const ae_config &c);
 
-cudaError_t launch_closest_plain(const DevScene &S, const ae_ray *rays, uint32_t n, ae_hit *hits, cudaStream_t st);
+// watertight: the watertight triangle test in the same walk (AE_VARIANT_PLAIN_WT).
+cudaError_t launch_closest_plain(const DevScene &S, const ae_ray *rays, uint32_t n, ae_hit *hits, cudaStream_t st,
+                                 bool watertight = false);
 cudaError_t launch_count_plain(const DevScene &S, const ae_ray *rays, uint32_t n, unsigned long long *totals,
                                cudaStream_t st);
 cudaError_t launch_render_plain(const DevScene &S, const FrameParams &F, float4 *accum, uchar4 *display,

@@ -94,6 +94,54 @@ struct DHit {
     float alpha, beta;
 };
 
+// Watertight test: shear the triangle into the ray's frame and decide inside
+// by the signs of the three 2D edge functions, falling back to double when an
+// edge function is exactly zero (Woop, Benthin and Wald 2013, sections 3-4).
+struct WtRay {
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+AE_DEV WtRay wt_setup(f3 d) {
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    int kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    const float dk[3] = {d.x, d.y, d.z};
+    if (dk[kz] < 0.0f) { const int tmp = kx; kx = ky; ky = tmp; }
+    WtRay w;
+    w.kx = kx; w.ky = ky; w.kz = kz;
+    w.sx = __fdiv_rn(dk[kx], dk[kz]);
+    w.sy = __fdiv_rn(dk[ky], dk[kz]);
+    w.sz = __fdiv_rn(1.0f, dk[kz]);
+    return w;
+}
+AE_DEV float comp(f3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+AE_DEV bool tri_wt(f3 o, const WtRay &W, float tn, float tf, f3 p0, f3 p1, f3 p2, float &t, float &a, float &b) {
+    const f3 A = p0 - o, B = p1 - o, C = p2 - o;
+    const float Az = comp(A, W.kz), Bz = comp(B, W.kz), Cz = comp(C, W.kz);
+    const float Ax = __fsub_rn(comp(A, W.kx), __fmul_rn(W.sx, Az)), Ay = __fsub_rn(comp(A, W.ky), __fmul_rn(W.sy, Az));
+    const float Bx = __fsub_rn(comp(B, W.kx), __fmul_rn(W.sx, Bz)), By = __fsub_rn(comp(B, W.ky), __fmul_rn(W.sy, Bz));
+    const float Cx = __fsub_rn(comp(C, W.kx), __fmul_rn(W.sx, Cz)), Cy = __fsub_rn(comp(C, W.ky), __fmul_rn(W.sy, Cz));
+    float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+    float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+    float Wv = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+    if (U == 0.0f || V == 0.0f || Wv == 0.0f) {
+        U = float(double(Cx) * double(By) - double(Cy) * double(Bx));
+        V = float(double(Ax) * double(Cy) - double(Ay) * double(Cx));
+        Wv = float(double(Bx) * double(Ay) - double(By) * double(Ax));
+    }
+    if ((U < 0.0f || V < 0.0f || Wv < 0.0f) && (U > 0.0f || V > 0.0f || Wv > 0.0f)) return false;
+    const float det = __fadd_rn(__fadd_rn(U, V), Wv);
+    if (det == 0.0f) return false;
+    const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, __fmul_rn(W.sz, Az)), __fmul_rn(V, __fmul_rn(W.sz, Bz))),
+                              __fmul_rn(Wv, __fmul_rn(W.sz, Cz)));
+    t = __fdiv_rn(T, det);
+    if (!(t >= tn) || t > tf) return false;
+    a = __fdiv_rn(V, det);
+    b = __fdiv_rn(Wv, det);
+    return true;
+}
+
 // HitMeshTriangle, hybrid:564-598.
 AE_DEV bool tri_ref(f3 o, f3 d, float tn, float tf, f3 p0, f3 p1, f3 p2, float &t, float &a, float &b, f3 &geo) {
     const f3 e1 = p1 - p0, e2 = p2 - p0;
@@ -119,6 +167,10 @@ AE_DEV f3 vtx_pos(const ae_vertex *v, uint32_t i) {
 }
 
 // HitMesh, hybrid:600-707 (ToLocal hybrid:534-543; pad0 scale extension).
+// WT = true swaps HitMeshTriangle for the watertight test above and keeps
+// everything else, visit order and tie rule included: the FP32-node form of
+// the precision variant's triangle test.
+template <bool WT = false>
 AE_DEV bool hit_mesh_ref(const DevScene &S, uint32_t inst_index, f3 o, f3 d, float tn, float tf, DHit &h,
                          Touch *T = nullptr) {
     if (T) T->instances++;
@@ -133,6 +185,8 @@ AE_DEV bool hit_mesh_ref(const DevScene &S, uint32_t inst_index, f3 o, f3 d, flo
         ld = ld * inv;
     }
     const f3 invd = 1.0f / ld;
+    WtRay W;
+    if (WT) W = wt_setup(ld);
     int stack[kBlasStack];
     int sp = 0;
     stack[sp++] = 0;
@@ -154,8 +208,11 @@ AE_DEV bool hit_mesh_ref(const DevScene &S, uint32_t inst_index, f3 o, f3 d, flo
                          p2 = vtx_pos(S.vertices, vbase + a2);
                 float t, a, b;
                 f3 g;
-                if (tri_ref(lo, ld, tn, closest, p0, p1, p2, t, a, b, g)) {
-                    closest = t; found = true; ba = a; bb = b; best = base; bgeo = g;
+                const bool hit = WT ? tri_wt(lo, W, tn, closest, p0, p1, p2, t, a, b)
+                                    : tri_ref(lo, ld, tn, closest, p0, p1, p2, t, a, b, g);
+                if (hit) {
+                    closest = t; found = true; ba = a; bb = b; best = base;
+                    if (!WT) bgeo = g;
                 }
             }
         } else if (sp + 2 <= kBlasStack) {
@@ -171,6 +228,10 @@ AE_DEV bool hit_mesh_ref(const DevScene &S, uint32_t inst_index, f3 o, f3 d, flo
     const float4 a1 = ld4(reinterpret_cast<const char *>(A) + 16), b1 = ld4(reinterpret_cast<const char *>(B) + 16),
                  c1 = ld4(reinterpret_cast<const char *>(C) + 16);
     const float4 a0 = ld4(A), b0 = ld4(B), c0 = ld4(C);
+    if (WT) {
+        const f3 n = cross(mk(b0.x, b0.y, b0.z) - mk(a0.x, a0.y, a0.z), mk(c0.x, c0.y, c0.z) - mk(a0.x, a0.y, a0.z));
+        bgeo = n / AE_SQRT(dot(n, n));
+    }
     const float w0 = AE_SUB(AE_SUB(1.0f, ba), bb);
     const f3 sh = normalize(w0 * mk(a0.w, a1.x, a1.y) + ba * mk(b0.w, b1.x, b1.y) + bb * mk(c0.w, c1.x, c1.y));
     f3 geo = bgeo;
@@ -341,6 +402,8 @@ AE_DEV bool hit_volume_ref(const ae_object *obj, uint32_t shape, f3 o, f3 d, flo
 }
 
 // TraverseBVH, hybrid:862-917, and HitObject dispatch, hybrid:827-856.
+// WT selects the watertight triangle test inside meshes (hit_mesh_ref).
+template <bool WT = false>
 AE_DEV bool traverse_ref(const DevScene &S, f3 o, f3 d, float time, float tn, DHit &out, uint32_t &seed,
                          Touch *T = nullptr) {
     if (S.n_nodes == 0) return false;
@@ -368,7 +431,7 @@ AE_DEV bool traverse_ref(const DevScene &S, f3 o, f3 d, float time, float tn, DH
                 else if (hd.shape == AE_SHAPE_TRIANGLE) hit = hit_planar_ref(obj, true, o, d, tn, tf, h);
                 else if (hd.shape == AE_SHAPE_MESH) {
                     const uint32_t inst = __float_as_uint(ld4(reinterpret_cast<const char *>(obj) + 80).z);
-                    hit = hit_mesh_ref(S, inst, o, d, tn, tf, h, T);
+                    hit = hit_mesh_ref<WT>(S, inst, o, d, tn, tf, h, T);
                 } else hit = hit_box_ref(obj, o, d, tn, tf, h);
                 if (hit) {
                     tf = h.t;

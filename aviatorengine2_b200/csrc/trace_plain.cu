@@ -11,6 +11,8 @@ namespace ae {
 // ---------------------------------------------------------------------------
 // Closest hit over a ray batch
 // ---------------------------------------------------------------------------
+// WT: the watertight triangle test in the same walk (AE_VARIANT_PLAIN_WT).
+template <bool WT>
 __global__ void __launch_bounds__(128) k_closest_plain(DevScene S, const ae_ray *__restrict__ rays, uint32_t n,
                                                        ae_hit *__restrict__ hits) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -21,7 +23,7 @@ __global__ void __launch_bounds__(128) k_closest_plain(DevScene S, const ae_ray 
     DHit h;
     ae_hit out;
     out.t = 0.0f; out.alpha = 0.0f; out.beta = 0.0f; out.object = AE_MISS; out.prim = AE_MISS;
-    if (traverse_ref(S, mk(r0.x, r0.y, r0.z), mk(r1.x, r1.y, r1.z), r1.w, r0.w, h, seed)) {
+    if (traverse_ref<WT>(S, mk(r0.x, r0.y, r0.z), mk(r1.x, r1.y, r1.z), r1.w, r0.w, h, seed)) {
         out.t = h.t; out.alpha = h.alpha; out.beta = h.beta; out.object = h.slot; out.prim = h.prim;
     }
     hits[i] = out;
@@ -139,9 +141,11 @@ __global__ void __launch_bounds__(128) k_render_plain(DevScene S, FrameParams F,
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
-cudaError_t launch_closest_plain(const DevScene &S, const ae_ray *rays, uint32_t n, ae_hit *hits, cudaStream_t st) {
+cudaError_t launch_closest_plain(const DevScene &S, const ae_ray *rays, uint32_t n, ae_hit *hits, cudaStream_t st,
+                                 bool watertight) {
     if (n == 0) return cudaSuccess;
-    k_closest_plain<<<(n + 127) / 128, 128, 0, st>>>(S, rays, n, hits);
+    if (watertight) k_closest_plain<true><<<(n + 127) / 128, 128, 0, st>>>(S, rays, n, hits);
+    else k_closest_plain<false><<<(n + 127) / 128, 128, 0, st>>>(S, rays, n, hits);
     return cudaGetLastError();
 }
 

@@ -348,8 +348,10 @@ typedef struct ae_settings {
  * FAST is the optimised closest-hit (ordered traversal, packed triangles);
  * QUANT adds 8-bit child bounds and the watertight triangle test; FAST_WALK
  * is FAST's walk run one step at a time per thread on a persistent grid (the
- * same hits; for incoherent sets such as bounce rays). */
-enum { AE_VARIANT_PLAIN = 0, AE_VARIANT_FAST = 1, AE_VARIANT_QUANT = 2, AE_VARIANT_FAST_WALK = 3 };
+ * same hits; for incoherent sets such as bounce rays); PLAIN_WT is PLAIN's
+ * walk over the FP32 binary BVH with QUANT's watertight triangle test - the
+ * FP32-node form QUANT's 8-bit nodes are checked against (identical hits). */
+enum { AE_VARIANT_PLAIN = 0, AE_VARIANT_FAST = 1, AE_VARIANT_QUANT = 2, AE_VARIANT_FAST_WALK = 3, AE_VARIANT_PLAIN_WT = 4 };
 
 /* Render modes for ae_render_frame.  AE_MODE_WAVEFRONT_PRECISION is the
  * wavefront tracer in the precision form: watertight triangle test, FP16
