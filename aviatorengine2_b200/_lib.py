@@ -130,6 +130,7 @@ SIGNATURES = {
     "ae_build_gbuffer": (_I, [_P]),
     "ae_read_image": (_I, [_P, _I, _P, ctypes.c_size_t]),
     "ae_image_error": (_I, [_P, _I, _P, ctypes.c_double, _P]),
+    "ae_image_error_pixels": (_I, [_P, _I, _P, _U32, _P, ctypes.c_double, _P]),
     "ae_closest_hit": (_I, [_P, _P, _U32, _P, _I]),
     "ae_closest_hit_device": (_I, [_P, _P, _U32, _P, _I]),
     "ae_closest_hit_noalloc": (_I, [_P, _P, _U32, _P, _I]),
@@ -137,6 +138,8 @@ SIGNATURES = {
     "ae_camera_rays": (_I, [_P, _P]),
     "ae_bounce_rays": (_I, [_P, _P, _P, _U32, _P, _P]),
     "ae_trace_counters": (_I, [_P, _P, _U32, _P]),
+    "ae_trace_counters_variant": (_I, [_P, _P, _U32, _I, _P]),
+    "ae_path_counters": (_I, [_P, _P]),
     "ae_wavefront_info": (_I, [_P, _P, _P, _P, _P]),
     "ae_synchronize": (_I, [_P]),
     "ae_last_kernel_ms": (_I, [_P, _P]),

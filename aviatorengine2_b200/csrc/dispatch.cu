@@ -51,17 +51,51 @@ int closest_hit_dispatch(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, i
 
 }  // namespace ae
 
-extern "C" int ae_trace_counters(ae_ctx *ctx, const ae_ray *d_rays, uint32_t n, uint64_t *counters) {
-    ae::Ctx *c = reinterpret_cast<ae::Ctx *>(ctx);
-    if (!c || !counters || (n && !d_rays)) return AE_ERR_INVALID;
+static int trace_counters(ae::Ctx *c, const ae_ray *d_rays, uint32_t n, int variant, uint64_t *counters) {
     if (!c->scene_uploaded) return c->fail(AE_ERR_STATE, "counters before ae_upload_scene");
+    if (variant != AE_VARIANT_PLAIN && variant != AE_VARIANT_FAST && variant != AE_VARIANT_QUANT)
+        return c->fail(AE_ERR_INVALID, "touch counters exist for PLAIN, FAST and QUANT (got variant %d)", variant);
+    int rc = ae::prepare_variant(c, variant);
+    if (rc) return rc;
     ae::DevBuf<unsigned long long> tot;
     if (tot.reserve(6)) return c->fail(AE_ERR_OOM, "counter buffer");
-    int rc = c->cuda(cudaMemsetAsync(tot.ptr, 0, 6 * sizeof(unsigned long long), c->stream), "memset");
-    if (!rc) rc = c->cuda(ae::launch_count_plain(c->scene(), d_rays, n, tot.ptr, c->stream), "count launch");
+    rc = c->cuda(cudaMemsetAsync(tot.ptr, 0, 6 * sizeof(unsigned long long), c->stream), "memset");
+    if (!rc)
+        rc = c->cuda(variant == AE_VARIANT_PLAIN
+                         ? ae::launch_count_plain(c->scene(), d_rays, n, tot.ptr, c->stream)
+                         : ae::launch_count_fast(c, d_rays, n, variant == AE_VARIANT_QUANT, tot.ptr, c->stream),
+                     "count launch");
     c->launches++;
     if (!rc) rc = c->cuda(cudaMemcpyAsync(counters, tot.ptr, 6 * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream), "copy");
     if (!rc) rc = c->cuda(cudaStreamSynchronize(c->stream), "counters");
+    return rc;
+}
+
+extern "C" int ae_trace_counters(ae_ctx *ctx, const ae_ray *d_rays, uint32_t n, uint64_t *counters) {
+    ae::Ctx *c = reinterpret_cast<ae::Ctx *>(ctx);
+    if (!c || !counters || (n && !d_rays)) return AE_ERR_INVALID;
+    return trace_counters(c, d_rays, n, AE_VARIANT_PLAIN, counters);
+}
+
+extern "C" int ae_trace_counters_variant(ae_ctx *ctx, const ae_ray *d_rays, uint32_t n, int variant,
+                                         uint64_t *counters) {
+    ae::Ctx *c = reinterpret_cast<ae::Ctx *>(ctx);
+    if (!c || !counters || (n && !d_rays)) return AE_ERR_INVALID;
+    return trace_counters(c, d_rays, n, variant, counters);
+}
+
+extern "C" int ae_path_counters(ae_ctx *ctx, uint64_t *counters) {
+    ae::Ctx *c = reinterpret_cast<ae::Ctx *>(ctx);
+    if (!c || !counters) return AE_ERR_INVALID;
+    if (!c->scene_uploaded || !c->geometry_uploaded) return c->fail(AE_ERR_STATE, "path counters before the uploads");
+    const ae::FrameParams F = ae::make_frame_params(c->config);
+    ae::DevBuf<unsigned long long> tot;
+    if (tot.reserve(7)) return c->fail(AE_ERR_OOM, "counter buffer");
+    int rc = c->cuda(cudaMemsetAsync(tot.ptr, 0, 7 * sizeof(unsigned long long), c->stream), "memset");
+    if (!rc) rc = c->cuda(ae::launch_count_paths(c->scene(), F, tot.ptr, c->stream), "count launch");
+    c->launches++;
+    if (!rc) rc = c->cuda(cudaMemcpyAsync(counters, tot.ptr, 7 * sizeof(uint64_t), cudaMemcpyDeviceToHost, c->stream), "copy");
+    if (!rc) rc = c->cuda(cudaStreamSynchronize(c->stream), "path counters");
     return rc;
 }
 

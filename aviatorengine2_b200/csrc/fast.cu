@@ -401,6 +401,30 @@ __global__ void __launch_bounds__(128, 8) k_closest_fast(DevScene S, FastView V,
     hits[i] = out;
 }
 
+// The optimised walk with its touches counted (outside timed regions): per
+// ray set, TLAS nodes, object metadata records, instance records, wide BLAS
+// nodes and triangle records fetched, summed in 64-bit.
+template <bool WT>
+__global__ void __launch_bounds__(128) k_count_fast(DevScene S, FastView V, const ae_ray *__restrict__ rays,
+                                                    uint32_t n, unsigned long long *__restrict__ totals) {
+    extern __shared__ uint2 stk[];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    Touch T = {0, 0, 0, 0, 0, 0, 0};
+    if (i < n) {
+        const float4 *rp = reinterpret_cast<const float4 *>(rays + i);
+        const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
+        const Best best = closest_fast<WT>(S, V, mk(r0.x, r0.y, r0.z), mk(r1.x, r1.y, r1.z), r0.w, r1.w, stk,
+                                           threadIdx.x, blockDim.x, &T);
+        T.winners = best.object != AE_MISS ? 1u : 0u;
+    }
+    const uint32_t v[6] = {T.tlas, T.objects, T.instances, T.blas, T.tris, T.winners};
+    for (int k = 0; k < 6; k++) {
+        unsigned long long x = v[k];
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+        if ((threadIdx.x & 31) == 0 && x) atomicAdd(totals + k, x);
+    }
+}
+
 // The same closest hit on the step-wise Walker, for incoherent ray sets
 // (bounce rays): a persistent grid where each lane starts its next ray as soon
 // as one finishes.  Bit-identical hits.
@@ -535,6 +559,23 @@ cudaError_t launch_closest_walk(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *
     cudaError_t e = cudaMemsetAsync(next, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     k_closest_walk<true><<<grid, threads, smem, st>>>(c->scene(), V, rays, n, hits, next);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count_fast(Ctx *c, const ae_ray *rays, uint32_t n, bool quant, unsigned long long *totals,
+                              cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    FastScene &F = *c->fast;
+    FastView V{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr};
+    const int threads = 128;
+    const size_t smem = size_t(kSharedStack) * threads * sizeof(uint2);
+    if (quant) {
+        cudaFuncSetAttribute(k_count_fast<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        k_count_fast<true><<<(n + threads - 1) / threads, threads, smem, st>>>(c->scene(), V, rays, n, totals);
+    } else {
+        cudaFuncSetAttribute(k_count_fast<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        k_count_fast<false><<<(n + threads - 1) / threads, threads, smem, st>>>(c->scene(), V, rays, n, totals);
+    }
     return cudaGetLastError();
 }
 

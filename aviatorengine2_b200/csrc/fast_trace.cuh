@@ -175,9 +175,11 @@ AE_DEV void child_hits(const QNode *nodep, f3 o, f3 inv, float tn, float tf, flo
 // value of the same sign, so products stay finite (no 0 * inf).
 AE_DEV float slab_inv(float x) { return fabsf(x) > 1e-20f ? 1.0f / x : copysignf(1e20f, x); }
 
+// T (optional): touch counters - wide nodes in `blas`, 48-byte triangle
+// records in `tris`.
 template <bool WT, int SS = kSharedStack>
 AE_DEV void trace_mesh(const FastView &V, const FastInst &I, uint32_t slot, uint64_t orank, f3 o, f3 d, float tn,
-                       Best &best, uint2 *stk, int tid, int nthreads) {
+                       Best &best, uint2 *stk, int tid, int nthreads, Touch *T = nullptr) {
     // ToLocal (hybrid:534-543) exactly as the reference, so the local ray and
     // every triangle's t are bit-identical to the plain kernel's.
     f3 lo = quat_rotate(-I.qx, -I.qy, -I.qz, I.qw, o - mk(I.px, I.py, I.pz));
@@ -197,6 +199,7 @@ AE_DEV void trace_mesh(const FastView &V, const FastInst &I, uint32_t slot, uint
     for (;;) {
         if (cur & kLeafBit) {
             const uint32_t first = leaf_first(cur), cnt = leaf_count(cur);
+            if (T) T->tris += cnt;
             for (uint32_t k = 0; k < cnt; k++) {
                 const uint32_t s = first + k;
                 const float4 *r = tris + size_t(s) * 3;
@@ -213,6 +216,7 @@ AE_DEV void trace_mesh(const FastView &V, const FastInst &I, uint32_t slot, uint
         } else {
             float tm[4];
             uint32_t ch[4];
+            if (T) T->blas++;
             child_hits(V.nodes + cur, lo, inv, tn, best.t, tm, ch);
             // Sort the four (distance, child) pairs, nearest first.
 #define AE_SWAP(i, j)                                            \
@@ -257,10 +261,11 @@ AE_DEV void trace_mesh(const FastView &V, const FastInst &I, uint32_t slot, uint
 // Closest hit of one ray over the whole scene: TLAS (the reference's binary
 // nodes, nearest child first), analytic objects by the reference intersectors,
 // meshes by the 4-wide quantised BLAS.  `stk` is this thread's column of the
-// block's shared-memory stack.
+// block's shared-memory stack.  T (optional) counts the touches: TLAS nodes,
+// object metadata records, instance records, wide BLAS nodes, triangle records.
 template <bool WT, int SS = kSharedStack>
 AE_DEV Best closest_fast(const DevScene &S, const FastView &V, f3 o, f3 d, float tn, float time, uint2 *stk, int tid,
-                         int nt) {
+                         int nt, Touch *T = nullptr) {
     Best best;
     best.t = kFarStart; best.alpha = 0.0f; best.beta = 0.0f;
     best.object = AE_MISS; best.prim = AE_MISS; best.orank = 0; best.lrank = 0;
@@ -271,6 +276,7 @@ AE_DEV Best closest_fast(const DevScene &S, const FastView &V, f3 o, f3 d, float
     float tdist[kTlasStack];
     int sp = 0;
     NodeBox nb = load_node(S.tlas, 0);
+    if (T) T->tlas++;
     bool live = slab_ref(o, rinv, nb.lo, nb.hi, tn, kFarStart);
     while (live) {
         if (nb.count > 0) {
@@ -280,14 +286,16 @@ AE_DEV Best closest_fast(const DevScene &S, const FastView &V, f3 o, f3 d, float
                 const uint64_t orank = (uint64_t(~first) << 32) | slot;
                 const uint4 m = __ldg(V.meta + slot);
                 const uint32_t shape = m.x & 0xff;
+                if (T) T->objects++;
                 if (shape == AE_SHAPE_MESH) {
+                    if (T) T->instances++;
                     const float4 *ip = reinterpret_cast<const float4 *>(V.inst + m.y);
                     const float4 a = __ldg(ip), b = __ldg(ip + 1), c = __ldg(ip + 2);
                     FastInst I;
                     I.px = a.x; I.py = a.y; I.pz = a.z; I.scale = a.w;
                     I.qx = b.x; I.qy = b.y; I.qz = b.z; I.qw = b.w;
                     I.root = __float_as_uint(c.x); I.tri_base = __float_as_uint(c.y);
-                    trace_mesh<WT, SS>(V, I, slot, orank, o, d, tn, best, stk, tid, nt);
+                    trace_mesh<WT, SS>(V, I, slot, orank, o, d, tn, best, stk, tid, nt, T);
                 } else {
                     DHit h;
                     const ae_object *obj = S.objects + slot;
@@ -304,6 +312,7 @@ AE_DEV Best closest_fast(const DevScene &S, const FastView &V, f3 o, f3 d, float
             }
         } else {
             const NodeBox L = load_node(S.tlas, uint32_t(nb.left)), R = load_node(S.tlas, uint32_t(nb.right));
+            if (T) T->tlas += 2;
             const f3 lt0 = (L.lo - o) * inv, lt1 = (L.hi - o) * inv;
             const f3 rt0 = (R.lo - o) * inv, rt1 = (R.hi - o) * inv;
             const float lmin = fmaxf(fmaxf(fminf(lt0.x, lt1.x), fminf(lt0.y, lt1.y)), fmaxf(fminf(lt0.z, lt1.z), tn));

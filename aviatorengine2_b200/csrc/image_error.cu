@@ -44,12 +44,15 @@ __device__ ErrPartial block_reduce(ErrPartial v) {
     return v;
 }
 
+// Pixel p of the comparison is image pixel p, or (xy[2p], xy[2p+1]) when a
+// pixel list is given (coordinates checked on the host).
 __global__ void __launch_bounds__(kErrThreads) k_image_error(const float4 *__restrict__ img,
                                                              const double *__restrict__ ref, size_t n, double eps,
+                                                             const uint32_t *__restrict__ xy, uint32_t width,
                                                              ErrPartial *partials) {
     ErrPartial acc{0.0, 0.0, 0.0, 0.0};
     for (size_t p = size_t(blockIdx.x) * kErrThreads + threadIdx.x; p < n; p += size_t(gridDim.x) * kErrThreads) {
-        const float4 x = img[p];
+        const float4 x = img[xy ? size_t(xy[2 * p + 1]) * width + xy[2 * p] : p];
         const double xs[3] = {double(x.x), double(x.y), double(x.z)};
         for (int k = 0; k < 3; k++) {
             const double r = ref[4 * p + k];
@@ -88,7 +91,8 @@ __global__ void __launch_bounds__(kErrThreads) k_image_error_final(const ErrPart
 
 using namespace ae;
 
-extern "C" int ae_image_error(ae_ctx *ctx, int which, const double *reference, double eps, double *out4) {
+static int image_error(ae_ctx *ctx, int which, const uint32_t *xy, uint32_t n_px, const double *reference,
+                       double eps, double *out4) {
     Ctx *c = reinterpret_cast<Ctx *>(ctx);
     if (!c) return AE_ERR_INVALID;
     if (!reference || !out4) return c->fail(AE_ERR_INVALID, "null reference or output");
@@ -97,22 +101,36 @@ extern "C" int ae_image_error(ae_ctx *ctx, int which, const double *reference, d
     if (which == AE_IMAGE_ACCUM) img = c->accum.ptr;
     else if (which == AE_IMAGE_FRAME) img = c->frame.ptr;
     else return c->fail(AE_ERR_INVALID, "image error compares AE_IMAGE_ACCUM or AE_IMAGE_FRAME");
-    const size_t n = size_t(c->settings.width) * c->settings.height;
-    if (!img || n == 0) return c->fail(AE_ERR_STATE, "no image yet");
+    const uint32_t W = c->settings.width, H = c->settings.height;
+    const size_t n = xy ? size_t(n_px) : size_t(W) * H;
+    if (!img || size_t(W) * H == 0) return c->fail(AE_ERR_STATE, "no image yet");
+    if (xy) {
+        if (n_px == 0) return c->fail(AE_ERR_INVALID, "empty pixel list");
+        for (uint32_t i = 0; i < n_px; i++)
+            if (xy[2 * i] >= W || xy[2 * i + 1] >= H)
+                return c->fail(AE_ERR_INVALID, "pixel %u (%u, %u) outside the %ux%u image", i, xy[2 * i], xy[2 * i + 1],
+                               W, H);
+    }
     int rc = c->cuda(cudaSetDevice(c->settings.device), "cudaSetDevice");
     if (rc) return rc;
-    // Scratch for the reference copy, the partials and the result.
+    // Scratch for the reference copy, the pixel list, the partials and the result.
     const size_t ref_bytes = n * 4 * sizeof(double);
+    const size_t xy_bytes = xy ? ((n * 2 * sizeof(uint32_t) + 15) / 16) * 16 : 0;
     const size_t part_bytes = kErrBlocks * sizeof(ErrPartial);
     void *scratch = nullptr;
-    if ((rc = c->cuda(cudaMalloc(&scratch, ref_bytes + part_bytes + 4 * sizeof(double)), "image error scratch")))
+    if ((rc = c->cuda(cudaMalloc(&scratch, ref_bytes + xy_bytes + part_bytes + 4 * sizeof(double)),
+                      "image error scratch")))
         return rc;
     double *d_ref = static_cast<double *>(scratch);
-    ErrPartial *d_part = reinterpret_cast<ErrPartial *>(static_cast<char *>(scratch) + ref_bytes);
-    double *d_out = reinterpret_cast<double *>(static_cast<char *>(scratch) + ref_bytes + part_bytes);
+    uint32_t *d_xy = xy ? reinterpret_cast<uint32_t *>(static_cast<char *>(scratch) + ref_bytes) : nullptr;
+    ErrPartial *d_part = reinterpret_cast<ErrPartial *>(static_cast<char *>(scratch) + ref_bytes + xy_bytes);
+    double *d_out = reinterpret_cast<double *>(static_cast<char *>(scratch) + ref_bytes + xy_bytes + part_bytes);
     rc = c->cuda(cudaMemcpyAsync(d_ref, reference, ref_bytes, cudaMemcpyHostToDevice, c->stream), "upload reference");
+    if (!rc && xy)
+        rc = c->cuda(cudaMemcpyAsync(d_xy, xy, n * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream),
+                     "upload pixel list");
     if (!rc) {
-        k_image_error<<<kErrBlocks, kErrThreads, 0, c->stream>>>(img, d_ref, n, eps, d_part);
+        k_image_error<<<kErrBlocks, kErrThreads, 0, c->stream>>>(img, d_ref, n, eps, d_xy, W, d_part);
         k_image_error_final<<<1, kErrThreads, 0, c->stream>>>(d_part, kErrBlocks, double(n) * 3.0, d_out);
         c->launches += 2;
         rc = c->cuda(cudaGetLastError(), "image error launch");
@@ -121,4 +139,14 @@ extern "C" int ae_image_error(ae_ctx *ctx, int which, const double *reference, d
     if (!rc) rc = c->cuda(cudaStreamSynchronize(c->stream), "image error");
     cudaFree(scratch);
     return rc;
+}
+
+extern "C" int ae_image_error(ae_ctx *ctx, int which, const double *reference, double eps, double *out4) {
+    return image_error(ctx, which, nullptr, 0, reference, eps, out4);
+}
+
+extern "C" int ae_image_error_pixels(ae_ctx *ctx, int which, const uint32_t *xy, uint32_t n_px,
+                                     const double *reference, double eps, double *out4) {
+    if (ctx && !xy) return reinterpret_cast<Ctx *>(ctx)->fail(AE_ERR_INVALID, "null pixel list");
+    return image_error(ctx, which, xy, n_px, reference, eps, out4);
 }

@@ -27,6 +27,7 @@ cudaError_t launch_closest_plain(const DevScene &S, const ae_ray *rays, uint32_t
                                  bool watertight = false);
 cudaError_t launch_count_plain(const DevScene &S, const ae_ray *rays, uint32_t n, unsigned long long *totals,
                                cudaStream_t st);
+cudaError_t launch_count_paths(const DevScene &S, const FrameParams &F, unsigned long long *totals, cudaStream_t st);
 cudaError_t launch_render_plain(const DevScene &S, const FrameParams &F, float4 *accum, uchar4 *display,
                                 float4 *frame, cudaStream_t st);
 

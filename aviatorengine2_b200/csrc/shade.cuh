@@ -71,7 +71,9 @@ AE_DEV void sample_light(const ae_object *L, uint32_t shape, f3 from, f3 &p, flo
 }
 
 // CalculateDirectLight, hybrid:1122-1212.
-AE_DEV f3 direct_light(const DevScene &S, const DHit &h, f3 surf_albedo, float time, uint32_t &seed) {
+// T (optional): touch counters of the shadow traversals.
+AE_DEV f3 direct_light(const DevScene &S, const DHit &h, f3 surf_albedo, float time, uint32_t &seed,
+                       Touch *T = nullptr) {
     f3 acc = splat(0.0f);
     for (uint32_t i = 0; i < S.n_lights; i++) {
         const ae_object *L = S.objects + __ldg(S.lights + i);
@@ -90,7 +92,7 @@ AE_DEV f3 direct_light(const DevScene &S, const DHit &h, f3 surf_albedo, float t
         bool occluded = false;
         for (int k = 0; k < 4; k++) {
             DHit sh;
-            if (!traverse_ref(S, so, sd, time, 0.001f, sh, seed)) break;
+            if (!traverse_ref(S, so, sd, time, 0.001f, sh, seed, T)) break;
             if (sh.t >= AE_SUB(distance(lp, so), 0.001f)) break;
             const uint32_t mt = load_head(S.objects + sh.slot).material;
             if (mt == AE_MAT_DIFFUSE_LIGHT) break;

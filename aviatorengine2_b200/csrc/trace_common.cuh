@@ -28,6 +28,7 @@ constexpr float kFarStart = 1000000.0f;  // hybrid:869
 // TLAS nodes, object records, instance records, BLAS nodes, triangles, winners.
 struct Touch {
     uint32_t tlas, objects, instances, blas, tris, winners;
+    uint32_t rays;  // traversals started (TraverseBVH calls)
 };
 
 struct DevScene {
@@ -406,6 +407,7 @@ AE_DEV bool hit_volume_ref(const ae_object *obj, uint32_t shape, f3 o, f3 d, flo
 template <bool WT = false>
 AE_DEV bool traverse_ref(const DevScene &S, f3 o, f3 d, float time, float tn, DHit &out, uint32_t &seed,
                          Touch *T = nullptr) {
+    if (T) T->rays++;
     if (S.n_nodes == 0) return false;
     const f3 inv = 1.0f / d;
     int stack[kTlasStack];

@@ -34,7 +34,7 @@ __global__ void __launch_bounds__(128) k_closest_plain(DevScene S, const ae_ray 
 __global__ void __launch_bounds__(128) k_count_plain(DevScene S, const ae_ray *__restrict__ rays, uint32_t n,
                                                      unsigned long long *__restrict__ totals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    Touch T = {0, 0, 0, 0, 0, 0};
+    Touch T = {0, 0, 0, 0, 0, 0, 0};
     if (i < n) {
         const float4 *rp = reinterpret_cast<const float4 *>(rays + i);
         const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
@@ -53,12 +53,13 @@ __global__ void __launch_bounds__(128) k_count_plain(DevScene S, const ae_ray *_
 // ---------------------------------------------------------------------------
 // Compute-only path tracer (hybrid:1230-1404)
 // ---------------------------------------------------------------------------
-// ColorRay, hybrid:1230-1325.
-AE_DEV f3 color_ray(const DevScene &S, const FrameParams &F, f3 o, f3 d, float time, uint32_t &seed) {
+// ColorRay, hybrid:1230-1325.  T (optional) counts every traversal's touches.
+AE_DEV f3 color_ray(const DevScene &S, const FrameParams &F, f3 o, f3 d, float time, uint32_t &seed,
+                    Touch *T = nullptr) {
     f3 thr = splat(1.0f), acc = splat(0.0f);
     for (uint32_t b = 0; b < F.depth; b++) {
         DHit h;
-        if (!traverse_ref(S, o, d, time, 0.001f, h, seed)) {
+        if (!traverse_ref(S, o, d, time, 0.001f, h, seed, T)) {
             acc = acc + thr * F.sky;
             break;
         }
@@ -70,7 +71,7 @@ AE_DEV f3 color_ray(const DevScene &S, const FrameParams &F, f3 o, f3 d, float t
         // SurfaceAlbedo (textured when the material has a layer).
         const f3 alb = m.type != AE_MAT_DIELECTRIC ? surface_albedo(S, h, m, o, d) : m.albedo;
         if (m.type == AE_MAT_LAMBERTIAN) {
-            f3 dl = direct_light(S, h, alb, time, seed);
+            f3 dl = direct_light(S, h, alb, time, seed, T);
             const float luma = maxc(dl);
             if (luma > 8.0f) dl = dl * AE_DIV(8.0f, luma);
             acc = acc + thr * dl;
@@ -138,6 +139,44 @@ __global__ void __launch_bounds__(128) k_render_plain(DevScene S, FrameParams F,
     display[px] = display_texel(acc, F.exposure);
 }
 
+// The frame's paths (main's camera ray and ColorRay, spp samples per pixel)
+// with every traversal's touches counted - the algorithmic traffic per path
+// of the reference's megakernel.  Writes no image; outside timed regions.
+__global__ void __launch_bounds__(128) k_count_paths(DevScene S, FrameParams F,
+                                                     unsigned long long *__restrict__ totals) {
+    const uint32_t x = blockIdx.x * 16 + (threadIdx.x & 15);
+    const uint32_t y = blockIdx.y * 8 + (threadIdx.x >> 4);
+    Touch T = {0, 0, 0, 0, 0, 0, 0};
+    if (x < F.width && y < F.height) {
+        uint32_t seed = x + y * F.width + F.batch * F.width * F.height + 1u;
+        for (uint32_t s = 0; s < F.spp; s++) {
+            const float jx = AE_SUB(rng_next(seed), 0.5f);
+            const float jy = AE_SUB(rng_next(seed), 0.5f);
+            const f3 tgt = F.pixel0 + AE_ADD(AE_U2F(x), jx) * F.pixel_u + AE_ADD(AE_U2F(y), jy) * F.pixel_v;
+            f3 o = F.source;
+            if (F.defocus_angle > 0.0f) {
+                float px_, py_;
+                for (;;) {
+                    const float a = rng_next(seed), b = rng_next(seed);
+                    px_ = AE_SUB(AE_MUL(a, 2.0f), 1.0f);
+                    py_ = AE_SUB(AE_MUL(b, 2.0f), 1.0f);
+                    if (length(mk(px_, py_, 0.0f)) < 1.0f) break;
+                }
+                o = F.source + px_ * F.defocus_u + py_ * F.defocus_v;
+            }
+            const f3 d = normalize(tgt - o);
+            const float time = rng_next(seed);
+            color_ray(S, F, o, d, time, seed, &T);
+        }
+    }
+    const uint32_t v[7] = {T.tlas, T.objects, T.instances, T.blas, T.tris, T.winners, T.rays};
+    for (int k = 0; k < 7; k++) {
+        unsigned long long c = v[k];
+        for (int off = 16; off > 0; off >>= 1) c += __shfl_down_sync(0xffffffffu, c, off);
+        if ((threadIdx.x & 31) == 0 && c) atomicAdd(totals + k, c);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
@@ -153,6 +192,12 @@ cudaError_t launch_count_plain(const DevScene &S, const ae_ray *rays, uint32_t n
                                cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     k_count_plain<<<(n + 127) / 128, 128, 0, st>>>(S, rays, n, totals);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count_paths(const DevScene &S, const FrameParams &F, unsigned long long *totals, cudaStream_t st) {
+    dim3 grid((F.width + 15) / 16, (F.height + 7) / 8);
+    k_count_paths<<<grid, 128, 0, st>>>(S, F, totals);
     return cudaGetLastError();
 }
 

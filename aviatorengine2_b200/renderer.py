@@ -211,6 +211,16 @@ class Context:
         self._chk(lib().ae_image_error(self._h, which, ptr(ref), eps, ptr(out)))
         return {"mre": out[0], "mae": out[1], "max": out[2], "rmse": out[3]}
 
+    def image_error_pixels(self, pixels, reference, which=_lib.IMAGE_ACCUM, eps=1e-3):
+        """image_error over a pixel subset: `pixels` (n, 2) as (x, y),
+        `reference` (n, 4) float64 in the same order."""
+        xy = np.ascontiguousarray(pixels, dtype=np.uint32).reshape(-1, 2)
+        ref = np.ascontiguousarray(reference, dtype=np.float64).reshape(-1, 4)
+        assert len(ref) == len(xy), (ref.shape, xy.shape)
+        out = np.zeros(4, np.float64)
+        self._chk(lib().ae_image_error_pixels(self._h, which, ptr(xy), len(xy), ptr(ref), eps, ptr(out)))
+        return {"mre": out[0], "mae": out[1], "max": out[2], "rmse": out[3]}
+
     def prepare_fast(self):
         self._chk(lib().ae_prepare_fast(self._h))
 

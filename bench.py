@@ -215,7 +215,74 @@ def cpu_reference(scene, rays, budget_s=12.0, impl="port"):
             "sample": f"{what}, {dt:.2f} s"}
 
 
-def measure_paths(local, width, height, frames=2):
+EDGE_EPS = 1e-3  # minimum barycentric of a hit counted as lying on a triangle edge
+MRE_EPS = 1e-3
+
+
+def classify_ids(ref, wt):
+    """Primary-ray ID disagreements between the reference's triangle test
+    (hybrid:564-598) and the watertight one, split into rays whose hit (on
+    either side) lies within EDGE_EPS of an edge - where the reference's
+    test has cracks - and the rest."""
+    from aviatorengine2_b200 import _lib
+
+    def min_bary(h):
+        a, b = h["alpha"].astype(np.float64), h["beta"].astype(np.float64)
+        return np.where(h["prim"] != _lib.MISS, np.minimum(np.minimum(a, b), 1.0 - a - b), np.inf)
+
+    dis = (ref["object"] != wt["object"]) | (ref["prim"] != wt["prim"])
+    edge = (min_bary(ref) < EDGE_EPS) | (min_bary(wt) < EDGE_EPS)
+    on_edge = int((dis & edge).sum())
+    unexplained = int((dis & ~edge).sum())
+    return {"rays": int(len(ref)), "agreement": float(1.0 - dis.mean()), "disagree": int(dis.sum()),
+            "on_shared_edge": on_edge, "unexplained": unexplained,
+            "agreement_excluding_edges": float(1.0 - unexplained / max(1, len(ref) - on_edge)),
+            "edge_eps": EDGE_EPS}
+
+
+def precision_ids(ctx, rays):
+    """The precision closest hit's primary-ray IDs: against the FP32-node form
+    with the same watertight test (must be identical: 8-bit outward-rounded
+    bounds lose no hit) and against the reference's triangle test
+    (classified)."""
+    from aviatorengine2_b200 import _lib
+    plain = ctx.closest_hit(rays, _lib.VARIANT_PLAIN)
+    fp32 = ctx.closest_hit(rays, _lib.VARIANT_PLAIN_WT)
+    quant = ctx.closest_hit(rays, _lib.VARIANT_QUANT)
+    ids = (quant["object"] == fp32["object"]) & (quant["prim"] == fp32["prim"])
+    return {"vs_fp32_nodes_same_test": {"agreement": float(ids.mean()),
+                                        "bit_exact_hits": bool(np.array_equal(quant.view(np.uint8),
+                                                                              fp32.view(np.uint8)))},
+            "vs_reference_triangle_test": classify_ids(plain, quant)}
+
+
+def fp64_reference(scene, config, frames, pixels):
+    """The FP64 oracle's accumulation after `frames` frames at `pixels` only
+    (the checker of the MRE figures; host cores).  The buffers are reused
+    across frames: only the listed pixels are written."""
+    O, _ = _oracle_modules()
+    s = O.oscene(scene)
+    c = np.ascontiguousarray(np.array(config, dtype=O._lib.CONFIG).reshape(1))
+    w, h = int(c["width"][0]), int(c["height"][0])
+    acc = np.zeros((h, w, 4), np.float64)
+    disp = np.zeros((h, w, 4), np.float64)
+    frame = np.zeros((h, w, 4), np.float64)
+    xy = np.ascontiguousarray(pixels, dtype=np.uint32).reshape(-1, 2)
+    fn = O.oracle().oracle_render_frame_f64
+    for b in range(frames):
+        c["batch"][0] = b
+        fn(ctypes.byref(s), O.ptr(c), O.ptr(acc), O.ptr(disp), O.ptr(frame), O.ptr(xy), ctypes.c_uint32(len(xy)),
+           ctypes.c_int(os.cpu_count() or 1))
+    return acc[xy[:, 1], xy[:, 0]].copy()
+
+
+def seeded_pixels(width, height, n, seed):
+    rng = np.random.default_rng(seed)
+    pick = np.sort(rng.choice(width * height, min(n, width * height), replace=False))
+    return np.stack([pick % width, pick // width], 1).astype(np.uint32)
+
+
+def measure_paths(local, width, height, frames=2, mre_pixels=1024):
     """Mpaths/s of compute-only frames (1 spp) on the wavefront workload:
     the plain megakernel against the wavefront form (4-wide 8-bit quantised
     BVH, persistent stages, CUDA graph) and its precision form (watertight
@@ -229,16 +296,27 @@ def measure_paths(local, width, height, frames=2):
                        f"{len(scene.lights)} lights", "triangles": int(scene.triangles),
            "instances": int(len(scene.instances)), "paths_per_frame": width * height}
     imgs = {}
+    px = seeded_pixels(width, height, mre_pixels, 17) if mre_pixels > 0 else None
+    ref64 = fp64_reference(scene, scene.config, frames + 1, px) if px is not None else None
+    mre = {}
     with Context(width, height, device=local) as ctx:
         ctx.upload(scene)
         # Primary-ray instance and triangle IDs of the optimised closest hits
         # against the reference-order kernel, on this frame's camera rays.
         rays = ctx.camera_rays()
         ref = ctx.closest_hit(rays, _lib.VARIANT_PLAIN)
-        for name, var in (("fast", _lib.VARIANT_FAST), ("precision", _lib.VARIANT_QUANT)):
-            h = ctx.closest_hit(rays, var)
-            out[f"primary_id_agreement_{name}"] = float(((h["object"] == ref["object"]) &
-                                                         (h["prim"] == ref["prim"])).mean())
+        h = ctx.closest_hit(rays, _lib.VARIANT_FAST)
+        out["primary_id_agreement_fast"] = float(((h["object"] == ref["object"]) & (h["prim"] == ref["prim"])).mean())
+        out["primary_ids_precision"] = precision_ids(ctx, rays)
+        out["primary_id_agreement_precision"] = \
+            out["primary_ids_precision"]["vs_reference_triangle_test"]["agreement"]
+        # Algorithmic bytes of one frame of paths (the reference megakernel's
+        # traversals, counted on the device): the Mpaths/s roofline.
+        ctx.set_config(scene.config)
+        pc = np.zeros(7, np.uint64)
+        _lib.check(_lib.lib().ae_path_counters(ctx.handle, _lib.ptr(pc)), ctx.handle)
+        per = np.array([48, 128, 48, 48, 48, 60], np.float64)
+        bytes_per_path = float((pc[:6].astype(np.float64) * per).sum()) / (width * height)
         for name, mode in (("plain", _lib.MODE_COMPUTE_ONLY), ("wavefront", _lib.MODE_WAVEFRONT),
                            ("precision", _lib.MODE_WAVEFRONT_PRECISION)):
             c = scene.config.copy()
@@ -253,13 +331,126 @@ def measure_paths(local, width, height, frames=2):
             imgs[name] = ctx.read_image(_lib.IMAGE_FRAME)
             out[f"{name}_ms"] = float(np.mean(ms))
             out[f"{name}_mpaths"] = width * height / (float(np.mean(ms)) / 1e3) / 1e6
+            if ref64 is not None:
+                mre[name] = ctx.image_error_pixels(px, ref64, eps=MRE_EPS)["mre"]
         info = ctx.wavefront_info()
         out["wavefront_extend"] = {"threads": info["threads"], "stack": info["stack"]}
     out["speedup"] = out["wavefront_mpaths"] / out["plain_mpaths"]
     out["precision_speedup"] = out["precision_mpaths"] / out["plain_mpaths"]
+    peak, peak_kind = load_peaks()
+    roof = peak * 1e9 / bytes_per_path / 1e6
+    out["roofline"] = {"bound": "hbm", "algorithmic_bytes_per_path": bytes_per_path,
+                       "traversals_per_path": float(pc[6]) / (width * height), "peak_gbs": peak,
+                       "peak_source": peak_kind, "roofline_mpaths": roof,
+                       "frac": {k: out[f"{k}_mpaths"] / roof for k in ("plain", "wavefront", "precision")}}
+    if mre:
+        out["mre"] = {"reference": f"FP64 oracle (same estimator and RNG stream in double) after {frames + 1} "
+                                   f"frames at {len(px)} seeded pixels; reduced on the GPU in FP64; eps {MRE_EPS}",
+                      **mre, "precision_over_plain": mre["precision"] / max(mre["plain"], 1e-300),
+                      "wavefront_over_plain": mre["wavefront"] / max(mre["plain"], 1e-300)}
     a, b = imgs["plain"], imgs["wavefront"]
     out["frames_bit_exact"] = bool(np.array_equal(a.view(np.uint32), b.view(np.uint32)))
     out["pixels_differing"] = int(np.any(a.view(np.uint32) != b.view(np.uint32), axis=-1).sum())
+    return out
+
+
+def timed_closest_hit(ctx, d_rays, n, d_hits, variant, flush, reps=5):
+    """Mean CUDA-event time (ms) of one closest-hit launch over device rays,
+    L2 flushed before each, on the context's stream."""
+    import torch
+    ext = torch.cuda.ExternalStream(ctx.stream)
+    ctx.closest_hit_device(d_rays, n, d_hits, variant)  # warm-up (and prepare)
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(ext):
+            e0.record()
+            ctx.closest_hit_device(d_rays, n, d_hits, variant)
+            e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return float(np.mean(ms))
+
+
+def measure_config4(local, frames=1024, mre_pixels=2048, width=960, height=540):
+    """The precision variant of the closest-hit workload (the 2.1M-triangle
+    instanced scene at 960x540):
+      * primary-ray IDs of the precision closest hit (4-wide BVH, 8-bit child
+        bounds rounded outward, watertight test) against the FP32-node form
+        with the same test (identical when no hit is lost) and against the
+        reference's triangle test (disagreements classified);
+      * node bytes per ray, counted on the device over camera + bounce rays:
+        the reference walk's 48-byte binary nodes against the precision
+        walk's 48-byte TLAS nodes and 64-byte quantised BLAS nodes;
+      * closest-hit Mrays/s (CUDA events, L2 flushed) of the FP32-node forms
+        and the precision form;
+      * `frames` frames of 1 spp each, the plain FP32 megakernel against the
+        precision wavefront form (Kahan-compensated accumulation): ms/frame,
+        Mpaths/s and MRE of the accumulation against the FP64 oracle at
+        `mre_pixels` seeded pixels."""
+    import torch
+    from aviatorengine2_b200 import Context, _lib, scenes
+    scene = scenes.instanced_meshes(width=width, height=height, gpu_build=True)
+    out = {"workload": f"instanced_meshes {width}x{height}, {frames} frames of 1 spp, depth "
+                       f"{int(scene.config['depth'])}", "triangles": int(scene.triangles)}
+    dev = torch.device("cuda", local)
+    with Context(width, height, device=local) as ctx:
+        ctx.upload(scene)
+        ctx.prepare_fast()
+        prim = ctx.camera_rays()
+        out["primary_ids"] = precision_ids(ctx, prim)
+        hits = ctx.closest_hit(prim, _lib.VARIANT_PLAIN)
+        bounce, valid = ctx.bounce_rays(prim, hits)
+        rays = np.concatenate([prim, bounce[valid]])
+        d_rays = torch.from_numpy(rays.view(np.uint8)).to(dev)
+        d_hits = torch.empty(len(rays) * 20, dtype=torch.uint8, device=dev)
+        flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=dev)
+        torch.cuda.synchronize()
+        L = _lib.lib()
+        cnt = {}
+        for name, var in (("plain", _lib.VARIANT_PLAIN), ("precision", _lib.VARIANT_QUANT)):
+            c6 = np.zeros(6, np.uint64)
+            _lib.check(L.ae_trace_counters_variant(ctx.handle, d_rays.data_ptr(), len(rays), var, _lib.ptr(c6)),
+                       ctx.handle)
+            cnt[name] = c6.astype(np.float64) / len(rays)
+        out["node_bytes_per_ray"] = {
+            "plain_fp32_binary": 48.0 * (cnt["plain"][0] + cnt["plain"][3]),
+            "precision_quantised": 48.0 * cnt["precision"][0] + 64.0 * cnt["precision"][3],
+            "plain_nodes_per_ray": float(cnt["plain"][0] + cnt["plain"][3]),
+            "precision_nodes_per_ray": float(cnt["precision"][0] + cnt["precision"][3]),
+            "plain_triangle_bytes_per_ray": 48.0 * cnt["plain"][4],
+            "precision_triangle_bytes_per_ray": 48.0 * cnt["precision"][4],
+            "rays": int(len(rays)), "note": "camera rays + one diffuse bounce per primary hit"}
+        chit = {}
+        for name, var in (("plain_fp32_nodes", _lib.VARIANT_PLAIN),
+                          ("plain_fp32_nodes_watertight", _lib.VARIANT_PLAIN_WT), ("precision", _lib.VARIANT_QUANT)):
+            ms = timed_closest_hit(ctx, d_rays.data_ptr(), len(rays), d_hits.data_ptr(), var, flush)
+            chit[name] = {"ms": ms, "mrays": len(rays) / (ms / 1e3) / 1e6}
+        out["closest_hit"] = chit
+        del flush
+        px = seeded_pixels(width, height, mre_pixels, 23) if mre_pixels > 0 else None
+        ref64 = fp64_reference(scene, scene.config, frames, px) if px is not None else None
+        for name, mode in (("plain", _lib.MODE_COMPUTE_ONLY), ("precision", _lib.MODE_WAVEFRONT_PRECISION)):
+            c = scene.config.copy()
+            ms = []
+            for b in range(frames):
+                c["batch"] = b
+                ctx.set_config(c)
+                ctx.render_frame(mode)
+                ms.append(ctx.last_kernel_ms())
+            ctx.synchronize()
+            r = {"ms_per_frame": float(np.mean(ms[1:])) if frames > 1 else float(ms[0])}
+            r["mpaths"] = width * height / (r["ms_per_frame"] / 1e3) / 1e6
+            if ref64 is not None:
+                r["mre"] = ctx.image_error_pixels(px, ref64, eps=MRE_EPS)["mre"]
+            out[name] = r
+    out["speedup"] = out["precision"]["mpaths"] / out["plain"]["mpaths"]
+    if ref64 is not None:
+        out["mre_reference"] = (f"FP64 oracle (same estimator and RNG stream in double) after {frames} frames at "
+                                f"{len(px)} seeded pixels; reduced on the GPU in FP64; eps {MRE_EPS}")
+        out["mre_precision_over_plain"] = out["precision"]["mre"] / max(out["plain"]["mre"], 1e-300)
     return out
 
 
@@ -489,6 +680,9 @@ def main():
     ap.add_argument("--no-paths", action="store_true", help="skip the Mpaths/s leg (plain vs wavefront frames)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-build", action="store_true", help="skip the BVH build leg")
+    ap.add_argument("--no-config4", action="store_true", help="skip the precision-variant leg (960x540)")
+    ap.add_argument("--c4-frames", type=int, default=1024, help="frames (1 spp each) of the precision-variant leg")
+    ap.add_argument("--mre-pixels", type=int, default=2048, help="seeded pixels scored against the FP64 oracle")
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-rate", type=float, default=0.5, help="Poisson arrivals per second")
     ap.add_argument("--serve-sweep", default="", help="comma-separated arrival rates: also run the serving "
@@ -650,10 +844,13 @@ def main():
     # Frame-level legs: rank 0 only (the other replicas would repeat them).
     paths = None
     if not args.no_paths and rank == 0:
-        paths = measure_paths(local, args.width, args.height)
+        paths = measure_paths(local, args.width, args.height, mre_pixels=args.mre_pixels // 2)
     build = None
     if not args.no_build and rank == 0:
         build = measure_build(local)
+    config4 = None
+    if not args.no_config4 and rank == 0:
+        config4 = measure_config4(local, args.c4_frames, args.mre_pixels)
     serving = None
     if not args.no_serve and rank == 0:
         serving = measure_serving(local, args.serve_requests, args.serve_rate)
@@ -670,7 +867,7 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "per_step_ms": [round(t, 4) for t in times],
-            "paths": paths, "serving": serving, "bvh_build": build}
+            "paths": paths, "config4": config4, "serving": serving, "bvh_build": build}
     if sweep is not None:
         line["serving_sweep"] = sweep
     if rank == 0:

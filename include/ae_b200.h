@@ -447,6 +447,11 @@ int ae_read_image(ae_ctx *ctx, int which, void *dst, size_t dst_bytes);
  * absolute error, out[3] = root mean square error.  The sums are reduced in a
  * fixed order, so the result is the same on every run. */
 int ae_image_error(ae_ctx *ctx, int which, const double *reference, double eps, double *out4);
+/* The same over a pixel subset: xy holds n_px (x, y) pairs, reference n_px
+ * RGBA doubles in that order (e.g. the FP64 oracle rendered at those pixels
+ * only).  Coordinates outside the image are refused with AE_ERR_INVALID. */
+int ae_image_error_pixels(ae_ctx *ctx, int which, const uint32_t *xy, uint32_t n_px, const double *reference,
+                          double eps, double *out4);
 
 /* Closest hit for a batch of HOST rays: copies in, traces, copies out,
  * pipelined in chunks over streams.  variant = AE_VARIANT_*. */
@@ -495,6 +500,17 @@ int ae_bounce_rays(ae_ctx *ctx, const ae_ray *primary, const ae_hit *hits, uint3
  * triangles tested, closest-hit winners.  The roofline's bytes per ray are
  * 48, 128, 48, 48, 48 and 60 bytes per touch respectively. */
 int ae_trace_counters(ae_ctx *ctx, const ae_ray *d_rays, uint32_t n, uint64_t *counters);
+/* The fetches of one kernel family's walk over DEVICE rays (no counterpart in
+ * the reference).  PLAIN: as ae_trace_counters.  FAST / QUANT (after
+ * ae_prepare_fast): counters[6] = TLAS nodes (48 B), object metadata records
+ * (16 B), instance records (48 B), 4-wide quantised BLAS nodes (64 B),
+ * triangle records (48 B), rays that hit. */
+int ae_trace_counters_variant(ae_ctx *ctx, const ae_ray *d_rays, uint32_t n, int variant, uint64_t *counters);
+/* Algorithmic traffic of one compute-only frame of the current config: every
+ * traversal of main/ColorRay/CalculateDirectLight (hybrid:1122-1404) with its
+ * touches counted as in ae_trace_counters, summed over all pixels.
+ * counters[7] = the six touch counts, then the number of traversals. */
+int ae_path_counters(ae_ctx *ctx, uint64_t *counters);
 
 /* Wavefront path tracer state after an AE_MODE_WAVEFRONT frame: the extend
  * stage's autotuned block size and shared-memory stack depth, the nine
