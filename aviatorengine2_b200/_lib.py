@@ -80,7 +80,7 @@ for _dt, _size in ((VERTEX, 32), (NODE, 48), (OBJECT, 128), (INSTANCE, 48), (RAY
 
 # Enumerations (include/ae_b200.h)
 SHAPE_SPHERE, SHAPE_QUAD, SHAPE_BOX, SHAPE_TRIANGLE, SHAPE_MESH = range(5)
-MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_DIFFUSE_LIGHT, MAT_ISOTROPIC = range(5)
+MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_DIFFUSE_LIGHT, MAT_ISOTROPIC, MAT_GGX_METAL = range(6)
 NO_TEXTURE = 0xFFFFFFFF
 MISS = 0xFFFFFFFF
 VARIANT_PLAIN, VARIANT_FAST, VARIANT_QUANT, VARIANT_FAST_WALK, VARIANT_PLAIN_WT = 0, 1, 2, 3, 4

@@ -336,6 +336,9 @@ int ae_upload_scene(ae_ctx *ctx, const ae_object *objects, uint32_t n_objects, c
     c->host_tlas.assign(tlas, tlas + n_nodes);
     c->host_instances.assign(instances, instances + n_instances);
     c->host_lights.assign(light_ids, light_ids + n_lights);
+    c->scene_has_ggx = false;
+    for (uint32_t i = 0; i < n_objects; i++)
+        if (objects[i].colorType == AE_MAT_GGX_METAL) c->scene_has_ggx = true;
     c->scene_uploaded = true;
     c->scene_version++;
     c->scene_version_layout++;
@@ -384,6 +387,9 @@ int ae_render_frame(ae_ctx *ctx, int mode, const ae_gbuffer *gb) {
             return rc;
         return c->timed_end();
     case AE_MODE_DEFERRED:
+        if (c->scene_has_ggx)
+            return c->fail(AE_ERR_STATE, "the hybrid passes have no GGX metal (an extension of the compute-only "
+                                         "forms); render this scene compute-only, wavefront or served");
         return render_deferred(c, gb);
     case AE_MODE_WAVEFRONT:
         return render_wavefront(c, false);

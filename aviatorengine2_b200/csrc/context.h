@@ -80,6 +80,7 @@ struct Ctx {
     std::vector<ae_instance> host_instances;
     std::vector<uint32_t> host_lights;
     bool scene_uploaded = false;
+    bool scene_has_ggx = false;  // an object uses AE_MAT_GGX_METAL (not shaded by the hybrid passes)
     uint64_t scene_version = 0;         // bumps on every change of scene content
     uint64_t scene_version_layout = 0;  // bumps when arrays are re-uploaded (topology may change)
     DevBuf<float> obj_box;              // world box per object (refit)

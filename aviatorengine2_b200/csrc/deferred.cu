@@ -1000,6 +1000,7 @@ extern "C" int ae_build_gbuffer(ae_ctx *ctx) {
     Ctx *c = reinterpret_cast<Ctx *>(ctx);
     if (!c) return AE_ERR_INVALID;
     if (!c->scene_uploaded) return c->fail(AE_ERR_STATE, "G-buffer before ae_upload_scene");
+    if (c->scene_has_ggx) return c->fail(AE_ERR_STATE, "the hybrid passes have no GGX metal");
     int rc = ensure(c);
     if (rc) return rc;
     Deferred &D = *c->deferred;

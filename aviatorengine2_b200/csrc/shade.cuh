@@ -108,10 +108,65 @@ AE_DEV f3 direct_light(const DevScene &S, const DHit &h, f3 surf_albedo, float t
     return acc;
 }
 
-// GetBounce, hybrid:965-1033.
-AE_DEV bool get_bounce(f3 d, const DHit &h, const MatRec &m, f3 &dir, uint32_t &seed) {
+// Rough metal with GGX microfacet reflection - an extension: the
+// reference's METAL is a mirror blurred by fuzz (hybrid:988-991).  The model
+// is Walter, Marschner, Li and Torrance, "Microfacet Models for Refraction
+// through Rough Surfaces" (EGSR 2007), with alpha = the material's roughness
+// (Object_GPU::fuzz):
+//   * a microfacet normal m drawn with density D(m)|m.n| (eqs. 35-36):
+//     cos^2(theta_m) = (1 - u1) / (1 + (alpha^2 - 1) u1), phi_m = 2 pi u2,
+//     placed in an orthonormal basis around n (Duff et al., "Building an
+//     Orthonormal Basis, Revisited", JCGT 2017);
+//   * the mirror direction o = 2 (i.m) m - i about m (eq. 39), i = -d;
+//   * the sample weight F(i.m) |i.m| G(i,o,m) / (|i.n| |m.n|) (eq. 41), with
+//     the Smith shadowing G = G1(i) G1(o), G1(v) = 2 / (1 + sqrt(1 + alpha^2
+//     tan^2 theta_v)) (eq. 34), and Schlick's Fresnel with F0 = albedo.
+// Two RNG draws, always taken.  Returns false when the path ends (i or o
+// below the shading surface).
+AE_DEV float ggx_g1(float cv, float a2) {
+    const float c2 = AE_MUL(cv, cv);
+    const float t2 = AE_DIV(AE_SUB(1.0f, c2), c2);
+    return AE_DIV(2.0f, AE_ADD(1.0f, AE_SQRT(AE_ADD(1.0f, AE_MUL(a2, t2)))));
+}
+AE_DEV bool ggx_bounce(f3 d, f3 n, f3 albedo, float alpha, f3 &dir, f3 &weight, uint32_t &seed) {
+    const f3 i = -normalize(d);
+    const float u1 = rng_next(seed);
+    const float u2 = rng_next(seed);
+    const float cin = dot(i, n);
+    if (cin <= 0.0f) return false;
+    const float a2 = AE_MUL(alpha, alpha);
+    const float c2 = AE_DIV(AE_SUB(1.0f, u1), AE_ADD(1.0f, AE_MUL(AE_SUB(a2, 1.0f), u1)));
+    const float cm = AE_SQRT(c2);
+    const float sm = AE_SQRT(fmax_(0.0f, AE_SUB(1.0f, c2)));
+    const float phi = AE_MUL(6.2831853f, u2);
+    const float cp = cosf_(phi), sp = sinf_(phi);
+    const float sg = n.z >= 0.0f ? 1.0f : -1.0f;
+    const float a = AE_DIV(-1.0f, AE_ADD(sg, n.z));
+    const float b = AE_MUL(AE_MUL(n.x, n.y), a);
+    const f3 t = mk(AE_ADD(1.0f, AE_MUL(AE_MUL(sg, AE_MUL(n.x, n.x)), a)), AE_MUL(sg, b), -AE_MUL(sg, n.x));
+    const f3 bt = mk(b, AE_ADD(sg, AE_MUL(AE_MUL(n.y, n.y), a)), -n.y);
+    const f3 m = t * AE_MUL(sm, cp) + bt * AE_MUL(sm, sp) + n * cm;
+    const float im = dot(i, m);
+    if (im <= 0.0f) return false;
+    dir = m * AE_MUL(2.0f, im) - i;
+    const float con = dot(dir, n);
+    if (con <= 0.0f) return false;
+    const float g = AE_MUL(ggx_g1(cin, a2), ggx_g1(con, a2));
+    const float w = AE_DIV(AE_MUL(im, g), AE_MUL(cin, cm));
+    const float f5 = powf_(AE_SUB(1.0f, im), 5.0f);
+    const f3 fr = albedo + (splat(1.0f) - albedo) * f5;
+    weight = fr * w;
+    return true;
+}
+
+// GetBounce, hybrid:965-1033, and the GGX metal extension above.  `alb` is
+// the surface albedo (GGX's F0); `ggx_w` receives the GGX sample weight,
+// which replaces the albedo in the throughput update for that material.
+AE_DEV bool get_bounce(f3 d, const DHit &h, const MatRec &m, f3 alb, f3 &dir, f3 &ggx_w, uint32_t &seed) {
     dir = splat(0.0f);
     switch (m.type) {
+    case AE_MAT_GGX_METAL:
+        return ggx_bounce(d, h.n, alb, m.fuzz, dir, ggx_w, seed);
     case AE_MAT_LAMBERTIAN:
         dir = h.n + random_direction(seed);
         if (dot(dir, dir) < 0.001f) dir = h.n;

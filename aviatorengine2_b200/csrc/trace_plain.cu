@@ -76,12 +76,13 @@ AE_DEV f3 color_ray(const DevScene &S, const FrameParams &F, f3 o, f3 d, float t
             if (luma > 8.0f) dl = dl * AE_DIV(8.0f, luma);
             acc = acc + thr * dl;
         }
-        f3 sd;
-        if (!get_bounce(d, h, m, sd, seed)) break;
+        f3 sd, gw;
+        if (!get_bounce(d, h, m, alb, sd, gw, seed)) break;
         d = normalize(sd);
         const float sgn = dot(d, h.n) < 0.0f ? -1.0f : 1.0f;
         o = h.p + h.n * AE_MUL(0.001f, sgn);
-        if (m.type != AE_MAT_DIELECTRIC) thr = thr * alb;
+        if (m.type == AE_MAT_GGX_METAL) thr = thr * gw;
+        else if (m.type != AE_MAT_DIELECTRIC) thr = thr * alb;
         if (b > 0) {
             const float p = clampf(maxc(thr), 0.1f, 1.0f);
             if (rng_next(seed) > p) break;

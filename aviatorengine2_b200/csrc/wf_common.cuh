@@ -191,12 +191,13 @@ AE_DEV bool shade_vertex(const DevScene &S, const FastView &V, const PrecView &P
             SH.occ[e] = 0;
         }
     }
-    f3 sd;
-    if (!get_bounce(d, h, m, sd, seed)) return false;
+    f3 sd, gw;
+    if (!get_bounce(d, h, m, alb, sd, gw, seed)) return false;
     const f3 nd = normalize(sd);
     const float sgn = dot(nd, h.n) < 0.0f ? -1.0f : 1.0f;
     const f3 no = h.p + h.n * AE_MUL(0.001f, sgn);
-    if (m.type != AE_MAT_DIELECTRIC) thr = thr * alb;
+    if (m.type == AE_MAT_GGX_METAL) thr = thr * gw;
+    else if (m.type != AE_MAT_DIELECTRIC) thr = thr * alb;
     if (bounce > 0) {
         const float p = clampf(maxc(thr), 0.1f, 1.0f);
         if (rng_next(seed) > p) return false;

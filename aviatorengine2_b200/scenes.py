@@ -17,7 +17,8 @@ Workloads (all inputs seeded; no dataset is involved):
   wavefront_scene  1024 instances of 32 meshes (heightfields and icospheres
                    from the generators above), about 10M unique triangles;
                    materials per mesh 60% Lambertian, 25% metal (fuzz =
-                   roughness in [0.05, 0.6]), 15% dielectric (IOR 1.5); 16
+                   roughness in [0.05, 0.6], or GGX rough metal of that
+                   roughness with ggx=True), 15% dielectric (IOR 1.5); 16
                    emissive quads above the field.
   hybrid_box       the Cornell box plus analytic spheres and boxes, for the
                    hybrid renderer's raster/analytic split.
@@ -456,10 +457,11 @@ def media_box(seed=7, width=128, height=96, depth=6):
     return _finish(ents, meshes, cfg, "media_box")
 
 
-def wavefront_meshes(rng, n_meshes=32, target_tris=10_000_000):
+def wavefront_meshes(rng, n_meshes=32, target_tris=10_000_000, metal=_lib.MAT_METAL):
     """wavefront_scene's unique meshes, alternating heightfields and
     icospheres sized to share `target_tris` triangles, and a material kind
-    per mesh (60 % Lambertian, 25 % metal, 15 % dielectric)."""
+    per mesh (60 % Lambertian, 25 % metal, 15 % dielectric); `metal` is the
+    metal kind: MAT_METAL (the reference's fuzzed mirror) or MAT_GGX_METAL."""
     geometry, kinds = [], []
     budget = target_tris
     for k in range(n_meshes):
@@ -474,18 +476,22 @@ def wavefront_meshes(rng, n_meshes=32, target_tris=10_000_000):
         budget -= len(i) // 3
         geometry.append((v, i))
         r = rng.random()
-        kinds.append(_lib.MAT_LAMBERTIAN if r < 0.6 else (_lib.MAT_METAL if r < 0.85 else _lib.MAT_DIELECTRIC))
+        kinds.append(_lib.MAT_LAMBERTIAN if r < 0.6 else (metal if r < 0.85 else _lib.MAT_DIELECTRIC))
     return geometry, kinds
 
 
 def wavefront_scene(seed=4, width=1920, height=1080, depth=12, n_meshes=32, n_instances=1024, n_lights=16,
-                    target_tris=10_000_000, gpu_build=False):
+                    target_tris=10_000_000, gpu_build=False, ggx=False):
     """The wavefront workload: meshes drawn from the heightfield and icosphere
     generators until about `target_tris` unique triangles, instanced 1024
-    times, lit by 16 emissive quads.  gpu_build: BLAS builds on the GPU."""
+    times, lit by 16 emissive quads.  Metal meshes are the reference's fuzzed
+    mirror (fuzz = roughness in [0.05, 0.6]) or, with ggx=True, GGX rough
+    metal of that roughness (MAT_GGX_METAL; the same random draws, so the
+    scene is otherwise identical).  gpu_build: BLAS builds on the GPU."""
     rng = np.random.default_rng(seed)
     meshes = MeshLibrary(gpu=gpu_build)
-    geometry, kinds = wavefront_meshes(rng, n_meshes, target_tris)
+    geometry, kinds = wavefront_meshes(rng, n_meshes, target_tris,
+                                       metal=_lib.MAT_GGX_METAL if ggx else _lib.MAT_METAL)
     handles = meshes.add_many(geometry)
     mat = []
     for k in range(n_meshes):

@@ -291,9 +291,10 @@ def measure_paths(local, width, height, frames=2, mre_pixels=1024):
     compared, and primary-ray IDs of both optimised closest hits against the
     plain kernel's."""
     from aviatorengine2_b200 import Context, _lib, scenes
-    scene = scenes.wavefront_scene(width=width, height=height, gpu_build=True)
+    scene = scenes.wavefront_scene(width=width, height=height, gpu_build=True, ggx=True)
     out = {"workload": f"wavefront_scene {width}x{height}, 1 spp, depth {int(scene.config['depth'])}, "
-                       f"{len(scene.lights)} lights", "triangles": int(scene.triangles),
+                       f"{len(scene.lights)} lights, materials 60% Lambertian / 25% GGX metal / 15% dielectric",
+           "triangles": int(scene.triangles),
            "instances": int(len(scene.instances)), "paths_per_frame": width * height}
     imgs = {}
     px = seeded_pixels(width, height, mre_pixels, 17) if mre_pixels > 0 else None

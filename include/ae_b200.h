@@ -58,8 +58,13 @@ typedef enum ae_status {
 
 /* BodyShape, scene/gpu_types.h:14-21 */
 enum { AE_SHAPE_SPHERE = 0, AE_SHAPE_QUAD = 1, AE_SHAPE_BOX = 2, AE_SHAPE_TRIANGLE = 3, AE_SHAPE_MESH = 4 };
-/* MaterialType, scene/material.h:11-18 */
-enum { AE_MAT_LAMBERTIAN = 0, AE_MAT_METAL = 1, AE_MAT_DIELECTRIC = 2, AE_MAT_DIFFUSE_LIGHT = 3, AE_MAT_ISOTROPIC = 4 };
+/* MaterialType, scene/material.h:11-18, plus one extension: GGX_METAL, a
+ * rough metal with GGX microfacet reflection (Walter et al., EGSR 2007;
+ * roughness alpha in Object_GPU::fuzz, F0 = albedo).  The compute-only,
+ * wavefront, precision and serving forms shade it; the hybrid (deferred)
+ * passes refuse scenes that use it. */
+enum { AE_MAT_LAMBERTIAN = 0, AE_MAT_METAL = 1, AE_MAT_DIELECTRIC = 2, AE_MAT_DIFFUSE_LIGHT = 3, AE_MAT_ISOTROPIC = 4,
+       AE_MAT_GGX_METAL = 5 };
 /* kNoTexture, scene/texture.h:19 */
 #define AE_NO_TEXTURE 0xFFFFFFFFu
 

@@ -47,6 +47,7 @@ CONFIG = np.dtype([("source_x", "<f4"), ("source_y", "<f4"), ("source_z", "<f4")
 # Shape and material enumerations (scene/gpu_types.h, scene/material.h:9-16).
 SHAPE_MESH = 4
 MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_DIFFUSE_LIGHT, MAT_ISOTROPIC = range(5)
+MAT_GGX_METAL = 5  # the library's extension (rough metal, GGX microfacets); not a reference material
 NO_TEXTURE = 0xFFFFFFFF  # kNoTexture, scene/texture.h
 MISS = 0xFFFFFFFF
 

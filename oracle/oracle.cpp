@@ -556,6 +556,52 @@ template <class T> V<T> random_direction(Rng &rng) {
     return v3<T>(rr * M<T>::cos(a), rr * M<T>::sin(a), z);
 }
 
+// GGX metal, the library's extension of the materials (not a reference
+// material): Walter, Marschner, Li and Torrance, "Microfacet Models for
+// Refraction through Rough Surfaces" (EGSR 2007), alpha = roughness (fuzz).
+// The half vector m is drawn with density D(m)|m.n| (eqs. 35-36), the
+// direction is the mirror of i = -d about m (eq. 39), and the sample weight
+// is F(i.m) |i.m| G(i,o,m) / (|i.n| |m.n|) (eq. 41) with Smith's
+// G1(v) = 2 / (1 + sqrt(1 + alpha^2 tan^2 theta_v)) (eq. 34) and Schlick's
+// Fresnel with F0 = albedo.  The tangent frame around n is Duff et al.'s
+// (JCGT 2017).  Two RNG draws, always taken.
+template <class T> T ggx_g1(T cv, T a2) {
+    const T c2 = cv * cv;
+    const T t2 = (T(1) - c2) / c2;
+    return T(2) / (T(1) + M<T>::sqrt(T(1) + a2 * t2));
+}
+template <class T>
+bool ggx_bounce(V<T> d, V<T> n, V<T> alb, T alpha, V<T> &dir, V<T> &weight, Rng &rng) {
+    const V<T> i = -nrm(d);
+    const T u1 = rng.next<T>();
+    const T u2 = rng.next<T>();
+    const T cin = dot(i, n);
+    if (cin <= 0) return false;
+    const T a2 = alpha * alpha;
+    const T c2 = (T(1) - u1) / (T(1) + (a2 - T(1)) * u1);
+    const T cm = M<T>::sqrt(c2);
+    const T sm = M<T>::sqrt(M<T>::fmax(T(0), T(1) - c2));
+    const T phi = T(6.2831853f) * u2;
+    const T cp = M<T>::cos(phi), sp = M<T>::sin(phi);
+    const T sg = n.z >= 0 ? T(1) : T(-1);
+    const T a = T(-1) / (sg + n.z);
+    const T b = (n.x * n.y) * a;
+    const V<T> t = v3<T>(T(1) + (sg * (n.x * n.x)) * a, sg * b, -(sg * n.x));
+    const V<T> bt = v3<T>(b, sg + (n.y * n.y) * a, -n.y);
+    const V<T> m = t * (sm * cp) + bt * (sm * sp) + n * cm;
+    const T im = dot(i, m);
+    if (im <= 0) return false;
+    dir = m * (T(2) * im) - i;
+    const T con = dot(dir, n);
+    if (con <= 0) return false;
+    const T g = ggx_g1(cin, a2) * ggx_g1(con, a2);
+    const T w = (im * g) / (cin * cm);
+    const T f5 = M<T>::pow(T(1) - im, T(5));
+    const V<T> fr = alb + (v3<T>(1, 1, 1) - alb) * f5;
+    weight = fr * w;
+    return true;
+}
+
 // GetBounce, hybrid:965-1033.
 template <class T> bool bounce(const Ray<T> &r, const Hit<T> &h, V<T> &dir, Rng &rng) {
     dir = v3<T>(0, 0, 0);
@@ -681,12 +727,16 @@ template <class T> V<T> color_ray(const Scene &S, const ae_config &cfg, Ray<T> r
             if (luma > T(8)) dl = dl * (T(8) / luma);
             acc = acc + thr * dl;
         }
-        V<T> sd;
-        if (!bounce(ray, h, sd, rng)) break;
+        V<T> sd, gw;
+        const bool ggx = h.obj->colorType == AE_MAT_GGX_METAL;
+        if (ggx ? !ggx_bounce(ray.d, h.n, surface_albedo(S, h), T(h.obj->fuzz), sd, gw, rng)
+                : !bounce(ray, h, sd, rng))
+            break;
         ray.d = nrm(sd);
         const T sign = dot(ray.d, h.n) < 0 ? T(-1) : T(1);
         ray.o = h.p + h.n * (T(0.001f) * sign);
-        if (h.obj->colorType != AE_MAT_DIELECTRIC) thr = thr * surface_albedo(S, h);
+        if (ggx) thr = thr * gw;
+        else if (h.obj->colorType != AE_MAT_DIELECTRIC) thr = thr * surface_albedo(S, h);
         if (b > 0) {
             T p = maxc(thr);
             p = M<T>::fmin(M<T>::fmax(p, T(0.1f)), T(1));
@@ -890,6 +940,25 @@ int oracle_math(int fn, const float *x, const float *y, float *out, uint32_t n) 
         case 7: out[i] = ae::acosf_(x[i]); break;
         default: { uint32_t sd; std::memcpy(&sd, &x[i], 4); out[i] = ae::rng_next(sd); }
         }
+    }
+    return 0;
+}
+
+// `count` GGX metal samples in double (ggx_bounce above) for incoming
+// direction d, shading normal n, albedo alb and roughness alpha, RNG seeds
+// seed, seed + 1, ...: out[7 k ..] = direction xyz, weight xyz, 1 if the path
+// continues (else 0 and the rest zero).
+int oracle_ggx_samples(const double *d, const double *n, const double *alb, double alpha, uint32_t seed,
+                       uint32_t count, double *out) {
+    for (uint32_t k = 0; k < count; k++) {
+        Rng rng{seed + k};
+        V<double> dir = v3<double>(0, 0, 0), w = v3<double>(0, 0, 0);
+        const bool ok = ggx_bounce<double>(v3<double>(d[0], d[1], d[2]), v3<double>(n[0], n[1], n[2]),
+                                           v3<double>(alb[0], alb[1], alb[2]), alpha, dir, w, rng);
+        double *o = out + 7 * size_t(k);
+        o[0] = ok ? dir.x : 0; o[1] = ok ? dir.y : 0; o[2] = ok ? dir.z : 0;
+        o[3] = ok ? w.x : 0; o[4] = ok ? w.y : 0; o[5] = ok ? w.z : 0;
+        o[6] = ok ? 1 : 0;
     }
     return 0;
 }

@@ -329,3 +329,13 @@ def any_hit(scene, rays, tmax, threads=0):
     out = np.zeros(len(r), np.uint8)
     oracle().oracle_any_hit(ctypes.byref(s), ptr(r), ptr(t), ctypes.c_uint32(len(r)), ptr(out), ctypes.c_int(threads))
     return out
+
+
+def ggx_samples(d, n, albedo, alpha, seed, count):
+    """`count` GGX metal samples of the FP64 oracle: (directions (count, 3),
+    weights (count, 3), continues (count,) bool)."""
+    out = np.zeros((count, 7), np.float64)
+    a = [np.ascontiguousarray(x, np.float64) for x in (d, n, albedo)]
+    oracle().oracle_ggx_samples(ptr(a[0]), ptr(a[1]), ptr(a[2]), ctypes.c_double(alpha), ctypes.c_uint32(seed),
+                                ctypes.c_uint32(count), ptr(out))
+    return out[:, 0:3], out[:, 3:6], out[:, 6] > 0.5
