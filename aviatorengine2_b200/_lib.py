@@ -67,7 +67,7 @@ SERVE_STATS = np.dtype([("submitted", "<u8"), ("completed", "<u8"), ("rejected",
                         ("paths", "<u8"), ("rays", "<u8"), ("first_submit_ms", "<f8"), ("last_done_ms", "<f8"),
                         ("p50_ms", "<f8"), ("p99_ms", "<f8"), ("mean_ms", "<f8"), ("max_ms", "<f8"),
                         ("launches", "<u8"), ("peak_arena_bytes", "<u8"), ("peak_resident", "<u4"),
-                        ("moves_applied", "<u4"), ("errors", "<u4"), ("pad", "<u4")])
+                        ("moves_applied", "<u4"), ("errors", "<u4"), ("cancelled", "<u4")])
 POLICY_EVENT = np.dtype([("kind", "<u4"), ("scene", "<u4"), ("tick", "<u4"), ("service_ticks", "<u4"),
                          ("footprint", "<u8")])
 POLICY_OUTCOME = np.dtype([("admit_tick", "<i4"), ("done_tick", "<i4"), ("version", "<u4"), ("status", "<i4"),
@@ -86,10 +86,11 @@ MISS = 0xFFFFFFFF
 VARIANT_PLAIN, VARIANT_FAST, VARIANT_QUANT, VARIANT_FAST_WALK, VARIANT_PLAIN_WT = 0, 1, 2, 3, 4
 MODE_COMPUTE_ONLY, MODE_DEFERRED, MODE_WAVEFRONT, MODE_WAVEFRONT_PRECISION = 0, 1, 2, 3
 IMAGE_ACCUM, IMAGE_DISPLAY, IMAGE_FRAME, IMAGE_REDUCED, IMAGE_HISTORY_GEOMETRY = range(5)
-POLICY_REQUEST, POLICY_MOVE = 0, 1
+POLICY_REQUEST, POLICY_MOVE, POLICY_CANCEL = 0, 1, 2
 CLAIM_OLDEST_FIRST, CLAIM_SHARED = 0, 1
 STATUS = {0: "AE_OK", -1: "AE_ERR_INVALID", -2: "AE_ERR_OOM", -3: "AE_ERR_OVERSIZE", -4: "AE_ERR_LAYOUT",
-          -5: "AE_ERR_CUDA", -6: "AE_ERR_TIMEOUT", -7: "AE_ERR_STATE", -8: "AE_ERR_REJECTED"}
+          -5: "AE_ERR_CUDA", -6: "AE_ERR_TIMEOUT", -7: "AE_ERR_STATE", -8: "AE_ERR_REJECTED", -9: "AE_ERR_CANCELLED"}
+FAULT_TILE_WAIT = 1
 
 # Every symbol include/ae_b200.h declares, with (restype, argtypes).
 _P = ctypes.c_void_p
@@ -157,11 +158,17 @@ SIGNATURES = {
     "ae_serve_add_scene": (_I, [_P, _P, _P]),
     "ae_serve_submit": (_I, [_P, _P, _P]),
     "ae_serve_move_instances": (_I, [_P, _U32, _P, _U32]),
+    "ae_serve_cancel": (_I, [_P, ctypes.c_uint64]),
     "ae_serve_wait": (_I, [_P, ctypes.c_uint64, ctypes.c_int32, _P]),
     "ae_serve_drain": (_I, [_P, ctypes.c_int32]),
     "ae_serve_get_stats": (_I, [_P, _P]),
     "ae_serve_reset_stats": (_I, [_P]),
     "ae_serve_policy_simulate": (_I, [_P, _U32, ctypes.c_uint64, _U32, _U32, _U32, _U32, _P]),
+    "ae_debug_fail_alloc_after": (_I, [ctypes.c_int64]),
+    "ae_debug_live_allocations": (ctypes.c_int64, []),
+    "ae_create_status": (_I, []),
+    "ae_debug_inject": (_I, [_P, _I, _U32]),
+    "ae_serve_debug_inject": (_I, [_P, _I, _U32]),
 }
 
 _lib = None

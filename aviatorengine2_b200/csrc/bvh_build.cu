@@ -44,6 +44,7 @@
 
 #include "../../include/ae_b200.h"
 #include "ae_math.h"
+#include "devmem.h"
 
 namespace ae {
 namespace {
@@ -750,16 +751,18 @@ template <class T> struct Grow {
     size_t cap = 0;
     cudaError_t need(size_t n) {
         if (n <= cap && p) return cudaSuccess;
-        if (p) cudaFree(p);
+        if (p) dev_free(p);
         p = nullptr;
         cap = 0;
         const size_t want = n + n / 4 + 16;
-        const cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+        void *q = nullptr;
+        const cudaError_t e = dev_alloc(&q, want * sizeof(T));
+        p = static_cast<T *>(q);
         if (e == cudaSuccess) cap = want;
         return e;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) dev_free(p);
         p = nullptr;
         cap = 0;
     }

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -23,6 +24,34 @@
 using namespace ae;
 
 namespace ae {
+
+// Device allocations (devmem.h): live count and the failure injected by
+// ae_debug_fail_alloc_after (the n-th call from now fails; -1 = none).
+static std::atomic<long long> g_fail_after{-1};
+static std::atomic<long long> g_live_allocations{0};
+
+cudaError_t dev_alloc(void **p, size_t bytes) {
+    long long n = g_fail_after.load();
+    while (n >= 0 && !g_fail_after.compare_exchange_weak(n, n - 1)) {
+    }
+    if (n == 0) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    const cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess && *p) g_live_allocations++;
+    return e;
+}
+
+void dev_free(void *p) {
+    if (!p) return;
+    cudaFree(p);
+    g_live_allocations--;
+}
+
+static thread_local int g_create_status = AE_OK;
+void set_create_status(int status) { g_create_status = status; }
+int create_status() { return g_create_status; }
 
 int Ctx::fail(int code, const char *fmt, ...) {
     char buf[512];
@@ -182,12 +211,17 @@ int validate_scene(Ctx *c, const ae_object *objects, uint32_t n_objects, const a
 extern "C" {
 
 ae_ctx *ae_create(const ae_settings *s) {
+    ae::set_create_status(AE_OK);
     if (!s || s->width == 0 || s->height == 0) {
         fprintf(stderr, "ae_create: invalid settings\n");
+        ae::set_create_status(AE_ERR_INVALID);
         return nullptr;
     }
     Ctx *c = new (std::nothrow) Ctx();
-    if (!c) return nullptr;
+    if (!c) {
+        ae::set_create_status(AE_ERR_OOM);
+        return nullptr;
+    }
     c->settings = *s;
     if (c->settings.trace_scale <= 0.0f) c->settings.trace_scale = 1.0f;
     if (c->settings.hybrid_max_depth == 0) c->settings.hybrid_max_depth = 3;
@@ -198,7 +232,9 @@ ae_ctx *ae_create(const ae_settings *s) {
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
     if (e != cudaSuccess) {
         fprintf(stderr, "ae_create: %s\n", cudaGetErrorString(e));
+        cudaGetLastError();
         delete c;
+        ae::set_create_status(AE_ERR_CUDA);
         return nullptr;
     }
     // Config defaults of Renderer::Initialize (renderer/renderer.cpp:104-120).
@@ -218,6 +254,7 @@ ae_ctx *ae_create(const ae_settings *s) {
     if (c->accum.reserve(px) || c->frame.reserve(px) || c->display.reserve(px)) {
         fprintf(stderr, "ae_create: image allocation failed\n");
         delete c;
+        ae::set_create_status(AE_ERR_OOM);
         return nullptr;
     }
     cudaMemsetAsync(c->accum.ptr, 0, px * sizeof(float4), c->stream);
@@ -258,6 +295,10 @@ int ae_upload_geometry(ae_ctx *ctx, const ae_vertex *v, uint32_t nv, const uint3
     c->host_blas.assign(blas, blas + nb);
     c->host_vertices.assign(v, v + nv);
     c->fast_ready = false;
+    // The optimised structures and any captured frame graph derive from the
+    // old geometry: both are rebuilt on next use.
+    c->geometry_version++;
+    c->scene_version++;
     c->geometry_uploaded = true;
     return c->cuda(cudaStreamSynchronize(c->stream), "upload geometry");
 }
@@ -369,6 +410,23 @@ int ae_reset_accumulation(ae_ctx *ctx) {
     if (!c) return AE_ERR_INVALID;
     c->config.batch = 0;
     c->config.historyReset = 1;
+    return AE_OK;
+}
+
+int ae_debug_fail_alloc_after(int64_t n) {
+    ae::g_fail_after.store(n < 0 ? -1 : (long long)n);
+    return AE_OK;
+}
+
+int64_t ae_debug_live_allocations(void) { return (int64_t)ae::g_live_allocations.load(); }
+
+int ae_create_status(void) { return ae::create_status(); }
+
+int ae_debug_inject(ae_ctx *ctx, int fault, uint32_t on) {
+    Ctx *c = reinterpret_cast<Ctx *>(ctx);
+    if (!c) return AE_ERR_INVALID;
+    if (fault != AE_FAULT_TILE_WAIT) return c->fail(AE_ERR_INVALID, "unknown fault %d", fault);
+    c->fault_tile_wait = on ? 1u : 0u;
     return AE_OK;
 }
 

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/ae_b200.h"
+#include "devmem.h"
 #include "trace_common.cuh"
 
 namespace ae {
@@ -25,7 +26,7 @@ template <class T> struct DevBuf {
         if (n <= cap) return AE_OK;
         release();
         void *p = nullptr;
-        if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) {
+        if (dev_alloc(&p, n * sizeof(T)) != cudaSuccess) {
             cudaGetLastError();
             return AE_ERR_OOM;
         }
@@ -34,7 +35,7 @@ template <class T> struct DevBuf {
         return AE_OK;
     }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) dev_free(ptr);
         ptr = nullptr;
         cap = 0;
     }
@@ -81,7 +82,9 @@ struct Ctx {
     std::vector<uint32_t> host_lights;
     bool scene_uploaded = false;
     bool scene_has_ggx = false;  // an object uses AE_MAT_GGX_METAL (not shaded by the hybrid passes)
+    uint32_t fault_tile_wait = 0;  // ae_debug_inject(AE_FAULT_TILE_WAIT)
     uint64_t scene_version = 0;         // bumps on every change of scene content
+    uint64_t geometry_version = 0;      // bumps on every ae_upload_geometry
     uint64_t scene_version_layout = 0;  // bumps when arrays are re-uploaded (topology may change)
     DevBuf<float> obj_box;              // world box per object (refit)
 

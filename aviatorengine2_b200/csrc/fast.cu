@@ -246,6 +246,17 @@ int prepare_fast(Ctx *c) {
     if (!c->fast) c->fast = new (std::nothrow) FastScene();
     if (!c->fast) return c->fail(AE_ERR_OOM, "fast scene");
     FastScene &F = *c->fast;
+    if (F.geometry_key != c->geometry_version) {
+        // New geometry arrays: every mesh is converted again (the device
+        // buffers are reused).
+        F.mesh_roots.clear();
+        F.host_nodes.clear();
+        F.host_tris.clear();
+        F.max_stack = 0;
+        F.shade16_tris = 0;
+        F.geometry_key = c->geometry_version;
+        F.geometry_dirty = true;
+    }
     // Geometry-derived part: rebuilt when new meshes appear.
     bool rebuilt = false;
     for (uint32_t i = 0; i < c->n_instances; i++) {
@@ -280,12 +291,13 @@ int prepare_fast(Ctx *c) {
         F.host_nodes.insert(F.host_nodes.end(), local.begin(), local.end());
         F.max_stack = std::max(F.max_stack, need);
         F.mesh_roots[key] = std::make_pair(root, tri_base);
-        rebuilt = true;
+        F.geometry_dirty = true;
     }
     if (F.max_stack + 1 > kFastStack)
         return c->fail(AE_ERR_LAYOUT, "4-wide BVH needs %d stack entries (> %d)", F.max_stack + 1, kFastStack);
     int rc;
-    if (rebuilt) {
+    if (F.geometry_dirty) {
+        rebuilt = true;
         F.n_nodes = uint32_t(F.host_nodes.size());
         F.n_tris = uint32_t(F.host_tris.size() / 12);
         if (F.nodes.reserve(std::max<size_t>(F.n_nodes, 1)) || F.tris.reserve(std::max<size_t>(size_t(F.n_tris) * 3, 1)))
@@ -296,6 +308,7 @@ int prepare_fast(Ctx *c) {
         if ((rc = c->cuda(cudaMemcpyAsync(F.tris.ptr, F.host_tris.data(), F.host_tris.size() * sizeof(float),
                                           cudaMemcpyHostToDevice, c->stream), "upload triangles")))
             return rc;
+        F.geometry_dirty = false;
     }
     // Scene-derived part: instances and object metadata, per upload.
     if (F.scene_key != c->scene_version || rebuilt) {

@@ -58,8 +58,11 @@ struct FastScene {
     uint32_t walk_pos = 0;
     uint32_t n_nodes = 0, n_tris = 0;
     int max_stack = 0;
-    uint64_t geometry_key = 0, scene_key = ~0ull;
+    uint64_t geometry_key = ~0ull, scene_key = ~0ull;
     bool has_volumes = false;
+    // host_nodes / host_tris grew and are not on the device yet (an upload
+    // that failed is retried by the next prepare_fast)
+    bool geometry_dirty = false;
     // per distinct mesh (vertexBase, indexBase, triangleCount, blasBase)
     std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>, std::pair<uint32_t, uint32_t>> mesh_roots;
     std::vector<QNode> host_nodes;

@@ -118,9 +118,10 @@ static int image_error(ae_ctx *ctx, int which, const uint32_t *xy, uint32_t n_px
     const size_t xy_bytes = xy ? ((n * 2 * sizeof(uint32_t) + 15) / 16) * 16 : 0;
     const size_t part_bytes = kErrBlocks * sizeof(ErrPartial);
     void *scratch = nullptr;
-    if ((rc = c->cuda(cudaMalloc(&scratch, ref_bytes + xy_bytes + part_bytes + 4 * sizeof(double)),
-                      "image error scratch")))
-        return rc;
+    if (dev_alloc(&scratch, ref_bytes + xy_bytes + part_bytes + 4 * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return c->fail(AE_ERR_OOM, "image error scratch");
+    }
     double *d_ref = static_cast<double *>(scratch);
     uint32_t *d_xy = xy ? reinterpret_cast<uint32_t *>(static_cast<char *>(scratch) + ref_bytes) : nullptr;
     ErrPartial *d_part = reinterpret_cast<ErrPartial *>(static_cast<char *>(scratch) + ref_bytes + xy_bytes);
@@ -137,7 +138,7 @@ static int image_error(ae_ctx *ctx, int which, const uint32_t *xy, uint32_t n_px
     }
     if (!rc) rc = c->cuda(cudaMemcpyAsync(out4, d_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
     if (!rc) rc = c->cuda(cudaStreamSynchronize(c->stream), "image error");
-    cudaFree(scratch);
+    dev_free(scratch);
     return rc;
 }
 

@@ -80,7 +80,9 @@ struct ReqDev {
     uint32_t scene, n_pixels, frames, spp;
 };
 
-enum { SV_Q0 = 0, SV_Q1 = 1, SV_SH = 2, SV_ERR = 3, SV_TILE = 4, SV_IDLE0 = 5, SV_IDLE1 = 6, SV_NORDER = 7, SV_COUNT = 8 };
+// SV_FAULT: the injected tile-wait failure of ae_serve_debug_inject (0 = none).
+enum { SV_Q0 = 0, SV_Q1 = 1, SV_SH = 2, SV_ERR = 3, SV_TILE = 4, SV_IDLE0 = 5, SV_IDLE1 = 6, SV_NORDER = 7,
+       SV_FAULT = 8, SV_COUNT = 9 };
 enum { ST_RAYS = 0, ST_SHADOW = 1, ST_COUNT = 2 };
 
 struct SvView {
@@ -128,6 +130,16 @@ __global__ void k_sv_begin(SvView W, int q) {
     W.cnt[SV_IDLE0 + (q ^ 1)] = 0;
 }
 
+// Withdraws request-table entry t from pixel claims: its claim counter is
+// set to its pixel count (claim_pixel then passes it over), and the pixels
+// claimed before - the ones still to finish - are reported.  Runs on the
+// serving stream between replays, so no claim races with it.
+__global__ void k_sv_cancel(SvView W, uint32_t t, uint32_t *claimed) {
+    const uint32_t n = W.reqs[t].n_pixels;
+    const uint32_t old = atomicExch(W.next + t, n);
+    *claimed = old < n ? old : n;
+}
+
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS) k_sv_extend(SvView W, int q) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -136,6 +148,8 @@ __global__ void __launch_bounds__(THREADS) k_sv_extend(SvView W, int q) {
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tile_index;
     const uint32_t count = W.cnt[q];
+    // An injected failure issues no copy: the wait runs out with nothing in flight.
+    const bool inject = W.cnt[SV_FAULT] != 0;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     uint32_t phase = 0;
@@ -145,13 +159,15 @@ __global__ void __launch_bounds__(THREADS) k_sv_extend(SvView W, int q) {
         const uint32_t start = tile_index * THREADS;
         if (start >= count) break;
         const uint32_t m = min(uint32_t(THREADS), count - start);
-        if (threadIdx.x == 0) {
+        if (threadIdx.x == 0 && !inject) {
             mbar_expect_tx(&bar, m * uint32_t(sizeof(ae_ray)));
             bulk_g2s(tile, W.qray[q] + start, m * uint32_t(sizeof(ae_ray)), &bar);
         }
-        const bool ok = __syncthreads_and(mbar_wait(&bar, phase, 1u << 24) ? 1 : 0) != 0;
+        const bool ok = __syncthreads_and(mbar_wait(&bar, phase, inject ? 64u : (1u << 24)) ? 1 : 0) != 0;
         if (!ok) {
-            mbar_wait(&bar, phase, 1u << 24);
+            // As in the wavefront extend: a second bounded wait for a copy in
+            // flight, then the block exits and reports the timeout.
+            if (!inject) mbar_wait(&bar, phase, 1u << 24);
             if (threadIdx.x == 0) atomicOr(&W.cnt[SV_ERR], 1u);
             break;
         }
@@ -219,6 +235,9 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_sv_extend_walk(SvView
 }
 
 __global__ void __launch_bounds__(256) k_sv_shade(SvView W, int q) {
+    // After an extend that gave up, hit records past its last tile were never
+    // written: nothing of this queue is shaded (the host fails the requests).
+    if (W.cnt[SV_ERR]) return;
     const uint32_t count = W.cnt[q];
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
         const uint32_t slot = W.qslot[q][k];
@@ -477,6 +496,8 @@ struct HostReq {
     double t_submit = 0, t_admit = -1, t_done = -1;
     int status = 1;  // 1 = not finished
     int stage = 0;   // 0 queued, 1 on the GPU, 2 result being copied
+    uint32_t target = 0;  // finished pixels that complete it (lowered to the claimed ones on cancel)
+    bool cancel = false;  // withdrawn by ae_serve_cancel while on the GPU
 };
 
 struct MoveOp {
@@ -541,6 +562,8 @@ struct Server {
     std::map<uint64_t, std::unique_ptr<HostReq>> reqs;
     std::vector<std::deque<MoveOp>> moves;
     std::deque<HostReq *> copy_queue;
+    std::vector<HostReq *> cancels;  // admitted requests withdrawn, for the scheduler
+    DevBuf<uint32_t> cancel_claimed;
     std::vector<HostReq *> table;
     std::vector<int> table_free;
     std::vector<int> order_host;  // table entries in admission order
@@ -555,7 +578,7 @@ struct Server {
     uint64_t submitted = 0, completed = 0, rejected = 0, n_failed = 0, paths = 0, launches = 0;
     double first_submit = -1, last_done = -1;
     uint64_t peak_arena = 0;
-    uint32_t peak_resident = 0, moves_applied = 0, dev_errors = 0;
+    uint32_t peak_resident = 0, moves_applied = 0, dev_errors = 0, n_cancelled = 0;
     unsigned long long rays_base = 0;
 
     int fail_locked(int code, const char *fmt, ...) {
@@ -605,11 +628,11 @@ int Server::init() {
         qray.reserve(size_t(S) * 2) || qslot.reserve(size_t(S) * 2) || idle.reserve(size_t(S) * 2) ||
         qhit.reserve(S) || sh4.reserve(SL * 4) || sh8.reserve(SL * 2) || sq.reserve(SL) || cnt.reserve(SV_COUNT) ||
         next.reserve(R) || done.reserve(R) || order.reserve(R) || stats.reserve(ST_COUNT) ||
-        scenes_d.reserve(size_t(st.max_scenes) * kFrameSets) || reqs_d.reserve(R)) {
+        scenes_d.reserve(size_t(st.max_scenes) * kFrameSets) || reqs_d.reserve(R) || cancel_claimed.reserve(1)) {
         err = "slot pool allocation failed";
         return AE_ERR_OOM;
     }
-    if (cudaMalloc(&arena, st.arena_bytes) != cudaSuccess) {
+    if (dev_alloc(reinterpret_cast<void **>(&arena), st.arena_bytes) != cudaSuccess) {
         cudaGetLastError();
         arena = nullptr;
         err = "image arena allocation failed";
@@ -789,11 +812,12 @@ void Server::run() {
     uint64_t issued = 0, observed = 0;
     for (;;) {
         std::vector<MoveOp> todo_moves;
-        std::vector<HostReq *> admitted;
+        std::vector<HostReq *> admitted, todo_cancels;
         bool active;
         {
             std::unique_lock<std::mutex> lk(mu);
             if (stop || failed) break;
+            todo_cancels.swap(cancels);
             uint32_t s;
             while (policy.next_move(s)) {
                 if (moves[s].empty()) break;
@@ -812,6 +836,7 @@ void Server::run() {
                 table[r->table] = r;
                 r->t_admit = now_ms(t0);
                 r->stage = 1;
+                r->target = r->width * r->height;
                 r->admit_launch = issued;
                 order_host.push_back(r->table);
                 order_dirty = true;
@@ -875,6 +900,22 @@ void Server::run() {
                                                      cudaMemcpyHostToDevice, stream);
             cudaMemcpyAsync(cnt.ptr + SV_NORDER, ho + st.max_requests, sizeof(uint32_t), cudaMemcpyHostToDevice, stream);
         }
+        // Withdrawn requests stop claiming pixels before the next replay; the
+        // pixels already claimed finish and complete them.
+        for (HostReq *r : todo_cancels) {
+            if (r->stage != 1 || r->table < 0) continue;
+            uint32_t claimed = 0;
+            k_sv_cancel<<<1, 1, 0, stream>>>(view, uint32_t(r->table), cancel_claimed.ptr);
+            cudaError_t ce = cudaMemcpyAsync(&claimed, cancel_claimed.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                             stream);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(stream);
+            std::lock_guard<std::mutex> lk(mu);
+            if (ce != cudaSuccess) {
+                fail_all(AE_ERR_CUDA, std::string("cancel: ") + cudaGetErrorString(ce));
+                break;
+            }
+            r->target = claimed;
+        }
         if (active) {
             cudaGraphLaunch(graph, stream);
             uint32_t *hd = h_done + size_t(h) * (st.max_requests + 1);
@@ -920,7 +961,7 @@ void Server::run() {
             for (size_t i = 0; i < order_host.size();) {
                 const int t = order_host[i];
                 HostReq *r = table[t];
-                if (r && r->admit_launch <= observed && hd[t] >= r->width * r->height) {
+                if (r && r->admit_launch <= observed && hd[t] >= r->target) {
                     table[t] = nullptr;
                     table_free.push_back(t);
                     order_host.erase(order_host.begin() + long(i));
@@ -951,6 +992,20 @@ void Server::run_completer() {
             copy_queue.pop_front();
         }
         cudaError_t e = cudaSuccess;
+        if (r->cancel) {
+            // Withdrawn: its pixels in flight have finished; nothing is copied.
+            std::lock_guard<std::mutex> lk(mu);
+            policy.completed(r->id);
+            if (r->status == 1) {
+                r->status = AE_ERR_CANCELLED;
+                r->t_done = now_ms(t0);
+                n_cancelled++;
+                if (outstanding) outstanding--;
+            }
+            cv_done.notify_all();
+            cv_sched.notify_one();
+            continue;
+        }
         if (r->dst_accum)
             e = cudaMemcpyAsync(r->dst_accum, arena + r->offset, r->accum_bytes, cudaMemcpyDeviceToHost, copy_stream);
         if (e == cudaSuccess && r->dst_display)
@@ -997,7 +1052,7 @@ Server::~Server() {
     if (completer.joinable()) completer.join();
     if (graph) cudaGraphExecDestroy(graph);
     if (stream) cudaStreamSynchronize(stream);
-    if (arena) cudaFree(arena);
+    if (arena) dev_free(arena);
     if (h_req) cudaFreeHost(h_req);
     if (h_order) cudaFreeHost(h_order);
     if (h_done) cudaFreeHost(h_done);
@@ -1015,6 +1070,7 @@ using namespace ae;
 struct ae_server : Server {};
 
 extern "C" ae_server *ae_serve_create(const ae_serve_settings *settings) {
+    set_create_status(AE_ERR_INVALID);
     ae_serve_settings s{};
     if (settings) s = *settings;
     if (!s.slots) s.slots = 1u << 20;
@@ -1030,13 +1086,19 @@ extern "C" ae_server *ae_serve_create(const ae_serve_settings *settings) {
         s.slots > (1u << 26) || uint64_t(s.slots) * s.max_lights > 0xffffffffull)
         return nullptr;
     ae_server *srv = new (std::nothrow) ae_server();
-    if (!srv) return nullptr;
-    srv->st = s;
-    if (srv->init() != AE_OK) {
-        std::fprintf(stderr, "ae_serve_create: %s\n", srv->err.c_str());
-        delete srv;
+    if (!srv) {
+        set_create_status(AE_ERR_OOM);
         return nullptr;
     }
+    srv->st = s;
+    const int rc = srv->init();
+    if (rc != AE_OK) {
+        std::fprintf(stderr, "ae_serve_create: %s\n", srv->err.c_str());
+        delete srv;
+        set_create_status(rc);
+        return nullptr;
+    }
+    set_create_status(AE_OK);
     return srv;
 }
 
@@ -1166,6 +1228,45 @@ extern "C" int ae_serve_move_instances(ae_server *srv, uint32_t scene, const ae_
     return AE_OK;
 }
 
+extern "C" int ae_serve_cancel(ae_server *srv, uint64_t id) {
+    if (!srv) return AE_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    auto it = srv->reqs.find(id);
+    if (it == srv->reqs.end()) return srv->fail_locked(AE_ERR_INVALID, "unknown request %llu", (unsigned long long)id);
+    HostReq *r = it->second.get();
+    if (r->status != 1 || r->stage == 2 || r->cancel)
+        return srv->fail_locked(AE_ERR_STATE, "request %llu has finished or is being cancelled", (unsigned long long)id);
+    if (r->stage == 0) {
+        if (!srv->policy.withdraw(id)) return srv->fail_locked(AE_ERR_STATE, "request %llu is not queued", (unsigned long long)id);
+        r->status = AE_ERR_CANCELLED;
+        r->t_done = now_ms(srv->t0);
+        srv->n_cancelled++;
+        if (srv->outstanding) srv->outstanding--;
+        srv->cv_done.notify_all();
+        srv->cv_sched.notify_one();
+        return AE_OK;
+    }
+    r->cancel = true;
+    srv->cancels.push_back(r);
+    srv->cv_sched.notify_one();
+    return AE_OK;
+}
+
+// Test hook: the tile-staged extend of every later replay issues no copy and
+// lets its bounded wait run out (AE_FAULT_TILE_WAIT), so the timeout path runs
+// with nothing in flight.
+extern "C" int ae_serve_debug_inject(ae_server *srv, int fault, uint32_t on) {
+    if (!srv) return AE_ERR_INVALID;
+    if (fault != AE_FAULT_TILE_WAIT) return AE_ERR_INVALID;
+    const uint32_t v = on ? 1u : 0u;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (cudaMemcpy(srv->cnt.ptr + SV_FAULT, &v, sizeof(v), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        return AE_ERR_CUDA;
+    }
+    return AE_OK;
+}
+
 extern "C" int ae_serve_wait(ae_server *srv, uint64_t id, int32_t timeout_ms, ae_serve_result *out) {
     if (!srv) return AE_ERR_INVALID;
     std::unique_lock<std::mutex> lk(srv->mu);
@@ -1239,6 +1340,7 @@ extern "C" int ae_serve_get_stats(ae_server *srv, ae_serve_stats *out) {
     out->peak_resident = srv->peak_resident;
     out->moves_applied = srv->moves_applied;
     out->errors = srv->dev_errors;
+    out->cancelled = srv->n_cancelled;
     return AE_OK;
 }
 
@@ -1253,6 +1355,7 @@ extern "C" int ae_serve_reset_stats(ae_server *srv) {
     std::lock_guard<std::mutex> lk(srv->mu);
     srv->latencies.clear();
     srv->submitted = srv->completed = srv->rejected = srv->n_failed = srv->paths = srv->launches = 0;
+    srv->n_cancelled = 0;
     srv->first_submit = srv->last_done = -1;
     srv->peak_arena = srv->policy.arena().used();
     srv->peak_resident = srv->policy.resident();

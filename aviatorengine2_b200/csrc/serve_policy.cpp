@@ -141,6 +141,17 @@ void Policy::completed(uint64_t id) {
     active_.erase(it);
 }
 
+bool Policy::withdraw(uint64_t id) {
+    for (auto it = pending_.begin(); it != pending_.end(); ++it) {
+        if (it->id != id) continue;
+        auto o = outstanding_.find({it->scene, it->version});
+        if (o != outstanding_.end() && o->second) o->second--;
+        pending_.erase(it);
+        return true;
+    }
+    return false;
+}
+
 std::vector<uint64_t> Policy::cancel_pending() {
     std::vector<uint64_t> ids;
     for (const PolicyRequest &r : pending_) {
@@ -183,6 +194,27 @@ extern "C" int ae_serve_policy_simulate(const ae_policy_event *events, uint32_t 
             if (e.kind == AE_POLICY_MOVE) {
                 P.move(e.scene);
                 moves[e.scene].push_back(next_event);
+            } else if (e.kind == AE_POLICY_CANCEL) {
+                // Withdraw request event `footprint`: a queued one at once, an
+                // admitted one as if its work in flight drained this tick.  A
+                // request that has not arrived yet or has finished is left as is.
+                const uint64_t target = e.footprint;
+                out[next_event].admit_tick = out[next_event].done_tick = int32_t(t);
+                finished++;
+                if (target < n && events[target].kind == AE_POLICY_REQUEST && out[target].done_tick < 0 &&
+                    out[target].status == AE_OK) {
+                    if (P.withdraw(target)) {
+                        out[target].status = AE_ERR_CANCELLED;
+                        out[target].done_tick = int32_t(t);
+                        finished++;
+                    } else if (remaining.count(target)) {
+                        remaining.erase(target);
+                        P.completed(target);
+                        out[target].status = AE_ERR_CANCELLED;
+                        out[target].done_tick = int32_t(t);
+                        finished++;
+                    }
+                }
             } else {
                 PolicyRequest r;
                 r.id = next_event;

@@ -70,6 +70,10 @@ class Policy {
     bool next_admission(PolicyRequest &out, uint64_t &offset);
     // Releases a completed request's arena block and resident slot.
     void completed(uint64_t id);
+    // Removes a request still queued (not admitted); false when it is not
+    // queued.  An admitted request is withdrawn through completed() once its
+    // work in flight has drained.
+    bool withdraw(uint64_t id);
     // Drops every queued request (server shutdown); returns their ids.
     std::vector<uint64_t> cancel_pending();
 

@@ -54,7 +54,9 @@ struct WfParams {
 // Device counters: [0],[1] ray queue sizes (ping-pong), [2] shadow queue,
 // [3] error flags, [4..4+kMaxBounce) extend tile counters, then shadow tiles.
 constexpr int kMaxBounce = 64;
-enum { C_Q0 = 0, C_Q1 = 1, C_SH = 2, C_ERR = 3, C_TILE = 4, C_SHTILE = 4 + kMaxBounce, C_COUNT = 4 + 2 * kMaxBounce };
+// C_FAULT: the injected tile-wait failure of ae_debug_inject (0 = none).
+enum { C_Q0 = 0, C_Q1 = 1, C_SH = 2, C_ERR = 3, C_TILE = 4, C_SHTILE = 4 + kMaxBounce, C_FAULT = 4 + 2 * kMaxBounce,
+       C_COUNT = 5 + 2 * kMaxBounce };
 
 struct WfView {
     ae_ray *qray[2];
@@ -154,6 +156,10 @@ __global__ void __launch_bounds__(THREADS) k_wf_extend(DevScene S, FastView V, W
     __shared__ uint32_t tile_index;
     const int q = bounce & 1;
     const uint32_t count = W.cnt[q];
+    // An injected failure (ae_debug_inject) issues no copy and waits on the
+    // unarmed phase for a few polls: the timeout path runs with nothing in
+    // flight.
+    const bool inject = W.cnt[C_FAULT] != 0;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     uint32_t phase = 0;
@@ -163,17 +169,22 @@ __global__ void __launch_bounds__(THREADS) k_wf_extend(DevScene S, FastView V, W
         const uint32_t start = tile_index * THREADS;
         if (start >= count) break;
         const uint32_t m = min(uint32_t(THREADS), count - start);
-        if (threadIdx.x == 0) {
+        if (threadIdx.x == 0 && !inject) {
             mbar_expect_tx(&bar, m * uint32_t(sizeof(ae_ray)));
             bulk_g2s(tile, W.qray[q] + start, m * uint32_t(sizeof(ae_ray)), &bar);
         }
         // Every thread polls the barrier (bounded); the block then agrees on
         // the outcome so no thread leaves while others wait at a barrier.
-        const bool ok = __syncthreads_and(mbar_wait(&bar, phase, 1u << 24) ? 1 : 0) != 0;
+        const bool ok = __syncthreads_and(mbar_wait(&bar, phase, inject ? 64u : (1u << 24)) ? 1 : 0) != 0;
         if (!ok) {
-            // Give the copy in flight a second bounded chance to land before
-            // the block exits, then report the timeout.
-            mbar_wait(&bar, phase, 1u << 24);
+            // A copy that has not landed after 2^24 polls gets a second
+            // bounded wait before the block exits and reports the timeout.
+            // Should it still be outstanding then, the block exits with a
+            // bulk copy into its shared memory in flight, which PTX leaves
+            // undefined; the bound keeps a kernel from hanging the GPU
+            // instead.  A global-to-shared copy of at most 8 KB has never
+            // come near it.
+            if (!inject) mbar_wait(&bar, phase, 1u << 24);
             if (threadIdx.x == 0) atomicOr(&W.cnt[C_ERR], 1u);
             break;
         }
@@ -239,6 +250,9 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_wf_extend_walk(DevSce
 // Shade: one queued path per thread (ColorRay's body after the traversal).
 template <bool PREC>
 __global__ void __launch_bounds__(256) k_wf_shade(DevScene S, FastView V, WfView W, int bounce) {
+    // After an extend that gave up, hit records past its last tile were never
+    // written: nothing is shaded, the frame ends and reports the timeout.
+    if (W.cnt[C_ERR]) return;
     const WfParams &P = *W.P;
     const int q = bounce & 1;
     const uint32_t count = W.cnt[q];
@@ -633,6 +647,12 @@ int render_wavefront(Ctx *c, bool prec) {
         if ((rc = c->cuda(ce, "graph instantiate"))) return rc;
         Wf.graph_key = key;
     }
+    // The error word counts this frame only; the fault word carries an
+    // injected failure (ae_debug_inject) into the extend kernels.
+    if ((rc = c->cuda(cudaMemsetAsync(Wf.cnt.ptr + C_ERR, 0, sizeof(uint32_t), c->stream), "reset error word")) ||
+        (rc = c->cuda(cudaMemsetAsync(Wf.cnt.ptr + C_FAULT, c->fault_tile_wait ? 0xff : 0, sizeof(uint32_t),
+                                      c->stream), "fault word")))
+        return rc;
     if ((rc = c->timed_begin())) return rc;
     for (uint32_t s = 0; s < hp.spp; s++) {
         hp.sample = s;
@@ -647,6 +667,13 @@ int render_wavefront(Ctx *c, bool prec) {
     }
     c->launches--;  // timed_end counts one
     if ((rc = c->timed_end())) return rc;
+    // A bounded device-side wait that gave up makes the frame incomplete.
+    uint32_t e = 0;
+    if ((rc = c->cuda(cudaMemcpyAsync(&e, Wf.cnt.ptr + C_ERR, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream),
+                      "read error word")) ||
+        (rc = c->cuda(cudaStreamSynchronize(c->stream), "frame")))
+        return rc;
+    if (e) return c->fail(AE_ERR_TIMEOUT, "a bounded queue-tile wait gave up on the device; the frame is incomplete");
     return AE_OK;
 }
 

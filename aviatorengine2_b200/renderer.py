@@ -33,7 +33,7 @@ class Context:
         s["trace_scale"], s["history_while_moving"], s["device"] = trace_scale, history_while_moving, device
         self._h = lib().ae_create(ptr(s))
         if not self._h:
-            raise _lib.AeError(-5, "ae_create failed (see stderr)")
+            raise _lib.AeError(lib().ae_create_status(), "ae_create failed (see stderr)")
         self.width, self.height = width, height
         self.scene = None
 
@@ -220,6 +220,10 @@ class Context:
         out = np.zeros(4, np.float64)
         self._chk(lib().ae_image_error_pixels(self._h, which, ptr(xy), len(xy), ptr(ref), eps, ptr(out)))
         return {"mre": out[0], "mae": out[1], "max": out[2], "rmse": out[3]}
+
+    def debug_inject(self, fault, on=True):
+        """Test hook (ae_debug_inject): e.g. _lib.FAULT_TILE_WAIT."""
+        self._chk(lib().ae_debug_inject(self._h, fault, 1 if on else 0))
 
     def prepare_fast(self):
         self._chk(lib().ae_prepare_fast(self._h))

@@ -27,7 +27,7 @@ class Server:
         s["extend_threads"], s["max_scenes"], s["claim_policy"] = extend_threads, max_scenes, claim_policy
         self._h = lib().ae_serve_create(ptr(s))
         if not self._h:
-            raise _lib.AeError(-5, "ae_serve_create failed (see stderr)")
+            raise _lib.AeError(lib().ae_create_status(), "ae_serve_create failed (see stderr)")
         self._scenes = []    # contexts stay alive while the server holds them
         self._outputs = {}   # request id -> (accum, display) host buffers
 
@@ -83,6 +83,15 @@ class Server:
         ins = np.ascontiguousarray(instances, _lib.INSTANCE)
         self._chk(lib().ae_serve_move_instances(self._h, scene, ptr(ins), len(ins)))
 
+    def cancel(self, rid):
+        """Withdraws a request (ae_serve_cancel); wait() then raises AeError
+        with code -9 (AE_ERR_CANCELLED) for it."""
+        self._chk(lib().ae_serve_cancel(self._h, rid))
+
+    def debug_inject(self, fault, on=True):
+        """Test hook (ae_serve_debug_inject)."""
+        self._chk(lib().ae_serve_debug_inject(self._h, fault, 1 if on else 0))
+
     def wait(self, rid, timeout_ms=-1):
         """(result record, accum image, display image) of a finished request."""
         out = np.zeros(1, _lib.SERVE_RESULT)
@@ -99,7 +108,7 @@ class Server:
     def stats(self):
         out = np.zeros(1, _lib.SERVE_STATS)
         self._chk(lib().ae_serve_get_stats(self._h, ptr(out)))
-        return {k: out[0][k].item() for k in _lib.SERVE_STATS.names if k != "pad"}
+        return {k: out[0][k].item() for k in _lib.SERVE_STATS.names}
 
     def reset_stats(self):
         self._chk(lib().ae_serve_reset_stats(self._h))

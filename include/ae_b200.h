@@ -49,7 +49,8 @@ typedef enum ae_status {
     AE_ERR_CUDA = -5,        /* a CUDA runtime call failed                        */
     AE_ERR_TIMEOUT = -6,     /* a bounded device-side wait gave up                */
     AE_ERR_STATE = -7,       /* call order violated (e.g. trace before upload)    */
-    AE_ERR_REJECTED = -8     /* serving: request refused at admission             */
+    AE_ERR_REJECTED = -8,    /* serving: request refused at admission             */
+    AE_ERR_CANCELLED = -9    /* serving: request withdrawn by ae_serve_cancel      */
 } ae_status;
 
 /* ------------------------------------------------------------------------ */
@@ -639,7 +640,7 @@ typedef struct ae_serve_stats {
     uint64_t peak_arena_bytes;
     uint32_t peak_resident, moves_applied;
     uint32_t errors;           /* device error flags (bounded waits that gave up) */
-    uint32_t pad;
+    uint32_t cancelled;        /* requests ended by ae_serve_cancel */
 } ae_serve_stats;
 
 ae_server *ae_serve_create(const ae_serve_settings *settings);
@@ -656,6 +657,13 @@ int ae_serve_submit(ae_server *srv, const ae_serve_request *req, uint64_t *id);
  * instances), so a move is applied while requests of the previous version
  * still run; only requests two versions back must have finished. */
 int ae_serve_move_instances(ae_server *srv, uint32_t scene, const ae_instance *instances, uint32_t n);
+/* Withdraws a request (no counterpart in the reference).  A queued request
+ * ends at once; one on the GPU stops claiming pixels, its pixels in flight
+ * finish, and then its slots and its image block in the arena go back to the
+ * pool; requests beside it are unaffected.  Its result is not copied out;
+ * ae_serve_wait returns AE_ERR_CANCELLED for it.  AE_ERR_STATE when the
+ * request has already finished or is having its result copied. */
+int ae_serve_cancel(ae_server *srv, uint64_t id);
 /* Waits for a request (timeout_ms < 0: forever); returns its status, or
  * AE_ERR_TIMEOUT.  The record is released once it has been returned. */
 int ae_serve_wait(ae_server *srv, uint64_t id, int32_t timeout_ms, ae_serve_result *out);
@@ -669,9 +677,10 @@ int ae_serve_reset_stats(ae_server *srv);
  * host, with no GPU: requests (footprint, service ticks) and instance moves
  * arrive at ticks; out[i] tells when each was admitted / applied and done.
  * frame_sets = copies of each scene's per-frame arrays (the server uses 2). */
-enum { AE_POLICY_REQUEST = 0, AE_POLICY_MOVE = 1 };
+enum { AE_POLICY_REQUEST = 0, AE_POLICY_MOVE = 1, AE_POLICY_CANCEL = 2 };
 typedef struct ae_policy_event {
-    uint32_t kind;             /* AE_POLICY_REQUEST or AE_POLICY_MOVE */
+    uint32_t kind;             /* AE_POLICY_REQUEST, AE_POLICY_MOVE, or AE_POLICY_CANCEL:
+                                  footprint = index of the request event withdrawn */
     uint32_t scene;
     uint32_t tick;             /* arrival; non-decreasing over the list */
     uint32_t service_ticks;    /* requests: ticks on the GPU once admitted */
@@ -681,12 +690,41 @@ typedef struct ae_policy_outcome {
     int32_t admit_tick;        /* -1 = never; moves: the tick it was applied */
     int32_t done_tick;
     uint32_t version;          /* requests: moves of the scene before it; moves: version after */
-    int32_t status;            /* AE_OK or AE_ERR_REJECTED */
+    int32_t status;            /* AE_OK, AE_ERR_REJECTED or AE_ERR_CANCELLED */
     uint64_t offset;           /* requests: arena offset */
 } ae_policy_outcome;
 int ae_serve_policy_simulate(const ae_policy_event *events, uint32_t n, uint64_t arena_bytes,
                              uint32_t max_resident, uint32_t n_scenes, uint32_t frame_sets,
                              uint32_t max_ticks, ae_policy_outcome *out);
+
+/* ------------------------------------------------------------------------ */
+/* Test hooks (no counterpart in the reference): failures made on purpose so */
+/* the error paths can be exercised without faulting or exhausting a GPU.    */
+/* ------------------------------------------------------------------------ */
+
+/* The n-th device allocation of the library from now fails (n = 0: the next
+ * one) as if the GPU were out of memory; the ones after it succeed again.
+ * n < 0 clears a pending failure.  Process-wide. */
+int ae_debug_fail_alloc_after(int64_t n);
+/* Device allocations of the library currently live (all contexts, servers
+ * and builders of the process): equal before and after a failed call when
+ * nothing leaked. */
+int64_t ae_debug_live_allocations(void);
+/* Why the last ae_create or ae_serve_create on the calling thread returned
+ * NULL (AE_ERR_INVALID, AE_ERR_OOM, AE_ERR_CUDA), or AE_OK after a success.
+ * Both constructors return a handle as the reference's Renderer::Initialize
+ * returns a bool; this gives the failure class. */
+int ae_create_status(void);
+/* AE_FAULT_TILE_WAIT: the tile-staged extend kernels issue no bulk copy and
+ * their bounded wait on the (unarmed) mbarrier phase runs out after a few
+ * polls, as a copy that never lands would; no copy is in flight when they
+ * give up.  ae_render_frame (wavefront forms) then returns AE_ERR_TIMEOUT;
+ * on a server, every unfinished request ends with AE_ERR_TIMEOUT (serving
+ * uses the tile-staged extend when extend_threads != 0).  on = 0 turns the
+ * fault off. */
+enum { AE_FAULT_TILE_WAIT = 1 };
+int ae_debug_inject(ae_ctx *ctx, int fault, uint32_t on);
+int ae_serve_debug_inject(ae_server *srv, int fault, uint32_t on);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -155,3 +155,43 @@ def test_random_streams_keep_invariants(seed, frame_sets):
             assert out[i]["version"] == moves_before[s]
             if out[i]["version"] > 0 and out[i]["status"] == 0:
                 assert out[i]["admit_tick"] >= applied_at[(s, int(out[i]["version"]))]
+
+
+def _cancel(tick, target):
+    return dict(kind=_lib.POLICY_CANCEL, tick=tick, footprint=target)
+
+
+def test_cancel_queued_request_frees_its_turn():
+    # Request 1 waits behind request 0; withdrawn while queued, it never runs
+    # and request 3 takes the arena after request 0.
+    ev = [_req(0, 60 * MB, 5), _req(1, 60 * MB, 5), _cancel(2, 1), _req(3, 60 * MB, 1)]
+    code, out = simulate_policy(ev, 100 * MB, 16, 1)
+    assert code == 0
+    assert out[1]["status"] == -9 and out[1]["admit_tick"] == -1 and out[1]["done_tick"] == 2
+    assert out[3]["admit_tick"] == 5
+
+
+def test_cancel_admitted_request_releases_arena_and_slot():
+    # Request 0 holds most of the arena for 50 ticks; withdrawn at tick 3,
+    # its block is released and request 1 is admitted that tick.
+    ev = [_req(0, 90 * MB, 50), _req(1, 90 * MB, 2), _cancel(3, 0)]
+    code, out = simulate_policy(ev, 100 * MB, 1, 1)
+    assert code == 0
+    assert out[0]["status"] == -9 and out[0]["done_tick"] == 3
+    assert out[1]["status"] == 0 and out[1]["admit_tick"] == 3
+
+
+def test_cancel_of_finished_request_changes_nothing():
+    ev = [_req(0, 10 * MB, 1), _cancel(5, 0)]
+    code, out = simulate_policy(ev, 100 * MB, 4, 1)
+    assert code == 0 and out[0]["status"] == 0 and out[0]["done_tick"] == 0
+
+
+def test_cancel_unblocks_move_waiting_for_its_version():
+    # With one frame set a move waits for every request of the old version;
+    # withdrawing the long one lets the move apply at the cancel tick.
+    ev = [_req(0, 1 * MB, 100), _move(1), _cancel(4, 0)]
+    code, out = simulate_policy(ev, 100 * MB, 4, 1, frame_sets=1)
+    assert code == 0
+    assert out[0]["status"] == -9
+    assert out[1]["admit_tick"] == 4
