@@ -355,6 +355,64 @@ def measure_paths(local, width, height, frames=2, mre_pixels=1024):
     return out
 
 
+def measure_config1(local, frames=16, budget_s=8.0, check_pixels=1024):
+    """The plain method's small case: the Cornell box (8 objects, 36
+    triangles) at 320x240, `frames` frames of 1 spp (16 spp accumulated),
+    depth 8.  GPU: the plain megakernel and the wavefront form, each frame
+    timed on the device.  CPU: the reference's own compute shader compiled
+    for the CPU (oracle/_ref), all host cores, whole frames until about
+    `budget_s`; its accumulation after all frames at `check_pixels` seeded
+    pixels is compared with the GPU's bit for bit."""
+    from aviatorengine2_b200 import Context, _lib, scenes
+    O, _ = _oracle_modules()
+    scene = scenes.cornell_box()
+    W, H = int(scene.config["width"]), int(scene.config["height"])
+    out = {"workload": f"cornell_box {W}x{H}, {frames} frames of 1 spp, depth {int(scene.config['depth'])}",
+           "triangles": int(scene.triangles), "objects": int(len(scene.objects))}
+    accs = {}
+    with Context(W, H, device=local) as ctx:
+        ctx.upload(scene)
+        for name, mode in (("plain", _lib.MODE_COMPUTE_ONLY), ("wavefront", _lib.MODE_WAVEFRONT)):
+            c = scene.config.copy()
+            ms = []
+            for rep in range(2):  # the first pass warms up (and tunes the wavefront)
+                for b in range(frames):
+                    c["batch"] = b
+                    ctx.set_config(c)
+                    ctx.render_frame(mode)
+                    ctx.synchronize()
+                    if rep:
+                        ms.append(ctx.last_kernel_ms())
+            accs[name] = ctx.read_image(_lib.IMAGE_ACCUM)
+            out[name] = {"ms_per_frame": float(np.mean(ms)), "ms_16spp": float(np.sum(ms)),
+                         "mpaths": W * H / (float(np.mean(ms)) / 1e3) / 1e6}
+    out["wavefront_equals_plain"] = bool(np.array_equal(accs["plain"].view(np.uint32),
+                                                        accs["wavefront"].view(np.uint32)))
+    if O.ref_available():
+        cores = os.cpu_count() or 1
+        px = seeded_pixels(W, H, check_pixels, 31)
+        c = scene.config.copy()
+        acc = None
+        for b in range(frames):
+            c["batch"] = b
+            acc, _ = O.ref_render(scene, c, acc, threads=cores, pixels=px)
+        out["bit_exact_vs_reference_sample"] = bool(np.array_equal(
+            acc[px[:, 1], px[:, 0]].view(np.uint32), accs["plain"][px[:, 1], px[:, 0]].view(np.uint32)))
+        acc = None
+        t0 = time.perf_counter()
+        done = 0
+        while done < frames and (done == 0 or time.perf_counter() - t0 < budget_s):
+            c["batch"] = done
+            acc, _ = O.ref_render(scene, c, acc, threads=cores)
+            done += 1
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": W * H * done / dt / 1e6, "unit": "Mpaths/s", "cores": cores,
+                               "kind": "reference", "ms_per_frame": dt / done * 1e3,
+                               "sample": f"{done} whole frames of the reference's compute shader on the CPU"}
+        out["speedup_plain_vs_cpu"] = out["plain"]["mpaths"] / out["cpu_baseline"]["value"]
+    return out
+
+
 def timed_closest_hit(ctx, d_rays, n, d_hits, variant, flush, reps=5):
     """Mean CUDA-event time (ms) of one closest-hit launch over device rays,
     L2 flushed before each, on the context's stream."""
@@ -682,6 +740,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-build", action="store_true", help="skip the BVH build leg")
     ap.add_argument("--no-config4", action="store_true", help="skip the precision-variant leg (960x540)")
+    ap.add_argument("--no-config1", action="store_true", help="skip the small plain-method leg (Cornell box)")
     ap.add_argument("--c4-frames", type=int, default=1024, help="frames (1 spp each) of the precision-variant leg")
     ap.add_argument("--mre-pixels", type=int, default=2048, help="seeded pixels scored against the FP64 oracle")
     ap.add_argument("--serve-requests", type=int, default=16)
@@ -849,6 +908,9 @@ def main():
     build = None
     if not args.no_build and rank == 0:
         build = measure_build(local)
+    config1 = None
+    if not args.no_config1 and rank == 0:
+        config1 = measure_config1(local)
     config4 = None
     if not args.no_config4 and rank == 0:
         config4 = measure_config4(local, args.c4_frames, args.mre_pixels)
@@ -868,7 +930,7 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "per_step_ms": [round(t, 4) for t in times],
-            "paths": paths, "config4": config4, "serving": serving, "bvh_build": build}
+            "paths": paths, "config1": config1, "config4": config4, "serving": serving, "bvh_build": build}
     if sweep is not None:
         line["serving_sweep"] = sweep
     if rank == 0:

@@ -1,7 +1,7 @@
 """Generates the golden fixtures of tests/golden/ from the REFERENCE's own code
 run on the CPU: its scene headers (BuildBVH, MeshLibrary::Add) and its
 compute-only shader, both compiled by oracle/Makefile into oracle/_ref/ from a
-reference checkout (REF, default /root/reference).  Run in a tree where
+reference checkout (located by oracle/Makefile, AE_REFERENCE_DIR).  Run in a tree where
 oracle/_ref/ is built:
 
     make -C oracle ref && python tests/golden/make_golden.py
