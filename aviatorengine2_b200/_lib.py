@@ -67,7 +67,8 @@ SERVE_STATS = np.dtype([("submitted", "<u8"), ("completed", "<u8"), ("rejected",
                         ("paths", "<u8"), ("rays", "<u8"), ("first_submit_ms", "<f8"), ("last_done_ms", "<f8"),
                         ("p50_ms", "<f8"), ("p99_ms", "<f8"), ("mean_ms", "<f8"), ("max_ms", "<f8"),
                         ("launches", "<u8"), ("peak_arena_bytes", "<u8"), ("peak_resident", "<u4"),
-                        ("moves_applied", "<u4"), ("errors", "<u4"), ("cancelled", "<u4")])
+                        ("moves_applied", "<u4"), ("errors", "<u4"), ("cancelled", "<u4"),
+                        ("moves_coalesced", "<u4"), ("pad", "<u4")])
 POLICY_EVENT = np.dtype([("kind", "<u4"), ("scene", "<u4"), ("tick", "<u4"), ("service_ticks", "<u4"),
                          ("footprint", "<u8")])
 POLICY_OUTCOME = np.dtype([("admit_tick", "<i4"), ("done_tick", "<i4"), ("version", "<u4"), ("status", "<i4"),
@@ -75,7 +76,7 @@ POLICY_OUTCOME = np.dtype([("admit_tick", "<i4"), ("done_tick", "<i4"), ("versio
 
 for _dt, _size in ((VERTEX, 32), (NODE, 48), (OBJECT, 128), (INSTANCE, 48), (RAY, 32), (HIT, 20), (CONFIG, 240),
                    (AABB, 24), (SETTINGS, 64), (QNODE, 64), (SERVE_SETTINGS, 56), (SERVE_REQUEST, 280),
-                   (SERVE_RESULT, 64), (SERVE_STATS, 128), (POLICY_EVENT, 24), (POLICY_OUTCOME, 24)):
+                   (SERVE_RESULT, 64), (SERVE_STATS, 136), (POLICY_EVENT, 24), (POLICY_OUTCOME, 24)):
     assert _dt.itemsize == _size, (_dt, _size)
 
 # Enumerations (include/ae_b200.h)

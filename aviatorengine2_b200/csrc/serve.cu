@@ -30,8 +30,9 @@
 //
 // Host side.  A scheduler thread admits queued requests (serve_policy.h:
 // arrival order, by image footprint inside an arena allocated once, and by
-// resident request slots), applies instance moves with the GPU refit when no
-// request of the scene's previous version is outstanding, replays the graph
+// resident request slots), applies instance moves with the GPU refit into a
+// copy of the scene's per-frame arrays that no outstanding request renders
+// (coalescing moves no request needs, serve_policy.h), replays the graph
 // while any request is on the GPU (two replays in flight), and watches the
 // per-request pixel counters.  A completion thread copies finished images to
 // the caller's memory and releases their arena blocks.
@@ -497,12 +498,14 @@ struct HostReq {
     int status = 1;  // 1 = not finished
     int stage = 0;   // 0 queued, 1 on the GPU, 2 result being copied
     uint32_t target = 0;  // finished pixels that complete it (lowered to the claimed ones on cancel)
+    uint32_t copy = 0;    // the copy of its scene's per-frame arrays it renders from
     bool cancel = false;  // withdrawn by ae_serve_cancel while on the GPU
 };
 
 struct MoveOp {
     uint32_t scene;
     uint32_t version = 0;  // the scene version this move creates
+    uint32_t copy = 0;     // the copy of the per-frame arrays it is written into
     std::vector<ae_instance> inst;
 };
 
@@ -515,7 +518,7 @@ struct FrameSet {
     DevBuf<ae_instance> instances;
     DevBuf<FastInst> inst;
 };
-constexpr uint32_t kFrameSets = 2;
+constexpr uint32_t kFrameSets = AE_SERVE_FRAME_SETS;
 
 typedef void (*SvExtendFn)(SvView, int);
 
@@ -578,7 +581,7 @@ struct Server {
     uint64_t submitted = 0, completed = 0, rejected = 0, n_failed = 0, paths = 0, launches = 0;
     double first_submit = -1, last_done = -1;
     uint64_t peak_arena = 0;
-    uint32_t peak_resident = 0, moves_applied = 0, dev_errors = 0, n_cancelled = 0;
+    uint32_t peak_resident = 0, moves_applied = 0, moves_coalesced = 0, dev_errors = 0, n_cancelled = 0;
     unsigned long long rays_base = 0;
 
     int fail_locked(int code, const char *fmt, ...) {
@@ -783,7 +786,7 @@ int Server::apply_move(MoveOp &m) {
     int rc = ae_refit_instances(reinterpret_cast<ae_ctx *>(c), m.inst.data(), uint32_t(m.inst.size()));
     if (rc == AE_OK) rc = prepare_fast(c);
     if (rc == AE_OK) rc = c->cuda(cudaStreamSynchronize(c->stream), "refit");
-    if (rc == AE_OK) rc = fill_frame_set(m.scene, m.version % kFrameSets);
+    if (rc == AE_OK) rc = fill_frame_set(m.scene, m.copy);
     if (rc != AE_OK) {
         std::lock_guard<std::mutex> lk(mu);
         err = "instance move: " + (c->err.empty() ? std::string("frame set copy failed") : c->err);
@@ -818,14 +821,23 @@ void Server::run() {
             std::unique_lock<std::mutex> lk(mu);
             if (stop || failed) break;
             todo_cancels.swap(cancels);
-            uint32_t s;
-            while (policy.next_move(s)) {
-                if (moves[s].empty()) break;
+            uint32_t s, v, cp;
+            bool coalesced = false;
+            while (policy.next_move(s, v, cp)) {
+                // Moves below version v are superseded by it (absolute transforms).
+                while (!moves[s].empty() && moves[s].front().version < v) {
+                    moves[s].pop_front();
+                    moves_coalesced++;
+                    coalesced = true;
+                    if (outstanding) outstanding--;
+                }
+                if (moves[s].empty() || moves[s].front().version != v) break;  // not reached: v was submitted
                 todo_moves.push_back(std::move(moves[s].front()));
                 moves[s].pop_front();
-                policy.move_applied(s);  // requests of the new version wait for this iteration's upload
-                todo_moves.back().version = policy.applied(s);
+                todo_moves.back().copy = cp;
+                policy.move_applied(s, v, cp);  // requests of version v wait for this iteration's upload
             }
+            if (coalesced) cv_done.notify_all();
             PolicyRequest pr;
             uint64_t off;
             while (!table_free.empty() && policy.next_admission(pr, off)) {
@@ -836,6 +848,7 @@ void Server::run() {
                 table[r->table] = r;
                 r->t_admit = now_ms(t0);
                 r->stage = 1;
+                r->copy = pr.copy;
                 r->target = r->width * r->height;
                 r->admit_launch = issued;
                 order_host.push_back(r->table);
@@ -881,7 +894,7 @@ void Server::run() {
                 d.F = make_frame_params(cfg);
                 d.accum = reinterpret_cast<float4 *>(arena + r->offset);
                 d.display = reinterpret_cast<uchar4 *>(arena + r->offset + r->accum_bytes);
-                d.scene = r->scene * kFrameSets + r->version % kFrameSets;
+                d.scene = r->scene * kFrameSets + r->copy;
                 d.n_pixels = r->width * r->height;
                 d.frames = r->frames;
                 d.spp = d.F.spp;
@@ -1221,8 +1234,8 @@ extern "C" int ae_serve_move_instances(ae_server *srv, uint32_t scene, const ae_
     MoveOp m;
     m.scene = scene;
     m.inst.assign(instances, instances + n);
+    m.version = srv->policy.move(scene);
     srv->moves[scene].push_back(std::move(m));
-    srv->policy.move(scene);
     srv->outstanding++;
     srv->cv_sched.notify_one();
     return AE_OK;
@@ -1339,6 +1352,7 @@ extern "C" int ae_serve_get_stats(ae_server *srv, ae_serve_stats *out) {
     out->peak_arena_bytes = srv->peak_arena;
     out->peak_resident = srv->peak_resident;
     out->moves_applied = srv->moves_applied;
+    out->moves_coalesced = srv->moves_coalesced;
     out->errors = srv->dev_errors;
     out->cancelled = srv->n_cancelled;
     return AE_OK;
@@ -1360,6 +1374,7 @@ extern "C" int ae_serve_reset_stats(ae_server *srv) {
     srv->peak_arena = srv->policy.arena().used();
     srv->peak_resident = srv->policy.resident();
     srv->moves_applied = 0;
+    srv->moves_coalesced = 0;
     srv->rays_base = dev[ST_RAYS] + dev[ST_SHADOW];
     return AE_OK;
 }

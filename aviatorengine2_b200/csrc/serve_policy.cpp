@@ -67,13 +67,16 @@ void Policy::configure(uint64_t arena_bytes, uint32_t max_resident, uint32_t fra
 }
 
 uint32_t Policy::add_scene() {
-    applied_.push_back(0);
+    newest_.push_back(0);
     submitted_moves_.push_back(0);
-    return uint32_t(applied_.size() - 1);
+    std::vector<int64_t> copies(frame_sets_, -1);
+    copies[0] = 0;
+    copy_version_.push_back(copies);
+    return uint32_t(newest_.size() - 1);
 }
 
 bool Policy::submit(PolicyRequest &r) {
-    if (r.scene >= applied_.size()) return false;
+    if (r.scene >= newest_.size()) return false;
     if (align_up(r.footprint, Arena::kAlign) > arena_.capacity()) return false;
     r.version = submitted_moves_[r.scene];
     pending_.push_back(r);
@@ -81,46 +84,68 @@ bool Policy::submit(PolicyRequest &r) {
     return true;
 }
 
-bool Policy::move(uint32_t scene) {
-    if (scene >= applied_.size()) return false;
-    submitted_moves_[scene]++;
-    return true;
+uint32_t Policy::move(uint32_t scene) {
+    if (scene >= newest_.size()) return 0;
+    return ++submitted_moves_[scene];
 }
 
-bool Policy::next_move(uint32_t &scene) const {
-    for (uint32_t s = 0; s < applied_.size(); s++) {
-        if (submitted_moves_[s] == applied_[s]) continue;
-        // The new version applied_ + 1 overwrites the copy of version
-        // applied_ + 1 - frame_sets (none while that is negative).
-        if (applied_[s] + 1 < frame_sets_) {
-            scene = s;
-            return true;
+uint32_t Policy::outstanding(uint32_t scene, int64_t version) const {
+    if (version < 0) return 0;
+    auto it = outstanding_.find({scene, uint32_t(version)});
+    return it == outstanding_.end() ? 0 : it->second;
+}
+
+int Policy::copy_of(uint32_t scene, uint32_t version) const {
+    const std::vector<int64_t> &cv = copy_version_[scene];
+    for (uint32_t c = 0; c < cv.size(); c++)
+        if (cv[c] == int64_t(version)) return int(c);
+    return -1;
+}
+
+bool Policy::next_move(uint32_t &scene, uint32_t &version, uint32_t &copy) const {
+    for (uint32_t s = 0; s < newest_.size(); s++) {
+        if (submitted_moves_[s] == newest_[s]) continue;
+        // The oldest version above the newest that a queued request renders;
+        // with none, the newest submitted state.
+        uint32_t target = submitted_moves_[s];
+        for (auto it = outstanding_.lower_bound({s, newest_[s] + 1}); it != outstanding_.end() && it->first.first == s;
+             ++it) {
+            if (it->second) {
+                target = it->first.second;
+                break;
+            }
         }
-        const uint32_t victim = applied_[s] + 1 - frame_sets_;
-        auto it = outstanding_.find({s, victim});
-        if (it == outstanding_.end() || it->second == 0) {
-            scene = s;
-            return true;
+        const std::vector<int64_t> &cv = copy_version_[s];
+        for (uint32_t c = 0; c < cv.size(); c++) {
+            if (cv[c] < 0 || outstanding(s, cv[c]) == 0) {
+                scene = s;
+                version = target;
+                copy = c;
+                return true;
+            }
         }
     }
     return false;
 }
 
-void Policy::move_applied(uint32_t scene) {
-    if (applied_[scene] + 1 >= frame_sets_) outstanding_.erase({scene, applied_[scene] + 1 - frame_sets_});
-    applied_[scene]++;
+void Policy::move_applied(uint32_t scene, uint32_t version, uint32_t copy) {
+    const int64_t old = copy_version_[scene][copy];
+    if (old >= 0) outstanding_.erase({scene, uint32_t(old)});
+    copy_version_[scene][copy] = version;
+    newest_[scene] = version;
 }
 
 bool Policy::next_admission(PolicyRequest &out, uint64_t &offset) {
     if (resident_ >= max_resident_) return false;
     for (auto it = pending_.begin(); it != pending_.end(); ++it) {
-        // A request waits for the moves submitted before it; its version's
-        // copy stays intact until every request of that version is done.
-        const uint32_t cur = applied_[it->scene];
-        if (it->version > cur || cur - it->version >= frame_sets_) continue;
+        // A request waits until its version is materialized; that copy stays
+        // intact until every request of the version is done.
+        const int copy = copy_of(it->scene, it->version);
+        if (copy < 0) continue;
         const uint64_t off = arena_.alloc(it->footprint);
         if (off == Arena::kNone) return false;  // arrival order: later requests wait too
         out = *it;
+        out.copy = uint32_t(copy);
         offset = off;
         pending_.erase(it);
         active_[out.id] = {out, off};
@@ -168,8 +193,9 @@ std::vector<uint64_t> Policy::cancel_pending() {
 using namespace ae;
 
 // Discrete-time run of the admission policy: events arrive at their tick (in
-// list order within a tick); each tick applies every move that may apply,
-// admits what fits, then advances admitted requests by one tick of service.
+// list order within a tick); each tick applies every move that may apply
+// (coalescing the ones no request needs), admits what fits, then advances
+// admitted requests by one tick of service.
 extern "C" int ae_serve_policy_simulate(const ae_policy_event *events, uint32_t n, uint64_t arena_bytes,
                                         uint32_t max_resident, uint32_t n_scenes, uint32_t frame_sets,
                                         uint32_t max_ticks, ae_policy_outcome *out) {
@@ -192,7 +218,7 @@ extern "C" int ae_serve_policy_simulate(const ae_policy_event *events, uint32_t 
         while (next_event < n && events[next_event].tick <= t) {
             const ae_policy_event &e = events[next_event];
             if (e.kind == AE_POLICY_MOVE) {
-                P.move(e.scene);
+                out[next_event].version = P.move(e.scene);
                 moves[e.scene].push_back(next_event);
             } else if (e.kind == AE_POLICY_CANCEL) {
                 // Withdraw request event `footprint`: a queued one at once, an
@@ -232,14 +258,18 @@ extern "C" int ae_serve_policy_simulate(const ae_policy_event *events, uint32_t 
         bool progress = true;
         while (progress) {
             progress = false;
-            uint32_t s;
-            while (P.next_move(s)) {
-                const uint32_t mi = moves[s].front();
-                moves[s].pop_front();
-                P.move_applied(s);
-                out[mi].admit_tick = out[mi].done_tick = int32_t(t);
-                out[mi].version = P.applied(s);
-                finished++;
+            uint32_t s, v, c;
+            while (P.next_move(s, v, c)) {
+                // Moves below the materialized version are coalesced into it.
+                while (!moves[s].empty()) {
+                    const uint32_t mi = moves[s].front();
+                    if (out[mi].version > v) break;
+                    moves[s].pop_front();
+                    out[mi].admit_tick = out[mi].done_tick = int32_t(t);
+                    out[mi].offset = out[mi].version == v ? uint64_t(c) : ~0ull;
+                    finished++;
+                }
+                P.move_applied(s, v, c);
                 progress = true;
             }
             PolicyRequest r;

@@ -6,10 +6,12 @@
 //   * Policy: admission in arrival order by memory footprint and resident
 //     slots, and the ordering of instance moves against the requests of a
 //     scene (a request renders the scene as it was when it was submitted).
-//     Each scene has `frame_sets` copies of its per-frame arrays; version v
-//     lives in copy v % frame_sets, so a move to version v + 1 may be applied
-//     once no request of version v + 1 - frame_sets is outstanding, while
-//     requests of the newer versions still run.
+//     Each scene has `frame_sets` copies of its per-frame arrays.  A version
+//     is materialized (refit, then written into a free copy) when a queued
+//     request needs it, or eagerly as the newest state when a copy is free;
+//     moves that no request will see are coalesced into the next one (moves
+//     carry absolute transforms).  A copy is free when no outstanding request
+//     renders the version it holds.
 #pragma once
 #include <cstdint>
 #include <deque>
@@ -48,25 +50,32 @@ struct PolicyRequest {
     uint32_t scene = 0;
     uint64_t footprint = 0;
     uint32_t version = 0;  // moves of its scene submitted before it
+    uint32_t copy = 0;     // set at admission: the copy holding its version
 };
 
 class Policy {
   public:
     void configure(uint64_t arena_bytes, uint32_t max_resident, uint32_t frame_sets = 2);
+    // A new scene; its version 0 lives in copy 0.
     uint32_t add_scene();
-    uint32_t scenes() const { return uint32_t(applied_.size()); }
+    uint32_t scenes() const { return uint32_t(newest_.size()); }
     // Queues a request; fills in its scene version.  False when it can never
     // fit (footprint above the whole arena) or the scene is unknown.
     bool submit(PolicyRequest &r);
-    // Queues an instance move of `scene`; requests submitted after it see it.
-    bool move(uint32_t scene);
-    // A scene whose oldest queued move may be applied now: every request of
-    // the version whose copy the move overwrites has completed.
-    bool next_move(uint32_t &scene) const;
-    void move_applied(uint32_t scene);
-    // The next request to admit (arrival order; requests waiting for a move
-    // of their scene are passed over, a request that does not fit stops the
-    // scan so large requests are not starved).  Places it in the arena.
+    // Queues an instance move of `scene`; returns the version it creates
+    // (0 for an unknown scene).  Requests submitted after it see it.
+    uint32_t move(uint32_t scene);
+    // The next move to apply: its scene, the version to materialize (the
+    // oldest version a queued request needs, else the newest submitted; the
+    // versions below it that no request needs are coalesced) and the copy
+    // to write it into.  False when nothing is to be applied or no copy of
+    // the scene is free.
+    bool next_move(uint32_t &scene, uint32_t &version, uint32_t &copy) const;
+    void move_applied(uint32_t scene, uint32_t version, uint32_t copy);
+    // The next request to admit (arrival order; requests whose version is
+    // not materialized yet are passed over, a request that does not fit stops
+    // the scan so large requests are not starved).  Places it in the arena
+    // and names the copy it renders from.
     bool next_admission(PolicyRequest &out, uint64_t &offset);
     // Releases a completed request's arena block and resident slot.
     void completed(uint64_t id);
@@ -80,14 +89,20 @@ class Policy {
     uint32_t resident() const { return resident_; }
     size_t pending() const { return pending_.size(); }
     const Arena &arena() const { return arena_; }
-    uint32_t applied(uint32_t scene) const { return applied_[scene]; }
+    uint32_t newest(uint32_t scene) const { return newest_[scene]; }
+    uint32_t submitted(uint32_t scene) const { return submitted_moves_[scene]; }
+    uint32_t frame_sets() const { return frame_sets_; }
+    // The copy holding `version` of `scene`, or -1.
+    int copy_of(uint32_t scene, uint32_t version) const;
 
   private:
+    uint32_t outstanding(uint32_t scene, int64_t version) const;
     Arena arena_;
     uint32_t max_resident_ = 1, resident_ = 0, frame_sets_ = 2;
     std::deque<PolicyRequest> pending_;
     std::map<uint64_t, std::pair<PolicyRequest, uint64_t>> active_;  // id -> (request, offset)
-    std::vector<uint32_t> applied_, submitted_moves_;
+    std::vector<uint32_t> newest_, submitted_moves_;
+    std::vector<std::vector<int64_t>> copy_version_;                  // per scene, per copy; -1 = empty
     std::map<std::pair<uint32_t, uint32_t>, uint32_t> outstanding_;  // (scene, version) -> pending + active
 };
 

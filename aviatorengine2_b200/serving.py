@@ -108,7 +108,7 @@ class Server:
     def stats(self):
         out = np.zeros(1, _lib.SERVE_STATS)
         self._chk(lib().ae_serve_get_stats(self._h, ptr(out)))
-        return {k: out[0][k].item() for k in _lib.SERVE_STATS.names}
+        return {k: out[0][k].item() for k in _lib.SERVE_STATS.names if k != "pad"}
 
     def reset_stats(self):
         self._chk(lib().ae_serve_reset_stats(self._h))

@@ -595,20 +595,23 @@ def measure_build(local, reps=3):
             "gpu_ms_per_mesh_calls": per_mesh_ms}
 
 
-def measure_serving(local, n_requests=16, rate=0.5, seed=7, claim_policy=1):
+def measure_serving(local, n_requests=48, rate=0.5, seed=7, claim_policy=1, frame_hz=30.0):
     """The serving loop under a Poisson stream of requests over the 8 resident
     serving scenes: resolution uniform over {256^2, 640x480, 960x540,
-    1920x1080}, spp from {1, 4, 16, 64} (as that many progressive frames),
-    and before each request a random-walk step of all 512 instances of its
-    scene (a GPU refit).  Latency = submit to images in host memory."""
+    1920x1080}, spp from {1, 4, 16, 64} (as that many progressive frames).
+    While the requests run, the world moves every frame: at `frame_hz` all
+    4096 instances (512 per scene) take a random-walk step, submitted to the
+    server as one move per scene (a GPU TLAS refit when applied; moves that
+    no request renders are coalesced).  Latency = submit to images in host
+    memory."""
     from aviatorengine2_b200 import Context, Server, scenes
     rng = np.random.default_rng(seed)
     t0 = time.perf_counter()
     S = scenes.serving_scenes(gpu_build=True)
     ctxs = []
-    for s in S:
+    for sc in S:
         c = Context(256, 256, device=local)
-        c.upload(s)
+        c.upload(sc)
         ctxs.append(c)
     build_s = time.perf_counter() - t0
     res_choices = [(256, 256), (640, 480), (960, 540), (1920, 1080)]
@@ -616,7 +619,7 @@ def measure_serving(local, n_requests=16, rate=0.5, seed=7, claim_policy=1):
     plan = [(int(rng.integers(0, len(S))), res_choices[int(rng.integers(0, 4))], spp_choices[int(rng.integers(0, 4))])
             for _ in range(n_requests)]
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
-    inst = [s.instances.copy() for s in S]
+    inst = [sc.instances.copy() for sc in S]
     with Server(device=local, arena_bytes=4 << 30, max_requests=64, claim_policy=claim_policy) as srv:
         ids = [srv.add_scene(c) for c in ctxs]
         # warm-up: one small request per scene
@@ -625,13 +628,29 @@ def measure_serving(local, n_requests=16, rate=0.5, seed=7, claim_policy=1):
             c["samples"], c["batches"] = 1, 1
             srv.wait(srv.submit(ids[k], 64, 64, 1, c, accum=False, display=False), 600000)
         srv.reset_stats()
+        stop = threading.Event()
+        moved = {"frames": 0, "moves": 0}
+        mover_rng = np.random.default_rng(seed + 1000)
+
+        def mover():
+            period = 1.0 / frame_hz
+            nxt = time.perf_counter()
+            while not stop.is_set():
+                for k in range(len(S)):
+                    inst[k] = scenes.random_walk(inst[k], mover_rng)
+                    srv.move_instances(ids[k], inst[k])
+                    moved["moves"] += 1
+                moved["frames"] += 1
+                nxt += period
+                stop.wait(max(0.0, nxt - time.perf_counter()))
+
+        th = threading.Thread(target=mover, daemon=True)
         start = time.perf_counter()
+        th.start()
         rids = []
         for i, (sc, (w, h), spp) in enumerate(plan):
             while time.perf_counter() - start < arrivals[i]:
                 time.sleep(0.0005)
-            inst[sc] = scenes.random_walk(inst[sc], rng)
-            srv.move_instances(ids[sc], inst[sc])
             c = S[sc].config.copy()
             c["samples"], c["batches"] = 1, 1
             rids.append(srv.submit(ids[sc], w, h, spp, c))
@@ -639,18 +658,25 @@ def measure_serving(local, n_requests=16, rate=0.5, seed=7, claim_policy=1):
         for r in rids:
             res, _, _ = srv.wait(r, 1800000)
             lat.append(res["done_ms"] - res["submit_ms"])
+        stop.set()
+        th.join()
+        mover_s = time.perf_counter() - start
+        srv.drain(600000)
         st = srv.stats()
     for c in ctxs:
         c.close()
     wall = (st["last_done_ms"] - st["first_submit_ms"]) / 1e3
-    return {"workload": "8 resident scenes " + "/".join(f"{s.triangles // 1000}k" for s in S) +
-                        " tris, 512 moving instances each; Poisson arrivals",
+    return {"workload": "8 resident scenes " + "/".join(f"{sc.triangles // 1000}k" for sc in S) +
+                        " tris, 512 instances each (4096 in all) moving every frame; Poisson arrivals",
             "requests": n_requests, "rate_per_s": rate, "claim_policy": "shared" if claim_policy else "oldest_first",
             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
             "mpaths": st["paths"] / wall / 1e6, "mrays": st["rays"] / wall / 1e6, "paths": int(st["paths"]),
-            "wall_s": wall, "moves_applied": int(st["moves_applied"]), "peak_resident": int(st["peak_resident"]),
-            "peak_arena_bytes": int(st["peak_arena_bytes"]), "errors": int(st["errors"]),
-            "scene_build_s": build_s}
+            "wall_s": wall, "frame_hz": frame_hz, "world_frames": int(moved["frames"]),
+            "moves_submitted": int(moved["moves"]), "moves_applied": int(st["moves_applied"]),
+            "moves_coalesced": int(st["moves_coalesced"]),
+            "refits_per_s": st["moves_applied"] / mover_s, "instances_moved_per_frame": int(sum(len(i) for i in inst)),
+            "peak_resident": int(st["peak_resident"]), "peak_arena_bytes": int(st["peak_arena_bytes"]),
+            "errors": int(st["errors"]), "scene_build_s": build_s}
 
 
 def run_reference_arm(args):
@@ -743,7 +769,9 @@ def main():
     ap.add_argument("--no-config1", action="store_true", help="skip the small plain-method leg (Cornell box)")
     ap.add_argument("--c4-frames", type=int, default=1024, help="frames (1 spp each) of the precision-variant leg")
     ap.add_argument("--mre-pixels", type=int, default=2048, help="seeded pixels scored against the FP64 oracle")
-    ap.add_argument("--serve-requests", type=int, default=16)
+    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--serve-frame-hz", type=float, default=30.0, help="world frames per second (every frame moves "
+                    "all 4096 instances of the serving scenes)")
     ap.add_argument("--serve-rate", type=float, default=0.5, help="Poisson arrivals per second")
     ap.add_argument("--serve-sweep", default="", help="comma-separated arrival rates: also run the serving "
                     "leg at each (reported as serving_sweep)")
@@ -916,10 +944,11 @@ def main():
         config4 = measure_config4(local, args.c4_frames, args.mre_pixels)
     serving = None
     if not args.no_serve and rank == 0:
-        serving = measure_serving(local, args.serve_requests, args.serve_rate)
+        serving = measure_serving(local, args.serve_requests, args.serve_rate, frame_hz=args.serve_frame_hz)
     sweep = None
     if args.serve_sweep and rank == 0:
-        sweep = [measure_serving(local, args.serve_requests, float(r)) for r in args.serve_sweep.split(",")]
+        sweep = [measure_serving(local, args.serve_requests, float(r), frame_hz=args.serve_frame_hz)
+                 for r in args.serve_sweep.split(",")]
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",

@@ -641,6 +641,8 @@ typedef struct ae_serve_stats {
     uint32_t peak_resident, moves_applied;
     uint32_t errors;           /* device error flags (bounded waits that gave up) */
     uint32_t cancelled;        /* requests ended by ae_serve_cancel */
+    uint32_t moves_coalesced;  /* moves superseded by a later one before any request needed them */
+    uint32_t pad;
 } ae_serve_stats;
 
 ae_server *ae_serve_create(const ae_serve_settings *settings);
@@ -653,9 +655,13 @@ int ae_serve_add_scene(ae_server *srv, ae_ctx *scene, uint32_t *scene_id);
 int ae_serve_submit(ae_server *srv, const ae_serve_request *req, uint64_t *id);
 /* Queues new transforms for every instance of a scene (refit on the GPU);
  * requests submitted earlier render the old ones, later ones the new.  The
- * server keeps two copies of each scene's per-frame arrays (objects, TLAS,
- * instances), so a move is applied while requests of the previous version
- * still run; only requests two versions back must have finished. */
+ * server keeps AE_SERVE_FRAME_SETS copies of each scene's per-frame arrays
+ * (objects, TLAS, instances): a move is refit into a copy that no
+ * outstanding request renders, while requests of older versions still run.
+ * Moves that no request will render (several per frame interval, none
+ * submitted between them) are coalesced into the next: a move carries
+ * absolute transforms. */
+#define AE_SERVE_FRAME_SETS 8u
 int ae_serve_move_instances(ae_server *srv, uint32_t scene, const ae_instance *instances, uint32_t n);
 /* Withdraws a request (no counterpart in the reference).  A queued request
  * ends at once; one on the GPU stops claiming pixels, its pixels in flight
@@ -687,11 +693,12 @@ typedef struct ae_policy_event {
     uint64_t footprint;        /* requests: image bytes */
 } ae_policy_event;
 typedef struct ae_policy_outcome {
-    int32_t admit_tick;        /* -1 = never; moves: the tick it was applied */
+    int32_t admit_tick;        /* -1 = never; moves: the tick it was applied or coalesced */
     int32_t done_tick;
     uint32_t version;          /* requests: moves of the scene before it; moves: version after */
     int32_t status;            /* AE_OK, AE_ERR_REJECTED or AE_ERR_CANCELLED */
-    uint64_t offset;           /* requests: arena offset */
+    uint64_t offset;           /* requests: arena offset; moves: the copy of the per-frame
+                                  arrays written, or ~0 when coalesced into a later move */
 } ae_policy_outcome;
 int ae_serve_policy_simulate(const ae_policy_event *events, uint32_t n, uint64_t arena_bytes,
                              uint32_t max_resident, uint32_t n_scenes, uint32_t frame_sets,
@@ -755,7 +762,7 @@ static_assert(sizeof(ae_hit) == 20, "hit record");
 static_assert(sizeof(ae_serve_settings) == 56, "serve settings");
 static_assert(sizeof(ae_serve_request) == 280, "serve request");
 static_assert(sizeof(ae_serve_result) == 64, "serve result");
-static_assert(sizeof(ae_serve_stats) == 128, "serve stats");
+static_assert(sizeof(ae_serve_stats) == 136, "serve stats");
 static_assert(sizeof(ae_policy_event) == 24, "policy event");
 static_assert(sizeof(ae_policy_outcome) == 24, "policy outcome");
 #endif

@@ -143,6 +143,47 @@ def test_moves_between_requests():
             assert np.array_equal(out[k][2], twin.read_image(_lib.IMAGE_DISPLAY))
 
 
+def test_frame_rate_moves_coalesce_and_requests_see_their_version():
+    """Moves submitted faster than requests (several per request, as a world
+    moving every frame): a request renders the transforms of the last move
+    submitted before it, bit for bit, while moves no request sees are
+    coalesced or refit eagerly; every move is accounted for."""
+    s = scenes.wavefront_scene(seed=12, width=64, height=48, depth=4, n_meshes=4, n_instances=48,
+                               n_lights=4, target_tris=30_000)
+    cfg = config_for(s, 64, 48, samples=1)
+    rng = np.random.default_rng(9)
+    walk = [s.instances]
+    for _ in range(15):
+        walk.append(scenes.random_walk(walk[-1], rng, step=1.0, angle=0.1))
+    ctx = resident(s)
+    with Server(slots=4096, max_requests=8, arena_bytes=1 << 24) as srv:
+        sid = srv.add_scene(ctx)
+        r0 = srv.submit(sid, 64, 48, 3, cfg)
+        for k in range(1, 11):
+            srv.move_instances(sid, walk[k])
+        r1 = srv.submit(sid, 64, 48, 2, cfg)
+        for k in range(11, 16):
+            srv.move_instances(sid, walk[k])
+        r2 = srv.submit(sid, 64, 48, 1, cfg)
+        out = [srv.wait(r, 60000) for r in (r0, r1, r2)]
+        srv.drain(60000)
+        st = srv.stats()
+    ctx.close()
+    assert [int(o[0]["scene_version"]) for o in out] == [0, 10, 15]
+    assert st["moves_applied"] + st["moves_coalesced"] == 15 and st["moves_applied"] >= 2
+    with Context(64, 48) as twin:
+        twin.upload(s)
+        for k, (inst, frames) in enumerate(((None, 3), (walk[10], 2), (walk[15], 1))):
+            if inst is not None:
+                twin.refit_instances(inst)
+            c = cfg.copy()
+            for b in range(frames):
+                c["batch"] = b
+                twin.set_config(c)
+                twin.render_frame(_lib.MODE_WAVEFRONT)
+            assert same(out[k][1], twin.read_image(_lib.IMAGE_ACCUM)), f"request {k}"
+
+
 def test_admission_by_footprint_and_rejection():
     s = scenes.cornell_box(depth=3)
     ctx = resident(s)

@@ -73,6 +73,9 @@ def test_oversize_rejected():
     assert out[1]["admit_tick"] == 0
 
 
+NONE = (1 << 64) - 1  # outcome offset of a coalesced move
+
+
 def test_move_waits_for_earlier_requests_one_frame_set():
     # With a single copy of the per-frame arrays a move waits for every
     # earlier request of its scene.
@@ -81,7 +84,7 @@ def test_move_waits_for_earlier_requests_one_frame_set():
     code, out = simulate_policy(ev, 100 * MB, 16, 2, frame_sets=1)
     assert code == 0
     assert out[2]["admit_tick"] > max(out[0]["done_tick"], out[1]["done_tick"])
-    assert out[2]["version"] == 1
+    assert out[2]["version"] == 1 and out[2]["offset"] == 0
     for i in (3, 5):  # later scene-0 requests see the move
         assert out[i]["version"] == 1 and out[i]["admit_tick"] >= out[2]["admit_tick"]
     assert out[4]["version"] == 0 and out[4]["admit_tick"] == 1  # scene 1 is not held up
@@ -89,16 +92,17 @@ def test_move_waits_for_earlier_requests_one_frame_set():
 
 
 def test_two_frame_sets_overlap_versions():
-    # With two copies a move is applied while the previous version still
-    # renders; the next move waits for the version it overwrites.
+    # With two copies a move is refit into the copy no request renders while
+    # the older version still runs; the next move takes whichever copy frees
+    # first - here the one of version 1, long before version 0's request ends.
     ev = [_req(0, 1 * MB, 6), _move(1), _req(1, 1 * MB, 2), _move(2), _req(2, 1 * MB, 1)]
     code, out = simulate_policy(ev, 100 * MB, 16, 1, frame_sets=2)
     assert code == 0
-    assert out[1]["admit_tick"] == 1 and out[1]["version"] == 1  # applied at once
+    assert out[1]["admit_tick"] == 1 and out[1]["version"] == 1 and out[1]["offset"] == 1
     assert out[2]["version"] == 1 and out[2]["admit_tick"] == 1  # overlaps request 0
-    assert out[0]["done_tick"] > out[2]["admit_tick"]
-    assert out[3]["admit_tick"] > out[0]["done_tick"]             # version 2 overwrites version 0's copy
-    assert out[4]["version"] == 2 and out[4]["admit_tick"] >= out[3]["admit_tick"]
+    assert out[3]["admit_tick"] == out[2]["done_tick"] + 1 and out[3]["offset"] == 1
+    assert out[3]["admit_tick"] < out[0]["done_tick"]
+    assert out[4]["version"] == 2 and out[4]["admit_tick"] == out[3]["admit_tick"]
     _check_invariants(ev, out, 100 * MB, 16)
 
 
@@ -113,24 +117,56 @@ def test_pending_request_of_previous_version_still_admitted():
     assert out[3]["version"] == 1
 
 
-def test_back_to_back_moves_apply_in_order():
+def test_back_to_back_moves_coalesce():
+    # Two moves before any request: the first is superseded (moves carry
+    # absolute transforms) and only version 2 is refit.
     ev = [_move(0), _move(0), _req(0, 1 * MB, 1), _move(1), _req(1, 1 * MB, 1)]
     code, out = simulate_policy(ev, 100 * MB, 16, 1, frame_sets=1)
     assert code == 0
-    assert out[0]["version"] == 1 and out[1]["version"] == 2
+    assert out[0]["version"] == 1 and out[0]["offset"] == NONE and out[0]["admit_tick"] == 0
+    assert out[1]["version"] == 2 and out[1]["offset"] == 0
     assert out[2]["version"] == 2 and out[4]["version"] == 3
     assert out[3]["admit_tick"] > out[2]["done_tick"]
     assert out[4]["admit_tick"] >= out[3]["admit_tick"]
 
 
-@pytest.mark.parametrize("frame_sets", [1, 2])
+def test_moves_every_tick_are_refit_every_tick():
+    # A move per tick and no requests: each is refit at its tick (the newest
+    # state is materialized eagerly whenever a copy is free).
+    ev = [_move(t) for t in range(10)]
+    code, out = simulate_policy(ev, 100 * MB, 16, 1, frame_sets=2)
+    assert code == 0
+    assert [int(o["admit_tick"]) for o in out] == list(range(10))
+    assert all(o["offset"] != NONE for o in out)
+
+
+def test_frame_rate_moves_do_not_hold_up_requests():
+    # A move every tick while requests of 20 ticks arrive every 4 ticks:
+    # with 8 copies every request is admitted when it arrives, and the moves
+    # keep being refit (or coalesced when every copy is pinned).
+    ev = []
+    for t in range(60):
+        ev.append(_move(t))
+        if t % 4 == 0:
+            ev.append(_req(t, 1 * MB, 20))
+    code, out = simulate_policy(ev, 100 * MB, 64, 1, frame_sets=8)
+    assert code == 0
+    for i, e in enumerate(ev):
+        if e["kind"] == _lib.POLICY_REQUEST:
+            assert out[i]["admit_tick"] == e["tick"], (i, out[i])
+    applied = [o for o, e in zip(out, ev) if e["kind"] == _lib.POLICY_MOVE and o["offset"] != NONE]
+    assert len(applied) >= 45
+    _check_invariants(ev, out, 100 * MB, 64)
+
+
+@pytest.mark.parametrize("frame_sets", [1, 2, 8])
 @pytest.mark.parametrize("seed", [0, 1, 2, 3])
 def test_random_streams_keep_invariants(seed, frame_sets):
     rng = np.random.default_rng(seed)
     ev, t = [], 0
     for _ in range(300):
         t += int(rng.poisson(1.0))
-        if rng.random() < 0.1:
+        if rng.random() < 0.3:
             ev.append(_move(t, scene=int(rng.integers(0, 4))))
         else:
             ev.append(_req(t, int(rng.choice([1, 4, 16, 33]) * MB), int(rng.integers(1, 8)), scene=int(rng.integers(0, 4))))
@@ -138,23 +174,33 @@ def test_random_streams_keep_invariants(seed, frame_sets):
     assert code == 0
     _check_invariants(ev, out, 64 * MB, 8)
     moves_before = {s: 0 for s in range(4)}
-    applied_at = {}
+    made = {(s, 0): (0, 0) for s in range(4)}  # (scene, version) -> (tick, copy) it was materialized
     for i, e in enumerate(ev):
         s = e["scene"]
         if e["kind"] == _lib.POLICY_MOVE:
             moves_before[s] += 1
-            v = int(out[i]["version"])
-            assert v == moves_before[s]
-            applied_at[(s, v)] = int(out[i]["admit_tick"])
-            # the copy it overwrites held version v - frame_sets: all done
-            victims = [j for j in range(len(ev)) if ev[j]["kind"] == _lib.POLICY_REQUEST and ev[j]["scene"] == s
-                       and out[j]["status"] == 0 and out[j]["version"] == v - frame_sets]
-            assert all(out[j]["done_tick"] < out[i]["admit_tick"] for j in victims)
+            assert int(out[i]["version"]) == moves_before[s]
+            if out[i]["offset"] != NONE:
+                made[(s, moves_before[s])] = (int(out[i]["admit_tick"]), int(out[i]["offset"]))
         else:
             # every request renders the version of its scene current at its arrival
             assert out[i]["version"] == moves_before[s]
-            if out[i]["version"] > 0 and out[i]["status"] == 0:
-                assert out[i]["admit_tick"] >= applied_at[(s, int(out[i]["version"]))]
+    reqs = [i for i, e in enumerate(ev) if e["kind"] == _lib.POLICY_REQUEST and out[i]["status"] == 0]
+    for i in reqs:
+        key = (ev[i]["scene"], int(out[i]["version"]))
+        assert key in made, f"request {i} renders version {key} that was coalesced"
+        assert out[i]["admit_tick"] >= made[key][0]
+    # A copy is overwritten only after every request of the version it held is done.
+    for s in range(4):
+        timeline = sorted((tick, copy, v) for (ss, v), (tick, copy) in made.items() if ss == s)
+        held = {}
+        for tick, copy, v in timeline:
+            if copy in held:
+                old = held[copy]
+                for i in reqs:
+                    if ev[i]["scene"] == s and int(out[i]["version"]) == old:
+                        assert out[i]["done_tick"] < tick, (s, copy, old, v, i)
+            held[copy] = v
 
 
 def _cancel(tick, target):
