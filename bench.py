@@ -930,24 +930,27 @@ def main():
                        "--impl reference prints the reference's own compiled traversal on the rigid twin beside it")
 
     # Frame-level legs: rank 0 only (the other replicas would repeat them).
-    paths = None
-    if not args.no_paths and rank == 0:
-        paths = measure_paths(local, args.width, args.height, mre_pixels=args.mre_pixels // 2)
-    build = None
-    if not args.no_build and rank == 0:
-        build = measure_build(local)
-    config1 = None
-    if not args.no_config1 and rank == 0:
-        config1 = measure_config1(local)
-    config4 = None
-    if not args.no_config4 and rank == 0:
-        config4 = measure_config4(local, args.c4_frames, args.mre_pixels)
-    serving = None
-    if not args.no_serve and rank == 0:
-        serving = measure_serving(local, args.serve_requests, args.serve_rate, frame_hz=args.serve_frame_hz)
+    # A leg that fails reports its error in its own block; the closest-hit
+    # line above stands.
+    def leg(enabled, fn, *a, **kw):
+        if not enabled or rank != 0:
+            return None
+        try:
+            return fn(*a, **kw)
+        except Exception as e:  # noqa: BLE001 - reported in the JSON line
+            import traceback
+            traceback.print_exc()
+            return {"error": f"{type(e).__name__}: {e}"}
+
+    paths = leg(not args.no_paths, measure_paths, local, args.width, args.height, mre_pixels=args.mre_pixels // 2)
+    build = leg(not args.no_build, measure_build, local)
+    config1 = leg(not args.no_config1, measure_config1, local)
+    config4 = leg(not args.no_config4, measure_config4, local, args.c4_frames, args.mre_pixels)
+    serving = leg(not args.no_serve, measure_serving, local, args.serve_requests, args.serve_rate,
+                  frame_hz=args.serve_frame_hz)
     sweep = None
-    if args.serve_sweep and rank == 0:
-        sweep = [measure_serving(local, args.serve_requests, float(r), frame_hz=args.serve_frame_hz)
+    if args.serve_sweep:
+        sweep = [leg(True, measure_serving, local, args.serve_requests, float(r), frame_hz=args.serve_frame_hz)
                  for r in args.serve_sweep.split(",")]
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
