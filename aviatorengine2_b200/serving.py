@@ -96,7 +96,9 @@ class Server:
         """(result record, accum image, display image) of a finished request."""
         out = np.zeros(1, _lib.SERVE_RESULT)
         code = lib().ae_serve_wait(self._h, rid, timeout_ms, ptr(out))
-        if code == -6 and timeout_ms >= 0:
+        # AE_ERR_TIMEOUT is either the wait running out (the record is left
+        # untouched) or the request's own status (a device wait gave up).
+        if code == -6 and timeout_ms >= 0 and int(out[0]["id"]) != rid:
             raise TimeoutError(f"request {rid} not finished after {timeout_ms} ms")
         acc, dsp = self._outputs.pop(rid, (None, None))
         self._chk(code)

@@ -233,11 +233,15 @@ def classify_ids(ref, wt):
     dis = (ref["object"] != wt["object"]) | (ref["prim"] != wt["prim"])
     edge = (min_bary(ref) < EDGE_EPS) | (min_bary(wt) < EDGE_EPS)
     on_edge = int((dis & edge).sum())
-    unexplained = int((dis & ~edge).sum())
+    rest = np.flatnonzero(dis & ~edge)
+    examples = [{"ray": int(i), "ref": [int(ref["object"][i]), int(ref["prim"][i]), float(ref["t"][i]),
+                                        float(min_bary(ref[i:i + 1])[0])],
+                 "wt": [int(wt["object"][i]), int(wt["prim"][i]), float(wt["t"][i]), float(min_bary(wt[i:i + 1])[0])]}
+                for i in rest[:8]]
     return {"rays": int(len(ref)), "agreement": float(1.0 - dis.mean()), "disagree": int(dis.sum()),
-            "on_shared_edge": on_edge, "unexplained": unexplained,
-            "agreement_excluding_edges": float(1.0 - unexplained / max(1, len(ref) - on_edge)),
-            "edge_eps": EDGE_EPS}
+            "on_shared_edge": on_edge, "unexplained": int(len(rest)),
+            "agreement_excluding_edges": float(1.0 - len(rest) / max(1, len(ref) - on_edge)),
+            "edge_eps": EDGE_EPS, "unexplained_examples": examples}
 
 
 def precision_ids(ctx, rays):
@@ -644,9 +648,10 @@ def measure_serving(local, n_requests=48, rate=0.5, seed=7, claim_policy=1, fram
                 nxt += period
                 stop.wait(max(0.0, nxt - time.perf_counter()))
 
-        th = threading.Thread(target=mover, daemon=True)
+        th = threading.Thread(target=mover, daemon=True) if frame_hz > 0 else None
         start = time.perf_counter()
-        th.start()
+        if th:
+            th.start()
         rids = []
         for i, (sc, (w, h), spp) in enumerate(plan):
             while time.perf_counter() - start < arrivals[i]:
@@ -659,7 +664,8 @@ def measure_serving(local, n_requests=48, rate=0.5, seed=7, claim_policy=1, fram
             res, _, _ = srv.wait(r, 1800000)
             lat.append(res["done_ms"] - res["submit_ms"])
         stop.set()
-        th.join()
+        if th:
+            th.join()
         mover_s = time.perf_counter() - start
         srv.drain(600000)
         st = srv.stats()

@@ -671,7 +671,10 @@ int ae_serve_move_instances(ae_server *srv, uint32_t scene, const ae_instance *i
  * request has already finished or is having its result copied. */
 int ae_serve_cancel(ae_server *srv, uint64_t id);
 /* Waits for a request (timeout_ms < 0: forever); returns its status, or
- * AE_ERR_TIMEOUT.  The record is released once it has been returned. */
+ * AE_ERR_TIMEOUT when the wait runs out.  A finished request fills `out`
+ * (its status too, which is AE_ERR_TIMEOUT itself for a request ended by a
+ * device wait that gave up); a wait that ran out leaves `out` untouched.  The
+ * record is released once it has been returned. */
 int ae_serve_wait(ae_server *srv, uint64_t id, int32_t timeout_ms, ae_serve_result *out);
 /* Waits until every submitted request and move has finished. */
 int ae_serve_drain(ae_server *srv, int32_t timeout_ms);
