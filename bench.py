@@ -215,15 +215,23 @@ def cpu_reference(scene, rays, budget_s=12.0, impl="port"):
             "sample": f"{what}, {dt:.2f} s"}
 
 
-EDGE_EPS = 1e-3  # minimum barycentric of a hit counted as lying on a triangle edge
+EDGE_EPS = 1e-2   # minimum barycentric of a hit counted as lying at a triangle edge
+TIE_REL = 1e-6    # relative depth difference of two hits counted as a tie
 MRE_EPS = 1e-3
 
 
 def classify_ids(ref, wt):
     """Primary-ray ID disagreements between the reference's triangle test
-    (hybrid:564-598) and the watertight one, split into rays whose hit (on
-    either side) lies within EDGE_EPS of an edge - where the reference's
-    test has cracks - and the rest."""
+    (hybrid:564-598) and the watertight one, by cause:
+      crack     - the watertight hit is nearer (or the reference missed) and
+                  lies within EDGE_EPS (barycentric) of an edge: the
+                  reference's test let the ray through between triangles;
+      leak      - the reference's hit is nearer (or the watertight test
+                  missed) and lies within EDGE_EPS of an edge: the
+                  reference's test took a ray just outside its triangle;
+      depth tie - two different surfaces within TIE_REL of the same depth,
+                  ranked by each test's own rounding of t;
+    and the rest, unexplained (must be none)."""
     from aviatorengine2_b200 import _lib
 
     def min_bary(h):
@@ -231,17 +239,24 @@ def classify_ids(ref, wt):
         return np.where(h["prim"] != _lib.MISS, np.minimum(np.minimum(a, b), 1.0 - a - b), np.inf)
 
     dis = (ref["object"] != wt["object"]) | (ref["prim"] != wt["prim"])
-    edge = (min_bary(ref) < EDGE_EPS) | (min_bary(wt) < EDGE_EPS)
-    on_edge = int((dis & edge).sum())
-    rest = np.flatnonzero(dis & ~edge)
+    rh, wh = ref["object"] != _lib.MISS, wt["object"] != _lib.MISS
+    tr, tw = ref["t"].astype(np.float64), wt["t"].astype(np.float64)
+    crack = dis & wh & (~rh | (tw < tr)) & (min_bary(wt) < EDGE_EPS)
+    leak = dis & rh & (~wh | (tr < tw)) & (min_bary(ref) < EDGE_EPS)
+    tie = dis & rh & wh & (np.abs(tr - tw) <= TIE_REL * np.maximum(tr, tw))
+    explained = crack | leak | tie
+    rest = np.flatnonzero(dis & ~explained)
     examples = [{"ray": int(i), "ref": [int(ref["object"][i]), int(ref["prim"][i]), float(ref["t"][i]),
                                         float(min_bary(ref[i:i + 1])[0])],
                  "wt": [int(wt["object"][i]), int(wt["prim"][i]), float(wt["t"][i]), float(min_bary(wt[i:i + 1])[0])]}
                 for i in rest[:8]]
+    n_expl = int((dis & explained).sum())
     return {"rays": int(len(ref)), "agreement": float(1.0 - dis.mean()), "disagree": int(dis.sum()),
-            "on_shared_edge": on_edge, "unexplained": int(len(rest)),
-            "agreement_excluding_edges": float(1.0 - len(rest) / max(1, len(ref) - on_edge)),
-            "edge_eps": EDGE_EPS, "unexplained_examples": examples}
+            "crack": int(crack.sum()), "leak": int((leak & ~crack).sum()), "depth_tie": int((tie & ~crack & ~leak).sum()),
+            "within_1e-3_of_an_edge": int((dis & ((min_bary(wt) < 1e-3) | (min_bary(ref) < 1e-3))).sum()),
+            "unexplained": int(len(rest)),
+            "agreement_excluding_explained": float(1.0 - len(rest) / max(1, len(ref) - n_expl)),
+            "edge_eps": EDGE_EPS, "tie_rel": TIE_REL, "unexplained_examples": examples}
 
 
 def precision_ids(ctx, rays):
