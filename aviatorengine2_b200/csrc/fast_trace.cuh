@@ -137,10 +137,23 @@ AE_DEV bool tri_test_wt(f3 o, const WtRay &W, float tn, float tf, const float4 &
 constexpr float kEntryShrink = 0.99999904632568359375f;  // 1 - 2^-20
 constexpr float kExitGrow = 1.00000095367431640625f;     // 1 + 2^-20
 
+// Byte k (0..3) of w as an exact float: the byte permute builds the bits
+// 0x4B0000bb, which are 2^23 + bb, and the subtraction is exact.  Same value
+// as float(bb), without a conversion on the XU pipe.
+AE_DEV float byte_as_float(uint32_t w, int k) {
+    const uint32_t bits = __byte_perm(w, 0x4B000000u, 0x7440u | uint32_t(k));
+    return __fsub_rn(__uint_as_float(bits), 8388608.0f);
+}
+
 // Entry distance of the 4 quantised child boxes; an inverted slot or a miss
 // yields +inf.  Computed as q * (s/d) + (o - p)/d per slab with a relative
 // widening of 2^-20 on the exit side, which covers the rounding of this
 // formulation (the decoded boxes already contain the exact ones).
+//
+// The near and far planes of each slab are picked once per node from the sign
+// of the direction term: the rounded fma is monotone in q, so for a valid
+// child (lo <= hi) the pick gives exactly min and max of the two plane
+// distances, and the intervals are bit for bit those of the min/max form.
 AE_DEV void child_hits(const QNode *nodep, f3 o, f3 inv, float tn, float tf, float tmin[4], uint32_t child[4]) {
     const float4 *p = reinterpret_cast<const float4 *>(nodep);
     const float4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2), w3 = __ldg(p + 3);
@@ -150,26 +163,28 @@ AE_DEV void child_hits(const QNode *nodep, f3 o, f3 inv, float tn, float tf, flo
                 sz = __int_as_float((ez + 127) << 23);
     const float ix = sx * inv.x, iy = sy * inv.y, iz = sz * inv.z;
     const float bx = (w0.x - o.x) * inv.x, by = (w0.y - o.y) * inv.y, bz = (w0.z - o.z) * inv.z;
-    const uint32_t qlo[3] = {__float_as_uint(w1.x), __float_as_uint(w1.y), __float_as_uint(w1.z)};
-    const uint32_t qhi[3] = {__float_as_uint(w1.w), __float_as_uint(w2.x), __float_as_uint(w2.y)};
+    const uint32_t lox = __float_as_uint(w1.x), loy = __float_as_uint(w1.y), loz = __float_as_uint(w1.z);
+    const uint32_t hix = __float_as_uint(w1.w), hiy = __float_as_uint(w2.x), hiz = __float_as_uint(w2.y);
+    // Near-plane and far-plane bytes per axis.
+    const uint32_t nx = ix >= 0.0f ? lox : hix, fx = ix >= 0.0f ? hix : lox;
+    const uint32_t ny = iy >= 0.0f ? loy : hiy, fy = iy >= 0.0f ? hiy : loy;
+    const uint32_t nz = iz >= 0.0f ? loz : hiz, fz = iz >= 0.0f ? hiz : loz;
+    // A slot is in use when its x range is not inverted (one byte-wise compare).
+    const uint32_t valid = __vcmpleu4(lox, hix);
     child[0] = __float_as_uint(w2.z); child[1] = __float_as_uint(w2.w);
     child[2] = __float_as_uint(w3.x); child[3] = __float_as_uint(w3.y);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        const float lx = float((qlo[0] >> (8 * k)) & 0xff), hx = float((qhi[0] >> (8 * k)) & 0xff);
-        const float ly = float((qlo[1] >> (8 * k)) & 0xff), hy = float((qhi[1] >> (8 * k)) & 0xff);
-        const float lz = float((qlo[2] >> (8 * k)) & 0xff), hz = float((qhi[2] >> (8 * k)) & 0xff);
-        const float t0x = fmaf(lx, ix, bx), t1x = fmaf(hx, ix, bx);
-        const float t0y = fmaf(ly, iy, by), t1y = fmaf(hy, iy, by);
-        const float t0z = fmaf(lz, iz, bz), t1z = fmaf(hz, iz, bz);
-        const float lo = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), tn));
-        const float hi = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fmaxf(t0z, t1z));
-        const bool valid = (qlo[0] >> (8 * k) & 0xff) <= (qhi[0] >> (8 * k) & 0xff);
+        const float t0x = fmaf(byte_as_float(nx, k), ix, bx), t1x = fmaf(byte_as_float(fx, k), ix, bx);
+        const float t0y = fmaf(byte_as_float(ny, k), iy, by), t1y = fmaf(byte_as_float(fy, k), iy, by);
+        const float t0z = fmaf(byte_as_float(nz, k), iz, bz), t1z = fmaf(byte_as_float(fz, k), iz, bz);
+        const float lo = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, tn));
+        const float hi = fminf(fminf(t1x, t1y), t1z);
         // Widened by 2^-20 relative on both sides: the interval computed here
         // then contains the exact one, so neither a closer hit nor one lying
         // on the box's face is pruned by rounding.
         const float lo_c = lo * kEntryShrink;
-        const bool hit = valid && lo_c <= fminf(hi * kExitGrow, tf);
+        const bool hit = ((valid >> (8 * k)) & 1u) && lo_c <= fminf(hi * kExitGrow, tf);
         tmin[k] = hit ? lo_c : __int_as_float(0x7f800000);
     }
 }
