@@ -301,23 +301,29 @@ def seeded_pixels(width, height, n, seed):
     return np.stack([pick % width, pick // width], 1).astype(np.uint32)
 
 
-def measure_paths(local, width, height, frames=2, mre_pixels=1024):
+def measure_paths(local, width, height, frames=2, mre_pixels=1024, mre_frames=16, target_tris=10_000_000,
+                  n_instances=1024):
     """Mpaths/s of compute-only frames (1 spp) on the wavefront workload:
     the plain megakernel against the wavefront form (4-wide 8-bit quantised
     BVH, persistent stages, CUDA graph) and its precision form (watertight
     test, FP16 shading normals, compensated accumulation).  Frames are timed
     on the device around the whole frame; the plain and wavefront images are
     compared, and primary-ray IDs of both optimised closest hits against the
-    plain kernel's."""
+    plain kernel's.  The images are scored against the FP64 oracle after
+    `mre_frames` frames (the frames past the timed ones continue the same
+    accumulation)."""
     from aviatorengine2_b200 import Context, _lib, scenes
-    scene = scenes.wavefront_scene(width=width, height=height, gpu_build=True, ggx=True)
+    scene = scenes.wavefront_scene(width=width, height=height, gpu_build=True, ggx=True, target_tris=target_tris,
+                                   n_instances=n_instances)
+    _lib.lib().ae_bvh_builder_release()  # the device builder's scratch is not needed past the build
     out = {"workload": f"wavefront_scene {width}x{height}, 1 spp, depth {int(scene.config['depth'])}, "
                        f"{len(scene.lights)} lights, materials 60% Lambertian / 25% GGX metal / 15% dielectric",
            "triangles": int(scene.triangles),
            "instances": int(len(scene.instances)), "paths_per_frame": width * height}
     imgs = {}
     px = seeded_pixels(width, height, mre_pixels, 17) if mre_pixels > 0 else None
-    ref64 = fp64_reference(scene, scene.config, frames + 1, px) if px is not None else None
+    n_frames = max(frames + 1, mre_frames if px is not None else 0)
+    ref64 = fp64_reference(scene, scene.config, n_frames, px) if px is not None else None
     mre = {}
     with Context(width, height, device=local) as ctx:
         ctx.upload(scene)
@@ -341,14 +347,15 @@ def measure_paths(local, width, height, frames=2, mre_pixels=1024):
                            ("precision", _lib.MODE_WAVEFRONT_PRECISION)):
             c = scene.config.copy()
             ms = []
-            for b in range(frames + 1):  # frame 0 warms up (and autotunes the wavefront)
+            for b in range(n_frames):  # frame 0 warms up (and autotunes the wavefront)
                 c["batch"] = b
                 ctx.set_config(c)
                 ctx.render_frame(mode)
                 ctx.synchronize()
-                if b:
+                if 1 <= b <= frames:
                     ms.append(ctx.last_kernel_ms())
-            imgs[name] = ctx.read_image(_lib.IMAGE_FRAME)
+                if b == frames:
+                    imgs[name] = ctx.read_image(_lib.IMAGE_FRAME)
             out[f"{name}_ms"] = float(np.mean(ms))
             out[f"{name}_mpaths"] = width * height / (float(np.mean(ms)) / 1e3) / 1e6
             if ref64 is not None:
@@ -364,7 +371,7 @@ def measure_paths(local, width, height, frames=2, mre_pixels=1024):
                        "peak_source": peak_kind, "roofline_mpaths": roof,
                        "frac": {k: out[f"{k}_mpaths"] / roof for k in ("plain", "wavefront", "precision")}}
     if mre:
-        out["mre"] = {"reference": f"FP64 oracle (same estimator and RNG stream in double) after {frames + 1} "
+        out["mre"] = {"reference": f"FP64 oracle (same estimator and RNG stream in double) after {n_frames} "
                                    f"frames at {len(px)} seeded pixels; reduced on the GPU in FP64; eps {MRE_EPS}",
                       **mre, "precision_over_plain": mre["precision"] / max(mre["plain"], 1e-300),
                       "wavefront_over_plain": mre["wavefront"] / max(mre["plain"], 1e-300)}
@@ -471,6 +478,7 @@ def measure_config4(local, frames=1024, mre_pixels=2048, width=960, height=540):
     import torch
     from aviatorengine2_b200 import Context, _lib, scenes
     scene = scenes.instanced_meshes(width=width, height=height, gpu_build=True)
+    _lib.lib().ae_bvh_builder_release()
     out = {"workload": f"instanced_meshes {width}x{height}, {frames} frames of 1 spp, depth "
                        f"{int(scene.config['depth'])}", "triangles": int(scene.triangles)}
     dev = torch.device("cuda", local)
@@ -627,6 +635,8 @@ def measure_serving(local, n_requests=48, rate=0.5, seed=7, claim_policy=1, fram
     rng = np.random.default_rng(seed)
     t0 = time.perf_counter()
     S = scenes.serving_scenes(gpu_build=True)
+    from aviatorengine2_b200 import _lib
+    _lib.lib().ae_bvh_builder_release()
     ctxs = []
     for sc in S:
         c = Context(256, 256, device=local)
@@ -790,6 +800,10 @@ def main():
     ap.add_argument("--no-config1", action="store_true", help="skip the small plain-method leg (Cornell box)")
     ap.add_argument("--c4-frames", type=int, default=1024, help="frames (1 spp each) of the precision-variant leg")
     ap.add_argument("--mre-pixels", type=int, default=2048, help="seeded pixels scored against the FP64 oracle")
+    ap.add_argument("--paths-tris", type=int, default=10_000_000, help="unique triangles of the wavefront scene")
+    ap.add_argument("--paths-instances", type=int, default=1024, help="instances of the wavefront scene")
+    ap.add_argument("--paths-mre-frames", type=int, default=16, help="frames accumulated before the MRE of the "
+                    "wavefront-scene images")
     ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--serve-frame-hz", type=float, default=30.0, help="world frames per second (every frame moves "
                     "all 4096 instances of the serving scenes)")
@@ -815,6 +829,7 @@ def main():
     # BLAS built on the GPU: the same bytes as the host build (tests), and
     # seconds less of set-up per run.
     scene = scenes.instanced_meshes(width=args.width, height=args.height, gpu_build=True)
+    _lib.lib().ae_bvh_builder_release()
     W, H = int(scene.config["width"]), int(scene.config["height"])
     ctx = Context(W, H, device=local)
     ctx.upload(scene)
@@ -963,7 +978,8 @@ def main():
             traceback.print_exc()
             return {"error": f"{type(e).__name__}: {e}"}
 
-    paths = leg(not args.no_paths, measure_paths, local, args.width, args.height, mre_pixels=args.mre_pixels // 2)
+    paths = leg(not args.no_paths, measure_paths, local, args.width, args.height, mre_pixels=args.mre_pixels,
+                mre_frames=args.paths_mre_frames, target_tris=args.paths_tris, n_instances=args.paths_instances)
     build = leg(not args.no_build, measure_build, local)
     config1 = leg(not args.no_config1, measure_config1, local)
     config4 = leg(not args.no_config4, measure_config4, local, args.c4_frames, args.mre_pixels)
