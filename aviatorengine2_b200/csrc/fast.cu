@@ -176,6 +176,146 @@ int stack_need(const std::vector<QNode> &nodes, uint32_t root) {
     return (q.nchild - 1) + best;
 }
 
+// Boxes of a mesh's binary BLAS nodes at depth kSubBoxDepth (leaves above
+// that depth count as they are), appended to `out` as six floats each; they
+// cover every triangle of the mesh.  Returns how many.
+uint32_t mesh_sub_boxes(const ae_bvh_node *bin, std::vector<float> &out) {
+    std::vector<uint32_t> level = {0};
+    for (int d = 0; d < kSubBoxDepth; d++) {
+        std::vector<uint32_t> next;
+        for (uint32_t i : level) {
+            if (bin[i].count > 0) next.push_back(i);
+            else { next.push_back(uint32_t(bin[i].left)); next.push_back(uint32_t(bin[i].right)); }
+        }
+        level.swap(next);
+    }
+    for (uint32_t i : level) {
+        const ae_bvh_node &n = bin[i];
+        const float b[6] = {n.min_x, n.min_y, n.min_z, n.max_x, n.max_y, n.max_z};
+        out.insert(out.end(), b, b + 6);
+    }
+    return uint32_t(level.size());
+}
+
+// World box of a mesh instance from its sub-boxes (double precision; the
+// device refresh computes the conservative version of the same bound).
+Box instance_box_host(const ae_instance &m, const float *sub, uint32_t count) {
+    const double s = (m.scale != 0.0f && m.scale != 1.0f) ? double(m.scale) : 1.0;
+    const double qx = m.qx, qy = m.qy, qz = m.qz, qw = m.qw;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (uint32_t b = 0; b < count; b++) {
+        const float *x = sub + 6 * size_t(b);
+        for (int k = 0; k < 8; k++) {
+            const double v[3] = {(k & 1 ? x[3] : x[0]) * s, (k & 2 ? x[4] : x[1]) * s, (k & 4 ? x[5] : x[2]) * s};
+            const double t[3] = {2 * (qy * v[2] - qz * v[1]), 2 * (qz * v[0] - qx * v[2]), 2 * (qx * v[1] - qy * v[0])};
+            const double w[3] = {v[0] + qw * t[0] + (qy * t[2] - qz * t[1]) + m.px,
+                                 v[1] + qw * t[1] + (qz * t[0] - qx * t[2]) + m.py,
+                                 v[2] + qw * t[2] + (qx * t[1] - qy * t[0]) + m.pz};
+            for (int a = 0; a < 3; a++) { lo[a] = std::min(lo[a], w[a]); hi[a] = std::max(hi[a], w[a]); }
+        }
+    }
+    Box r;
+    for (int a = 0; a < 3; a++) { r.lo[a] = float(lo[a]); r.hi[a] = float(hi[a]); }
+    return r;
+}
+
+// Binary tree over object boxes with one object per leaf, in ae_bvh_node
+// form (a leaf holds its object slot in `left`, count 1): binned SAH over the
+// centroids, 16 bins per axis; a median split where the centroids coincide
+// or the tree gets deep.
+struct ObjectTree {
+    const std::vector<Box> &box;
+    std::vector<uint32_t> idx;
+    std::vector<ae_bvh_node> nodes;
+
+    static float centre(const Box &b, int a) { return 0.5f * (b.lo[a] + b.hi[a]); }
+
+    uint32_t build(uint32_t b, uint32_t e, int depth) {
+        const uint32_t self = uint32_t(nodes.size());
+        nodes.push_back(ae_bvh_node{});
+        Box u = box[idx[b]];
+        for (uint32_t i = b + 1; i < e; i++)
+            for (int a = 0; a < 3; a++) {
+                u.lo[a] = std::min(u.lo[a], box[idx[i]].lo[a]);
+                u.hi[a] = std::max(u.hi[a], box[idx[i]].hi[a]);
+            }
+        ae_bvh_node n;
+        std::memset(&n, 0, sizeof(n));
+        n.min_x = u.lo[0]; n.min_y = u.lo[1]; n.min_z = u.lo[2];
+        n.max_x = u.hi[0]; n.max_y = u.hi[1]; n.max_z = u.hi[2];
+        if (e - b == 1) {
+            n.left = int32_t(idx[b]);
+            n.count = 1;
+            nodes[self] = n;
+            return self;
+        }
+        float clo[3] = {1e30f, 1e30f, 1e30f}, chi[3] = {-1e30f, -1e30f, -1e30f};
+        for (uint32_t i = b; i < e; i++)
+            for (int a = 0; a < 3; a++) {
+                clo[a] = std::min(clo[a], centre(box[idx[i]], a));
+                chi[a] = std::max(chi[a], centre(box[idx[i]], a));
+            }
+        constexpr int kBins = 16;
+        int axis = -1, split = 0;
+        double best = 1e300;
+        for (int a = 0; a < 3 && depth < 48; a++) {
+            const float ext = chi[a] - clo[a];
+            if (!(ext > 0.0f)) continue;
+            uint32_t cnt[kBins] = {};
+            Box bb[kBins];
+            for (int k = 0; k < kBins; k++)
+                for (int j = 0; j < 3; j++) { bb[k].lo[j] = 1e30f; bb[k].hi[j] = -1e30f; }
+            for (uint32_t i = b; i < e; i++) {
+                const Box &x = box[idx[i]];
+                const int k = std::min(kBins - 1, int((centre(x, a) - clo[a]) / ext * kBins));
+                cnt[k]++;
+                for (int j = 0; j < 3; j++) { bb[k].lo[j] = std::min(bb[k].lo[j], x.lo[j]); bb[k].hi[j] = std::max(bb[k].hi[j], x.hi[j]); }
+            }
+            double right_area[kBins];
+            uint32_t right_cnt[kBins];
+            Box acc = bb[kBins - 1];
+            uint32_t rc = 0;
+            for (int k = kBins - 1; k >= 1; k--) {
+                if (k < kBins - 1)
+                    for (int j = 0; j < 3; j++) { acc.lo[j] = std::min(acc.lo[j], bb[k].lo[j]); acc.hi[j] = std::max(acc.hi[j], bb[k].hi[j]); }
+                rc += cnt[k];
+                right_area[k] = rc ? half_area(acc) : 0.0;
+                right_cnt[k] = rc;
+            }
+            Box lacc = bb[0];
+            uint32_t lc = 0;
+            for (int k = 1; k < kBins; k++) {
+                if (k > 1)
+                    for (int j = 0; j < 3; j++) { lacc.lo[j] = std::min(lacc.lo[j], bb[k - 1].lo[j]); lacc.hi[j] = std::max(lacc.hi[j], bb[k - 1].hi[j]); }
+                lc += cnt[k - 1];
+                if (!lc || !right_cnt[k]) continue;
+                const double cost = double(lc) * half_area(lacc) + double(right_cnt[k]) * right_area[k];
+                if (cost < best) { best = cost; axis = a; split = k; }
+            }
+        }
+        uint32_t m = b;
+        if (axis >= 0) {
+            const float ext = chi[axis] - clo[axis];
+            m = uint32_t(std::partition(idx.begin() + b, idx.begin() + e, [&](uint32_t o) {
+                            return std::min(kBins - 1, int((centre(box[o], axis) - clo[axis]) / ext * kBins)) < split;
+                        }) - idx.begin());
+        }
+        if (m == b || m == e) {
+            int a = 0;
+            for (int j = 1; j < 3; j++) if (chi[j] - clo[j] > chi[a] - clo[a]) a = j;
+            m = (b + e) / 2;
+            std::nth_element(idx.begin() + b, idx.begin() + m, idx.begin() + e,
+                             [&](uint32_t x, uint32_t y) { return centre(box[x], a) < centre(box[y], a); });
+        }
+        const uint32_t l = build(b, m, depth + 1), r = build(m, e, depth + 1);
+        n.left = int32_t(l);
+        n.right = int32_t(r);
+        n.count = 0;
+        nodes[self] = n;
+        return self;
+    }
+};
+
 }  // namespace
 
 // The 4-wide quantised BVH of one mesh from its binary BLAS (mesh-relative
@@ -238,6 +378,255 @@ bool build_qbvh(const ae_bvh_node *bin, uint32_t n_bin, uint32_t tri_count, std:
     return true;
 }
 
+// ---------------------------------------------------------------------------
+// Instance-level tree
+// ---------------------------------------------------------------------------
+
+// Conservative world box of every object, one warp per object: a mesh
+// instance's sub-boxes (its BLAS nodes at depth kSubBoxDepth) with each
+// corner through the instance transform in double precision, the extremes
+// rounded outward to float; an analytic object's packed box.  Both are
+// widened by `margin` on every side, which covers the rounding of the
+// kernels' ToLocal and triangle arithmetic for rays that start within the
+// scene's coordinate range (the margin is 2^-14 of it).
+__global__ void k_object_boxes(const uint4 *__restrict__ meta, const FastInst *__restrict__ inst,
+                               const float *__restrict__ sub, const float *__restrict__ static_box, uint32_t n,
+                               float margin, float *__restrict__ out) {
+    const uint32_t slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (slot >= n) return;  // whole warps
+    const uint4 m = meta[slot];
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    if ((m.x & 0xff) == AE_SHAPE_MESH) {
+        const FastInst I = inst[m.y];
+        const double s = (I.scale != 0.0f && I.scale != 1.0f) ? double(I.scale) : 1.0;
+        const double qx = I.qx, qy = I.qy, qz = I.qz, qw = I.qw;
+        const uint32_t first = I.pad[0], cnt = I.pad[1];
+        for (uint32_t j = lane; j < cnt * 8u; j += 32) {
+            const float *x = sub + 6 * size_t(first + j / 8);
+            const uint32_t k = j & 7u;
+            const double v0 = double(k & 1u ? x[3] : x[0]) * s, v1 = double(k & 2u ? x[4] : x[1]) * s,
+                         v2 = double(k & 4u ? x[5] : x[2]) * s;
+            const double t0 = 2.0 * (qy * v2 - qz * v1), t1 = 2.0 * (qz * v0 - qx * v2), t2 = 2.0 * (qx * v1 - qy * v0);
+            const double w[3] = {v0 + qw * t0 + (qy * t2 - qz * t1) + double(I.px),
+                                 v1 + qw * t1 + (qz * t0 - qx * t2) + double(I.py),
+                                 v2 + qw * t2 + (qx * t1 - qy * t0) + double(I.pz)};
+            for (int a = 0; a < 3; a++) { lo[a] = fmin(lo[a], w[a]); hi[a] = fmax(hi[a], w[a]); }
+        }
+        for (int off = 16; off > 0; off >>= 1)
+            for (int a = 0; a < 3; a++) {
+                lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], off));
+                hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
+            }
+    } else {
+        const float *x = static_box + 6 * size_t(slot);
+        for (int a = 0; a < 3; a++) { lo[a] = x[a]; hi[a] = x[3 + a]; }
+    }
+    if (lane == 0) {
+        float *o = out + 6 * size_t(slot);
+        for (int a = 0; a < 3; a++) {
+            o[a] = __fsub_rd(__double2float_rd(lo[a]), margin);
+            o[3 + a] = __fadd_ru(__double2float_ru(hi[a]), margin);
+        }
+    }
+}
+
+// Smallest power-of-two scale whose 255 steps from `org` reach `top`
+// (the host collapser's frame rule); false when none fits the exponent range.
+__device__ bool frame_exponent(float org, float top, int &e) {
+    const float extent = top - org;
+    e = -126;
+    if (extent > 0.0f) {
+        e = int(ceil(log2(double(extent) / 255.0)));
+        while (ldexp(255.0, e) < double(extent)) e++;
+        e = max(e, -126);
+    }
+    while (e <= 127 && fmaf(255.0f, ldexpf(1.0f, e), org) < top) e++;
+    return e <= 127;
+}
+
+// Child interval [a, b] quantised outward in the frame (org, 2^e): the
+// decoded bounds org + q 2^e (fmaf) contain it.
+__device__ bool quantise_outward(float org, int e, float a, float b, uint8_t &qa, uint8_t &qb) {
+    const float sc = ldexpf(1.0f, e);
+    double la = floor((double(a) - double(org)) / double(sc)), lb = ceil((double(b) - double(org)) / double(sc));
+    la = fmin(fmax(la, 0.0), 255.0);
+    lb = fmin(fmax(lb, 0.0), 255.0);
+    int ia = int(la), ib = int(lb);
+    while (ia > 0 && fmaf(float(ia), sc, org) > a) ia--;
+    while (ib < 255 && fmaf(float(ib), sc, org) < b) ib++;
+    qa = uint8_t(ia);
+    qb = uint8_t(ib);
+    return fmaf(float(ia), sc, org) <= a && fmaf(float(ib), sc, org) >= b;
+}
+
+// One level of the instance tree's bottom-up refresh (levels deepest first):
+// a node's float box is the union of its children's (objects' boxes for leaf
+// children), and its children are re-quantised in the node's new frame.  A
+// child whose box is empty or not finite becomes an unused slot.  Sets *bad
+// when a box cannot be quantised conservatively.
+__global__ void k_instance_tree_level(QNode *__restrict__ nodes, float *__restrict__ nbox,
+                                      const float *__restrict__ obj_box, const int32_t *__restrict__ level,
+                                      int32_t count, uint32_t *bad) {
+    const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int32_t ni = level[k];
+    QNode q = nodes[ni];
+    float cb[4][6];
+    bool cv[4];
+    float u[6] = {3.402823466e38f, 3.402823466e38f, 3.402823466e38f, -3.402823466e38f, -3.402823466e38f,
+                  -3.402823466e38f};
+    bool any = false;
+    for (int c = 0; c < 4; c++) {
+        cv[c] = false;
+        if (c >= q.nchild) continue;
+        const uint32_t ref = q.child[c];
+        const float *x = (ref & kLeafBit) ? obj_box + 6 * size_t(leaf_first(ref)) : nbox + 6 * size_t(ref);
+        bool ok = true;
+        for (int a = 0; a < 6; a++) { cb[c][a] = x[a]; ok = ok && isfinite(x[a]); }
+        for (int a = 0; a < 3; a++) ok = ok && cb[c][a] <= cb[c][3 + a];
+        cv[c] = ok;
+        if (!ok) continue;
+        any = true;
+        for (int a = 0; a < 3; a++) { u[a] = fminf(u[a], cb[c][a]); u[3 + a] = fmaxf(u[3 + a], cb[c][3 + a]); }
+    }
+    bool good = true;
+    int ex[3] = {0, 0, 0};
+    if (any) {
+        q.ox = u[0]; q.oy = u[1]; q.oz = u[2];
+        for (int a = 0; a < 3; a++) good = frame_exponent(u[a], u[3 + a], ex[a]) && good;
+    } else {
+        q.ox = q.oy = q.oz = 0.0f;
+        u[0] = u[1] = u[2] = __int_as_float(0x7f800000);
+        u[3] = u[4] = u[5] = -__int_as_float(0x7f800000);
+    }
+    q.ex = int8_t(good ? ex[0] : 0); q.ey = int8_t(good ? ex[1] : 0); q.ez = int8_t(good ? ex[2] : 0);
+    const float org[3] = {q.ox, q.oy, q.oz};
+    for (int c = 0; c < 4; c++) {
+        if (cv[c] && any && good) {
+            for (int a = 0; a < 3; a++)
+                good = quantise_outward(org[a], ex[a], cb[c][a], cb[c][3 + a], q.lo[a][c], q.hi[a][c]) && good;
+        } else {
+            for (int a = 0; a < 3; a++) { q.lo[a][c] = 255; q.hi[a][c] = 0; }
+        }
+    }
+    if (!good) atomicExch(bad, 1u);
+    nodes[ni] = q;
+    float *o = nbox + 6 * size_t(ni);
+    for (int a = 0; a < 6; a++) o[a] = u[a];
+}
+
+// Topology of the instance-level tree for the current objects (host, per
+// scene layout): an object tree over host bounds, collapsed 4-wide by the
+// BLAS collapser.  The boxes uploaded here are replaced by the device
+// refresh.
+static int build_instance_tree(Ctx *c, FastScene &F) {
+    const uint32_t n = c->n_objects;
+    F.n_tnodes = 0;
+    F.tlas_stack = 0;
+    F.troot = kEmptyTlas;
+    F.static_range = 0.0f;
+    if (n == 0) return AE_OK;
+    if (n >= kMaxLeafFirst) return c->fail(AE_ERR_LAYOUT, "%u objects: the instance tree addresses at most %u", n, kMaxLeafFirst);
+    std::vector<Box> boxes(n);
+    std::vector<float> stat(size_t(n) * 6, 0.0f);
+    for (uint32_t s = 0; s < n; s++) {
+        const ae_object &o = c->host_objects[s];
+        if (o.shapeType == AE_SHAPE_MESH) {
+            const ae_instance &m = c->host_instances[o.instanceIndex];
+            const FastScene::MeshSub &ms = F.mesh_sub.at(std::make_tuple(m.vertexBase, m.indexBase, m.triangleCount, m.blasBase));
+            boxes[s] = instance_box_host(m, F.host_sub.data() + 6 * size_t(ms.first), ms.count);
+        } else {
+            const ae_aabb b = analytic_box(o);
+            boxes[s] = Box{{b.min_x, b.min_y, b.min_z}, {b.max_x, b.max_y, b.max_z}};
+            std::memcpy(&stat[6 * size_t(s)], &b, 24);
+            for (int a = 0; a < 3; a++)
+                F.static_range = std::max(F.static_range, std::max(std::fabs(boxes[s].lo[a]), std::fabs(boxes[s].hi[a])));
+        }
+    }
+    ObjectTree T{boxes, {}, {}};
+    T.idx.resize(n);
+    for (uint32_t s = 0; s < n; s++) T.idx[s] = s;
+    T.nodes.reserve(2 * size_t(n));
+    T.build(0, n, 0);
+    std::vector<QNode> out;
+    uint32_t root;
+    if (T.nodes[0].count > 0) {
+        root = leaf_ref(uint32_t(T.nodes[0].left), 1);
+    } else {
+        Collapser col{T.nodes.data(), out};
+        root = col.emit(0);
+        F.tlas_stack = stack_need(out, root);
+        if (F.tlas_stack > kTlas4Stack)
+            return c->fail(AE_ERR_LAYOUT, "instance tree needs %d stack entries (> %d)", F.tlas_stack, kTlas4Stack);
+    }
+    // Nodes by depth, deepest first, for the bottom-up refresh.
+    std::vector<int32_t> depth(out.size(), 0), order;
+    int maxd = 0;
+    for (size_t i = 0; i < out.size(); i++)
+        for (int k = 0; k < out[i].nchild; k++)
+            if (!(out[i].child[k] & kLeafBit)) {
+                depth[out[i].child[k]] = depth[i] + 1;
+                maxd = std::max(maxd, depth[i] + 1);
+            }
+    F.tlevel_start.assign(1, 0);
+    for (int d = maxd; d >= 0 && !out.empty(); d--) {
+        for (size_t i = 0; i < out.size(); i++)
+            if (depth[i] == d) order.push_back(int32_t(i));
+        F.tlevel_start.push_back(int32_t(order.size()));
+    }
+    const size_t nn = std::max<size_t>(out.size(), 1);
+    if (F.tnodes.reserve(nn) || F.tbox.reserve(nn * 6) || F.tlevels.reserve(std::max<size_t>(order.size(), 1)) ||
+        F.obj_box.reserve(size_t(n) * 6) || F.static_box.reserve(size_t(n) * 6) || F.tflag.reserve(1))
+        return c->fail(AE_ERR_OOM, "instance tree");
+    int rc;
+    if (!out.empty() &&
+        ((rc = c->cuda(cudaMemcpyAsync(F.tnodes.ptr, out.data(), out.size() * sizeof(QNode), cudaMemcpyHostToDevice,
+                                       c->stream), "upload instance tree")) ||
+         (rc = c->cuda(cudaMemcpyAsync(F.tlevels.ptr, order.data(), order.size() * sizeof(int32_t),
+                                       cudaMemcpyHostToDevice, c->stream), "upload instance tree levels"))))
+        return rc;
+    if ((rc = c->cuda(cudaMemcpyAsync(F.static_box.ptr, stat.data(), stat.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                      c->stream), "upload object boxes")))
+        return rc;
+    // The host copies must outlive the asynchronous copies.
+    if ((rc = c->cuda(cudaStreamSynchronize(c->stream), "instance tree"))) return rc;
+    F.n_tnodes = uint32_t(out.size());
+    F.troot = root;
+    return AE_OK;
+}
+
+// Device refresh of the instance tree's boxes from the current instance
+// records (after every upload or refit).
+static int refresh_instance_tree(Ctx *c, FastScene &F) {
+    if (F.n_tnodes == 0) return AE_OK;
+    // Coordinate range of the scene for the margin of the object boxes.
+    float range = 1.0f;
+    for (uint32_t s = 0; s < c->n_objects; s++) {
+        const ae_object &o = c->host_objects[s];
+        if (o.shapeType == AE_SHAPE_MESH) {
+            const ae_instance &m = c->host_instances[o.instanceIndex];
+            const FastScene::MeshSub &ms = F.mesh_sub.at(std::make_tuple(m.vertexBase, m.indexBase, m.triangleCount, m.blasBase));
+            const float sc = (m.scale != 0.0f && m.scale != 1.0f) ? std::fabs(m.scale) : 1.0f;
+            const float r = std::max(std::fabs(m.px), std::max(std::fabs(m.py), std::fabs(m.pz))) + 1.75f * sc * ms.radius;
+            range = std::max(range, r);
+        }
+    }
+    range = std::max(range, F.static_range);
+    const float margin = std::ldexp(range, -14);
+    const uint32_t n = c->n_objects;
+    int rc;
+    if ((rc = c->cuda(cudaMemsetAsync(F.tflag.ptr, 0, sizeof(uint32_t), c->stream), "instance tree flag"))) return rc;
+    k_object_boxes<<<(n * 32 + 255) / 256, 256, 0, c->stream>>>(F.obj_meta.ptr, F.inst.ptr, F.sub_boxes.ptr,
+                                                                 F.static_box.ptr, n, margin, F.obj_box.ptr);
+    for (size_t l = 0; l + 1 < F.tlevel_start.size(); l++) {
+        const int32_t cnt = F.tlevel_start[l + 1] - F.tlevel_start[l];
+        if (cnt <= 0) continue;
+        k_instance_tree_level<<<(cnt + 127) / 128, 128, 0, c->stream>>>(F.tnodes.ptr, F.tbox.ptr, F.obj_box.ptr,
+                                                                       F.tlevels.ptr + F.tlevel_start[l], cnt, F.tflag.ptr);
+    }
+    return c->cuda(cudaGetLastError(), "instance tree refresh");
+}
+
 int prepare_fast(Ctx *c) {
     // Not ready until this call accepts the current scene: every early
     // return below leaves the optimised structures unusable.
@@ -252,6 +641,8 @@ int prepare_fast(Ctx *c) {
         F.mesh_roots.clear();
         F.host_nodes.clear();
         F.host_tris.clear();
+        F.mesh_sub.clear();
+        F.host_sub.clear();
         F.max_stack = 0;
         F.shade16_tris = 0;
         F.geometry_key = c->geometry_version;
@@ -291,6 +682,12 @@ int prepare_fast(Ctx *c) {
         F.host_nodes.insert(F.host_nodes.end(), local.begin(), local.end());
         F.max_stack = std::max(F.max_stack, need);
         F.mesh_roots[key] = std::make_pair(root, tri_base);
+        FastScene::MeshSub ms;
+        ms.first = uint32_t(F.host_sub.size() / 6);
+        ms.count = mesh_sub_boxes(c->host_blas.data() + m.blasBase, F.host_sub);
+        ms.radius = 0.0f;
+        for (size_t k = size_t(ms.first) * 6; k < F.host_sub.size(); k++) ms.radius = std::max(ms.radius, std::fabs(F.host_sub[k]));
+        F.mesh_sub[key] = ms;
         F.geometry_dirty = true;
     }
     if (F.max_stack + 1 > kFastStack)
@@ -308,6 +705,11 @@ int prepare_fast(Ctx *c) {
         if ((rc = c->cuda(cudaMemcpyAsync(F.tris.ptr, F.host_tris.data(), F.host_tris.size() * sizeof(float),
                                           cudaMemcpyHostToDevice, c->stream), "upload triangles")))
             return rc;
+        if (F.sub_boxes.reserve(std::max<size_t>(F.host_sub.size(), 1))) return c->fail(AE_ERR_OOM, "mesh sub-boxes");
+        if (!F.host_sub.empty() &&
+            (rc = c->cuda(cudaMemcpyAsync(F.sub_boxes.ptr, F.host_sub.data(), F.host_sub.size() * sizeof(float),
+                                          cudaMemcpyHostToDevice, c->stream), "upload mesh sub-boxes")))
+            return rc;
         F.geometry_dirty = false;
     }
     // Scene-derived part: instances and object metadata, per upload.
@@ -321,13 +723,21 @@ int prepare_fast(Ctx *c) {
             f.qx = m.qx; f.qy = m.qy; f.qz = m.qz; f.qw = m.qw;
             f.root = rt.first;
             f.tri_base = rt.second;
-            f.pad[0] = f.pad[1] = 0;
+            const FastScene::MeshSub &ms = F.mesh_sub.at(std::make_tuple(m.vertexBase, m.indexBase, m.triangleCount, m.blasBase));
+            f.pad[0] = ms.first;
+            f.pad[1] = ms.count;
         }
+        // Each object's rank comes from the reference TLAS leaf that holds it.
+        std::vector<uint32_t> leaf_first_of(std::max<uint32_t>(c->n_objects, 1), 0u);
+        for (const ae_bvh_node &nd : c->host_tlas)
+            if (nd.count > 0)
+                for (int32_t k = 0; k < nd.count; k++)
+                    if (uint32_t(nd.left + k) < c->n_objects) leaf_first_of[nd.left + k] = uint32_t(nd.left);
         std::vector<uint4> meta(std::max<uint32_t>(c->n_objects, 1));
         F.has_volumes = false;
         for (uint32_t s = 0; s < c->n_objects; s++) {
             const ae_object &o = c->host_objects[s];
-            meta[s] = make_uint4(o.shapeType | (o.colorType << 8), o.instanceIndex, 0u, 0u);
+            meta[s] = make_uint4(o.shapeType | (o.colorType << 8), o.instanceIndex, leaf_first_of[s], 0u);
             if (o.colorType == AE_MAT_ISOTROPIC) F.has_volumes = true;
         }
         if (F.inst.reserve(fi.size()) || F.obj_meta.reserve(meta.size())) return c->fail(AE_ERR_OOM, "fast scene");
@@ -337,7 +747,20 @@ int prepare_fast(Ctx *c) {
         if ((rc = c->cuda(cudaMemcpyAsync(F.obj_meta.ptr, meta.data(), meta.size() * sizeof(uint4),
                                           cudaMemcpyHostToDevice, c->stream), "upload metadata")))
             return rc;
+        if (F.tlas_key != c->scene_version_layout || F.sub_key != c->geometry_version) {
+            F.tlas_key = ~0ull;
+            if ((rc = build_instance_tree(c, F))) return rc;
+            F.tlas_key = c->scene_version_layout;
+            F.sub_key = c->geometry_version;
+        }
+        if ((rc = refresh_instance_tree(c, F))) return rc;
         if ((rc = c->cuda(cudaStreamSynchronize(c->stream), "prepare fast"))) return rc;
+        if (F.n_tnodes) {
+            uint32_t bad = 0;
+            if ((rc = c->cuda(cudaMemcpy(&bad, F.tflag.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost), "instance tree flag")))
+                return rc;
+            if (bad) return c->fail(AE_ERR_LAYOUT, "instance tree: an object box cannot be quantised conservatively");
+        }
         F.scene_key = c->scene_version;
     }
     if (F.has_volumes)
@@ -467,7 +890,7 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_closest_walk(DevScene
         bool active = k < n;
         if (active) {
             const ae_ray r = rays[k];
-            w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+            w.start(V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
         }
         uint32_t iter = 0;
         for (;;) {
@@ -488,7 +911,7 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_closest_walk(DevScene
             active = k < n;
             if (active) {
                 const ae_ray r = rays[k];
-                w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+                w.start(V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
             }
         }
         return;
@@ -521,7 +944,7 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_closest_walk(DevScene
                 need = false;
                 active = true;
                 const ae_ray r = rays[k];
-                w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+                w.start(V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
             }
             cbase += take;
             m = __ballot_sync(0xffffffffu, need);
@@ -549,7 +972,7 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_closest_walk(DevScene
 cudaError_t launch_closest_walk(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     FastScene &F = *c->fast;
-    FastView V{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr};
+    FastView V = fast_view(F);
     const int threads = 128;
     const size_t smem = size_t(kSharedStack) * threads * sizeof(uint2);
     static int per_sm = 0, sms = 0;
@@ -579,7 +1002,7 @@ cudaError_t launch_count_fast(Ctx *c, const ae_ray *rays, uint32_t n, bool quant
                               cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     FastScene &F = *c->fast;
-    FastView V{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr};
+    FastView V = fast_view(F);
     const int threads = 128;
     const size_t smem = size_t(kSharedStack) * threads * sizeof(uint2);
     if (quant) {
@@ -595,7 +1018,7 @@ cudaError_t launch_count_fast(Ctx *c, const ae_ray *rays, uint32_t n, bool quant
 cudaError_t launch_closest_fast(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, bool quant, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     FastScene &F = *c->fast;
-    FastView V{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr};
+    FastView V = fast_view(F);
     const int threads = 128;
     const size_t smem = size_t(kSharedStack) * threads * sizeof(uint2);
     if (quant) {

@@ -14,4 +14,7 @@ cudaError_t launch_count_fast(Ctx *c, const ae_ray *rays, uint32_t n, bool quant
 void destroy_wavefront(Ctx *c);
 void destroy_deferred(Ctx *c);
 void destroy_refit(Ctx *c);
+// World box of an analytic (non-mesh) object record, as the scene packer
+// computes it (refit.cu).
+ae_aabb analytic_box(const ae_object &o);
 }  // namespace ae

@@ -44,6 +44,19 @@ struct FastInst {            // 48 B
 };
 static_assert(sizeof(FastInst) == 48, "FastInst must be 48 bytes");
 
+// The instance-level tree of the optimised walks: 4-wide QNodes over every
+// object of the scene, one object per leaf (leaf_ref(slot, 1)), boxes from
+// conservative world bounds of each object (fast.cu: k_object_boxes) and
+// refreshed on the device whenever the instances move.  The ranking of equal
+// distances does not depend on this tree: an object's rank comes from the
+// reference TLAS leaf that holds it (the metadata's z word).
+constexpr uint32_t kEmptyTlas = kLeafBit;  // root of a scene without objects (a leaf of count 0)
+constexpr int kTlas4Stack = 40;
+// Depth of the BLAS nodes whose boxes bound a mesh for the instance tree: up
+// to 2^kSubBoxDepth local boxes per mesh, each corner through the instance
+// transform.
+constexpr int kSubBoxDepth = 8;
+
 struct FastScene {
     DevBuf<QNode> nodes;
     DevBuf<float4> tris;     // 3 float4 per triangle
@@ -67,6 +80,27 @@ struct FastScene {
     std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>, std::pair<uint32_t, uint32_t>> mesh_roots;
     std::vector<QNode> host_nodes;
     std::vector<float> host_tris;
+    // Instance-level tree.  Per mesh: its local sub-boxes (host_sub, six
+    // floats each) at sub_boxes[first .. first + count) and the largest
+    // coordinate magnitude they reach.
+    struct MeshSub {
+        uint32_t first, count;
+        float radius;
+    };
+    std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>, MeshSub> mesh_sub;
+    std::vector<float> host_sub;
+    DevBuf<float> sub_boxes;
+    DevBuf<QNode> tnodes;         // the tree's nodes (boxes rewritten on every refresh)
+    DevBuf<float> tbox;           // float box per tree node (6 floats)
+    DevBuf<float> obj_box;        // conservative world box per object (6 floats)
+    DevBuf<float> static_box;     // analytic objects' boxes (6 floats per object slot)
+    DevBuf<int32_t> tlevels;      // tree nodes by depth, deepest first
+    DevBuf<uint32_t> tflag;       // set by the refresh when a box cannot be quantised
+    std::vector<int32_t> tlevel_start;
+    uint32_t troot = kEmptyTlas, n_tnodes = 0;
+    int tlas_stack = 0;
+    float static_range = 0.0f;    // largest coordinate magnitude of the analytic objects' boxes
+    uint64_t tlas_key = ~0ull, sub_key = ~0ull;
 };
 
 // Traversal stack per thread: the first kSharedStack entries in shared
@@ -84,8 +118,21 @@ struct FastView {
     const QNode *nodes;
     const float4 *tris;
     const FastInst *inst;
-    const uint4 *meta;
+    const uint4 *meta;      // x: shape | material << 8, y: instance, z: first slot of its reference TLAS leaf
+    const QNode *tnodes;    // instance-level tree
+    uint32_t troot;         // its root: a node index, leaf_ref(slot, 1), or kEmptyTlas
 };
+
+// The view of a prepared scene; `inst` and `tnodes` may name another copy of
+// the per-frame arrays (serving frame sets).
+inline FastView fast_view(const FastScene &F, const FastInst *inst = nullptr, const QNode *tnodes = nullptr) {
+    return FastView{F.nodes.ptr, F.tris.ptr, inst ? inst : F.inst.ptr, F.obj_meta.ptr, tnodes ? tnodes : F.tnodes.ptr,
+                    F.troot};
+}
+
+// Rank of an object's candidates (see Best): ~first slot of the reference
+// TLAS leaf holding the object, then the slot.
+AE_DEV uint64_t object_rank(const uint4 &meta, uint32_t slot) { return (uint64_t(~meta.z) << 32) | slot; }
 
 // Best candidate so far with its visit rank (see the file comment).  A
 // candidate ranks by (object rank, leaf rank, slot): object rank is
@@ -193,6 +240,22 @@ AE_DEV void child_hits(const QNode *nodep, f3 o, f3 inv, float tn, float tf, flo
 // value of the same sign, so products stay finite (no 0 * inf).
 AE_DEV float slab_inv(float x) { return fabsf(x) > 1e-20f ? 1.0f / x : copysignf(1e20f, x); }
 
+// Sorts child_hits' four (distance, child) pairs nearest first and returns
+// how many were hit (misses carry +inf and sort last).
+AE_DEV int sort_hits(float tm[4], uint32_t ch[4]) {
+#define AE_SWAP(i, j)                                            \
+    if (tm[j] < tm[i]) {                                         \
+        const float tt = tm[i]; tm[i] = tm[j]; tm[j] = tt;       \
+        const uint32_t cc = ch[i]; ch[i] = ch[j]; ch[j] = cc;    \
+    }
+    AE_SWAP(0, 1) AE_SWAP(2, 3) AE_SWAP(0, 2) AE_SWAP(1, 3) AE_SWAP(1, 2)
+#undef AE_SWAP
+    int nh = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) nh += tm[k] != __int_as_float(0x7f800000) ? 1 : 0;
+    return nh;
+}
+
 // T (optional): touch counters - wide nodes in `blas`, 48-byte triangle
 // records in `tris`.
 template <bool WT, int SS = kSharedStack>
@@ -214,39 +277,27 @@ AE_DEV void trace_mesh(const FastView &V, const FastInst &I, uint32_t slot, uint
     uint2 spill[kFastStack - SS];
     int sp = 0;
     uint32_t cur = I.root;
-    for (;;) {
-        if (cur & kLeafBit) {
-            const uint32_t first = leaf_first(cur), cnt = leaf_count(cur);
-            if (T) T->tris += cnt;
-            for (uint32_t k = 0; k < cnt; k++) {
-                const uint32_t s = first + k;
-                const float4 *r = tris + size_t(s) * 3;
-                const float4 r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2);
-                float t, a, b;
-                const bool h = WT ? tri_test_wt(lo, W, tn, best.t, r0, r1, r2, t, a, b)
-                                  : tri_test_ref(lo, ld, tn, best.t, r0, r1, r2, t, a, b);
-                if (h && takes(best, t, orank, ~first, s)) {
-                    best.t = t; best.alpha = a; best.beta = b;
-                    best.object = slot; best.prim = s;
-                    best.orank = orank; best.lrank = ~first;
-                }
+    // Next stack entry still no farther than the best hit; false when none.
+    auto pop = [&]() {
+        while (sp > 0) {
+            sp--;
+            const uint2 e = sp < SS ? stk[sp * nthreads + tid] : spill[sp - SS];
+            if (__uint_as_float(e.y) <= best.t) {
+                cur = e.x;
+                return true;
             }
-        } else {
+        }
+        return false;
+    };
+    for (;;) {
+        // Interior nodes until this lane holds a leaf; the warp's lanes then
+        // test their leaves' triangles together.
+        while (!(cur & kLeafBit)) {
             float tm[4];
             uint32_t ch[4];
             if (T) T->blas++;
             child_hits(V.nodes + cur, lo, inv, tn, best.t, tm, ch);
-            // Sort the four (distance, child) pairs, nearest first.
-#define AE_SWAP(i, j)                                            \
-    if (tm[j] < tm[i]) {                                         \
-        const float tt = tm[i]; tm[i] = tm[j]; tm[j] = tt;       \
-        const uint32_t cc = ch[i]; ch[i] = ch[j]; ch[j] = cc;    \
-    }
-            AE_SWAP(0, 1) AE_SWAP(2, 3) AE_SWAP(0, 2) AE_SWAP(1, 3) AE_SWAP(1, 2)
-#undef AE_SWAP
-            int nh = 0;
-#pragma unroll
-            for (int k = 0; k < 4; k++) nh += tm[k] != __int_as_float(0x7f800000) ? 1 : 0;
+            const int nh = sort_hits(tm, ch);
             if (nh > 0) {
                 // Far hits onto the stack (farthest deepest), continue with the
                 // nearest.  prepare_fast checked that the tree never needs more
@@ -258,110 +309,113 @@ AE_DEV void trace_mesh(const FastView &V, const FastInst &I, uint32_t slot, uint
                     sp = sp < kFastStack ? sp + 1 : sp;
                 }
                 cur = ch[0];
-                continue;
+            } else if (!pop()) {
+                return;
             }
         }
-        // Pop the next entry still no farther than the best hit.
-        bool found = false;
-        while (sp > 0) {
-            sp--;
-            const uint2 e = sp < SS ? stk[sp * nthreads + tid] : spill[sp - SS];
-            if (__uint_as_float(e.y) <= best.t) {
-                cur = e.x;
-                found = true;
-                break;
+        const uint32_t first = leaf_first(cur), cnt = leaf_count(cur);
+        if (T) T->tris += cnt;
+        for (uint32_t k = 0; k < cnt; k++) {
+            const uint32_t s = first + k;
+            const float4 *r = tris + size_t(s) * 3;
+            const float4 r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2);
+            float t, a, b;
+            const bool h = WT ? tri_test_wt(lo, W, tn, best.t, r0, r1, r2, t, a, b)
+                              : tri_test_ref(lo, ld, tn, best.t, r0, r1, r2, t, a, b);
+            if (h && takes(best, t, orank, ~first, s)) {
+                best.t = t; best.alpha = a; best.beta = b;
+                best.object = slot; best.prim = s;
+                best.orank = orank; best.lrank = ~first;
             }
         }
-        if (!found) break;
+        if (!pop()) return;
     }
 }
 
-// Closest hit of one ray over the whole scene: TLAS (the reference's binary
-// nodes, nearest child first), analytic objects by the reference intersectors,
+// Closest hit of one ray over the whole scene: the instance-level tree
+// (nearest child first), analytic objects by the reference intersectors,
 // meshes by the 4-wide quantised BLAS.  `stk` is this thread's column of the
-// block's shared-memory stack.  T (optional) counts the touches: TLAS nodes,
-// object metadata records, instance records, wide BLAS nodes, triangle records.
+// block's shared-memory stack.  T (optional) counts the touches: instance-tree
+// nodes, object metadata records, instance records, wide BLAS nodes, triangle
+// records.
 template <bool WT, int SS = kSharedStack>
 AE_DEV Best closest_fast(const DevScene &S, const FastView &V, f3 o, f3 d, float tn, float time, uint2 *stk, int tid,
                          int nt, Touch *T = nullptr) {
     Best best;
     best.t = kFarStart; best.alpha = 0.0f; best.beta = 0.0f;
     best.object = AE_MISS; best.prim = AE_MISS; best.orank = 0; best.lrank = 0;
-    if (S.n_nodes == 0) return best;
+    if (V.troot == kEmptyTlas) return best;
     const f3 inv = mk(slab_inv(d.x), slab_inv(d.y), slab_inv(d.z));
-    const f3 rinv = 1.0f / d;
-    int tstack[kTlasStack];
-    float tdist[kTlasStack];
+    uint32_t tstack[kTlas4Stack];
+    float tdist[kTlas4Stack];
     int sp = 0;
-    NodeBox nb = load_node(S.tlas, 0);
-    if (T) T->tlas++;
-    bool live = slab_ref(o, rinv, nb.lo, nb.hi, tn, kFarStart);
-    while (live) {
-        if (nb.count > 0) {
-            const uint32_t first = uint32_t(nb.left);
-            for (int k = 0; k < nb.count; k++) {
-                const uint32_t slot = first + uint32_t(k);
-                const uint64_t orank = (uint64_t(~first) << 32) | slot;
-                const uint4 m = __ldg(V.meta + slot);
-                const uint32_t shape = m.x & 0xff;
-                if (T) T->objects++;
-                if (shape == AE_SHAPE_MESH) {
-                    if (T) T->instances++;
-                    const float4 *ip = reinterpret_cast<const float4 *>(V.inst + m.y);
-                    const float4 a = __ldg(ip), b = __ldg(ip + 1), c = __ldg(ip + 2);
-                    FastInst I;
-                    I.px = a.x; I.py = a.y; I.pz = a.z; I.scale = a.w;
-                    I.qx = b.x; I.qy = b.y; I.qz = b.z; I.qw = b.w;
-                    I.root = __float_as_uint(c.x); I.tri_base = __float_as_uint(c.y);
-                    trace_mesh<WT, SS>(V, I, slot, orank, o, d, tn, best, stk, tid, nt, T);
-                } else {
-                    DHit h;
-                    const ae_object *obj = S.objects + slot;
-                    bool hit;
-                    if (shape == AE_SHAPE_SPHERE) hit = hit_sphere_ref(obj, o, d, time, tn, best.t, h);
-                    else if (shape == AE_SHAPE_QUAD) hit = hit_planar_ref(obj, false, o, d, tn, best.t, h);
-                    else if (shape == AE_SHAPE_TRIANGLE) hit = hit_planar_ref(obj, true, o, d, tn, best.t, h);
-                    else hit = hit_box_ref(obj, o, d, tn, best.t, h);
-                    if (hit && takes(best, h.t, orank, 0u, 0u)) {
-                        best.t = h.t; best.alpha = h.alpha; best.beta = h.beta;
-                        best.object = slot; best.prim = AE_MISS; best.orank = orank; best.lrank = 0;
-                    }
-                }
-            }
-        } else {
-            const NodeBox L = load_node(S.tlas, uint32_t(nb.left)), R = load_node(S.tlas, uint32_t(nb.right));
-            if (T) T->tlas += 2;
-            const f3 lt0 = (L.lo - o) * inv, lt1 = (L.hi - o) * inv;
-            const f3 rt0 = (R.lo - o) * inv, rt1 = (R.hi - o) * inv;
-            const float lmin = fmaxf(fmaxf(fminf(lt0.x, lt1.x), fminf(lt0.y, lt1.y)), fmaxf(fminf(lt0.z, lt1.z), tn));
-            const float lmax = fminf(fminf(fmaxf(lt0.x, lt1.x), fmaxf(lt0.y, lt1.y)), fmaxf(lt0.z, lt1.z));
-            const float rmin = fmaxf(fmaxf(fminf(rt0.x, rt1.x), fminf(rt0.y, rt1.y)), fmaxf(fminf(rt0.z, rt1.z), tn));
-            const float rmax = fminf(fminf(fmaxf(rt0.x, rt1.x), fmaxf(rt0.y, rt1.y)), fmaxf(rt0.z, rt1.z));
-            const float lmin_c = lmin * kEntryShrink, rmin_c = rmin * kEntryShrink;
-            const bool lh = lmin_c <= fminf(lmax * kExitGrow, best.t);
-            const bool rh = rmin_c <= fminf(rmax * kExitGrow, best.t);
-            if (lh && rh) {
-                const bool lfirst = lmin <= rmin;
-                if (sp < kTlasStack) {
-                    tstack[sp] = lfirst ? nb.right : nb.left;
-                    tdist[sp] = lfirst ? rmin_c : lmin_c;
-                    sp++;
-                }
-                nb = lfirst ? L : R;
-                continue;
-            }
-            if (lh) { nb = L; continue; }
-            if (rh) { nb = R; continue; }
-        }
-        live = false;
+    uint32_t cur = V.troot;
+    // Next stack entry no farther than the best hit; false when none is left.
+    auto pop = [&]() {
         while (sp > 0) {
             sp--;
             if (tdist[sp] <= best.t) {
-                nb = load_node(S.tlas, uint32_t(tstack[sp]));
-                live = true;
+                cur = tstack[sp];
+                return true;
+            }
+        }
+        return false;
+    };
+    for (;;) {
+        // Inner nodes until this lane holds an object: the lanes of a warp
+        // leave this loop together and then enter their objects together
+        // (a lane at a node does not wait through another lane's whole mesh).
+        bool live = true;
+        while (!(cur & kLeafBit)) {
+            float tm[4];
+            uint32_t ch[4];
+            if (T) T->tlas++;
+            child_hits(V.tnodes + cur, o, inv, tn, best.t, tm, ch);
+            const int nh = sort_hits(tm, ch);
+            if (nh > 0) {
+                // prepare_fast checked the tree against kTlas4Stack.
+                for (int k = nh - 1; k >= 1; k--) {
+                    if (sp < kTlas4Stack) {
+                        tstack[sp] = ch[k];
+                        tdist[sp] = tm[k];
+                        sp++;
+                    }
+                }
+                cur = ch[0];
+            } else if (!pop()) {
+                live = false;
                 break;
             }
         }
+        if (!live) break;
+        const uint32_t slot = leaf_first(cur);
+        const uint4 m = __ldg(V.meta + slot);
+        const uint64_t orank = object_rank(m, slot);
+        const uint32_t shape = m.x & 0xff;
+        if (T) T->objects++;
+        if (shape == AE_SHAPE_MESH) {
+            if (T) T->instances++;
+            const float4 *ip = reinterpret_cast<const float4 *>(V.inst + m.y);
+            const float4 a = __ldg(ip), b = __ldg(ip + 1), c = __ldg(ip + 2);
+            FastInst I;
+            I.px = a.x; I.py = a.y; I.pz = a.z; I.scale = a.w;
+            I.qx = b.x; I.qy = b.y; I.qz = b.z; I.qw = b.w;
+            I.root = __float_as_uint(c.x); I.tri_base = __float_as_uint(c.y);
+            trace_mesh<WT, SS>(V, I, slot, orank, o, d, tn, best, stk, tid, nt, T);
+        } else {
+            DHit h;
+            const ae_object *obj = S.objects + slot;
+            bool hit;
+            if (shape == AE_SHAPE_SPHERE) hit = hit_sphere_ref(obj, o, d, time, tn, best.t, h);
+            else if (shape == AE_SHAPE_QUAD) hit = hit_planar_ref(obj, false, o, d, tn, best.t, h);
+            else if (shape == AE_SHAPE_TRIANGLE) hit = hit_planar_ref(obj, true, o, d, tn, best.t, h);
+            else hit = hit_box_ref(obj, o, d, tn, best.t, h);
+            if (hit && takes(best, h.t, orank, 0u, 0u)) {
+                best.t = h.t; best.alpha = h.alpha; best.beta = h.beta;
+                best.object = slot; best.prim = AE_MISS; best.orank = orank; best.lrank = 0;
+            }
+        }
+        if (!pop()) break;
     }
     return best;
 }

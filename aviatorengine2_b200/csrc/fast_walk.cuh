@@ -1,10 +1,11 @@
 // fast_walk.cuh - the optimised closest hit (closest_fast, fast_trace.cuh)
-// re-expressed as a state machine that advances one step per call: one TLAS
-// node, one TLAS-leaf object, or one BLAS node (a leaf's triangles included).
+// re-expressed as a state machine that advances one step per call: one node
+// of the instance-level tree, one object entry, or one BLAS node (a leaf's
+// triangles included).
 //
-// Why: the nested form runs a TLAS loop, a per-object loop and a BLAS loop
-// inside one another, and the lanes of a warp wait at the end of each inner
-// loop for the slowest lane.  On incoherent rays (bounces, shadow samples)
+// Why: the nested form runs an instance-tree loop and a BLAS loop inside one
+// another, and the lanes of a warp wait at the end of each inner loop for the
+// slowest lane.  On incoherent rays (bounces, shadow samples)
 // only a few lanes were active per instruction.  A kernel built on Walker
 // keeps every lane stepping its own ray and lets a lane that finishes start
 // its next ray at once, so warps stay full.
@@ -27,28 +28,26 @@ enum : uint32_t { kWalkTlas = 0, kWalkObject = 1, kWalkBlas = 2, kWalkDone = 3 }
 // wavefront frame 177 ms against 192 ms and 179 ms.
 constexpr int kWalkBlocksPerSm = 7;
 
-// The walk's per-thread local stacks: the TLAS stack and the BLAS entries
-// beyond the shared-memory part.  Kept out of Walker so its scalar state can
-// live in registers.
+// The walk's per-thread local stacks: the instance-tree stack and the BLAS
+// entries beyond the shared-memory part.  Kept out of Walker so its scalar
+// state can live in registers.
 template <int SS = kSharedStack>
 struct WalkStacks {
-    int tstack[kTlasStack];
-    float tdist[kTlasStack];
+    uint32_t tstack[kTlas4Stack];
+    float tdist[kTlas4Stack];
     uint2 spill[kFastStack - SS];
 };
 
 template <bool WT, int SS = kSharedStack>
 struct Walker {
     // ray
-    f3 o, d, tinv, rinv;
+    f3 o, d, tinv;
     float tn, time;
     Best best;
     uint32_t phase;
-    // TLAS
-    uint32_t tnode;
+    // instance tree: the current node, or the leaf (object) being entered
+    uint32_t tcur;
     int tsp;
-    // objects of the current TLAS leaf
-    uint32_t ofirst, ocount, ok;
     // current mesh instance
     f3 lo, ld, linv;
     WtRay W;
@@ -59,7 +58,7 @@ struct Walker {
     // tmax below kFarStart starts the walk as if a hit at tmax were already
     // found: every hit nearer than tmax is still found, with the same tie
     // ranking, and nothing at or beyond it is reported as nearer.
-    AE_DEV void start(const DevScene &S, f3 o_, f3 d_, float tn_, float time_, float tmax = kFarStart) {
+    AE_DEV void start(const FastView &V, f3 o_, f3 d_, float tn_, float time_, float tmax = kFarStart) {
         o = o_;
         d = d_;
         tn = tn_;
@@ -67,24 +66,18 @@ struct Walker {
         best.t = tmax; best.alpha = 0.0f; best.beta = 0.0f;
         best.object = AE_MISS; best.prim = AE_MISS; best.orank = 0; best.lrank = 0;
         tsp = 0;
-        phase = kWalkDone;
-        if (S.n_nodes == 0) return;
         tinv = mk(slab_inv(d.x), slab_inv(d.y), slab_inv(d.z));
-        rinv = 1.0f / d;
-        const NodeBox nb = load_node(S.tlas, 0);
-        if (slab_ref(o, rinv, nb.lo, nb.hi, tn, kFarStart)) {
-            tnode = 0;
-            phase = kWalkTlas;
-        }
+        tcur = V.troot;
+        phase = (tcur & kLeafBit) ? (leaf_count(tcur) ? kWalkObject : kWalkDone) : kWalkTlas;
     }
 
-    // Next TLAS stack entry no farther than the best hit, or done.
+    // Next instance-tree stack entry no farther than the best hit, or done.
     AE_DEV void tlas_pop(const WalkStacks<SS> &K) {
         while (tsp > 0) {
             tsp--;
             if (K.tdist[tsp] <= best.t) {
-                tnode = uint32_t(K.tstack[tsp]);
-                phase = kWalkTlas;
+                tcur = K.tstack[tsp];
+                phase = (tcur & kLeafBit) ? kWalkObject : kWalkTlas;
                 return;
             }
         }
@@ -92,7 +85,7 @@ struct Walker {
     }
 
     // Next BLAS stack entry no farther than the best hit, or back to the
-    // leaf's remaining objects.
+    // instance tree.
     AE_DEV void blas_pop(const WalkStacks<SS> &K, const uint2 *stk, int tid, int nt) {
         while (bsp > 0) {
             bsp--;
@@ -102,11 +95,11 @@ struct Walker {
                 return;
             }
         }
-        phase = kWalkObject;
+        tlas_pop(K);
     }
 
-    // The walk's phase group for warp-level step scheduling: 0 TLAS node,
-    // 1 object of a TLAS leaf, 2 BLAS interior node, 3 BLAS leaf.
+    // The walk's phase group for warp-level step scheduling: 0 instance-tree
+    // node, 1 object entry, 2 BLAS interior node, 3 BLAS leaf.
     AE_DEV uint32_t group() const {
         return phase == kWalkBlas ? ((cur & kLeafBit) ? 3u : 2u) : (phase == kWalkTlas ? 0u : 1u);
     }
@@ -135,16 +128,7 @@ struct Walker {
                 float tm[4];
                 uint32_t ch[4];
                 child_hits(V.nodes + cur, lo, linv, tn, best.t, tm, ch);
-#define AE_SWAP(i, j)                                            \
-    if (tm[j] < tm[i]) {                                         \
-        const float tt = tm[i]; tm[i] = tm[j]; tm[j] = tt;       \
-        const uint32_t cc = ch[i]; ch[i] = ch[j]; ch[j] = cc;    \
-    }
-                AE_SWAP(0, 1) AE_SWAP(2, 3) AE_SWAP(0, 2) AE_SWAP(1, 3) AE_SWAP(1, 2)
-#undef AE_SWAP
-                int nh = 0;
-#pragma unroll
-                for (int k = 0; k < 4; k++) nh += tm[k] != __int_as_float(0x7f800000) ? 1 : 0;
+                const int nh = sort_hits(tm, ch);
                 if (nh > 0) {
                     for (int k = nh - 1; k >= 1; k--) {
                         if (bsp < SS) stk[bsp * nt + tid] = make_uint2(ch[k], __float_as_uint(tm[k]));
@@ -156,17 +140,12 @@ struct Walker {
                     blas_pop(K, stk, tid, nt);
                 }
             }
-            return false;
+            return phase == kWalkDone;
         }
         if (phase == kWalkObject) {
-            if (ok >= ocount) {
-                tlas_pop(K);
-                return phase == kWalkDone;
-            }
-            slot = ofirst + ok;
-            ok++;
-            orank = (uint64_t(~ofirst) << 32) | slot;
+            slot = leaf_first(tcur);
             const uint4 m = __ldg(V.meta + slot);
+            orank = object_rank(m, slot);
             const uint32_t shape = m.x & 0xff;
             if (shape == AE_SHAPE_MESH) {
                 // ToLocal (hybrid:534-543), as trace_mesh.
@@ -185,52 +164,39 @@ struct Walker {
                 cur = __float_as_uint(c.x);
                 bsp = 0;
                 phase = kWalkBlas;
-            } else {
-                DHit h;
-                const ae_object *obj = S.objects + slot;
-                bool hit;
-                if (shape == AE_SHAPE_SPHERE) hit = hit_sphere_ref(obj, o, d, time, tn, best.t, h);
-                else if (shape == AE_SHAPE_QUAD) hit = hit_planar_ref(obj, false, o, d, tn, best.t, h);
-                else if (shape == AE_SHAPE_TRIANGLE) hit = hit_planar_ref(obj, true, o, d, tn, best.t, h);
-                else hit = hit_box_ref(obj, o, d, tn, best.t, h);
-                if (hit && takes(best, h.t, orank, 0u, 0u)) {
-                    best.t = h.t; best.alpha = h.alpha; best.beta = h.beta;
-                    best.object = slot; best.prim = AE_MISS; best.orank = orank; best.lrank = 0;
-                }
+                return false;
             }
-            return false;
+            DHit h;
+            const ae_object *obj = S.objects + slot;
+            bool hit;
+            if (shape == AE_SHAPE_SPHERE) hit = hit_sphere_ref(obj, o, d, time, tn, best.t, h);
+            else if (shape == AE_SHAPE_QUAD) hit = hit_planar_ref(obj, false, o, d, tn, best.t, h);
+            else if (shape == AE_SHAPE_TRIANGLE) hit = hit_planar_ref(obj, true, o, d, tn, best.t, h);
+            else hit = hit_box_ref(obj, o, d, tn, best.t, h);
+            if (hit && takes(best, h.t, orank, 0u, 0u)) {
+                best.t = h.t; best.alpha = h.alpha; best.beta = h.beta;
+                best.object = slot; best.prim = AE_MISS; best.orank = orank; best.lrank = 0;
+            }
+            tlas_pop(K);
+            return phase == kWalkDone;
         }
         if (phase == kWalkTlas) {
-            const NodeBox nb = load_node(S.tlas, tnode);
-            if (nb.count > 0) {
-                ofirst = uint32_t(nb.left);
-                ocount = uint32_t(nb.count);
-                ok = 0;
-                phase = kWalkObject;
-                return false;
-            }
-            const NodeBox L = load_node(S.tlas, uint32_t(nb.left)), R = load_node(S.tlas, uint32_t(nb.right));
-            const f3 lt0 = (L.lo - o) * tinv, lt1 = (L.hi - o) * tinv;
-            const f3 rt0 = (R.lo - o) * tinv, rt1 = (R.hi - o) * tinv;
-            const float lmin = fmaxf(fmaxf(fminf(lt0.x, lt1.x), fminf(lt0.y, lt1.y)), fmaxf(fminf(lt0.z, lt1.z), tn));
-            const float lmax = fminf(fminf(fmaxf(lt0.x, lt1.x), fmaxf(lt0.y, lt1.y)), fmaxf(lt0.z, lt1.z));
-            const float rmin = fmaxf(fmaxf(fminf(rt0.x, rt1.x), fminf(rt0.y, rt1.y)), fmaxf(fminf(rt0.z, rt1.z), tn));
-            const float rmax = fminf(fminf(fmaxf(rt0.x, rt1.x), fmaxf(rt0.y, rt1.y)), fmaxf(rt0.z, rt1.z));
-            const float lmin_c = lmin * kEntryShrink, rmin_c = rmin * kEntryShrink;
-            const bool lh = lmin_c <= fminf(lmax * kExitGrow, best.t);
-            const bool rh = rmin_c <= fminf(rmax * kExitGrow, best.t);
-            if (lh && rh) {
-                const bool lfirst = lmin <= rmin;
-                if (tsp < kTlasStack) {
-                    K.tstack[tsp] = lfirst ? nb.right : nb.left;
-                    K.tdist[tsp] = lfirst ? rmin_c : lmin_c;
-                    tsp++;
+            float tm[4];
+            uint32_t ch[4];
+            child_hits(V.tnodes + tcur, o, tinv, tn, best.t, tm, ch);
+            const int nh = sort_hits(tm, ch);
+            if (nh > 0) {
+                for (int k = nh - 1; k >= 1; k--) {
+                    if (tsp < kTlas4Stack) {
+                        K.tstack[tsp] = ch[k];
+                        K.tdist[tsp] = tm[k];
+                        tsp++;
+                    }
                 }
-                tnode = uint32_t(lfirst ? nb.left : nb.right);
+                tcur = ch[0];
+                phase = (tcur & kLeafBit) ? kWalkObject : kWalkTlas;
                 return false;
             }
-            if (lh) { tnode = uint32_t(nb.left); return false; }
-            if (rh) { tnode = uint32_t(nb.right); return false; }
             tlas_pop(K);
             return phase == kWalkDone;
         }

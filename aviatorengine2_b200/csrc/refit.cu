@@ -126,10 +126,10 @@ __global__ void k_refit_level(ae_bvh_node *nodes, float *raw, const float *obj_b
 
 using namespace ae;
 
-namespace {
-// World box of a non-mesh object as ae_pack_scene computed it: recover it
-// from the uploaded TLAS leaf?  Not recoverable per object, so the refit
-// recomputes analytic boxes from the object record with the host formulas.
+namespace ae {
+// World box of a non-mesh object as ae_pack_scene computed it.  The packed
+// TLAS holds only the union per leaf, so the box is recomputed from the
+// object record with the host formulas.
 ae_aabb analytic_box(const ae_object &o) {
     ae_entity e;
     std::memset(&e, 0, sizeof(e));
@@ -151,7 +151,7 @@ ae_aabb analytic_box(const ae_object &o) {
     ae_entity_bounds(&e, nullptr, &b);
     return b;
 }
-}  // namespace
+}  // namespace ae
 
 extern "C" int ae_refit_instances(ae_ctx *ctx, const ae_instance *instances, uint32_t n) {
     Ctx *c = reinterpret_cast<Ctx *>(ctx);

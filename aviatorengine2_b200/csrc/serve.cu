@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_sv_extend_walk(SvView
     if (active) {
         const ae_ray r = W.qray[q][k];
         R = W.scenes + W.s_scene[W.qslot[q][k]];
-        w.start(R->S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+        w.start(R->V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
     }
     uint32_t iter = 0;
     for (;;) {
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_sv_extend_walk(SvView
         if (active) {
             const ae_ray r = W.qray[q][k];
             R = W.scenes + W.s_scene[W.qslot[q][k]];
-            w.start(R->S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+            w.start(R->V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
         }
     }
 }
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_s
         R = W.scenes + W.s_scene[e / W.max_lights];
         const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
         so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
-        w.start(R->S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
+        w.start(R->V, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
     }
     uint32_t iter = 0;
     for (;;) {
@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_s
         if (verdict == 2) {
             so = (so + sd * b.t) + sd * 0.001f;
             if (++step < 4) {
-                w.start(R->S, so, sd, 0.001f, w.time, AE_SUB(distance(lp, so), 0.001f));
+                w.start(R->V, so, sd, 0.001f, w.time, AE_SUB(distance(lp, so), 0.001f));
                 continue;
             }
             verdict = 0;
@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_s
             const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
             so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
             step = 0;
-            w.start(R->S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
+            w.start(R->V, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
         }
     }
 }
@@ -517,6 +517,7 @@ struct FrameSet {
     DevBuf<ae_bvh_node> tlas;
     DevBuf<ae_instance> instances;
     DevBuf<FastInst> inst;
+    DevBuf<QNode> tnodes;  // the optimised walks' instance-level tree
 };
 constexpr uint32_t kFrameSets = AE_SERVE_FRAME_SETS;
 
@@ -746,7 +747,9 @@ int Server::fill_frame_set(uint32_t scene, uint32_t copy) {
     FastScene &F = *c->fast;
     const size_t no = std::max<size_t>(c->n_objects, 1), nn = std::max<size_t>(c->n_nodes, 1),
                  ni = std::max<size_t>(c->n_instances, 1);
-    if (fs.objects.reserve(no) || fs.tlas.reserve(nn) || fs.instances.reserve(ni) || fs.inst.reserve(ni))
+    const size_t nt = std::max<size_t>(F.n_tnodes, 1);
+    if (fs.objects.reserve(no) || fs.tlas.reserve(nn) || fs.instances.reserve(ni) || fs.inst.reserve(ni) ||
+        fs.tnodes.reserve(nt))
         return AE_ERR_OOM;
     cudaStream_t cs = c->stream;
     cudaError_t e = cudaSuccess;
@@ -759,6 +762,8 @@ int Server::fill_frame_set(uint32_t scene, uint32_t copy) {
                             cudaMemcpyDeviceToDevice, cs);
     if (e == cudaSuccess && c->n_instances)
         e = cudaMemcpyAsync(fs.inst.ptr, F.inst.ptr, c->n_instances * sizeof(FastInst), cudaMemcpyDeviceToDevice, cs);
+    if (e == cudaSuccess && F.n_tnodes)
+        e = cudaMemcpyAsync(fs.tnodes.ptr, F.tnodes.ptr, F.n_tnodes * sizeof(QNode), cudaMemcpyDeviceToDevice, cs);
     if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -768,7 +773,7 @@ int Server::fill_frame_set(uint32_t scene, uint32_t copy) {
     S.objects = fs.objects.ptr;
     S.tlas = fs.tlas.ptr;
     S.instances = fs.instances.ptr;
-    const SceneRec rec{S, FastView{F.nodes.ptr, F.tris.ptr, fs.inst.ptr, F.obj_meta.ptr}};
+    const SceneRec rec{S, fast_view(F, fs.inst.ptr, fs.tnodes.ptr)};
     // Stream order puts the row before any replay that reads it.
     if (cudaMemcpyAsync(scenes_d.ptr + size_t(scene) * kFrameSets + copy, &rec, sizeof(rec), cudaMemcpyHostToDevice,
                         stream) != cudaSuccess) {

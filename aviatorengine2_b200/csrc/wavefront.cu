@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_wf_extend_walk(DevSce
     bool active = k < count;
     if (active) {
         const ae_ray r = W.qray[q][k];
-        w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+        w.start(V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
     }
     uint32_t iter = 0;
     for (;;) {
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_wf_extend_walk(DevSce
         active = k < count;
         if (active) {
             const ae_ray r = W.qray[q][k];
-            w.start(S, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+            w.start(V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
         }
     }
 }
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_w
         e = W.sq[k];
         const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
         so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
-        w.start(S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
+        w.start(V, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
     }
     uint32_t iter = 0;
     for (;;) {
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_w
         if (verdict == 2) {
             so = (so + sd * b.t) + sd * 0.001f;
             if (++step < 4) {
-                w.start(S, so, sd, 0.001f, w.time, AE_SUB(distance(lp, so), 0.001f));
+                w.start(V, so, sd, 0.001f, w.time, AE_SUB(distance(lp, so), 0.001f));
                 continue;
             }
             verdict = 0;
@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_w
             const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
             so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
             step = 0;
-            w.start(S, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
+            w.start(V, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
         }
     }
 }
@@ -526,7 +526,7 @@ static int record_sample(Ctx *c, cudaStream_t st, int cfg_index, const Grids &G,
     const WfView W = view_of(c);
     const DevScene S = c->scene();
     FastScene &F = *c->fast;
-    const FastView V{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr};
+    const FastView V = fast_view(F);
     const ExtendCfg &e = kExtendCfgs[prec][cfg_index];
     const int grid256 = G.grid256, egrid = G.egrid, shgrid = G.shgrid;
     const size_t esmem = G.esmem, shsmem = G.shsmem;
@@ -561,7 +561,7 @@ static int autotune(Ctx *c) {
     const WfView W = view_of(c);
     const DevScene S = c->scene();
     FastScene &F = *c->fast;
-    const FastView V{F.nodes.ptr, F.tris.ptr, F.inst.ptr, F.obj_meta.ptr};
+    const FastView V = fast_view(F);
     int best = 4;
     float best_ms = 1e30f;
     for (int k = 0; k < 9; k++) {
