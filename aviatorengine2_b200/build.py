@@ -9,6 +9,7 @@ import hashlib
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -47,21 +48,20 @@ def build(force=False, verbose=False):
     if not force and os.path.exists(OUT) and os.path.exists(stamp) and open(stamp).read() == digest:
         return OUT
     os.makedirs(BUILD, exist_ok=True)
-    objs = []
-    for f in cu:
-        o = os.path.join(BUILD, f + ".o")
-        cmd = [NVCC] + NVFLAGS + ["-c", os.path.join(CSRC, f), "-o", o]
+    jobs = [([NVCC] + NVFLAGS + ["-c", os.path.join(CSRC, f), "-o", os.path.join(BUILD, f + ".o")]) for f in cu]
+    jobs += [(["g++"] + CXXFLAGS + ["-c", os.path.join(CSRC, f), "-o", os.path.join(BUILD, f + ".o")]) for f in cpp]
+    objs = [cmd[-1] for cmd in jobs]
+
+    def run(cmd):
         if verbose:
             print(" ".join(cmd))
         subprocess.check_call(cmd)
-        objs.append(o)
-    for f in cpp:
-        o = os.path.join(BUILD, f + ".o")
-        cmd = ["g++"] + CXXFLAGS + ["-c", os.path.join(CSRC, f), "-o", o]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.check_call(cmd)
-        objs.append(o)
+
+    # One compiler process per source file, as many at a time as there are
+    # cores; the first failure is raised.
+    with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as pool:
+        for fut in [pool.submit(run, cmd) for cmd in jobs]:
+            fut.result()
     tmp = OUT + ".tmp"
     cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-cudart=static", "-lpthread"]
     subprocess.check_call(cmd)

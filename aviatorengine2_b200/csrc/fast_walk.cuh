@@ -19,6 +19,8 @@
 namespace ae {
 
 enum : uint32_t { kWalkTlas = 0, kWalkObject = 1, kWalkBlas = 2, kWalkDone = 3 };
+// Phase groups of Walker::group().
+constexpr uint32_t kWalkGroups = 3;
 
 // Minimum resident 128-thread blocks per SM asked of the compiler for every
 // kernel built on Walker (extend and shadow, wavefront and serving): caps them
@@ -98,48 +100,32 @@ struct Walker {
         tlas_pop(K);
     }
 
-    // The walk's phase group for warp-level step scheduling: 0 instance-tree
-    // node, 1 object entry, 2 BLAS interior node, 3 BLAS leaf.
+    // The walk's phase group for warp-level step scheduling: 0 interior node
+    // of either tree (the instance-level tree and the BLAS share the 4-wide
+    // node format and its child test), 1 object entry, 2 BLAS leaf.
     AE_DEV uint32_t group() const {
-        return phase == kWalkBlas ? ((cur & kLeafBit) ? 3u : 2u) : (phase == kWalkTlas ? 0u : 1u);
+        return phase == kWalkObject ? 1u : ((phase == kWalkBlas && (cur & kLeafBit)) ? 2u : 0u);
     }
 
     // One step; returns true once the ray is finished (best is final).
     AE_DEV bool step(const DevScene &S, const FastView &V, WalkStacks<SS> &K, uint2 *stk, int tid, int nt) {
-        if (phase == kWalkBlas) {
-            if (cur & kLeafBit) {
-                const uint32_t first = leaf_first(cur), cnt = leaf_count(cur);
-                const float4 *tris = V.tris + size_t(tri_base) * 3;
-                for (uint32_t k = 0; k < cnt; k++) {
-                    const uint32_t s = first + k;
-                    const float4 *r = tris + size_t(s) * 3;
-                    const float4 r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2);
-                    float t, a, b;
-                    const bool h = WT ? tri_test_wt(lo, W, tn, best.t, r0, r1, r2, t, a, b)
-                                      : tri_test_ref(lo, ld, tn, best.t, r0, r1, r2, t, a, b);
-                    if (h && takes(best, t, orank, ~first, s)) {
-                        best.t = t; best.alpha = a; best.beta = b;
-                        best.object = slot; best.prim = s;
-                        best.orank = orank; best.lrank = ~first;
-                    }
-                }
-                blas_pop(K, stk, tid, nt);
-            } else {
-                float tm[4];
-                uint32_t ch[4];
-                child_hits(V.nodes + cur, lo, linv, tn, best.t, tm, ch);
-                const int nh = sort_hits(tm, ch);
-                if (nh > 0) {
-                    for (int k = nh - 1; k >= 1; k--) {
-                        if (bsp < SS) stk[bsp * nt + tid] = make_uint2(ch[k], __float_as_uint(tm[k]));
-                        else if (bsp < kFastStack) K.spill[bsp - SS] = make_uint2(ch[k], __float_as_uint(tm[k]));
-                        bsp = bsp < kFastStack ? bsp + 1 : bsp;
-                    }
-                    cur = ch[0];
-                } else {
-                    blas_pop(K, stk, tid, nt);
+        if (phase == kWalkBlas && (cur & kLeafBit)) {
+            const uint32_t first = leaf_first(cur), cnt = leaf_count(cur);
+            const float4 *tris = V.tris + size_t(tri_base) * 3;
+            for (uint32_t k = 0; k < cnt; k++) {
+                const uint32_t s = first + k;
+                const float4 *r = tris + size_t(s) * 3;
+                const float4 r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2);
+                float t, a, b;
+                const bool h = WT ? tri_test_wt(lo, W, tn, best.t, r0, r1, r2, t, a, b)
+                                  : tri_test_ref(lo, ld, tn, best.t, r0, r1, r2, t, a, b);
+                if (h && takes(best, t, orank, ~first, s)) {
+                    best.t = t; best.alpha = a; best.beta = b;
+                    best.object = slot; best.prim = s;
+                    best.orank = orank; best.lrank = ~first;
                 }
             }
+            blas_pop(K, stk, tid, nt);
             return phase == kWalkDone;
         }
         if (phase == kWalkObject) {
@@ -180,12 +166,17 @@ struct Walker {
             tlas_pop(K);
             return phase == kWalkDone;
         }
-        if (phase == kWalkTlas) {
-            float tm[4];
-            uint32_t ch[4];
-            child_hits(V.tnodes + tcur, o, tinv, tn, best.t, tm, ch);
-            const int nh = sort_hits(tm, ch);
-            if (nh > 0) {
+        if (phase == kWalkDone) return true;
+        // An interior node of the instance-level tree (world ray) or of the
+        // current mesh's BLAS (local ray): one code path for both, so the
+        // lanes of a warp at either level step together.
+        const bool top = phase == kWalkTlas;
+        float tm[4];
+        uint32_t ch[4];
+        child_hits(top ? V.tnodes + tcur : V.nodes + cur, top ? o : lo, top ? tinv : linv, tn, best.t, tm, ch);
+        const int nh = sort_hits(tm, ch);
+        if (nh > 0) {
+            if (top) {
                 for (int k = nh - 1; k >= 1; k--) {
                     if (tsp < kTlas4Stack) {
                         K.tstack[tsp] = ch[k];
@@ -195,12 +186,19 @@ struct Walker {
                 }
                 tcur = ch[0];
                 phase = (tcur & kLeafBit) ? kWalkObject : kWalkTlas;
-                return false;
+            } else {
+                for (int k = nh - 1; k >= 1; k--) {
+                    if (bsp < SS) stk[bsp * nt + tid] = make_uint2(ch[k], __float_as_uint(tm[k]));
+                    else if (bsp < kFastStack) K.spill[bsp - SS] = make_uint2(ch[k], __float_as_uint(tm[k]));
+                    bsp = bsp < kFastStack ? bsp + 1 : bsp;
+                }
+                cur = ch[0];
             }
-            tlas_pop(K);
-            return phase == kWalkDone;
+            return false;
         }
-        return true;
+        if (top) tlas_pop(K);
+        else blas_pop(K, stk, tid, nt);
+        return phase == kWalkDone;
     }
 };
 
@@ -212,7 +210,7 @@ struct Walker {
 // Scheduling only: each lane's own sequence of steps, and so its result, is
 // unchanged.
 AE_DEV uint32_t warp_pick_group(uint32_t group, bool active, uint32_t &iter) {
-    const uint32_t g = active ? group : 4u;
+    const uint32_t g = active ? group : kWalkGroups;
     uint32_t pick;
     if ((iter & 3u) == 3u) {
         const uint32_t am = __ballot_sync(0xffffffffu, active);
@@ -223,7 +221,7 @@ AE_DEV uint32_t warp_pick_group(uint32_t group, bool active, uint32_t &iter) {
     } else {
         uint32_t best = 0, bc = 0;
 #pragma unroll
-        for (uint32_t k = 0; k < 4; k++) {
+        for (uint32_t k = 0; k < kWalkGroups; k++) {
             const uint32_t c = uint32_t(__popc(__ballot_sync(0xffffffffu, g == k)));
             if (c > bc) { bc = c; best = k; }
         }
