@@ -19,8 +19,6 @@
 namespace ae {
 
 enum : uint32_t { kWalkTlas = 0, kWalkObject = 1, kWalkBlas = 2, kWalkDone = 3 };
-// Phase groups of Walker::group().
-constexpr uint32_t kWalkGroups = 3;
 
 // Minimum resident 128-thread blocks per SM asked of the compiler for every
 // kernel built on Walker (extend and shadow, wavefront and serving): caps them
@@ -205,27 +203,25 @@ struct Walker {
 // Which phase group a warp steps this iteration: the largest group among its
 // active lanes, so the lanes that step run the same code; every fourth
 // iteration the group of the next active lane at or after a rotating
-// position, so every lane steps at least once every 128 iterations.  `group`
-// of an inactive lane is ignored.  All 32 lanes must call this together.
-// Scheduling only: each lane's own sequence of steps, and so its result, is
-// unchanged.
-AE_DEV uint32_t warp_pick_group(uint32_t group, bool active, uint32_t &iter) {
-    const uint32_t g = active ? group : kWalkGroups;
+// position, so every lane steps at least once every 128 iterations.  `am` is
+// the warp's ballot of `active`; `group` of an inactive lane is ignored.  All
+// 32 lanes must call this together.  Scheduling only: each lane's own
+// sequence of steps, and so its result, is unchanged.
+AE_DEV uint32_t warp_pick_group(uint32_t group, bool active, uint32_t am, uint32_t &iter) {
     uint32_t pick;
     if ((iter & 3u) == 3u) {
-        const uint32_t am = __ballot_sync(0xffffffffu, active);
         const uint32_t r = (iter >> 2) & 31u;
         const uint32_t rot = (am >> r) | (r ? (am << (32u - r)) : 0u);
         const uint32_t src = (r + uint32_t(__ffs(rot)) - 1u) & 31u;
-        pick = __shfl_sync(0xffffffffu, g, int(src));
+        pick = __shfl_sync(0xffffffffu, group, int(src));
     } else {
-        uint32_t best = 0, bc = 0;
-#pragma unroll
-        for (uint32_t k = 0; k < kWalkGroups; k++) {
-            const uint32_t c = uint32_t(__popc(__ballot_sync(0xffffffffu, g == k)));
-            if (c > bc) { bc = c; best = k; }
-        }
-        pick = best;
+        // Lane counts of groups 0 and 1 by ballot, group 2 by difference;
+        // ties go to the lower group.
+        const uint32_t c0 = uint32_t(__popc(__ballot_sync(0xffffffffu, active && group == 0u)));
+        const uint32_t c1 = uint32_t(__popc(__ballot_sync(0xffffffffu, active && group == 1u)));
+        const uint32_t c2 = uint32_t(__popc(am)) - c0 - c1;
+        pick = c1 > c0 ? 1u : 0u;
+        if (c2 > max(c0, c1)) pick = 2u;
     }
     iter++;
     return pick;

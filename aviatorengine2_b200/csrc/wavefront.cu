@@ -225,9 +225,10 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_wf_extend_walk(DevSce
     }
     uint32_t iter = 0;
     for (;;) {
-        if (!__any_sync(0xffffffffu, active)) break;
+        const uint32_t am = __ballot_sync(0xffffffffu, active);
+        if (!am) break;
         // Only the warp's largest phase group steps (warp_pick_group).
-        const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, iter);
+        const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, am, iter);
         if (!active || w.group() != pick || !w.step(S, V, K, stk, threadIdx.x, blockDim.x)) continue;
         const Best &b = w.best;
         const bool any = b.object != AE_MISS;
@@ -309,9 +310,10 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_w
     }
     uint32_t iter = 0;
     for (;;) {
-        if (!__any_sync(0xffffffffu, active)) break;
+        const uint32_t am = __ballot_sync(0xffffffffu, active);
+        if (!am) break;
         // Only the warp's largest phase group steps (warp_pick_group).
-        const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, iter);
+        const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, am, iter);
         if (!active || w.group() != pick || !w.step(S, V, K, stk, threadIdx.x, THREADS)) continue;
         const Best &b = w.best;
         int verdict = 0;  // 0 unoccluded, 1 occluded, 2 through glass
