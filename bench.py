@@ -362,6 +362,7 @@ def measure_paths(local, width, height, frames=2, mre_pixels=1024, mre_frames=16
                 mre[name] = ctx.image_error_pixels(px, ref64, eps=MRE_EPS)["mre"]
         info = ctx.wavefront_info()
         out["wavefront_extend"] = {"threads": info["threads"], "stack": info["stack"]}
+        out["walker_runs"] = {"wavefront": ctx.wavefront_walk_info(False), "precision": ctx.wavefront_walk_info(True)}
     out["speedup"] = out["wavefront_mpaths"] / out["plain_mpaths"]
     out["precision_speedup"] = out["precision_mpaths"] / out["plain_mpaths"]
     peak, peak_kind = load_peaks()
@@ -630,7 +631,7 @@ def measure_serving(local, n_requests=48, rate=0.5, seed=7, claim_policy=1, fram
     4096 instances (512 per scene) take a random-walk step, submitted to the
     server as one move per scene (a GPU TLAS refit when applied; moves that
     no request renders are coalesced).  Latency = submit to images in host
-    memory."""
+    memory; frame latency = a request's latency over its progressive frames."""
     from aviatorengine2_b200 import Context, Server, scenes
     rng = np.random.default_rng(seed)
     t0 = time.perf_counter()
@@ -684,10 +685,11 @@ def measure_serving(local, n_requests=48, rate=0.5, seed=7, claim_policy=1, fram
             c = S[sc].config.copy()
             c["samples"], c["batches"] = 1, 1
             rids.append(srv.submit(ids[sc], w, h, spp, c))
-        lat = []
-        for r in rids:
+        lat, per_frame = [], []
+        for r, (_, _, spp) in zip(rids, plan):
             res, _, _ = srv.wait(r, 1800000)
             lat.append(res["done_ms"] - res["submit_ms"])
+            per_frame.append(lat[-1] / spp)
         stop.set()
         if th:
             th.join()
@@ -701,6 +703,8 @@ def measure_serving(local, n_requests=48, rate=0.5, seed=7, claim_policy=1, fram
                         " tris, 512 instances each (4096 in all) moving every frame; Poisson arrivals",
             "requests": n_requests, "rate_per_s": rate, "claim_policy": "shared" if claim_policy else "oldest_first",
             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
+            # per progressive frame: a request's latency over its frame count
+            "frame_p50_ms": float(np.percentile(per_frame, 50)), "frame_p99_ms": float(np.percentile(per_frame, 99)),
             "mpaths": st["paths"] / wall / 1e6, "mrays": st["rays"] / wall / 1e6, "paths": int(st["paths"]),
             "wall_s": wall, "frame_hz": frame_hz, "world_frames": int(moved["frames"]),
             "moves_submitted": int(moved["moves"]), "moves_applied": int(st["moves_applied"]),
@@ -957,7 +961,7 @@ def main():
                 "note": "algorithmic bytes = reference-walk touches (48 B node, 128 B object, 48 B instance, "
                         "48 B triangle, 60 B winner) counted on the device over each launch's ray set; achieved = "
                         "those bytes / that launch's CUDA-event time; the working set is mostly L2-resident, so "
-                        "DRAM traffic is far below the algorithmic bytes (l2_throughput_pct_of_peak: ncu, 960x540)"}
+                        "DRAM traffic is far below the algorithmic bytes (l2_throughput_pct_of_peak: the committed ncu summary, its case named)"}
 
     cpu = None
     if rank == 0 and not args.no_cpu:
