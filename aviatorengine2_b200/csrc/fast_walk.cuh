@@ -200,6 +200,42 @@ struct Walker {
     }
 };
 
+// Run assignment for a persistent walker grid: the lanes of a warp that need
+// work (need) take the next indices of the warp's current run of `run`
+// consecutive queue entries, in lane order, and the warp claims a new run from
+// `counter` when its run is used up, so the entries a warp has in flight stay
+// neighbours in the queue.  cbase, cend and exhausted are the same in every
+// lane.  Returns true in the lanes that got an index (k).  All 32 lanes must
+// call this together.
+AE_DEV bool run_take(uint32_t *counter, uint32_t n, uint32_t run, bool &need, uint32_t &k, uint32_t &cbase,
+                     uint32_t &cend, bool &exhausted) {
+    const uint32_t lane = threadIdx.x & 31u, below = (1u << lane) - 1u;
+    bool got = false;
+    uint32_t m = __ballot_sync(0xffffffffu, need);
+    while (m && !exhausted) {
+        if (cbase >= cend) {
+            uint32_t b = 0;
+            if (lane == 0) b = atomicAdd(counter, run);
+            b = __shfl_sync(0xffffffffu, b, 0);
+            if (b >= n) {
+                exhausted = true;
+                break;
+            }
+            cbase = b;
+            cend = min(b + run, n);
+        }
+        const uint32_t take = min(cend - cbase, uint32_t(__popc(m)));
+        if (need && uint32_t(__popc(m & below)) < take) {
+            k = cbase + uint32_t(__popc(m & below));
+            need = false;
+            got = true;
+        }
+        cbase += take;
+        m = __ballot_sync(0xffffffffu, need);
+    }
+    return got;
+}
+
 // Which phase group a warp steps this iteration: the largest group among its
 // active lanes, so the lanes that step run the same code; every fourth
 // iteration the group of the next active lane at or after a rotating

@@ -97,6 +97,11 @@ struct Wavefront {
     int ext_threads = 128, ext_stack = 24;
     bool tuned = false;
     float tune_ms[9] = {0};
+    // autotuned queue assignment of the walker stages, per form (index:
+    // precision form), as a run length (0: static assignment)
+    uint32_t walk_run[2] = {0, 0}, shadow_run[2] = {0, 0};
+    bool walk_tuned[2] = {false, false};
+    float walk_tune_ms[2][8] = {};  // shadow stage for kRunCfgs, then the bounce extend
     ~Wavefront() {
         if (graph) cudaGraphExecDestroy(graph);
         if (host_params) cudaFreeHost(host_params);
@@ -207,10 +212,14 @@ __global__ void __launch_bounds__(THREADS) k_wf_extend(DevScene S, FastView V, W
 }
 
 // Extend on the step-wise Walker: a persistent grid, each thread stepping
-// its own queued ray and taking the next (k + grid size) when one finishes.
-// For incoherent queues (bounces past the camera rays).
-template <bool WT>
-__global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_wf_extend_walk(DevScene S, FastView V, WfView W, int bounce) {
+// its own queued ray and taking the next one when one finishes - static
+// assignment (DYN false: k + grid size) or runs of `run` consecutive queue
+// entries per warp claimed from the bounce's counter (DYN true); the
+// autotuner picks per scene.  For incoherent queues (bounces past the camera
+// rays).
+template <bool WT, bool DYN>
+__global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_wf_extend_walk(DevScene S, FastView V, WfView W, int bounce,
+                                                                          uint32_t run) {
     extern __shared__ uint2 stk[];
     const int q = bounce & 1;
     const uint32_t count = W.cnt[q];
@@ -218,13 +227,20 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_wf_extend_walk(DevSce
     uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     Walker<WT> w;
     WalkStacks<> K;
-    bool active = k < count;
+    bool active = !DYN && k < count;
+    bool need = DYN, exhausted = false;
+    uint32_t cbase = 0, cend = 0;
     if (active) {
         const ae_ray r = W.qray[q][k];
         w.start(V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
     }
     uint32_t iter = 0;
     for (;;) {
+        if (DYN && run_take(&W.cnt[C_TILE + bounce], count, run, need, k, cbase, cend, exhausted)) {
+            active = true;
+            const ae_ray r = W.qray[q][k];
+            w.start(V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
+        }
         const uint32_t am = __ballot_sync(0xffffffffu, active);
         if (!am) break;
         // Only the warp's largest phase group steps (warp_pick_group).
@@ -239,6 +255,11 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_wf_extend_walk(DevSce
         h.object = b.object;
         h.prim = b.prim;
         W.qhit[k] = h;
+        if (DYN) {
+            active = false;
+            need = true;
+            continue;
+        }
         k += stride;
         active = k < count;
         if (active) {
@@ -290,8 +311,11 @@ __global__ void __launch_bounds__(256) k_wf_shade(DevScene S, FastView V, WfView
 // hit lies before |lp - so| - 0.001 (a hit at or beyond it, or none, leaves
 // the sample unoccluded), so each walk starts with that distance as its
 // bound: the verdict and the glass step are those of the unbounded walk.
-template <int THREADS, bool WT>
-__global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_wf_shadow(DevScene S, FastView V, WfView W) {
+// Entries are taken statically (k + grid size) or, DYN, in runs of `run`
+// consecutive queue entries per warp, as the autotuner picked.
+template <int THREADS, bool WT, bool DYN>
+__global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS)
+    k_wf_shadow(DevScene S, FastView V, WfView W, int bounce, uint32_t run) {
     extern __shared__ uint2 stk[];
     const uint32_t count = W.cnt[C_SH];
     const uint32_t stride = gridDim.x * THREADS;
@@ -301,15 +325,24 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_w
     uint32_t e = 0;
     f3 so, sd, lp;
     int step = 0;
-    bool active = k < count;
-    if (active) {
+    bool active = !DYN && k < count;
+    bool need = DYN, exhausted = false;
+    uint32_t cbase = 0, cend = 0;
+    // Starts sample k of the queue.
+    auto begin = [&]() {
         e = W.sq[k];
         const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
         so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
+        step = 0;
         w.start(V, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
-    }
+    };
+    if (active) begin();
     uint32_t iter = 0;
     for (;;) {
+        if (DYN && run_take(&W.cnt[C_SHTILE + bounce], count, run, need, k, cbase, cend, exhausted)) {
+            active = true;
+            begin();
+        }
         const uint32_t am = __ballot_sync(0xffffffffu, active);
         if (!am) break;
         // Only the warp's largest phase group steps (warp_pick_group).
@@ -330,15 +363,14 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_w
             verdict = 0;
         }
         W.sh.occ[e] = uint8_t(verdict);
+        if (DYN) {
+            active = false;
+            need = true;
+            continue;
+        }
         k += stride;
         active = k < count;
-        if (active) {
-            e = W.sq[k];
-            const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
-            so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
-            step = 0;
-            w.start(V, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
-        }
+        if (active) begin();
     }
 }
 
@@ -508,20 +540,50 @@ static Grids grids_for(Ctx *c, int cfg_index, bool prec) {
     g.egrid = extend_grid(c, e);
     g.esmem = extend_smem(e.threads, e.stack);
     g.shsmem = size_t(kSharedStack) * 128 * sizeof(uint2);
-    const void *shfn = prec ? reinterpret_cast<const void *>(k_wf_shadow<128, true>)
-                            : reinterpret_cast<const void *>(k_wf_shadow<128, false>);
+    const void *shfn = prec ? reinterpret_cast<const void *>(k_wf_shadow<128, true, false>)
+                            : reinterpret_cast<const void *>(k_wf_shadow<128, false, false>);
+    const void *shdyn = prec ? reinterpret_cast<const void *>(k_wf_shadow<128, true, true>)
+                             : reinterpret_cast<const void *>(k_wf_shadow<128, false, true>);
     cudaFuncSetAttribute(shfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(g.shsmem));
+    cudaFuncSetAttribute(shdyn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(g.shsmem));
     int sh_per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh_per_sm, shfn, 128, g.shsmem);
     g.shgrid = std::max(1, sh_per_sm) * Wf.sms;
     // The step-wise extend of the bounce queues (same block and stack shape).
-    const void *wfn = prec ? reinterpret_cast<const void *>(k_wf_extend_walk<true>)
-                           : reinterpret_cast<const void *>(k_wf_extend_walk<false>);
+    const void *wfn = prec ? reinterpret_cast<const void *>(k_wf_extend_walk<true, false>)
+                           : reinterpret_cast<const void *>(k_wf_extend_walk<false, false>);
+    const void *wdyn = prec ? reinterpret_cast<const void *>(k_wf_extend_walk<true, true>)
+                            : reinterpret_cast<const void *>(k_wf_extend_walk<false, true>);
     cudaFuncSetAttribute(wfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(g.shsmem));
+    cudaFuncSetAttribute(wdyn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(g.shsmem));
     int w_per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&w_per_sm, wfn, 128, g.shsmem);
     g.wgrid = std::max(1, w_per_sm) * Wf.sms;
     return g;
+}
+
+// The walker stages with a queue assignment: run 0 static, else runs of
+// `run` entries per warp.
+static void launch_extend_walk(bool prec, uint32_t run, const Grids &G, cudaStream_t st, const DevScene &S,
+                               const FastView &V, const WfView &W, int b) {
+    if (prec) {
+        if (run) k_wf_extend_walk<true, true><<<G.wgrid, 128, G.shsmem, st>>>(S, V, W, b, run);
+        else k_wf_extend_walk<true, false><<<G.wgrid, 128, G.shsmem, st>>>(S, V, W, b, 0u);
+    } else {
+        if (run) k_wf_extend_walk<false, true><<<G.wgrid, 128, G.shsmem, st>>>(S, V, W, b, run);
+        else k_wf_extend_walk<false, false><<<G.wgrid, 128, G.shsmem, st>>>(S, V, W, b, 0u);
+    }
+}
+
+static void launch_shadow(bool prec, uint32_t run, const Grids &G, cudaStream_t st, const DevScene &S,
+                          const FastView &V, const WfView &W, int b) {
+    if (prec) {
+        if (run) k_wf_shadow<128, true, true><<<G.shgrid, 128, G.shsmem, st>>>(S, V, W, b, run);
+        else k_wf_shadow<128, true, false><<<G.shgrid, 128, G.shsmem, st>>>(S, V, W, b, 0u);
+    } else {
+        if (run) k_wf_shadow<128, false, true><<<G.shgrid, 128, G.shsmem, st>>>(S, V, W, b, run);
+        else k_wf_shadow<128, false, false><<<G.shgrid, 128, G.shsmem, st>>>(S, V, W, b, 0u);
+    }
 }
 
 static int record_sample(Ctx *c, cudaStream_t st, int cfg_index, const Grids &G, bool prec) {
@@ -529,9 +591,10 @@ static int record_sample(Ctx *c, cudaStream_t st, int cfg_index, const Grids &G,
     const DevScene S = c->scene();
     FastScene &F = *c->fast;
     const FastView V = fast_view(F);
+    const Wavefront &Wf = *c->wave;
     const ExtendCfg &e = kExtendCfgs[prec][cfg_index];
-    const int grid256 = G.grid256, egrid = G.egrid, shgrid = G.shgrid;
-    const size_t esmem = G.esmem, shsmem = G.shsmem;
+    const int grid256 = G.grid256, egrid = G.egrid;
+    const size_t esmem = G.esmem;
     k_wf_generate<<<grid256, 256, 0, st>>>(W);
     for (uint32_t b = 0; b < c->config.depth; b++) {
         k_wf_reset<<<1, 1, 0, st>>>(W, int(b));
@@ -539,15 +602,10 @@ static int record_sample(Ctx *c, cudaStream_t st, int cfg_index, const Grids &G,
         // queues are not: the step-wise walk keeps warps full (measured 6 %
         // more paths/s on the 10M-triangle scene).
         if (b == 0) e.fn<<<egrid, e.threads, esmem, st>>>(S, V, W, int(b));
-        else if (prec) k_wf_extend_walk<true><<<G.wgrid, 128, shsmem, st>>>(S, V, W, int(b));
-        else k_wf_extend_walk<false><<<G.wgrid, 128, shsmem, st>>>(S, V, W, int(b));
-        if (prec) {
-            k_wf_shade<true><<<grid256, 256, 0, st>>>(S, V, W, int(b));
-            k_wf_shadow<128, true><<<shgrid, 128, shsmem, st>>>(S, V, W);
-        } else {
-            k_wf_shade<false><<<grid256, 256, 0, st>>>(S, V, W, int(b));
-            k_wf_shadow<128, false><<<shgrid, 128, shsmem, st>>>(S, V, W);
-        }
+        else launch_extend_walk(prec, Wf.walk_run[prec], G, st, S, V, W, int(b));
+        if (prec) k_wf_shade<true><<<grid256, 256, 0, st>>>(S, V, W, int(b));
+        else k_wf_shade<false><<<grid256, 256, 0, st>>>(S, V, W, int(b));
+        launch_shadow(prec, Wf.shadow_run[prec], G, st, S, V, W, int(b));
         k_wf_connect<<<grid256, 256, 0, st>>>(W, int(b));
     }
     k_wf_finish<<<grid256, 256, 0, st>>>(W);
@@ -598,6 +656,55 @@ static int best_cfg_index(const Wavefront &Wf) {
     return 4;
 }
 
+// Queue assignments the walker stages are timed with: static, then runs of
+// 32, 64 and 256 queue entries per warp.
+static const uint32_t kRunCfgs[4] = {0, 32, 64, 256};
+
+// Times the shadow stage on sample 0's first shadow queue and the step-wise
+// extend on its second ray queue under every assignment of kRunCfgs, and
+// keeps the fastest of each for this form.  Runs before the first frame of
+// the form; the frame's generate stage then starts every path afresh.
+static int autotune_walkers(Ctx *c, bool prec) {
+    Wavefront &Wf = *c->wave;
+    const WfView W = view_of(c);
+    const DevScene S = c->scene();
+    const FastView V = fast_view(*c->fast);
+    const int ci = best_cfg_index(Wf);
+    const Grids G = grids_for(c, ci, prec);
+    const ExtendCfg &e = kExtendCfgs[prec][ci];
+    cudaStream_t st = c->stream;
+    k_wf_generate<<<G.grid256, 256, 0, st>>>(W);
+    k_wf_reset<<<1, 1, 0, st>>>(W, 0);
+    e.fn<<<G.egrid, e.threads, G.esmem, st>>>(S, V, W, 0);
+    if (prec) k_wf_shade<true><<<G.grid256, 256, 0, st>>>(S, V, W, 0);
+    else k_wf_shade<false><<<G.grid256, 256, 0, st>>>(S, V, W, 0);
+    c->launches += 4;
+    int rc = c->cuda(cudaGetLastError(), "autotune");
+    if (rc) return rc;
+    for (int stage = 0; stage < 2; stage++) {
+        uint32_t *counter = Wf.cnt.ptr + (stage == 0 ? C_SHTILE + 0 : C_TILE + 1);
+        int best = 0;
+        for (int k = 0; k < 4; k++) {
+            float ms = 0.0f;
+            for (int rep = 0; rep < 2; rep++) {
+                if ((rc = c->cuda(cudaMemsetAsync(counter, 0, sizeof(uint32_t), st), "autotune"))) return rc;
+                cudaEventRecord(c->ev0, st);
+                if (stage == 0) launch_shadow(prec, kRunCfgs[k], G, st, S, V, W, 0);
+                else launch_extend_walk(prec, kRunCfgs[k], G, st, S, V, W, 1);
+                cudaEventRecord(c->ev1, st);
+                if ((rc = c->cuda(cudaEventSynchronize(c->ev1), "autotune"))) return rc;
+                if (rep == 1) cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+                c->launches++;
+            }
+            Wf.walk_tune_ms[prec][stage * 4 + k] = ms;
+            if (ms < Wf.walk_tune_ms[prec][stage * 4 + best]) best = k;
+        }
+        (stage == 0 ? Wf.shadow_run : Wf.walk_run)[prec] = kRunCfgs[best];
+    }
+    Wf.walk_tuned[prec] = true;
+    return c->cuda(cudaGetLastError(), "autotune");
+}
+
 int render_wavefront(Ctx *c, bool prec) {
     int rc = ensure_wavefront(c);
     if (rc) return rc;
@@ -623,12 +730,14 @@ int render_wavefront(Ctx *c, bool prec) {
             return rc;
         return c->timed_end();
     }
-    if (!Wf.tuned) {
+    if (!Wf.tuned || !Wf.walk_tuned[prec]) {
+        if ((rc = c->cuda(cudaStreamSynchronize(c->stream), "params"))) return rc;
         *Wf.host_params = hp;
         if ((rc = c->cuda(cudaMemcpyAsync(Wf.params.ptr, Wf.host_params, sizeof(WfParams), cudaMemcpyHostToDevice,
                                           c->stream), "params")))
             return rc;
-        if ((rc = autotune(c))) return rc;
+        if (!Wf.tuned && (rc = autotune(c))) return rc;
+        if (!Wf.walk_tuned[prec] && (rc = autotune_walkers(c, prec))) return rc;
     }
     // One graph per (scene upload, frame shape); frame parameters travel
     // through device memory so the graph is replayed unchanged.
@@ -682,6 +791,37 @@ int render_wavefront(Ctx *c, bool prec) {
 }  // namespace ae
 
 using namespace ae;
+
+extern "C" int ae_wavefront_walk_info(ae_ctx *ctx, int precision, uint32_t *shadow_run, uint32_t *extend_run,
+                                      float *tune_ms8) {
+    Ctx *c = reinterpret_cast<Ctx *>(ctx);
+    if (!c) return AE_ERR_INVALID;
+    const int f = precision ? 1 : 0;
+    if (!c->wave || !c->wave->walk_tuned[f]) return c->fail(AE_ERR_STATE, "no wavefront frame of this form yet");
+    if (shadow_run) *shadow_run = c->wave->shadow_run[f];
+    if (extend_run) *extend_run = c->wave->walk_run[f];
+    if (tune_ms8) std::memcpy(tune_ms8, c->wave->walk_tune_ms[f], sizeof(c->wave->walk_tune_ms[f]));
+    return AE_OK;
+}
+
+extern "C" int ae_wavefront_set_walk_runs(ae_ctx *ctx, int precision, uint32_t shadow_run, uint32_t extend_run) {
+    Ctx *c = reinterpret_cast<Ctx *>(ctx);
+    if (!c) return AE_ERR_INVALID;
+    if (shadow_run > (1u << 20) || extend_run > (1u << 20))
+        return c->fail(AE_ERR_INVALID, "run lengths above 2^20 (got %u, %u)", shadow_run, extend_run);
+    if (!c->wave) c->wave = new (std::nothrow) Wavefront();
+    if (!c->wave) return c->fail(AE_ERR_OOM, "wavefront state");
+    Wavefront &Wf = *c->wave;
+    const int f = precision ? 1 : 0;
+    Wf.shadow_run[f] = shadow_run;
+    Wf.walk_run[f] = extend_run;
+    Wf.walk_tuned[f] = true;
+    if (Wf.graph) {
+        cudaGraphExecDestroy(Wf.graph);
+        Wf.graph = nullptr;
+    }
+    return AE_OK;
+}
 
 // Wavefront statistics: the autotuned extend configuration and the error flag.
 extern "C" int ae_wavefront_info(ae_ctx *ctx, int32_t *threads, int32_t *stack, float *tune_ms9, uint32_t *errors) {

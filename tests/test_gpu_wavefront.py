@@ -118,3 +118,40 @@ def test_wavefront_equals_plain_full_size():
         assert hp[k]["object"] != _lib.MISS and hf[k]["object"] != _lib.MISS, detail
         tp, tf = float(hp[k]["t"]), float(hf[k]["t"])
         assert tf <= tp and tp - tf <= tp * 2.0 ** -20, detail
+
+
+@pytest.mark.parametrize("mode", [_lib.MODE_WAVEFRONT, _lib.MODE_WAVEFRONT_PRECISION])
+def test_walker_queue_assignments_give_the_same_frames(mode):
+    """The walker stages take their queue entries statically or in runs per
+    warp (the autotuner picks per scene and form); every assignment must give
+    the same frames bit for bit.  A small wavefront scene (glass, metal, 16
+    lights) rendered with the assignment pinned three ways, and once more
+    autotuned."""
+    s = scenes.wavefront_scene(width=240, height=136, depth=6, n_meshes=6, n_instances=96, target_tris=200_000)
+    prec = mode == _lib.MODE_WAVEFRONT_PRECISION
+    w, h = int(s.config["width"]), int(s.config["height"])
+    runs = [(0, 0), (32, 64), (256, 32), None]
+    out = []
+    for r in runs:
+        with Context(w, h) as ctx:
+            ctx.upload(s)
+            if r is not None:
+                ctx.set_wavefront_walk_runs(r[0], r[1], precision=prec)
+            frames = []
+            c = s.config.copy()
+            for b in range(2):
+                c["batch"] = b
+                ctx.set_config(c)
+                ctx.render_frame(mode)
+                frames.append(ctx.read_image(_lib.IMAGE_FRAME))
+            info = ctx.wavefront_walk_info(precision=prec)
+            if r is not None:
+                assert (info["shadow_run"], info["extend_run"]) == r
+            else:
+                assert info["shadow_run"] in (0, 32, 64, 256) and info["extend_run"] in (0, 32, 64, 256)
+                assert all(t > 0 for t in info["shadow_ms"] + info["extend_ms"]), info
+            assert ctx.wavefront_info()["errors"] == 0
+            out.append(frames)
+    for k in range(1, len(runs)):
+        for b in range(2):
+            assert same(out[k][b], out[0][b]), (runs[k], b)
