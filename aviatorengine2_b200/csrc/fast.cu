@@ -869,12 +869,13 @@ __global__ void __launch_bounds__(128) k_count_fast(DevScene S, FastView V, cons
 // from a global counter, and the lanes of a warp take theirs from the warp's
 // current chunk, so the rays a warp has in flight stay close in the input
 // order (neighbouring pixels: neighbouring origins and nodes).  On a
-// 1.3M-ray bounce set this took 3.70 -> 3.31 ms.  It keeps every block busy
+// 1.3M-ray bounce set this took 3.70 -> 3.31 ms; on the current walker, runs
+// of 32 rays beat 64 and 128 (1.72 / 1.76 / 1.96 ms).  It keeps every block busy
 // to the end of the launch, which suits a launch that has the GPU to itself;
 // the smaller launches of the pipelined host-buffer call, which overlap on
 // three streams, use the static assignment (lane i: rays i, i + grid size,
 // ...), whose blocks retire early and make room for the next launch.
-constexpr uint32_t kWalkChunk = 64;
+constexpr uint32_t kWalkChunk = 32;
 constexpr uint32_t kWalkDynamicMin = (1u << 19) + 1;  // above the host pipeline's largest chunk
 
 template <bool DYN>

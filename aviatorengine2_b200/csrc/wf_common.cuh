@@ -11,6 +11,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include "bulk.cuh"
 #include "fast_trace.cuh"
 #include "shade.cuh"
 #include "trace_common.cuh"
@@ -35,38 +36,6 @@ AE_DEV uint32_t warp_append(uint32_t *counter, uint32_t want) {
     if (int(lane) == leader) base = atomicAdd(counter, incl);
     base = __shfl_sync(mask, base, leader);
     return base + incl - want;
-}
-
-// ---------------------------------------------------------------------------
-// Bulk-copy staging of a queue tile into shared memory (no multicast).
-// ---------------------------------------------------------------------------
-AE_DEV uint32_t smem_addr(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
-
-AE_DEV void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-AE_DEV void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
-}
-AE_DEV void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_addr(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
-}
-// Waits for `phase` to complete; gives up after `limit` polls and reports it.
-AE_DEV bool mbar_wait(uint64_t *bar, uint32_t phase, uint32_t limit) {
-    for (uint32_t i = 0; i < limit; i++) {
-        uint32_t done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done)
-            : "r"(smem_addr(bar)), "r"(phase)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
 }
 
 // ---------------------------------------------------------------------------
