@@ -460,7 +460,11 @@ int ae_image_error_pixels(ae_ctx *ctx, int which, const uint32_t *xy, uint32_t n
                           double eps, double *out4);
 
 /* Closest hit for a batch of HOST rays: copies in, traces, copies out,
- * pipelined in chunks over streams.  variant = AE_VARIANT_*. */
+ * pipelined in chunks over streams.  variant = AE_VARIANT_*.  With FAST or
+ * QUANT and page-locked buffers the device can address (cudaHostAlloc'd or
+ * cudaHostRegister'd), the kernel reads the rays and writes the hits in host
+ * memory directly, in one launch.  The hits are ae_closest_hit_device's
+ * either way. */
 int ae_closest_hit(ae_ctx *ctx, const ae_ray *rays, uint32_t n, ae_hit *hits, int variant);
 /* Same with DEVICE pointers, on the context's stream, no synchronisation. */
 int ae_closest_hit_device(ae_ctx *ctx, const ae_ray *d_rays, uint32_t n, ae_hit *d_hits, int variant);

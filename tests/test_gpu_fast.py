@@ -215,3 +215,27 @@ def test_fast_refuses_media():
         c.upload(s)
         with pytest.raises(AeError):
             c.prepare_fast()
+
+
+@pytest.mark.parametrize("variant", [_lib.VARIANT_FAST, _lib.VARIANT_QUANT, _lib.VARIANT_FAST_WALK])
+def test_host_call_with_page_locked_buffers(instanced, variant):
+    """ae_closest_hit over page-locked host buffers: FAST and QUANT trace them
+    in place (the kernel reads rays and writes hits in host memory), the walker
+    variant through its staged pipeline; the hits equal the device-pointer
+    call's byte for byte, as with pageable buffers."""
+    import torch
+    s = instanced
+    with ctx_for(s) as c:
+        prim = c.camera_rays()
+        r = np.concatenate([prim, random_rays(70001, 0, 100, 11)])
+        h_r = torch.from_numpy(r.view(np.uint8).copy()).pin_memory()
+        h_h = torch.zeros(len(r) * 20, dtype=torch.uint8).pin_memory()
+        _lib.check(_lib.lib().ae_closest_hit(c.handle, h_r.data_ptr(), len(r), h_h.data_ptr(), variant), c.handle)
+        dev = torch.device("cuda", 0)
+        d_r = h_r.to(dev)
+        d_h = torch.zeros(len(r) * 20, dtype=torch.uint8, device=dev)
+        torch.cuda.synchronize(dev)
+        c.closest_hit_device(d_r.data_ptr(), len(r), d_h.data_ptr(), variant)
+        c.synchronize()
+        assert torch.equal(h_h, d_h.cpu())
+        assert same(h_h.numpy().view(_lib.HIT), c.closest_hit(r, variant))
