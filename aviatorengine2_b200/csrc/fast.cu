@@ -899,7 +899,7 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_closest_walk(DevScene
             if (!am) break;
             // Only the warp's largest phase group steps (warp_pick_group).
             const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, am, iter);
-            if (!active || w.group() != pick || !w.steps(pick, S, V, K, stk, threadIdx.x, blockDim.x)) continue;
+            if (!active || w.group() != pick || !w.step(S, V, K, stk, threadIdx.x, blockDim.x)) continue;
             const Best &b = w.best;
             const bool any = b.object != AE_MISS;
             ae_hit h;
@@ -956,7 +956,7 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_closest_walk(DevScene
         // Only the warp's largest phase group steps (warp_pick_group): on the
         // 1080p bounce set 3.31 -> 2.70 ms.
         const uint32_t pick = warp_pick_group(w.group(), active, am, iter);
-        if (active && w.group() == pick && w.steps(pick, S, V, K, stk, threadIdx.x, blockDim.x)) {
+        if (active && w.group() == pick && w.step(S, V, K, stk, threadIdx.x, blockDim.x)) {
             const Best &b = w.best;
             const bool any = b.object != AE_MISS;
             ae_hit h;

@@ -28,13 +28,6 @@ enum : uint32_t { kWalkTlas = 0, kWalkObject = 1, kWalkBlas = 2, kWalkDone = 3 }
 // wavefront frame 177 ms against 192 ms and 179 ms.
 constexpr int kWalkBlocksPerSm = 7;
 
-// Steps a lane may take in one warp iteration while it stays in the picked
-// phase group (Walker::steps).
-#ifndef AE_WALK_REPEAT
-#define AE_WALK_REPEAT 1
-#endif
-constexpr int kWalkRepeat = AE_WALK_REPEAT;
-
 // The walk's per-thread local stacks: the instance-tree stack and the BLAS
 // entries beyond the shared-memory part.  Kept out of Walker so its scalar
 // state can live in registers.
@@ -204,16 +197,6 @@ struct Walker {
         if (top) tlas_pop(K);
         else blas_pop(K, stk, tid, nt);
         return phase == kWalkDone;
-    }
-
-    // Up to kWalkRepeat steps while the walk stays in the warp's picked
-    // group `pick`; returns true once the ray is finished.
-    AE_DEV bool steps(uint32_t pick, const DevScene &S, const FastView &V, WalkStacks<SS> &K, uint2 *stk, int tid,
-                      int nt) {
-        bool done = step(S, V, K, stk, tid, nt);
-#pragma unroll 1
-        for (int r = 1; r < kWalkRepeat && !done && group() == pick; r++) done = step(S, V, K, stk, tid, nt);
-        return done;
     }
 };
 

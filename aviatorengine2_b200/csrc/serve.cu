@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_sv_extend_walk(SvView
         if (!am) break;
         // Only the warp's largest phase group steps (warp_pick_group).
         const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, am, iter);
-        if (!active || w.group() != pick || !w.steps(pick, R->S, R->V, K, stk, threadIdx.x, blockDim.x)) continue;
+        if (!active || w.group() != pick || !w.step(R->S, R->V, K, stk, threadIdx.x, blockDim.x)) continue;
         const Best &b = w.best;
         const bool any = b.object != AE_MISS;
         ae_hit h;
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_s
         if (!am) break;
         // Only the warp's largest phase group steps (warp_pick_group).
         const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, am, iter);
-        if (!active || w.group() != pick || !w.steps(pick, R->S, R->V, K, stk, threadIdx.x, THREADS)) continue;
+        if (!active || w.group() != pick || !w.step(R->S, R->V, K, stk, threadIdx.x, THREADS)) continue;
         const Best &b = w.best;
         int verdict = 0;  // 0 unoccluded, 1 occluded, 2 through glass
         if (b.object != AE_MISS && b.t < AE_SUB(distance(lp, so), 0.001f)) {

@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_wf_extend_walk(DevSce
         if (!am) break;
         // Only the warp's largest phase group steps (warp_pick_group).
         const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, am, iter);
-        if (!active || w.group() != pick || !w.steps(pick, S, V, K, stk, threadIdx.x, blockDim.x)) continue;
+        if (!active || w.group() != pick || !w.step(S, V, K, stk, threadIdx.x, blockDim.x)) continue;
         const Best &b = w.best;
         const bool any = b.object != AE_MISS;
         ae_hit h;
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS)
         if (!am) break;
         // Only the warp's largest phase group steps (warp_pick_group).
         const uint32_t pick = warp_pick_group(active ? w.group() : 0u, active, am, iter);
-        if (!active || w.group() != pick || !w.steps(pick, S, V, K, stk, threadIdx.x, THREADS)) continue;
+        if (!active || w.group() != pick || !w.step(S, V, K, stk, threadIdx.x, THREADS)) continue;
         const Best &b = w.best;
         int verdict = 0;  // 0 unoccluded, 1 occluded, 2 through glass
         if (b.object != AE_MISS && b.t < AE_SUB(distance(lp, so), 0.001f)) {

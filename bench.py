@@ -814,6 +814,8 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=0.5, help="Poisson arrivals per second")
     ap.add_argument("--serve-sweep", default="", help="comma-separated arrival rates: also run the serving "
                     "leg at each (reported as serving_sweep)")
+    ap.add_argument("--serve-claim", choices=["shared", "oldest"], default="shared",
+                    help="how free slots pick the next pixel: spread over the admitted requests, or the oldest first")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -987,11 +989,13 @@ def main():
     build = leg(not args.no_build, measure_build, local)
     config1 = leg(not args.no_config1, measure_config1, local)
     config4 = leg(not args.no_config4, measure_config4, local, args.c4_frames, args.mre_pixels)
+    claim = 0 if args.serve_claim == "oldest" else 1
     serving = leg(not args.no_serve, measure_serving, local, args.serve_requests, args.serve_rate,
-                  frame_hz=args.serve_frame_hz)
+                  claim_policy=claim, frame_hz=args.serve_frame_hz)
     sweep = None
     if args.serve_sweep:
-        sweep = [leg(True, measure_serving, local, args.serve_requests, float(r), frame_hz=args.serve_frame_hz)
+        sweep = [leg(True, measure_serving, local, args.serve_requests, float(r), claim_policy=claim,
+                     frame_hz=args.serve_frame_hz)
                  for r in args.serve_sweep.split(",")]
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
