@@ -57,7 +57,8 @@ MESH_RANGE = np.dtype([("vertexBase", "<u4"), ("indexBase", "<u4"), ("triangleCo
 
 SERVE_SETTINGS = np.dtype([("device", "<i4"), ("slots", "<u4"), ("max_lights", "<u4"), ("max_requests", "<u4"),
                            ("arena_bytes", "<u8"), ("ticks_per_launch", "<u4"), ("extend_threads", "<u4"),
-                           ("max_scenes", "<u4"), ("claim_policy", "<u4"), ("reserved", "<u4", 4)])
+                           ("max_scenes", "<u4"), ("claim_policy", "<u4"), ("queue_run", "<u4"),
+                           ("reserved", "<u4", 3)])
 SERVE_REQUEST = np.dtype([("scene", "<u4"), ("width", "<u4"), ("height", "<u4"), ("frames", "<u4"),
                           ("config", CONFIG), ("accum", "<u8"), ("display", "<u8"), ("user", "<u8")])
 SERVE_RESULT = np.dtype([("id", "<u8"), ("user", "<u8"), ("status", "<i4"), ("scene_version", "<u4"),

@@ -83,8 +83,11 @@ struct ReqDev {
 
 // SV_FAULT: the injected tile-wait failure of ae_serve_debug_inject (0 = none).
 enum { SV_Q0 = 0, SV_Q1 = 1, SV_SH = 2, SV_ERR = 3, SV_TILE = 4, SV_IDLE0 = 5, SV_IDLE1 = 6, SV_NORDER = 7,
-       SV_FAULT = 8, SV_COUNT = 9 };
+       SV_FAULT = 8, SV_RUN_EXT = 9, SV_RUN_SH = 10, SV_COUNT = 11 };
 enum { ST_RAYS = 0, ST_SHADOW = 1, ST_COUNT = 2 };
+// Default run of queue entries a warp of the walker stages takes at a time
+// (ae_serve_settings.queue_run 0).
+constexpr uint32_t kServeQueueRun = 32;
 
 struct SvView {
     const SceneRec *scenes;
@@ -128,6 +131,8 @@ __global__ void k_sv_begin(SvView W, int q) {
     W.cnt[q ^ 1] = 0;
     W.cnt[SV_SH] = 0;
     W.cnt[SV_TILE] = 0;
+    W.cnt[SV_RUN_EXT] = 0;
+    W.cnt[SV_RUN_SH] = 0;
     W.cnt[SV_IDLE0 + (q ^ 1)] = 0;
 }
 
@@ -195,8 +200,11 @@ __global__ void __launch_bounds__(THREADS) k_sv_extend(SvView W, int q) {
 }
 
 // Extend on the step-wise Walker: each thread steps its own queued ray (its
-// own scene's) and takes the next (k + grid size) as soon as one finishes.
-__global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_sv_extend_walk(SvView W, int q) {
+// own scene's) and takes the next one as soon as one finishes - k + grid size
+// (DYN false) or from its warp's run of `run` consecutive queue entries (DYN
+// true; ae_serve_settings.queue_run).
+template <bool DYN>
+__global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_sv_extend_walk(SvView W, int q, uint32_t run) {
     extern __shared__ uint2 stk[];
     const uint32_t count = W.cnt[q];
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -204,14 +212,21 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_sv_extend_walk(SvView
     Walker<false> w;
     WalkStacks<> K;
     const SceneRec *R = nullptr;
-    bool active = k < count;
-    if (active) {
+    bool active = !DYN && k < count;
+    bool need = DYN, exhausted = false;
+    uint32_t cbase = 0, cend = 0;
+    auto begin = [&]() {
         const ae_ray r = W.qray[q][k];
         R = W.scenes + W.s_scene[W.qslot[q][k]];
         w.start(R->V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
-    }
+    };
+    if (active) begin();
     uint32_t iter = 0;
     for (;;) {
+        if (DYN && run_take(&W.cnt[SV_RUN_EXT], count, run, need, k, cbase, cend, exhausted)) {
+            active = true;
+            begin();
+        }
         const uint32_t am = __ballot_sync(0xffffffffu, active);
         if (!am) break;
         // Only the warp's largest phase group steps (warp_pick_group).
@@ -226,13 +241,14 @@ __global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_sv_extend_walk(SvView
         h.object = b.object;
         h.prim = b.prim;
         W.qhit[k] = h;
+        if (DYN) {
+            active = false;
+            need = true;
+            continue;
+        }
         k += stride;
         active = k < count;
-        if (active) {
-            const ae_ray r = W.qray[q][k];
-            R = W.scenes + W.s_scene[W.qslot[q][k]];
-            w.start(R->V, mk(r.ox, r.oy, r.oz), mk(r.dx, r.dy, r.dz), r.tnear, r.time);
-        }
+        if (active) begin();
     }
 }
 
@@ -272,10 +288,11 @@ __global__ void __launch_bounds__(256) k_sv_shade(SvView W, int q) {
     }
 }
 
-template <int THREADS>
-__global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_sv_shadow(SvView W) {
+template <int THREADS, bool DYN>
+__global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_sv_shadow(SvView W, uint32_t run) {
     // The reference's shadow loop per light sample on the step-wise Walker:
-    // a lane that finishes a sample starts its next one at once.  The
+    // a lane that finishes a sample starts its next one at once (k + grid
+    // size, or from its warp's run of `run` queue entries when DYN).  The
     // sample's scene (its slot's) is read through the scene table.
     extern __shared__ uint2 stk[];
     const uint32_t count = W.cnt[SV_SH];
@@ -287,16 +304,24 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_s
     uint32_t e = 0;
     f3 so, sd, lp;
     int step = 0;
-    bool active = k < count;
-    if (active) {
+    bool active = !DYN && k < count;
+    bool need = DYN, exhausted = false;
+    uint32_t cbase = 0, cend = 0;
+    auto begin = [&]() {
         e = W.sq[k];
         R = W.scenes + W.s_scene[e / W.max_lights];
         const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
         so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
+        step = 0;
         w.start(R->V, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
-    }
+    };
+    if (active) begin();
     uint32_t iter = 0;
     for (;;) {
+        if (DYN && run_take(&W.cnt[SV_RUN_SH], count, run, need, k, cbase, cend, exhausted)) {
+            active = true;
+            begin();
+        }
         const uint32_t am = __ballot_sync(0xffffffffu, active);
         if (!am) break;
         // Only the warp's largest phase group steps (warp_pick_group).
@@ -317,16 +342,14 @@ __global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS) k_s
             verdict = 0;
         }
         W.sh.occ[e] = uint8_t(verdict);
+        if (DYN) {
+            active = false;
+            need = true;
+            continue;
+        }
         k += stride;
         active = k < count;
-        if (active) {
-            e = W.sq[k];
-            R = W.scenes + W.s_scene[e / W.max_lights];
-            const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
-            so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
-            step = 0;
-            w.start(R->V, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
-        }
+        if (active) begin();
     }
 }
 
@@ -703,16 +726,22 @@ int Server::build_graph() {
     const bool walk = st.extend_threads == 0;
     const int ei = extend_index(st.extend_threads);
     const int et = walk ? 128 : (ei == 2 ? 256 : ei == 1 ? 128 : 64);
-    const SvExtendFn efn = walk ? k_sv_extend_walk : kSvExtend[ei];
+    // Walker stages: runs of queue_run entries per warp, or (queue_run 1)
+    // the static assignment.
+    const bool dyn = st.queue_run > 1;
+    const uint32_t run = st.queue_run;
+    const void *wfn = dyn ? reinterpret_cast<const void *>(k_sv_extend_walk<true>)
+                          : reinterpret_cast<const void *>(k_sv_extend_walk<false>);
+    const void *efn = walk ? wfn : reinterpret_cast<const void *>(kSvExtend[ei]);
+    const void *shfn = dyn ? reinterpret_cast<const void *>(k_sv_shadow<128, true>)
+                           : reinterpret_cast<const void *>(k_sv_shadow<128, false>);
     const size_t shsmem = size_t(kSharedStack) * 128 * sizeof(uint2);
     const size_t esmem = walk ? shsmem : sv_extend_smem(et);
-    cudaFuncSetAttribute(reinterpret_cast<const void *>(efn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(esmem));
-    cudaFuncSetAttribute(reinterpret_cast<const void *>(k_sv_shadow<128>), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         int(shsmem));
+    cudaFuncSetAttribute(efn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(esmem));
+    cudaFuncSetAttribute(shfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shsmem));
     int e_per_sm = 0, sh_per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e_per_sm, reinterpret_cast<const void *>(efn), et, esmem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh_per_sm, reinterpret_cast<const void *>(k_sv_shadow<128>), 128,
-                                                  shsmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e_per_sm, efn, et, esmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh_per_sm, shfn, 128, shsmem);
     const int egrid = std::max(1, e_per_sm) * sms, shgrid = std::max(1, sh_per_sm) * sms, g256 = sms * 8;
     if (cudaGetLastError() != cudaSuccess) { err = "launch shape query failed"; return AE_ERR_CUDA; }
     cudaGraph_t g;
@@ -725,9 +754,12 @@ int Server::build_graph() {
     for (uint32_t t = 0; t < st.ticks_per_launch; t++) {
         const int q = int(t & 1);
         k_sv_begin<<<1, 1, 0, stream>>>(W, q);
-        efn<<<egrid, et, esmem, stream>>>(W, q);
+        if (!walk) kSvExtend[ei]<<<egrid, et, esmem, stream>>>(W, q);
+        else if (dyn) k_sv_extend_walk<true><<<egrid, et, esmem, stream>>>(W, q, run);
+        else k_sv_extend_walk<false><<<egrid, et, esmem, stream>>>(W, q, 0u);
         k_sv_shade<<<g256, 256, 0, stream>>>(W, q);
-        k_sv_shadow<128><<<shgrid, 128, shsmem, stream>>>(W);
+        if (dyn) k_sv_shadow<128, true><<<shgrid, 128, shsmem, stream>>>(W, run);
+        else k_sv_shadow<128, false><<<shgrid, 128, shsmem, stream>>>(W, 0u);
         k_sv_connect<<<g256, 256, 0, stream>>>(W, q);
         k_sv_advance<<<g256, 256, 0, stream>>>(W, q);
     }
@@ -1101,8 +1133,9 @@ extern "C" ae_server *ae_serve_create(const ae_serve_settings *settings) {
     if (s.extend_threads != 0 && s.extend_threads != 64 && s.extend_threads != 128 && s.extend_threads != 256)
         return nullptr;
     if (!s.max_scenes) s.max_scenes = 16;
+    if (!s.queue_run) s.queue_run = kServeQueueRun;
     if (s.max_lights > kServeMaxLights || s.max_requests > kServeMaxRequests || (s.ticks_per_launch & 1) ||
-        s.claim_policy > AE_CLAIM_SHARED ||
+        s.claim_policy > AE_CLAIM_SHARED || s.queue_run > 1024 ||
         s.slots > (1u << 26) || uint64_t(s.slots) * s.max_lights > 0xffffffffull)
         return nullptr;
     ae_server *srv = new (std::nothrow) ae_server();

@@ -20,11 +20,12 @@ from ._lib import lib, ptr
 
 class Server:
     def __init__(self, slots=0, max_lights=0, max_requests=0, arena_bytes=0, ticks_per_launch=0, extend_threads=0,
-                 max_scenes=0, claim_policy=_lib.CLAIM_OLDEST_FIRST, device=0):
+                 max_scenes=0, claim_policy=_lib.CLAIM_OLDEST_FIRST, device=0, queue_run=0):
         s = np.zeros(1, _lib.SERVE_SETTINGS)
         s["device"], s["slots"], s["max_lights"], s["max_requests"] = device, slots, max_lights, max_requests
         s["arena_bytes"], s["ticks_per_launch"] = arena_bytes, ticks_per_launch
         s["extend_threads"], s["max_scenes"], s["claim_policy"] = extend_threads, max_scenes, claim_policy
+        s["queue_run"] = queue_run
         self._h = lib().ae_serve_create(ptr(s))
         if not self._h:
             raise _lib.AeError(lib().ae_create_status(), "ae_serve_create failed (see stderr)")

@@ -618,7 +618,10 @@ typedef struct ae_serve_settings {
     uint32_t extend_threads;   /* 0 = step-wise walker (default); 64, 128 or 256 = tile-staged extend */
     uint32_t max_scenes;       /* resident scenes; 0 = 16 */
     uint32_t claim_policy;     /* AE_CLAIM_OLDEST_FIRST (0) or AE_CLAIM_SHARED (1) */
-    uint32_t reserved[4];
+    uint32_t queue_run;        /* walker extend and shadow stages: queue entries a warp takes at a time
+                                  (runs of consecutive entries); 0 = default (32), 1 = static assignment
+                                  (entry k + grid size); at most 1024 */
+    uint32_t reserved[3];
 } ae_serve_settings;
 
 /* How free slots pick the next pixel: from the oldest admitted request that
