@@ -494,7 +494,8 @@ int ae_closest_hit(ae_ctx *ctx, const ae_ray *rays, uint32_t n, ae_hit *hits, in
     int rc = prepare_variant(c, variant);
     if (rc) return rc;
     // The one-ray-per-thread optimised kernels over page-locked host buffers
-    // the device can address (cudaHostAlloc'd, or cudaHostRegister'd): the
+    // the device can address (cudaHostAlloc'd, or cudaHostRegister'd), rays
+    // on a 16-byte boundary (anything else takes the staged pipeline): the
     // kernel reads the rays and writes the hits over the bus itself, one
     // launch and no staging copies.  Each thread reads its ray once when its
     // block starts, and the resident blocks hide the bus latency (1080p
@@ -506,7 +507,8 @@ int ae_closest_hit(ae_ctx *ctx, const ae_ray *rays, uint32_t n, ae_hit *hits, in
         cudaPointerAttributes ar{}, ah{};
         const bool mapped = cudaPointerGetAttributes(&ar, rays) == cudaSuccess &&
                             cudaPointerGetAttributes(&ah, hits) == cudaSuccess && ar.type == cudaMemoryTypeHost &&
-                            ah.type == cudaMemoryTypeHost && ar.devicePointer && ah.devicePointer;
+                            ah.type == cudaMemoryTypeHost && ar.devicePointer && ah.devicePointer &&
+                            (reinterpret_cast<uintptr_t>(ar.devicePointer) & 15u) == 0;
         cudaGetLastError();  // pageable memory is not an error here
         if (mapped) {
             if ((rc = closest_hit_dispatch(c, static_cast<const ae_ray *>(ar.devicePointer), n,

@@ -34,6 +34,9 @@ int closest_hit_dispatch(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, i
     int rc = prepare_variant(c, variant);
     if (rc) return rc;
     if (n == 0) return AE_OK;
+    // The kernels read a ray as two 16-byte loads.
+    if (reinterpret_cast<uintptr_t>(rays) & 15u)
+        return c->fail(AE_ERR_INVALID, "device rays must start on a 16-byte boundary");
     if (timed && (rc = c->cuda(cudaEventRecord(c->ev0, st), "event"))) return rc;
     cudaError_t e;
     if (variant == AE_VARIANT_PLAIN || variant == AE_VARIANT_PLAIN_WT)
@@ -53,6 +56,8 @@ int closest_hit_dispatch(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, i
 
 static int trace_counters(ae::Ctx *c, const ae_ray *d_rays, uint32_t n, int variant, uint64_t *counters) {
     if (!c->scene_uploaded) return c->fail(AE_ERR_STATE, "counters before ae_upload_scene");
+    if (reinterpret_cast<uintptr_t>(d_rays) & 15u)
+        return c->fail(AE_ERR_INVALID, "device rays must start on a 16-byte boundary");
     if (variant != AE_VARIANT_PLAIN && variant != AE_VARIANT_FAST && variant != AE_VARIANT_QUANT)
         return c->fail(AE_ERR_INVALID, "touch counters exist for PLAIN, FAST and QUANT (got variant %d)", variant);
     int rc = ae::prepare_variant(c, variant);

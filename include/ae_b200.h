@@ -466,7 +466,8 @@ int ae_image_error_pixels(ae_ctx *ctx, int which, const uint32_t *xy, uint32_t n
  * memory directly, in one launch.  The hits are ae_closest_hit_device's
  * either way. */
 int ae_closest_hit(ae_ctx *ctx, const ae_ray *rays, uint32_t n, ae_hit *hits, int variant);
-/* Same with DEVICE pointers, on the context's stream, no synchronisation. */
+/* Same with DEVICE pointers, on the context's stream, no synchronisation.
+ * d_rays must start on a 16-byte boundary (AE_ERR_INVALID otherwise). */
 int ae_closest_hit_device(ae_ctx *ctx, const ae_ray *d_rays, uint32_t n, ae_hit *d_hits, int variant);
 /* Closest hit for HOST rays with no device allocation: the variant of
  * ae_closest_hit for callers that cannot let a library call cudaMalloc (a

@@ -239,3 +239,28 @@ def test_host_call_with_page_locked_buffers(instanced, variant):
         c.synchronize()
         assert torch.equal(h_h, d_h.cpu())
         assert same(h_h.numpy().view(_lib.HIT), c.closest_hit(r, variant))
+
+
+def test_misaligned_rays(instanced):
+    """Rays that do not start on a 16-byte boundary: the device-pointer call
+    refuses them (AE_ERR_INVALID, nothing launched); the host-buffer call
+    traces them through its aligned staging, page-locked or not."""
+    import torch
+    s = instanced
+    with ctx_for(s) as c:
+        r = random_rays(5000, 0, 100, 12)
+        want = c.closest_hit(r, _lib.VARIANT_FAST)
+        dev = torch.device("cuda", 0)
+        d_r = torch.zeros(len(r) * 32 + 16, dtype=torch.uint8, device=dev)
+        d_h = torch.zeros(len(r) * 20, dtype=torch.uint8, device=dev)
+        with pytest.raises(AeError) as e:
+            c.closest_hit_device(d_r.data_ptr() + 4, len(r), d_h.data_ptr(), _lib.VARIANT_FAST)
+        assert e.value.code == -1
+        h_buf = torch.zeros(len(r) * 32 + 16, dtype=torch.uint8).pin_memory()
+        h_buf[8:8 + len(r) * 32].copy_(torch.from_numpy(r.view(np.uint8)))
+        for variant in (_lib.VARIANT_FAST, _lib.VARIANT_QUANT):
+            h_h = torch.zeros(len(r) * 20, dtype=torch.uint8).pin_memory()
+            _lib.check(_lib.lib().ae_closest_hit(c.handle, h_buf.data_ptr() + 8, len(r), h_h.data_ptr(), variant),
+                       c.handle)
+            assert same(h_h.numpy().view(_lib.HIT), c.closest_hit(r, variant))
+        assert same(c.closest_hit(r, _lib.VARIANT_FAST), want)
