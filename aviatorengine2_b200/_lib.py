@@ -85,7 +85,7 @@ SHAPE_SPHERE, SHAPE_QUAD, SHAPE_BOX, SHAPE_TRIANGLE, SHAPE_MESH = range(5)
 MAT_LAMBERTIAN, MAT_METAL, MAT_DIELECTRIC, MAT_DIFFUSE_LIGHT, MAT_ISOTROPIC, MAT_GGX_METAL = range(6)
 NO_TEXTURE = 0xFFFFFFFF
 MISS = 0xFFFFFFFF
-VARIANT_PLAIN, VARIANT_FAST, VARIANT_QUANT, VARIANT_FAST_WALK, VARIANT_PLAIN_WT = 0, 1, 2, 3, 4
+VARIANT_PLAIN, VARIANT_FAST, VARIANT_QUANT, VARIANT_FAST_WALK, VARIANT_PLAIN_WT, VARIANT_PLAIN_CHECKED = 0, 1, 2, 3, 4, 5
 MODE_COMPUTE_ONLY, MODE_DEFERRED, MODE_WAVEFRONT, MODE_WAVEFRONT_PRECISION = 0, 1, 2, 3
 IMAGE_ACCUM, IMAGE_DISPLAY, IMAGE_FRAME, IMAGE_REDUCED, IMAGE_HISTORY_GEOMETRY = range(5)
 POLICY_REQUEST, POLICY_MOVE, POLICY_CANCEL = 0, 1, 2
@@ -93,6 +93,8 @@ CLAIM_OLDEST_FIRST, CLAIM_SHARED = 0, 1
 STATUS = {0: "AE_OK", -1: "AE_ERR_INVALID", -2: "AE_ERR_OOM", -3: "AE_ERR_OVERSIZE", -4: "AE_ERR_LAYOUT",
           -5: "AE_ERR_CUDA", -6: "AE_ERR_TIMEOUT", -7: "AE_ERR_STATE", -8: "AE_ERR_REJECTED", -9: "AE_ERR_CANCELLED"}
 FAULT_TILE_WAIT = 1
+FAULT_CHECK_LIMITS = 2
+CHECK_STACK, CHECK_INDEX = 1, 2
 
 # Every symbol include/ae_b200.h declares, with (restype, argtypes).
 _P = ctypes.c_void_p
@@ -172,6 +174,7 @@ SIGNATURES = {
     "ae_debug_live_allocations": (ctypes.c_int64, []),
     "ae_create_status": (_I, []),
     "ae_debug_inject": (_I, [_P, _I, _U32]),
+    "ae_debug_flags": (_I, [_P, _P]),
     "ae_serve_debug_inject": (_I, [_P, _I, _U32]),
 }
 

@@ -425,9 +425,22 @@ int ae_create_status(void) { return ae::create_status(); }
 int ae_debug_inject(ae_ctx *ctx, int fault, uint32_t on) {
     Ctx *c = reinterpret_cast<Ctx *>(ctx);
     if (!c) return AE_ERR_INVALID;
-    if (fault != AE_FAULT_TILE_WAIT) return c->fail(AE_ERR_INVALID, "unknown fault %d", fault);
-    c->fault_tile_wait = on ? 1u : 0u;
+    if (fault == AE_FAULT_TILE_WAIT) c->fault_tile_wait = on ? 1u : 0u;
+    else if (fault == AE_FAULT_CHECK_LIMITS) c->fault_check_limits = on ? 1u : 0u;
+    else return c->fail(AE_ERR_INVALID, "unknown fault %d", fault);
     return AE_OK;
+}
+
+int ae_debug_flags(ae_ctx *ctx, uint32_t *flags) {
+    Ctx *c = reinterpret_cast<Ctx *>(ctx);
+    if (!c || !flags) return AE_ERR_INVALID;
+    *flags = 0;
+    if (!c->check_word.ptr) return AE_OK;  // the debug walk has not run
+    int rc = c->cuda(cudaMemcpyAsync(flags, c->check_word.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream),
+                     "read check word");
+    if (!rc) rc = c->cuda(cudaMemsetAsync(c->check_word.ptr, 0, sizeof(uint32_t), c->stream), "clear check word");
+    if (!rc) rc = c->cuda(cudaStreamSynchronize(c->stream), "check word");
+    return rc;
 }
 
 int ae_render_frame(ae_ctx *ctx, int mode, const ae_gbuffer *gb) {

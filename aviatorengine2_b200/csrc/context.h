@@ -83,6 +83,8 @@ struct Ctx {
     bool scene_uploaded = false;
     bool scene_has_ggx = false;  // an object uses AE_MAT_GGX_METAL (not shaded by the hybrid passes)
     uint32_t fault_tile_wait = 0;  // ae_debug_inject(AE_FAULT_TILE_WAIT)
+    uint32_t fault_check_limits = 0;  // ae_debug_inject(AE_FAULT_CHECK_LIMITS)
+    DevBuf<uint32_t> check_word;      // AE_CHECK_* bits of the debug walk (ae_debug_flags)
     uint64_t scene_version = 0;         // bumps on every change of scene content
     uint64_t geometry_version = 0;      // bumps on every ae_upload_geometry
     uint64_t scene_version_layout = 0;  // bumps when arrays are re-uploaded (topology may change)

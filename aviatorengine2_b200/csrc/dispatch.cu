@@ -22,11 +22,35 @@ int prepare_variant(Ctx *c, int variant) {
     switch (variant) {
     case AE_VARIANT_PLAIN:
     case AE_VARIANT_PLAIN_WT: return AE_OK;
+    case AE_VARIANT_PLAIN_CHECKED:
+        if (!c->check_word.ptr) {
+            if (c->check_word.reserve(1)) return c->fail(AE_ERR_OOM, "check word");
+            return c->cuda(cudaMemset(c->check_word.ptr, 0, sizeof(uint32_t)), "check word");
+        }
+        return AE_OK;
     case AE_VARIANT_FAST:
     case AE_VARIANT_QUANT:
     case AE_VARIANT_FAST_WALK: return prepare_fast(c);
     default: return c->fail(AE_ERR_INVALID, "unknown kernel variant %d", variant);
     }
+}
+
+// The debug walk's limits: the uploaded arrays' true lengths and the walk's
+// stack capacities, or (AE_FAULT_CHECK_LIMITS) stacks of 2 and half of every
+// length, so the checks fire while every access made stays in bounds.
+static Checks checks_of(const Ctx *c) {
+    Checks C;
+    C.flags = c->check_word.ptr;
+    const bool lim = c->fault_check_limits != 0;
+    C.n_nodes = lim ? c->n_nodes / 2 : c->n_nodes;
+    C.n_objects = lim ? c->n_objects / 2 : c->n_objects;
+    C.n_instances = lim ? c->n_instances / 2 : c->n_instances;
+    C.n_blas = uint32_t(lim ? c->n_blas / 2 : c->n_blas);
+    C.n_indices = uint32_t(lim ? c->n_indices / 2 : c->n_indices);
+    C.n_vertices = uint32_t(lim ? c->n_vertices / 2 : c->n_vertices);
+    C.tlas_stack = lim ? 2 : kTlasStack;
+    C.blas_stack = lim ? 2 : kBlasStack;
+    return C;
 }
 
 int closest_hit_dispatch(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, int variant, cudaStream_t st,
@@ -41,6 +65,7 @@ int closest_hit_dispatch(Ctx *c, const ae_ray *rays, uint32_t n, ae_hit *hits, i
     cudaError_t e;
     if (variant == AE_VARIANT_PLAIN || variant == AE_VARIANT_PLAIN_WT)
         e = launch_closest_plain(c->scene(), rays, n, hits, st, variant == AE_VARIANT_PLAIN_WT);
+    else if (variant == AE_VARIANT_PLAIN_CHECKED) e = launch_closest_checked(c->scene(), checks_of(c), rays, n, hits, st);
     else if (variant == AE_VARIANT_FAST_WALK) e = launch_closest_walk(c, rays, n, hits, st);
     else e = launch_closest_fast(c, rays, n, hits, variant == AE_VARIANT_QUANT, st);
     if ((rc = c->cuda(e, "closest hit launch"))) return rc;

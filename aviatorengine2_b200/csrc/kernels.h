@@ -9,6 +9,7 @@
 namespace ae {
 
 struct DevScene;
+struct Checks;
 
 // Everything the frame kernels derive from Config once per frame (the camera
 // basis of hybrid:1347-1361), computed on the host with the same intrinsics
@@ -25,6 +26,8 @@ FrameParams make_frame_params(const ae_config &c);
 // watertight: the watertight triangle test in the same walk (AE_VARIANT_PLAIN_WT).
 cudaError_t launch_closest_plain(const DevScene &S, const ae_ray *rays, uint32_t n, ae_hit *hits, cudaStream_t st,
                                  bool watertight = false);
+cudaError_t launch_closest_checked(const DevScene &S, const Checks &C, const ae_ray *rays, uint32_t n, ae_hit *hits,
+                                   cudaStream_t st);
 cudaError_t launch_count_plain(const DevScene &S, const ae_ray *rays, uint32_t n, unsigned long long *totals,
                                cudaStream_t st);
 cudaError_t launch_count_paths(const DevScene &S, const FrameParams &F, unsigned long long *totals, cudaStream_t st);

@@ -162,6 +162,19 @@ AE_DEV bool tri_ref(f3 o, f3 d, float tn, float tf, f3 p0, f3 p1, f3 p2, float &
     return true;
 }
 
+// Debug checks of the reference walk (AE_VARIANT_PLAIN_CHECKED): every stack
+// push against the stack's capacity and every buffer index against its
+// array's length.  A violation skips the access - a node not visited, a
+// triangle or object not tested - and sets its bit (AE_CHECK_STACK,
+// AE_CHECK_INDEX) in *flags.  Passed as a null pointer, as by every other
+// caller, the checks compile away.
+struct Checks {
+    uint32_t *flags;
+    uint32_t n_nodes, n_objects, n_instances, n_blas, n_indices, n_vertices;
+    int tlas_stack, blas_stack;  // capacities checked (at most kTlasStack, kBlasStack)
+};
+AE_DEV void check_fail(const Checks *ck, uint32_t bit) { atomicOr(ck->flags, bit); }
+
 AE_DEV f3 vtx_pos(const ae_vertex *v, uint32_t i) {
     const float4 a = ld4(v + i);
     return mk(a.x, a.y, a.z);
@@ -173,8 +186,12 @@ AE_DEV f3 vtx_pos(const ae_vertex *v, uint32_t i) {
 // the precision variant's triangle test.
 template <bool WT = false>
 AE_DEV bool hit_mesh_ref(const DevScene &S, uint32_t inst_index, f3 o, f3 d, float tn, float tf, DHit &h,
-                         Touch *T = nullptr) {
+                         Touch *T = nullptr, const Checks *CK = nullptr) {
     if (T) T->instances++;
+    if (CK && inst_index >= CK->n_instances) {
+        check_fail(CK, AE_CHECK_INDEX);
+        return false;
+    }
     const float4 *ip = reinterpret_cast<const float4 *>(S.instances + inst_index);
     const float4 i0 = __ldg(ip), i1 = __ldg(ip + 1), i2 = __ldg(ip + 2);
     const uint32_t vbase = __float_as_uint(i2.x), ibase = __float_as_uint(i2.y), bbase = __float_as_uint(i2.w);
@@ -196,15 +213,29 @@ AE_DEV bool hit_mesh_ref(const DevScene &S, uint32_t inst_index, f3 o, f3 d, flo
     uint32_t best = 0;
     f3 bgeo = mk(0.0f, 0.0f, 1.0f);
     while (sp > 0) {
-        const NodeBox n = load_node(S.blas, bbase + uint32_t(stack[--sp]));
+        const uint32_t ni = bbase + uint32_t(stack[--sp]);
+        if (CK && ni >= CK->n_blas) {
+            check_fail(CK, AE_CHECK_INDEX);
+            continue;
+        }
+        const NodeBox n = load_node(S.blas, ni);
         if (T) T->blas++;
         if (!slab_ref(lo, invd, n.lo, n.hi, tn, closest)) continue;
         if (n.count > 0) {
             for (int i = 0; i < n.count; ++i) {
                 const uint32_t base = ibase + uint32_t(n.left + i) * 3u;
                 if (T) T->tris++;
+                if (CK && base + 2u >= CK->n_indices) {
+                    check_fail(CK, AE_CHECK_INDEX);
+                    continue;
+                }
                 const uint32_t a0 = __ldg(S.indices + base), a1 = __ldg(S.indices + base + 1),
                                a2 = __ldg(S.indices + base + 2);
+                if (CK && (vbase + a0 >= CK->n_vertices || vbase + a1 >= CK->n_vertices ||
+                          vbase + a2 >= CK->n_vertices)) {
+                    check_fail(CK, AE_CHECK_INDEX);
+                    continue;
+                }
                 const f3 p0 = vtx_pos(S.vertices, vbase + a0), p1 = vtx_pos(S.vertices, vbase + a1),
                          p2 = vtx_pos(S.vertices, vbase + a2);
                 float t, a, b;
@@ -216,9 +247,11 @@ AE_DEV bool hit_mesh_ref(const DevScene &S, uint32_t inst_index, f3 o, f3 d, flo
                     if (!WT) bgeo = g;
                 }
             }
-        } else if (sp + 2 <= kBlasStack) {
+        } else if (sp + 2 <= (CK ? CK->blas_stack : kBlasStack)) {
             stack[sp++] = n.left;
             stack[sp++] = n.right;
+        } else if (CK) {
+            check_fail(CK, AE_CHECK_STACK);
         }
     }
     if (!found) return false;
@@ -406,7 +439,7 @@ AE_DEV bool hit_volume_ref(const ae_object *obj, uint32_t shape, f3 o, f3 d, flo
 // WT selects the watertight triangle test inside meshes (hit_mesh_ref).
 template <bool WT = false>
 AE_DEV bool traverse_ref(const DevScene &S, f3 o, f3 d, float time, float tn, DHit &out, uint32_t &seed,
-                         Touch *T = nullptr) {
+                         Touch *T = nullptr, const Checks *CK = nullptr) {
     if (T) T->rays++;
     if (S.n_nodes == 0) return false;
     const f3 inv = 1.0f / d;
@@ -416,12 +449,21 @@ AE_DEV bool traverse_ref(const DevScene &S, f3 o, f3 d, float time, float tn, DH
     bool found = false;
     float tf = kFarStart;
     while (sp > 0) {
-        const NodeBox n = load_node(S.tlas, uint32_t(stack[--sp]));
+        const uint32_t ni = uint32_t(stack[--sp]);
+        if (CK && ni >= CK->n_nodes) {
+            check_fail(CK, AE_CHECK_INDEX);
+            continue;
+        }
+        const NodeBox n = load_node(S.tlas, ni);
         if (T) T->tlas++;
         if (!slab_ref(o, inv, n.lo, n.hi, tn, tf)) continue;
         if (n.count > 0) {
             for (int i = 0; i < n.count; i++) {
                 const uint32_t slot = uint32_t(n.left + i);
+                if (CK && slot >= CK->n_objects) {
+                    check_fail(CK, AE_CHECK_INDEX);
+                    continue;
+                }
                 const ae_object *obj = S.objects + slot;
                 if (T) T->objects++;
                 const ObjHead hd = load_head(obj);
@@ -433,7 +475,7 @@ AE_DEV bool traverse_ref(const DevScene &S, f3 o, f3 d, float time, float tn, DH
                 else if (hd.shape == AE_SHAPE_TRIANGLE) hit = hit_planar_ref(obj, true, o, d, tn, tf, h);
                 else if (hd.shape == AE_SHAPE_MESH) {
                     const uint32_t inst = __float_as_uint(ld4(reinterpret_cast<const char *>(obj) + 80).z);
-                    hit = hit_mesh_ref<WT>(S, inst, o, d, tn, tf, h, T);
+                    hit = hit_mesh_ref<WT>(S, inst, o, d, tn, tf, h, T, CK);
                 } else hit = hit_box_ref(obj, o, d, tn, tf, h);
                 if (hit) {
                     tf = h.t;
@@ -442,9 +484,11 @@ AE_DEV bool traverse_ref(const DevScene &S, f3 o, f3 d, float time, float tn, DH
                     found = true;
                 }
             }
-        } else if (sp + 2 <= kTlasStack) {
+        } else if (sp + 2 <= (CK ? CK->tlas_stack : kTlasStack)) {
             stack[sp++] = n.left;
             stack[sp++] = n.right;
+        } else if (CK) {
+            check_fail(CK, AE_CHECK_STACK);
         }
     }
     return found;

@@ -29,6 +29,31 @@ __global__ void __launch_bounds__(128) k_closest_plain(DevScene S, const ae_ray 
     hits[i] = out;
 }
 
+// The debug walk (AE_VARIANT_PLAIN_CHECKED): PLAIN's traversal with every
+// stack push and buffer index checked (Checks).
+__global__ void __launch_bounds__(128) k_closest_checked(DevScene S, Checks C, const ae_ray *__restrict__ rays,
+                                                         uint32_t n, ae_hit *__restrict__ hits) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 *rp = reinterpret_cast<const float4 *>(rays + i);
+    const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
+    uint32_t seed = 1u;
+    DHit h;
+    ae_hit out;
+    out.t = 0.0f; out.alpha = 0.0f; out.beta = 0.0f; out.object = AE_MISS; out.prim = AE_MISS;
+    if (traverse_ref<false>(S, mk(r0.x, r0.y, r0.z), mk(r1.x, r1.y, r1.z), r1.w, r0.w, h, seed, nullptr, &C)) {
+        out.t = h.t; out.alpha = h.alpha; out.beta = h.beta; out.object = h.slot; out.prim = h.prim;
+    }
+    hits[i] = out;
+}
+
+cudaError_t launch_closest_checked(const DevScene &S, const Checks &C, const ae_ray *rays, uint32_t n, ae_hit *hits,
+                                   cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_closest_checked<<<(n + 127) / 128, 128, 0, st>>>(S, C, rays, n, hits);
+    return cudaGetLastError();
+}
+
 // The same traversal with its touches counted: the algorithmic traffic of
 // the reference's walk, per ray set, summed in 64-bit.
 __global__ void __launch_bounds__(128) k_count_plain(DevScene S, const ae_ray *__restrict__ rays, uint32_t n,

@@ -236,6 +236,13 @@ class Context:
         self._chk(lib().ae_image_error_pixels(self._h, which, ptr(xy), len(xy), ptr(ref), eps, ptr(out)))
         return {"mre": out[0], "mae": out[1], "max": out[2], "rmse": out[3]}
 
+    def debug_flags(self):
+        """AE_CHECK_* bits the debug walk (VARIANT_PLAIN_CHECKED) set since the
+        last read (ae_debug_flags); reading clears them."""
+        f = ctypes.c_uint32()
+        self._chk(lib().ae_debug_flags(self._h, ctypes.byref(f)))
+        return f.value
+
     def debug_inject(self, fault, on=True):
         """Test hook (ae_debug_inject): e.g. _lib.FAULT_TILE_WAIT."""
         self._chk(lib().ae_debug_inject(self._h, fault, 1 if on else 0))

@@ -623,7 +623,7 @@ def measure_build(local, reps=3):
             "gpu_ms_per_mesh_calls": per_mesh_ms}
 
 
-def measure_serving(local, n_requests=48, rate=0.5, seed=7, claim_policy=1, frame_hz=30.0, queue_run=0):
+def measure_serving(local, n_requests=48, rate=0.5, seed=7, claim_policy=1, frame_hz=30.0, queue_run=0, slots=0):
     """The serving loop under a Poisson stream of requests over the 8 resident
     serving scenes: resolution uniform over {256^2, 640x480, 960x540,
     1920x1080}, spp from {1, 4, 16, 64} (as that many progressive frames).
@@ -651,7 +651,7 @@ def measure_serving(local, n_requests=48, rate=0.5, seed=7, claim_policy=1, fram
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
     inst = [sc.instances.copy() for sc in S]
     with Server(device=local, arena_bytes=4 << 30, max_requests=64, claim_policy=claim_policy,
-                queue_run=queue_run) as srv:
+                queue_run=queue_run, slots=slots) as srv:
         ids = [srv.add_scene(c) for c in ctxs]
         # warm-up: one small request per scene
         for k in range(len(S)):
@@ -703,7 +703,7 @@ def measure_serving(local, n_requests=48, rate=0.5, seed=7, claim_policy=1, fram
     return {"workload": "8 resident scenes " + "/".join(f"{sc.triangles // 1000}k" for sc in S) +
                         " tris, 512 instances each (4096 in all) moving every frame; Poisson arrivals",
             "requests": n_requests, "rate_per_s": rate, "claim_policy": "shared" if claim_policy else "oldest_first",
-            "queue_run": queue_run or "default (32)",
+            "queue_run": queue_run or "default (32)", "slots": slots or 1 << 20,
             "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
             # per progressive frame: a request's latency over its frame count
             "frame_p50_ms": float(np.percentile(per_frame, 50)), "frame_p99_ms": float(np.percentile(per_frame, 99)),
@@ -818,6 +818,7 @@ def main():
                     "leg at each (reported as serving_sweep)")
     ap.add_argument("--serve-claim", choices=["shared", "oldest"], default="shared",
                     help="how free slots pick the next pixel: spread over the admitted requests, or the oldest first")
+    ap.add_argument("--serve-slots", type=int, default=0, help="server path slots (0: the library default, 2^20)")
     ap.add_argument("--serve-run", type=int, default=0,
                     help="walker stages' queue entries per warp claim in the server (0: default, 1: static)")
     args = ap.parse_args()
@@ -995,11 +996,11 @@ def main():
     config4 = leg(not args.no_config4, measure_config4, local, args.c4_frames, args.mre_pixels)
     claim = 0 if args.serve_claim == "oldest" else 1
     serving = leg(not args.no_serve, measure_serving, local, args.serve_requests, args.serve_rate,
-                  claim_policy=claim, frame_hz=args.serve_frame_hz, queue_run=args.serve_run)
+                  claim_policy=claim, frame_hz=args.serve_frame_hz, queue_run=args.serve_run, slots=args.serve_slots)
     sweep = None
     if args.serve_sweep:
         sweep = [leg(True, measure_serving, local, args.serve_requests, float(r), claim_policy=claim,
-                     frame_hz=args.serve_frame_hz, queue_run=args.serve_run)
+                     frame_hz=args.serve_frame_hz, queue_run=args.serve_run, slots=args.serve_slots)
                  for r in args.serve_sweep.split(",")]
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -356,8 +356,16 @@ typedef struct ae_settings {
  * is FAST's walk run one step at a time per thread on a persistent grid (the
  * same hits; for incoherent sets such as bounce rays); PLAIN_WT is PLAIN's
  * walk over the FP32 binary BVH with QUANT's watertight triangle test - the
- * FP32-node form QUANT's 8-bit nodes are checked against (identical hits). */
-enum { AE_VARIANT_PLAIN = 0, AE_VARIANT_FAST = 1, AE_VARIANT_QUANT = 2, AE_VARIANT_FAST_WALK = 3, AE_VARIANT_PLAIN_WT = 4 };
+ * FP32-node form QUANT's 8-bit nodes are checked against (identical hits).
+ * PLAIN_CHECKED is PLAIN's walk in a debug mode: every stack push checked
+ * against the stack's capacity and every buffer index (TLAS node, object,
+ * instance, BLAS node, index triple, vertex) against its array's length; a
+ * violation skips that access and sets AE_CHECK_STACK or AE_CHECK_INDEX in
+ * the context's check word (ae_debug_flags).  On a valid scene its hits are
+ * PLAIN's. */
+enum { AE_VARIANT_PLAIN = 0, AE_VARIANT_FAST = 1, AE_VARIANT_QUANT = 2, AE_VARIANT_FAST_WALK = 3, AE_VARIANT_PLAIN_WT = 4,
+       AE_VARIANT_PLAIN_CHECKED = 5 };
+enum { AE_CHECK_STACK = 1, AE_CHECK_INDEX = 2 };
 
 /* Render modes for ae_render_frame.  AE_MODE_WAVEFRONT_PRECISION is the
  * wavefront tracer in the precision form: watertight triangle test, FP16
@@ -752,8 +760,16 @@ int ae_create_status(void);
  * on a server, every unfinished request ends with AE_ERR_TIMEOUT (serving
  * uses the tile-staged extend when extend_threads != 0).  on = 0 turns the
  * fault off. */
-enum { AE_FAULT_TILE_WAIT = 1 };
+/* AE_FAULT_CHECK_LIMITS: the debug walk (AE_VARIANT_PLAIN_CHECKED) checks
+ * against capacities and lengths below the true ones (stacks of 2 entries,
+ * half of every array), so its checks fire on a valid scene while every access
+ * it still makes stays inside the real arrays. */
+enum { AE_FAULT_TILE_WAIT = 1, AE_FAULT_CHECK_LIMITS = 2 };
 int ae_debug_inject(ae_ctx *ctx, int fault, uint32_t on);
+/* The check word of the debug walk (AE_CHECK_* bits set since the last read),
+ * then cleared.  Synchronises the context's stream.  No counterpart in the
+ * reference (its shaders have no checks). */
+int ae_debug_flags(ae_ctx *ctx, uint32_t *flags);
 int ae_serve_debug_inject(ae_server *srv, int fault, uint32_t on);
 
 #ifdef __cplusplus
