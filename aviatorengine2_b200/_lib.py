@@ -146,8 +146,8 @@ SIGNATURES = {
     "ae_trace_counters_variant": (_I, [_P, _P, _U32, _I, _P]),
     "ae_path_counters": (_I, [_P, _P]),
     "ae_wavefront_info": (_I, [_P, _P, _P, _P, _P]),
-    "ae_wavefront_walk_info": (_I, [_P, ctypes.c_int, _P, _P, _P]),
-    "ae_wavefront_set_walk_runs": (_I, [_P, ctypes.c_int, _U32, _U32]),
+    "ae_wavefront_walk_info": (_I, [_P, ctypes.c_int, _P, _P, _P, _P, _P]),
+    "ae_wavefront_set_walk_runs": (_I, [_P, ctypes.c_int, _U32, _U32, _U32, _U32]),
     "ae_synchronize": (_I, [_P]),
     "ae_last_kernel_ms": (_I, [_P, _P]),
     "ae_stream": (_P, [_P]),

@@ -100,8 +100,11 @@ struct Wavefront {
     // autotuned queue assignment of the walker stages, per form (index:
     // precision form), as a run length (0: static assignment)
     uint32_t walk_run[2] = {0, 0}, shadow_run[2] = {0, 0};
+    // and register bound, as an index into kWalkMinBlocks (6 or 7 blocks per SM)
+    int walk_mb[2] = {1, 1}, shadow_mb[2] = {1, 1};
     bool walk_tuned[2] = {false, false};
-    float walk_tune_ms[2][8] = {};  // shadow stage for kRunCfgs, then the bounce extend
+    // per stage (shadow, then the bounce extend): kRunCfgs x {6, 7} blocks per SM
+    float walk_tune_ms[2][16] = {};
     ~Wavefront() {
         if (graph) cudaGraphExecDestroy(graph);
         if (host_params) cudaFreeHost(host_params);
@@ -214,11 +217,11 @@ __global__ void __launch_bounds__(THREADS) k_wf_extend(DevScene S, FastView V, W
 // Extend on the step-wise Walker: a persistent grid, each thread stepping
 // its own queued ray and taking the next one when one finishes - static
 // assignment (DYN false: k + grid size) or runs of `run` consecutive queue
-// entries per warp claimed from the bounce's counter (DYN true); the
-// autotuner picks per scene.  For incoherent queues (bounces past the camera
-// rays).
-template <bool WT, bool DYN>
-__global__ void __launch_bounds__(128, kWalkBlocksPerSm) k_wf_extend_walk(DevScene S, FastView V, WfView W, int bounce,
+// entries per warp claimed from the bounce's counter (DYN true), compiled
+// for MINB resident blocks per SM; the autotuner picks per scene.  For
+// incoherent queues (bounces past the camera rays).
+template <bool WT, bool DYN, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_wf_extend_walk(DevScene S, FastView V, WfView W, int bounce,
                                                                           uint32_t run) {
     extern __shared__ uint2 stk[];
     const int q = bounce & 1;
@@ -312,9 +315,10 @@ __global__ void __launch_bounds__(256) k_wf_shade(DevScene S, FastView V, WfView
 // the sample unoccluded), so each walk starts with that distance as its
 // bound: the verdict and the glass step are those of the unbounded walk.
 // Entries are taken statically (k + grid size) or, DYN, in runs of `run`
-// consecutive queue entries per warp, as the autotuner picked.
-template <int THREADS, bool WT, bool DYN>
-__global__ void __launch_bounds__(THREADS, kWalkBlocksPerSm * 128 / THREADS)
+// consecutive queue entries per warp; MINB is the resident blocks per SM the
+// kernel is compiled for (its register bound).  The autotuner picks both.
+template <int THREADS, bool WT, bool DYN, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB * 128 / THREADS)
     k_wf_shadow(DevScene S, FastView V, WfView W, int bounce, uint32_t run) {
     extern __shared__ uint2 stk[];
     const uint32_t count = W.cnt[C_SH];
@@ -530,6 +534,37 @@ struct Grids {
     size_t esmem, shsmem;
 };
 
+// The walker stages' kernels by [precision form][runs][register bound]:
+// compiled for 6 or 7 resident 128-thread blocks per SM (kWalkMinBlocks).
+using ShadowFn = void (*)(DevScene, FastView, WfView, int, uint32_t);
+using ExtendWalkFn = void (*)(DevScene, FastView, WfView, int, uint32_t);
+constexpr int kWalkMinBlocks[2] = {6, 7};
+static const ShadowFn kShadowFns[2][2][2] = {
+    {{k_wf_shadow<128, false, false, 6>, k_wf_shadow<128, false, false, 7>},
+     {k_wf_shadow<128, false, true, 6>, k_wf_shadow<128, false, true, 7>}},
+    {{k_wf_shadow<128, true, false, 6>, k_wf_shadow<128, true, false, 7>},
+     {k_wf_shadow<128, true, true, 6>, k_wf_shadow<128, true, true, 7>}}};
+static const ExtendWalkFn kExtendWalkFns[2][2][2] = {
+    {{k_wf_extend_walk<false, false, 6>, k_wf_extend_walk<false, false, 7>},
+     {k_wf_extend_walk<false, true, 6>, k_wf_extend_walk<false, true, 7>}},
+    {{k_wf_extend_walk<true, false, 6>, k_wf_extend_walk<true, false, 7>},
+     {k_wf_extend_walk<true, true, 6>, k_wf_extend_walk<true, true, 7>}}};
+static const void *shadow_fn(bool prec, bool dyn, int mb) {
+    return reinterpret_cast<const void *>(kShadowFns[prec][dyn][mb]);
+}
+static const void *extend_walk_fn(bool prec, bool dyn, int mb) {
+    return reinterpret_cast<const void *>(kExtendWalkFns[prec][dyn][mb]);
+}
+// Persistent grid of a walker kernel: its resident blocks per SM x the SMs
+// (an occupancy query: never while a stream is being captured).
+static int walk_grid(Ctx *c, const void *fn) {
+    const size_t smem = size_t(kSharedStack) * 128 * sizeof(uint2);
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, smem);
+    return std::max(1, per_sm) * c->wave->sms;
+}
+
 // Launch shapes, fixed before capture (no attribute or occupancy query runs
 // while a stream is being captured).
 static Grids grids_for(Ctx *c, int cfg_index, bool prec) {
@@ -540,50 +575,24 @@ static Grids grids_for(Ctx *c, int cfg_index, bool prec) {
     g.egrid = extend_grid(c, e);
     g.esmem = extend_smem(e.threads, e.stack);
     g.shsmem = size_t(kSharedStack) * 128 * sizeof(uint2);
-    const void *shfn = prec ? reinterpret_cast<const void *>(k_wf_shadow<128, true, false>)
-                            : reinterpret_cast<const void *>(k_wf_shadow<128, false, false>);
-    const void *shdyn = prec ? reinterpret_cast<const void *>(k_wf_shadow<128, true, true>)
-                             : reinterpret_cast<const void *>(k_wf_shadow<128, false, true>);
-    cudaFuncSetAttribute(shfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(g.shsmem));
-    cudaFuncSetAttribute(shdyn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(g.shsmem));
-    int sh_per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh_per_sm, shfn, 128, g.shsmem);
-    g.shgrid = std::max(1, sh_per_sm) * Wf.sms;
-    // The step-wise extend of the bounce queues (same block and stack shape).
-    const void *wfn = prec ? reinterpret_cast<const void *>(k_wf_extend_walk<true, false>)
-                           : reinterpret_cast<const void *>(k_wf_extend_walk<false, false>);
-    const void *wdyn = prec ? reinterpret_cast<const void *>(k_wf_extend_walk<true, true>)
-                            : reinterpret_cast<const void *>(k_wf_extend_walk<false, true>);
-    cudaFuncSetAttribute(wfn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(g.shsmem));
-    cudaFuncSetAttribute(wdyn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(g.shsmem));
-    int w_per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&w_per_sm, wfn, 128, g.shsmem);
-    g.wgrid = std::max(1, w_per_sm) * Wf.sms;
+    g.shgrid = walk_grid(c, shadow_fn(prec, Wf.shadow_run[prec] != 0, Wf.shadow_mb[prec]));
+    g.wgrid = walk_grid(c, extend_walk_fn(prec, Wf.walk_run[prec] != 0, Wf.walk_mb[prec]));
     return g;
 }
 
-// The walker stages with a queue assignment: run 0 static, else runs of
-// `run` entries per warp.
-static void launch_extend_walk(bool prec, uint32_t run, const Grids &G, cudaStream_t st, const DevScene &S,
-                               const FastView &V, const WfView &W, int b) {
-    if (prec) {
-        if (run) k_wf_extend_walk<true, true><<<G.wgrid, 128, G.shsmem, st>>>(S, V, W, b, run);
-        else k_wf_extend_walk<true, false><<<G.wgrid, 128, G.shsmem, st>>>(S, V, W, b, 0u);
-    } else {
-        if (run) k_wf_extend_walk<false, true><<<G.wgrid, 128, G.shsmem, st>>>(S, V, W, b, run);
-        else k_wf_extend_walk<false, false><<<G.wgrid, 128, G.shsmem, st>>>(S, V, W, b, 0u);
-    }
+// The walker stages with a queue assignment (run 0: static, else runs of
+// `run` entries per warp) and a register bound (kWalkMinBlocks[mb] resident
+// blocks per SM), launched on `grid` blocks.
+static void launch_extend_walk(bool prec, uint32_t run, int mb, int grid, const Grids &G, cudaStream_t st,
+                               const DevScene &S, const FastView &V, const WfView &W, int b) {
+    const ExtendWalkFn fn = kExtendWalkFns[prec][run != 0][mb];
+    fn<<<grid, 128, G.shsmem, st>>>(S, V, W, b, run);
 }
 
-static void launch_shadow(bool prec, uint32_t run, const Grids &G, cudaStream_t st, const DevScene &S,
-                          const FastView &V, const WfView &W, int b) {
-    if (prec) {
-        if (run) k_wf_shadow<128, true, true><<<G.shgrid, 128, G.shsmem, st>>>(S, V, W, b, run);
-        else k_wf_shadow<128, true, false><<<G.shgrid, 128, G.shsmem, st>>>(S, V, W, b, 0u);
-    } else {
-        if (run) k_wf_shadow<128, false, true><<<G.shgrid, 128, G.shsmem, st>>>(S, V, W, b, run);
-        else k_wf_shadow<128, false, false><<<G.shgrid, 128, G.shsmem, st>>>(S, V, W, b, 0u);
-    }
+static void launch_shadow(bool prec, uint32_t run, int mb, int grid, const Grids &G, cudaStream_t st,
+                          const DevScene &S, const FastView &V, const WfView &W, int b) {
+    const ShadowFn fn = kShadowFns[prec][run != 0][mb];
+    fn<<<grid, 128, G.shsmem, st>>>(S, V, W, b, run);
 }
 
 static int record_sample(Ctx *c, cudaStream_t st, int cfg_index, const Grids &G, bool prec) {
@@ -602,10 +611,10 @@ static int record_sample(Ctx *c, cudaStream_t st, int cfg_index, const Grids &G,
         // queues are not: the step-wise walk keeps warps full (measured 6 %
         // more paths/s on the 10M-triangle scene).
         if (b == 0) e.fn<<<egrid, e.threads, esmem, st>>>(S, V, W, int(b));
-        else launch_extend_walk(prec, Wf.walk_run[prec], G, st, S, V, W, int(b));
+        else launch_extend_walk(prec, Wf.walk_run[prec], Wf.walk_mb[prec], G.wgrid, G, st, S, V, W, int(b));
         if (prec) k_wf_shade<true><<<grid256, 256, 0, st>>>(S, V, W, int(b));
         else k_wf_shade<false><<<grid256, 256, 0, st>>>(S, V, W, int(b));
-        launch_shadow(prec, Wf.shadow_run[prec], G, st, S, V, W, int(b));
+        launch_shadow(prec, Wf.shadow_run[prec], Wf.shadow_mb[prec], G.shgrid, G, st, S, V, W, int(b));
         k_wf_connect<<<grid256, 256, 0, st>>>(W, int(b));
     }
     k_wf_finish<<<grid256, 256, 0, st>>>(W);
@@ -661,8 +670,9 @@ static int best_cfg_index(const Wavefront &Wf) {
 static const uint32_t kRunCfgs[4] = {0, 32, 64, 256};
 
 // Times the shadow stage on sample 0's first shadow queue and the step-wise
-// extend on its second ray queue under every assignment of kRunCfgs, and
-// keeps the fastest of each for this form.  Runs before the first frame of
+// extend on its second ray queue under every assignment of kRunCfgs, each
+// compiled for 6 and for 7 resident blocks per SM, and keeps the fastest of
+// each for this form.  Runs before the first frame of
 // the form; the frame's generate stage then starts every path afresh.
 static int autotune_walkers(Ctx *c, bool prec) {
     Wavefront &Wf = *c->wave;
@@ -684,22 +694,26 @@ static int autotune_walkers(Ctx *c, bool prec) {
     for (int stage = 0; stage < 2; stage++) {
         uint32_t *counter = Wf.cnt.ptr + (stage == 0 ? C_SHTILE + 0 : C_TILE + 1);
         int best = 0;
-        for (int k = 0; k < 4; k++) {
+        for (int k = 0; k < 8; k++) {
+            const uint32_t run = kRunCfgs[k & 3];
+            const int mb = k >> 2;
+            const int grid = walk_grid(c, stage == 0 ? shadow_fn(prec, run != 0, mb) : extend_walk_fn(prec, run != 0, mb));
             float ms = 0.0f;
             for (int rep = 0; rep < 2; rep++) {
                 if ((rc = c->cuda(cudaMemsetAsync(counter, 0, sizeof(uint32_t), st), "autotune"))) return rc;
                 cudaEventRecord(c->ev0, st);
-                if (stage == 0) launch_shadow(prec, kRunCfgs[k], G, st, S, V, W, 0);
-                else launch_extend_walk(prec, kRunCfgs[k], G, st, S, V, W, 1);
+                if (stage == 0) launch_shadow(prec, run, mb, grid, G, st, S, V, W, 0);
+                else launch_extend_walk(prec, run, mb, grid, G, st, S, V, W, 1);
                 cudaEventRecord(c->ev1, st);
                 if ((rc = c->cuda(cudaEventSynchronize(c->ev1), "autotune"))) return rc;
                 if (rep == 1) cudaEventElapsedTime(&ms, c->ev0, c->ev1);
                 c->launches++;
             }
-            Wf.walk_tune_ms[prec][stage * 4 + k] = ms;
-            if (ms < Wf.walk_tune_ms[prec][stage * 4 + best]) best = k;
+            Wf.walk_tune_ms[prec][stage * 8 + k] = ms;
+            if (ms < Wf.walk_tune_ms[prec][stage * 8 + best]) best = k;
         }
-        (stage == 0 ? Wf.shadow_run : Wf.walk_run)[prec] = kRunCfgs[best];
+        (stage == 0 ? Wf.shadow_run : Wf.walk_run)[prec] = kRunCfgs[best & 3];
+        (stage == 0 ? Wf.shadow_mb : Wf.walk_mb)[prec] = best >> 2;
     }
     Wf.walk_tuned[prec] = true;
     return c->cuda(cudaGetLastError(), "autotune");
@@ -793,28 +807,39 @@ int render_wavefront(Ctx *c, bool prec) {
 using namespace ae;
 
 extern "C" int ae_wavefront_walk_info(ae_ctx *ctx, int precision, uint32_t *shadow_run, uint32_t *extend_run,
-                                      float *tune_ms8) {
+                                      uint32_t *shadow_blocks, uint32_t *extend_blocks, float *tune_ms16) {
     Ctx *c = reinterpret_cast<Ctx *>(ctx);
     if (!c) return AE_ERR_INVALID;
     const int f = precision ? 1 : 0;
     if (!c->wave || !c->wave->walk_tuned[f]) return c->fail(AE_ERR_STATE, "no wavefront frame of this form yet");
-    if (shadow_run) *shadow_run = c->wave->shadow_run[f];
-    if (extend_run) *extend_run = c->wave->walk_run[f];
-    if (tune_ms8) std::memcpy(tune_ms8, c->wave->walk_tune_ms[f], sizeof(c->wave->walk_tune_ms[f]));
+    const Wavefront &Wf = *c->wave;
+    if (shadow_run) *shadow_run = Wf.shadow_run[f];
+    if (extend_run) *extend_run = Wf.walk_run[f];
+    if (shadow_blocks) *shadow_blocks = uint32_t(kWalkMinBlocks[Wf.shadow_mb[f]]);
+    if (extend_blocks) *extend_blocks = uint32_t(kWalkMinBlocks[Wf.walk_mb[f]]);
+    if (tune_ms16) std::memcpy(tune_ms16, Wf.walk_tune_ms[f], sizeof(Wf.walk_tune_ms[f]));
     return AE_OK;
 }
 
-extern "C" int ae_wavefront_set_walk_runs(ae_ctx *ctx, int precision, uint32_t shadow_run, uint32_t extend_run) {
+extern "C" int ae_wavefront_set_walk_runs(ae_ctx *ctx, int precision, uint32_t shadow_run, uint32_t extend_run,
+                                          uint32_t shadow_blocks, uint32_t extend_blocks) {
     Ctx *c = reinterpret_cast<Ctx *>(ctx);
     if (!c) return AE_ERR_INVALID;
     if (shadow_run > (1u << 20) || extend_run > (1u << 20))
         return c->fail(AE_ERR_INVALID, "run lengths above 2^20 (got %u, %u)", shadow_run, extend_run);
+    auto mb_of = [](uint32_t blocks) { return blocks == 0 || blocks == 7 ? 1 : blocks == 6 ? 0 : -1; };
+    const int smb = mb_of(shadow_blocks), emb = mb_of(extend_blocks);
+    if (smb < 0 || emb < 0)
+        return c->fail(AE_ERR_INVALID, "resident blocks per SM must be 6 or 7 (got %u, %u)", shadow_blocks,
+                       extend_blocks);
     if (!c->wave) c->wave = new (std::nothrow) Wavefront();
     if (!c->wave) return c->fail(AE_ERR_OOM, "wavefront state");
     Wavefront &Wf = *c->wave;
     const int f = precision ? 1 : 0;
     Wf.shadow_run[f] = shadow_run;
     Wf.walk_run[f] = extend_run;
+    Wf.shadow_mb[f] = smb;
+    Wf.walk_mb[f] = emb;
     Wf.walk_tuned[f] = true;
     if (Wf.graph) {
         cudaGraphExecDestroy(Wf.graph);

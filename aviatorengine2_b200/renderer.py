@@ -203,19 +203,22 @@ class Context:
         return {"threads": th.value, "stack": st.value, "tune_ms": ms.tolist(), "errors": err.value}
 
     def wavefront_walk_info(self, precision=False):
-        """The walker stages' autotuned queue assignment for one form: run
-        lengths (0 = static) of the shadow stage and the bounce extend, and
-        the timings behind them (static, 32, 64, 256 for each)."""
-        sh, ex = ctypes.c_uint32(), ctypes.c_uint32()
-        ms = np.zeros(8, np.float32)
+        """The walker stages' autotuned launch for one form: run lengths (0 =
+        static) and resident blocks per SM of the shadow stage and the bounce
+        extend, and the timings behind them (static, 32, 64, 256 at 6 blocks,
+        then at 7, for each stage)."""
+        sh, ex, shb, exb = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        ms = np.zeros(16, np.float32)
         self._chk(lib().ae_wavefront_walk_info(self._h, 1 if precision else 0, ctypes.byref(sh), ctypes.byref(ex),
-                                               ptr(ms)))
-        return {"shadow_run": sh.value, "extend_run": ex.value, "shadow_ms": ms[:4].tolist(),
-                "extend_ms": ms[4:].tolist()}
+                                               ctypes.byref(shb), ctypes.byref(exb), ptr(ms)))
+        return {"shadow_run": sh.value, "extend_run": ex.value, "shadow_blocks": shb.value,
+                "extend_blocks": exb.value, "shadow_ms": ms[:8].tolist(), "extend_ms": ms[8:].tolist()}
 
-    def set_wavefront_walk_runs(self, shadow_run, extend_run, precision=False):
-        """Pin the walker stages' queue assignment of one form (0 = static)."""
-        self._chk(lib().ae_wavefront_set_walk_runs(self._h, 1 if precision else 0, shadow_run, extend_run))
+    def set_wavefront_walk_runs(self, shadow_run, extend_run, precision=False, shadow_blocks=0, extend_blocks=0):
+        """Pin the walker stages' launch of one form (runs: 0 = static;
+        blocks: 6 or 7, 0 = 7)."""
+        self._chk(lib().ae_wavefront_set_walk_runs(self._h, 1 if precision else 0, shadow_run, extend_run,
+                                                   shadow_blocks, extend_blocks))
 
     def image_error(self, reference, which=_lib.IMAGE_ACCUM, eps=1e-3):
         """FP64 error of an image against a reference (H, W, 4) float64 image,

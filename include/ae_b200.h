@@ -536,18 +536,23 @@ int ae_path_counters(ae_ctx *ctx, uint64_t *counters);
  * candidate timings in milliseconds (threads 64/128/256 x stack 16/24/32),
  * and the device error flags (non-zero: a bounded wait gave up). */
 int ae_wavefront_info(ae_ctx *ctx, int32_t *threads, int32_t *stack, float *tune_ms9, uint32_t *errors);
-/* The walker stages' autotuned queue assignment for one form (precision 0:
+/* The walker stages' autotuned launch for one form (precision 0:
  * AE_MODE_WAVEFRONT, 1: AE_MODE_WAVEFRONT_PRECISION), after that form's first
- * frame: run lengths of queue entries a warp claims at a time for the shadow
- * stage and the bounce extend (0: static assignment, entry k + grid size),
- * and the eight timings in milliseconds behind them (shadow stage, then
- * extend, each for static, 32, 64 and 256).  AE_ERR_STATE before that frame.
- * No counterpart in the reference (its passes have no autotuner). */
-int ae_wavefront_walk_info(ae_ctx *ctx, int precision, uint32_t *shadow_run, uint32_t *extend_run, float *tune_ms8);
-/* Pins that assignment for one form instead of autotuning it (0: static;
- * otherwise a run length, at most 2^20): every assignment gives the same
- * hits and images, so this only fixes the launch shape (comparisons, tests). */
-int ae_wavefront_set_walk_runs(ae_ctx *ctx, int precision, uint32_t shadow_run, uint32_t extend_run);
+ * frame: for the shadow stage and the bounce extend, the run length of queue
+ * entries a warp claims at a time (0: static assignment, entry k + grid
+ * size) and the resident blocks per SM the kernel is compiled for (6 or 7:
+ * its register bound), and the sixteen timings in milliseconds behind them
+ * (shadow stage, then extend; each for static, 32, 64 and 256 at 6 blocks,
+ * then the same at 7).  AE_ERR_STATE before that frame.  No counterpart in
+ * the reference (its passes have no autotuner). */
+int ae_wavefront_walk_info(ae_ctx *ctx, int precision, uint32_t *shadow_run, uint32_t *extend_run,
+                           uint32_t *shadow_blocks, uint32_t *extend_blocks, float *tune_ms16);
+/* Pins that launch for one form instead of autotuning it (runs: 0 static,
+ * otherwise a run length, at most 2^20; blocks: 6 or 7, 0 = 7): every choice
+ * gives the same hits and images, so this only fixes the launch shape
+ * (comparisons, tests). */
+int ae_wavefront_set_walk_runs(ae_ctx *ctx, int precision, uint32_t shadow_run, uint32_t extend_run,
+                               uint32_t shadow_blocks, uint32_t extend_blocks);
 
 /* Synchronise the context's stream.  Returns AE_ERR_CUDA on a sticky error. */
 int ae_synchronize(ae_ctx *ctx);

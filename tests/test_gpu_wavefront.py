@@ -123,20 +123,20 @@ def test_wavefront_equals_plain_full_size():
 @pytest.mark.parametrize("mode", [_lib.MODE_WAVEFRONT, _lib.MODE_WAVEFRONT_PRECISION])
 def test_walker_queue_assignments_give_the_same_frames(mode):
     """The walker stages take their queue entries statically or in runs per
-    warp (the autotuner picks per scene and form); every assignment must give
-    the same frames bit for bit.  A small wavefront scene (glass, metal, 16
+    warp, compiled for 6 or 7 resident blocks per SM (the autotuner picks per
+    scene and form); every choice must give the same frames bit for bit.  A small wavefront scene (glass, metal, 16
     lights) rendered with the assignment pinned three ways, and once more
     autotuned."""
     s = scenes.wavefront_scene(width=240, height=136, depth=6, n_meshes=6, n_instances=96, target_tris=200_000)
     prec = mode == _lib.MODE_WAVEFRONT_PRECISION
     w, h = int(s.config["width"]), int(s.config["height"])
-    runs = [(0, 0), (32, 64), (256, 32), None]
+    runs = [(0, 0, 7, 7), (32, 64, 6, 7), (256, 32, 7, 6), None]
     out = []
     for r in runs:
         with Context(w, h) as ctx:
             ctx.upload(s)
             if r is not None:
-                ctx.set_wavefront_walk_runs(r[0], r[1], precision=prec)
+                ctx.set_wavefront_walk_runs(r[0], r[1], precision=prec, shadow_blocks=r[2], extend_blocks=r[3])
             frames = []
             c = s.config.copy()
             for b in range(2):
@@ -146,9 +146,10 @@ def test_walker_queue_assignments_give_the_same_frames(mode):
                 frames.append(ctx.read_image(_lib.IMAGE_FRAME))
             info = ctx.wavefront_walk_info(precision=prec)
             if r is not None:
-                assert (info["shadow_run"], info["extend_run"]) == r
+                assert (info["shadow_run"], info["extend_run"], info["shadow_blocks"], info["extend_blocks"]) == r
             else:
                 assert info["shadow_run"] in (0, 32, 64, 256) and info["extend_run"] in (0, 32, 64, 256)
+                assert info["shadow_blocks"] in (6, 7) and info["extend_blocks"] in (6, 7)
                 assert all(t > 0 for t in info["shadow_ms"] + info["extend_ms"]), info
             assert ctx.wavefront_info()["errors"] == 0
             out.append(frames)
