@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(THREADS, MINB * 128 / THREADS)
     Walker<WT> w;
     WalkStacks<> K;
     uint32_t e = 0;
-    f3 so, sd, lp;
+    float lim = 0.0f;  // the sample's cut-off |lp - so| - 0.001; the ray itself lives in the walker (w.o, w.d)
     int step = 0;
     bool active = !DYN && k < count;
     bool need = DYN, exhausted = false;
@@ -336,9 +336,10 @@ __global__ void __launch_bounds__(THREADS, MINB * 128 / THREADS)
     auto begin = [&]() {
         e = W.sq[k];
         const float4 o4 = W.sh.o[e], d4 = W.sh.d[e], l4 = W.sh.lp[e];
-        so = mk(o4.x, o4.y, o4.z); sd = mk(d4.x, d4.y, d4.z); lp = mk(l4.x, l4.y, l4.z);
+        const f3 so = mk(o4.x, o4.y, o4.z);
         step = 0;
-        w.start(V, so, sd, 0.001f, d4.w, AE_SUB(distance(lp, so), 0.001f));
+        lim = AE_SUB(distance(mk(l4.x, l4.y, l4.z), so), 0.001f);
+        w.start(V, so, mk(d4.x, d4.y, d4.z), 0.001f, d4.w, lim);
     };
     if (active) begin();
     uint32_t iter = 0;
@@ -354,14 +355,18 @@ __global__ void __launch_bounds__(THREADS, MINB * 128 / THREADS)
         if (!active || w.group() != pick || !w.step(S, V, K, stk, threadIdx.x, THREADS)) continue;
         const Best &b = w.best;
         int verdict = 0;  // 0 unoccluded, 1 occluded, 2 through glass
-        if (b.object != AE_MISS && b.t < AE_SUB(distance(lp, so), 0.001f)) {
+        if (b.object != AE_MISS && b.t < lim) {
             const uint32_t mt = load_head(S.objects + b.object).material;
             verdict = mt == AE_MAT_DIFFUSE_LIGHT ? 0 : (mt != AE_MAT_DIELECTRIC ? 1 : 2);
         }
         if (verdict == 2) {
-            so = (so + sd * b.t) + sd * 0.001f;
+            // Through the glass: the reference's re-origin, from the walker's
+            // copy of the ray; the light point is read again.
+            const f3 so = (w.o + w.d * b.t) + w.d * 0.001f;
             if (++step < 4) {
-                w.start(V, so, sd, 0.001f, w.time, AE_SUB(distance(lp, so), 0.001f));
+                const float4 l4 = W.sh.lp[e];
+                lim = AE_SUB(distance(mk(l4.x, l4.y, l4.z), so), 0.001f);
+                w.start(V, so, w.d, 0.001f, w.time, lim);
                 continue;
             }
             verdict = 0;
