@@ -937,7 +937,10 @@ def main():
             et.append(time.perf_counter() - t0)
         e2e_s = max_over_ranks(float(np.mean(et)), pg, dev)
         e2e = {"value": replica_value(rays_step, world, e2e_s), "unit": UNIT, "h2d_bytes_per_step": int((n1 + n2) * 32),
-               "d2h_bytes_per_step": int((n1 + n2) * 20)}
+               "d2h_bytes_per_step": int((n1 + n2) * 20),
+               "note": "pinned host buffers, wall clock per step; the camera-ray call's kernel reads the rays and "
+                       "writes the hits in host memory over the bus, the bounce-ray call copies chunks in and out "
+                       "(cudaMemcpyAsync) around its launches"}
 
     peak, peak_kind = load_peaks()
     traffic = load_traffic()
