@@ -460,7 +460,7 @@ def timed_closest_hit(ctx, d_rays, n, d_hits, variant, flush, reps=5):
     return float(np.mean(ms))
 
 
-def measure_config4(local, frames=1024, mre_pixels=2048, width=960, height=540):
+def measure_config4(local, frames=4096, mre_pixels=2048, width=960, height=540):
     """The precision variant of the closest-hit workload (the 2.1M-triangle
     instanced scene at 960x540):
       * primary-ray IDs of the precision closest hit (4-wide BVH, 8-bit child
@@ -804,7 +804,7 @@ def main():
     ap.add_argument("--no-build", action="store_true", help="skip the BVH build leg")
     ap.add_argument("--no-config4", action="store_true", help="skip the precision-variant leg (960x540)")
     ap.add_argument("--no-config1", action="store_true", help="skip the small plain-method leg (Cornell box)")
-    ap.add_argument("--c4-frames", type=int, default=1024, help="frames (1 spp each) of the precision-variant leg")
+    ap.add_argument("--c4-frames", type=int, default=4096, help="frames (1 spp each) of the precision-variant leg")
     ap.add_argument("--mre-pixels", type=int, default=2048, help="seeded pixels scored against the FP64 oracle")
     ap.add_argument("--paths-tris", type=int, default=10_000_000, help="unique triangles of the wavefront scene")
     ap.add_argument("--paths-instances", type=int, default=1024, help="instances of the wavefront scene")
@@ -974,16 +974,17 @@ def main():
                         "DRAM traffic is far below the algorithmic bytes (l2_throughput_pct_of_peak: the committed ncu summary, its case named)"}
 
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference(scene, np.concatenate([prim, bounce]))
         cpu["note"] = ("the oracle's restatement of the reference traversal, which traces the scaled instances; "
                        "--impl reference prints the reference's own compiled traversal on the rigid twin beside it")
 
-    # Frame-level legs: rank 0 only (the other replicas would repeat them).
-    # A leg that fails reports its error in its own block; the closest-hit
-    # line above stands.
+    # Frame-level legs: single-GPU workloads, measured in the one-GPU run
+    # (with N replicas they would repeat the same numbers on rank 0 while the
+    # other GPUs wait).  A leg that fails reports its error in its own block;
+    # the closest-hit line above stands.
     def leg(enabled, fn, *a, **kw):
-        if not enabled or rank != 0:
+        if not enabled or rank != 0 or world > 1:
             return None
         try:
             return fn(*a, **kw)
